@@ -1,0 +1,186 @@
+"""ctypes binding of the CPU FP64 oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load this
+module.  It checks the CUDA product path; nothing in gemini_unified_b200 may
+import it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in
+                ("steps_ok", "steps_rej", "attempts", "sysmats", "matvecs", "flops")]
+
+    def asdict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+def build() -> str:
+    srcs = [os.path.join(HERE, f) for f in ("oracle_fk.cpp", "oracle_synth.cpp", "oracle_core.h")]
+    if not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(build())
+        L = _lib
+        vp = ctypes.c_void_p
+        L.oracle_create.restype = vp
+        L.oracle_create_nodes.restype = vp
+        L.oracle_destroy.argtypes = [vp]
+        L.oracle_nnod.argtypes = [vp]
+        L.oracle_nodes.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_node_index.argtypes = [vp, ctypes.c_double]
+        L.oracle_spline.argtypes = [vp, ctypes.c_double, ctypes.c_int] + [ctypes.c_void_p] * 4
+        L.oracle_start_radius.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        L.oracle_start_radius.restype = ctypes.c_double
+        L.oracle_nwn.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.oracle_fk_frequency.argtypes = [vp, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.oracle_legendre.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
+        L.oracle_fft.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_degree_sums.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_synthetics.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_void_p]
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Oracle:
+    """One earth model + external node set, as the FK driver holds them."""
+
+    def __init__(self, model, nodes):
+        self._desc = model.desc()
+        self.model = model
+        r = np.ascontiguousarray(nodes.r, dtype=np.float64)
+        s = np.ascontiguousarray(nodes.state, dtype=np.int32)
+        l = np.ascontiguousarray(nodes.layer, dtype=np.int32)
+        self.h = lib().oracle_create_nodes(ctypes.byref(self._desc), len(r), _p(r), _p(s), _p(l))
+        if not self.h:
+            raise RuntimeError("oracle_create_nodes failed")
+
+    @classmethod
+    def from_blocks(cls, model, nnodb, drb, shift, rearth):
+        self = cls.__new__(cls)
+        self._desc = model.desc()
+        self.model = model
+        nb = np.ascontiguousarray(nnodb, dtype=np.int32)
+        dr = np.ascontiguousarray(drb, dtype=np.float64)
+        self.h = lib().oracle_create(ctypes.byref(self._desc), len(nb), _p(nb), _p(dr),
+                                     ctypes.c_double(shift), ctypes.c_double(rearth))
+        if not self.h:
+            raise RuntimeError("oracle_create failed")
+        return self
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_destroy(self.h)
+            self.h = None
+
+    def nodes(self):
+        n = lib().oracle_nnod(self.h)
+        r = np.zeros(n); s = np.zeros(n, np.int32); l = np.zeros(n, np.int32)
+        lib().oracle_nodes(self.h, _p(r), _p(s), _p(l))
+        return r, s, l
+
+    def spline(self, f, attmode):
+        nk = self.model.nk
+        ro = np.zeros(nk); ro2 = np.zeros(nk); el = np.zeros(nk * 14); el2 = np.zeros(nk * 14)
+        rc = lib().oracle_spline(self.h, ctypes.c_double(f), attmode, _p(ro), _p(ro2), _p(el), _p(el2))
+        if rc:
+            raise RuntimeError("spline failed")
+        return ro, ro2, el.view(np.complex128).reshape(nk, 7), el2.view(np.complex128).reshape(nk, 7)
+
+    def start_radius(self, f, attmode, wn, tor):
+        return lib().oracle_start_radius(self.h, ctypes.c_double(f), attmode, ctypes.c_double(wn), int(tor))
+
+    def nwn(self, pc):
+        cap = 1 << 16
+        nwn = np.zeros(cap, np.int32)
+        nf1 = ctypes.c_int(); nf2 = ctypes.c_int()
+        rc = lib().oracle_nwn(self.h, ctypes.byref(pc), ctypes.byref(nf1), ctypes.byref(nf2), _p(nwn), cap)
+        if rc:
+            raise RuntimeError("oracle_nwn failed")
+        return nf1.value, nf2.value, nwn[: nf2.value].copy()
+
+    def fk_frequency(self, pc, jf, nwn, nsp, iwn_lo=1, iwn_hi=1 << 30):
+        """FK spectra of one frequency: complex128 [nnod, nsp, nwn] plus per-iwn status and stats."""
+        nnod = lib().oracle_nnod(self.h)
+        gf = np.zeros(nwn * nsp * nnod * 2)
+        status = np.zeros(nwn, np.int32)
+        st = Stats()
+        rc = lib().oracle_fk_frequency(self.h, ctypes.byref(pc), jf, nwn, _p(gf), _p(status), ctypes.byref(st),
+                                       iwn_lo, iwn_hi)
+        if rc < 0:
+            raise RuntimeError("oracle_fk_frequency: unsupported configuration")
+        if rc != nsp:
+            raise RuntimeError(f"nsp mismatch {rc} != {nsp}")
+        g = gf.view(np.complex128).reshape(nnod, nsp, nwn)
+        return g, status, st.asdict()
+
+
+def legendre(lmax, theta):
+    out = np.zeros(5 * 3 * (lmax + 1))
+    lib().oracle_legendre(lmax, ctypes.c_double(theta), _p(out))
+    return out.reshape(5, 3, lmax + 1)
+
+
+def fft(x, y, n, is_):
+    x = np.ascontiguousarray(x, np.float64).copy(); y = np.ascontiguousarray(y, np.float64).copy()
+    lib().oracle_fft(n, is_, _p(x), _p(y))
+    return x, y
+
+
+def degree_sums(nf1, nf2, nwn, nwnmax, gr, gi, theta):
+    """gr/gi: float32 [nsp, nkfmax] (row per spectrum).  Returns complex [nsta, nf2, 14]."""
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkf = gr.shape
+    th = np.ascontiguousarray(theta, np.float64)
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    hd = np.zeros(len(th) * nf2 * 14 * 2)
+    rc = lib().oracle_degree_sums(nf1, nf2, _p(nwn), nwnmax, nkf, nsp, _p(gr), _p(gi), len(th), _p(th), _p(hd))
+    if rc:
+        raise RuntimeError("oracle_degree_sums failed")
+    return hd.view(np.complex128).reshape(len(th), nf2, 14)
+
+
+def synthetics(nf1, nf2, nwn, nwnmax, df, sigma, gr, gi, theta, phi, propdir, mt, filspecs,
+               velocity, tred, nsamp, dt):
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkf = gr.shape
+    th = np.ascontiguousarray(theta, np.float64); ph = np.ascontiguousarray(phi, np.float64)
+    pd = np.ascontiguousarray(propdir, np.float64)
+    mt = np.ascontiguousarray(mt, np.float64).reshape(-1, 6)
+    fs = np.ascontiguousarray(filspecs, np.float64)
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    tr = np.zeros(len(th) * len(mt) * 3 * nsamp, np.float32)
+    rc = lib().oracle_synthetics(nf1, nf2, _p(nwn), nwnmax, df, sigma, nkf, nsp, _p(gr), _p(gi), len(th),
+                                 _p(th), _p(ph), _p(pd), len(mt), _p(mt), _p(fs), int(velocity), tred,
+                                 nsamp, dt, _p(tr))
+    if rc:
+        raise RuntimeError("oracle_synthetics failed")
+    return tr.reshape(len(th), len(mt), 3, nsamp)

@@ -1,0 +1,344 @@
+// =============================================================================
+//  GEMINI FK hot path -- CPU FP64 ORACLE, phase 2 (synthetic seismograms).
+//  Test infrastructure only; see oracle_core.h for the conventions.
+//
+//  Restates:
+//    legendreFunctions.f90:48-157            (P_l^m, m <= 2, and derivatives)
+//    harmonicDegreeSums.f90:231-369,34-45    (moment degree sums, cos^2 taper)
+//    displacementSpectra.f90:49-113          (frequency loop, sum -> FK index)
+//    singleFrequencyDisplacement.f90:108-125 (ZRT from the 14 sums)
+//    eventFilter.f90:40-83, butterworthFilter.f90:49-96 (complex-omega band-pass)
+//    computeSyntheticSeismograms.f90:355-388 (time shift, velocity, ZNE rotation)
+//    axesRotation.f90:560-568                (RLT -> ZNE)
+//    frequencyTime.f90:34-113, fourierTransform.f90:118-192 (iFFT, exp(sigma t))
+// =============================================================================
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "oracle_core.h"
+
+using namespace orc;
+
+namespace {
+
+struct Legendre {
+  int lmax;
+  // [m][l], m = 0..2 ; pdst/dtpdst use m = 1..2 (m = 0 row unused)
+  std::vector<double> plm[3], dpdt[3], pdst[3], d2pdt2[3], dtpdst[3];
+};
+
+// legendreFunctions.f90:48-157 (mmax = 2)
+void computeLegendre(int lmax, double theta, Legendre& a) {
+  const int mmax = 2;
+  a.lmax = lmax;
+  for (int m = 0; m < 3; ++m) {
+    a.plm[m].assign(lmax + 2, 0.0); a.dpdt[m].assign(lmax + 2, 0.0); a.pdst[m].assign(lmax + 2, 0.0);
+    a.d2pdt2[m].assign(lmax + 2, 0.0); a.dtpdst[m].assign(lmax + 2, 0.0);
+  }
+  double ct = std::cos(theta), st = std::sin(theta);
+  bool atpoles = !(st > 0.0);
+  for (int m = 0; m <= mmax; ++m) {
+    if (m > lmax) break;
+    a.plm[m][m] = 1.0;
+    double fact = 1.0;
+    for (int j = 1; j <= m; ++j) { a.plm[m][m] = a.plm[m][m] * fact * st; fact = fact + 2.0; }
+    if (m + 1 <= lmax) a.plm[m][m + 1] = ct * (double)(2 * m + 1) * a.plm[m][m];
+    for (int l = m + 2; l <= lmax; ++l)
+      a.plm[m][l] = (ct * (double)(2 * l - 1) * a.plm[m][l - 1] - (double)(l + m - 1) * a.plm[m][l - 2]) /
+                    (double)(l - m);
+  }
+  if (!atpoles) {
+    double rst = 1.0 / st;
+    for (int m = 0; m <= mmax; ++m) {
+      if (m > lmax) break;
+      a.dpdt[m][m] = (double)m * ct * a.plm[m][m] * rst;
+      for (int l = m + 1; l <= lmax; ++l)
+        a.dpdt[m][l] = ((double)l * ct * a.plm[m][l] - (double)(l + m) * a.plm[m][l - 1]) * rst;
+    }
+    for (int m = 1; m <= mmax; ++m)
+      for (int l = m; l <= lmax; ++l) a.pdst[m][l] = a.plm[m][l] * rst;
+    for (int m = 0; m <= mmax; ++m)
+      for (int l = m; l <= lmax; ++l)
+        a.d2pdt2[m][l] = (-ct) * rst * a.dpdt[m][l] + ((double)(m * m) * (rst * rst) - (double)(l * (l + 1))) * a.plm[m][l];
+    for (int m = 1; m <= mmax; ++m)
+      for (int l = m; l <= lmax; ++l) a.dtpdst[m][l] = rst * (a.dpdt[m][l] - ct * rst * a.plm[m][l]);
+  } else {
+    int isct = (int)std::copysign(1.0, ct);
+    auto ipow = [](int b, int e) { int r = 1; for (int i = 0; i < e; ++i) r *= b; return r; };
+    for (int l = 0; l <= lmax; ++l) {
+      a.dpdt[0][l] = 0.0;
+      a.dpdt[1][l] = 0.5 * (double)(l * (l + 1) * ipow(isct, l));
+      a.dpdt[2][l] = 0.0;
+    }
+    for (int l = 1; l <= lmax; ++l) {
+      a.pdst[1][l] = 0.5 * (double)(l * (l + 1) * ipow(isct, l + 1));
+      a.pdst[2][l] = 0.0;
+    }
+    for (int l = 0; l <= lmax; ++l) {
+      a.d2pdt2[0][l] = 0.5 * (double)(l * (l + 1) * ipow(isct, l));
+      a.d2pdt2[1][l] = 0.0;
+      a.d2pdt2[2][l] = 0.25 * (double)((l + 2) * (l + 1) * l * (l - 1) * ipow(isct, l));
+    }
+    for (int l = 1; l <= lmax; ++l) {
+      a.dtpdst[1][l] = 0.0;
+      a.dtpdst[2][l] = 0.125 * (double)((l + 2) * (l + 1) * l * (l - 1) * ipow(isct, l + 1));
+    }
+  }
+}
+
+// taperHarmonicDegreeSums (harmonicDegreeSums.f90:356-369)
+void taper(int lmax, double tapfrac, std::vector<double>& g) {
+  g.assign(lmax + 1, 0.0);
+  int jt = std::min((int)std::lround((double)lmax * (1.0 - tapfrac)), lmax);
+  jt = std::max(1, jt);
+  double c1 = (double)lmax * tapfrac * 2.0 / PI_F;
+  double c2 = (1.0 - tapfrac) / tapfrac * 0.5 * PI_F;
+  for (int j = 0; j <= jt - 1 && j <= lmax; ++j) g[j] = 1.0;
+  for (int j = jt; j <= lmax; ++j) {
+    double c = std::cos((double)(float)j / c1 - c2);
+    g[j] = c * c;
+  }
+}
+
+// table kind and factor of the 14 moment sums (harmonicDegreeSums.f90:297-351)
+// kind: 0 plm, 1 dpdt, 2 pdst ; m ; l start ; factor numerator (0 => none)
+struct SumDef { int kind, m, l0; double fnum; int comp, jump; };
+const SumDef MSUM[14] = {
+    {0, 0, 0, 0.0, 1, 1},  {0, 0, 0, 0.0, 1, 2},  {0, 1, 1, 2.0, 1, 3},  {0, 2, 2, 2.0, 1, 4},
+    {1, 0, 1, 0.0, 3, 1},  {1, 0, 1, 0.0, 3, 2},  {1, 1, 1, 2.0, 3, 3},  {1, 2, 2, 2.0, 3, 4},
+    {2, 1, 1, 2.0, 7, 1},  {2, 2, 2, 4.0, 7, 2},  {1, 1, 1, 2.0, 7, 1},  {1, 2, 2, -2.0, 7, 2},
+    {2, 1, 1, 2.0, 3, 3},  {2, 2, 2, -4.0, 3, 4}};
+
+// momentHarmonicDegreeSums for kint 1..14 over lmax = nwn-1 terms
+zc momentSum(int kint, const float* gr, const float* gi, int nwn, const Legendre& alf,
+             const std::vector<double>& tap) {
+  const SumDef& s = MSUM[kint - 1];
+  const std::vector<double>& T =
+      s.kind == 0 ? alf.plm[s.m] : (s.kind == 1 ? alf.dpdt[s.m] : alf.pdst[s.m]);
+  double fourpi = 4.0 * PI_F;
+  int lmax = nwn - 1;
+  zc z = Z(0.0);
+  for (int l = s.l0; l <= lmax; ++l) {
+    zc g = Z((double)gr[l], (double)gi[l]);
+    zc t;
+    if (s.fnum == 0.0) t = T[l] * g;
+    else t = ((T[l] * s.fnum) / (double)(float)(l * (l + 1))) * g;
+    t = ((t * (2.0 * (double)l + 1.0)) / fourpi) * tap[l];
+    z = z + t;
+  }
+  return z;
+}
+
+// doubleFastFourierTransform (fourierTransform.f90:118-192), 1-based x,y
+void fft(std::vector<double>& x, std::vector<double>& y, int n, int is) {
+  double piz = 2.0 * PI_F;
+  std::vector<int> zh(n + 2);
+  zh[1] = 1;
+  for (int l = 1; l <= n; ++l) zh[l + 1] = 2 * zh[l];
+  int ng = zh[n + 1];
+  double gn = 1.0 / (double)ng;
+  for (int m = 1; m <= n; ++m) {
+    int nar = zh[m], lar = ng / nar, larh = lar / 2;
+    double alpha = piz / (double)(is >= 0 ? lar : -lar);
+    for (int jr = 1; jr <= larh; ++jr) {
+      double beta = alpha * (double)(jr - 1);
+      double excos = std::cos(beta), exsin = std::sin(beta);
+      int ja = jr - lar;
+      for (int nr = 1; nr <= nar; ++nr) {
+        ja = ja + lar;
+        int jb = ja + larh;
+        double zx = x[ja] - x[jb], zy = y[ja] - y[jb];
+        x[ja] = x[ja] + x[jb];
+        y[ja] = y[ja] + y[jb];
+        x[jb] = zx * excos - zy * exsin;
+        y[jb] = zx * exsin + zy * excos;
+      }
+    }
+  }
+  int ais = is < 0 ? -is : is;
+  if (ais == 3) gn = std::sqrt(gn);
+  if (ais == 2 || ais == 3) for (int i = 1; i <= ng; ++i) { y[i] *= gn; x[i] *= gn; }
+  for (int j = 1; j <= ng; ++j) {
+    int js = j - 1, k = 1, nny = n + 1;
+    for (int ny = 1; ny <= n; ++ny) {
+      nny = nny - 1;
+      if (js < zh[nny]) continue;
+      js = js - zh[nny];
+      k = k + zh[ny];
+    }
+    if (j - k < 0) {
+      std::swap(x[j], x[k]); std::swap(y[j], y[k]);
+    }
+  }
+}
+
+// transformFrequencyTime (frequencyTime.f90:55-113); sp 1-based [1..nf2]
+int freqTime(int nf1, int nf2, double df, double sigma, const std::vector<zc>& sp, int nsamp,
+             double dt, float* ts) {
+  int nslog = (int)std::ceil((double)std::log((float)nf2) / std::log(2.0)) + 1;
+  int ns = 1 << nslog;
+  double dts; int ndec;
+  if (ns <= nsamp) {
+    ns = nsamp;
+    nslog = (int)std::ceil(-std::log(df * dt) / std::log(2.0));
+    dts = dt; ndec = 1;
+  } else {
+    dts = 1.0 / (df * ns);
+    ndec = (int)std::lround(dt / dts);
+    if (std::fabs(dt - ndec * dts) > 1.e-5) return 2;
+  }
+  if ((1 << nslog) != ns) return 2;   // inconsistent nsamp / dt
+  std::vector<double> x(ns + 1, 0.0), y(ns + 1, 0.0);
+  for (int i = nf1; i <= nf2; ++i) { x[i] = sp[i].re; y[i] = sp[i].im; }
+  for (int i = ns / 2 + 2; i <= ns; ++i) { x[i] = x[ns - i + 2]; y[i] = -y[ns - i + 2]; }
+  fft(x, y, nslog, +1);
+  double fac = 1.0, expo = std::exp(sigma * dts);
+  for (int i = 1; i <= nsamp; ++i) {
+    ts[i - 1] = (float)(x[ndec * (i - 1) + 1] * df * fac);
+    fac = fac * expo;
+  }
+  return 0;
+}
+
+// complex-omega Butterworth band-pass (eventFilter.f90:40-83, butterworthFilter.f90:49-96)
+void eventFilter(int nordh, double fch, int nordl, double fcl, int nf1, int nf2, double df,
+                 double sigma, std::vector<zc>& hfil) {
+  hfil.assign(nf2 + 1, Z(0.0));
+  int nf = nf2 - nf1 + 1;
+  double fmin = (double)(nf1 - 1) * df;
+  const zc ci = Z(0.0, 1.0);
+  std::vector<zc> hh(nf, Z(1.0)), hl(nf, Z(1.0));
+  zc zfna = (fmin - (ci * sigma) / TWO_PI_F) / fch;
+  for (int j = 1; j <= nordh; ++j) {
+    zc zfn = zfna;
+    zc ep = zexp(((ci * PI_F) * ((double)j - 0.5)) / (double)nordh);
+    for (int i = 0; i < nf; ++i) { hh[i] = (hh[i] * zfn) / (zfn - ep); zfn = zfn + df / fch; }
+  }
+  zfna = (fmin - (ci * sigma) / TWO_PI_F) / fcl;
+  for (int j = 1; j <= nordl; ++j) {
+    zc zfn = zfna;
+    zc ep = zexp(((ci * PI_F) * ((double)j - 0.5)) / (double)nordl);
+    for (int i = 0; i < nf; ++i) { hl[i] = (hl[i] * (-ci)) / (zfn - ep); zfn = zfn + df / fcl; }
+  }
+  for (int i = 0; i < nf; ++i) hfil[nf1 + i] = hh[i] * hl[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+// Legendre tables for the unit tests: out[kind*3*(lmax+1) + m*(lmax+1) + l], kinds
+// plm, dpdt, pdst, d2pdt2, dtpdst.
+void oracle_legendre(int lmax, double theta, double* out) {
+  Legendre a;
+  computeLegendre(lmax, theta, a);
+  int L = lmax + 1;
+  for (int m = 0; m < 3; ++m)
+    for (int l = 0; l <= lmax; ++l) {
+      out[0 * 3 * L + m * L + l] = a.plm[m][l];
+      out[1 * 3 * L + m * L + l] = a.dpdt[m][l];
+      out[2 * 3 * L + m * L + l] = a.pdst[m][l];
+      out[3 * 3 * L + m * L + l] = a.d2pdt2[m][l];
+      out[4 * 3 * L + m * L + l] = a.dtpdst[m][l];
+    }
+}
+
+void oracle_fft(int n, int is, double* x, double* y) {
+  int ng = 1 << n;
+  std::vector<double> xx(ng + 1), yy(ng + 1);
+  for (int i = 0; i < ng; ++i) { xx[i + 1] = x[i]; yy[i + 1] = y[i]; }
+  fft(xx, yy, n, is);
+  for (int i = 0; i < ng; ++i) { x[i] = xx[i + 1]; y[i] = yy[i + 1]; }
+}
+
+// Harmonic degree sums: hd[(sta*nf2 + jf-1)*14 + k] complex interleaved (jf in nf1..nf2)
+// gr/gi: FP32 FK spectra of one node, Fortran (nkfmax, nsp) layout.
+int oracle_degree_sums(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp,
+                       const float* gr, const float* gi, int nsta, const double* theta,
+                       double* hd) {
+  // offsets of the 10 moment FK spectra (greenFKSpectra.f90:204-212 with dsvmask U,V,W)
+  auto offset = [](int comp, int jump) { return comp == 1 ? jump : (comp == 3 ? 4 + jump : 8 + jump); };
+  for (int is = 0; is < nsta; ++is) {
+    Legendre alf;
+    computeLegendre(nwnmax - 1, theta[is], alf);
+    int nwe = 0;
+    for (int jf = nf1; jf <= nf2; ++jf) {
+      int nwa = nwe + 1;
+      nwe = nwe + nwn[jf - 1];
+      std::vector<double> tap;
+      taper(nwn[jf - 1] - 1, 0.2, tap);
+      for (int k = 1; k <= 14; ++k) {
+        int col = offset(MSUM[k - 1].comp, MSUM[k - 1].jump) - 1;
+        if (col >= nsp) return 2;
+        zc z = momentSum(k, gr + (size_t)col * nkfmax + (nwa - 1), gi + (size_t)col * nkfmax + (nwa - 1),
+                         nwn[jf - 1], alf, tap);
+        size_t o = (((size_t)is * nf2 + (jf - 1)) * 14 + (k - 1)) * 2;
+        hd[o] = z.re; hd[o + 1] = z.im;
+      }
+    }
+  }
+  return 0;
+}
+
+// Full phase 2 for moment tensor sources: traces[((sta*nmt + imt)*3 + comp)*nsamp + i]
+// comp order Z, N, E.  filspecs = {nord_hp, fc_hp, nord_lp, fc_lp}.
+int oracle_synthetics(int nf1, int nf2, const int* nwn, int nwnmax, double df, double sigma,
+                      int nkfmax, int nsp, const float* gr, const float* gi, int nsta,
+                      const double* theta, const double* phi, const double* propdir, int nmt,
+                      const double* mt, const double* filspecs, int velocity, double tred,
+                      int nsamp, double dt, float* traces) {
+  std::vector<double> hd((size_t)nsta * nf2 * 14 * 2, 0.0);
+  int rc = oracle_degree_sums(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, nsta, theta, hd.data());
+  if (rc) return rc;
+  std::vector<zc> evf;
+  eventFilter((int)std::lround(filspecs[0]), filspecs[1], (int)std::lround(filspecs[2]), filspecs[3],
+              nf1, nf2, df, sigma, evf);
+  const zc ci = Z(0.0, 1.0);
+  for (int is = 0; is < nsta; ++is) {
+    double sphi = std::sin(phi[is]), cphi = std::cos(phi[is]);
+    double s2phi = std::sin((double)2.0f * phi[is]), c2phi = std::cos((double)2.0f * phi[is]);
+    double ca = std::cos(propdir[is]), sa = std::sin(propdir[is]);
+    for (int im = 0; im < nmt; ++im) {
+      const double* m = mt + im * 6;
+      std::vector<zc> zsp[3];
+      for (int c = 0; c < 3; ++c) zsp[c].assign(nf2 + 1, Z(0.0));
+      for (int jf = nf1; jf <= nf2; ++jf) {
+        const double* h = &hd[(((size_t)is * nf2 + (jf - 1)) * 14) * 2];
+        zc w[15];
+        for (int k = 1; k <= 14; ++k) w[k] = Z(h[(k - 1) * 2], h[(k - 1) * 2 + 1]);
+        // singleFrequencyDisplacement.f90:108-125
+        double t1 = m[3] * cphi + m[4] * sphi;
+        double t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
+        double t3 = m[4] * cphi - m[3] * sphi;
+        double t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
+        zsp[0][jf] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
+        zsp[1][jf] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
+        zsp[2][jf] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+      }
+      for (int jf = nf1; jf <= nf2; ++jf) {
+        zc tsf = zexp(((ci * TWO_PI_F) * (double)(jf - 1)) * df * tred) * std::exp(sigma * tred);
+        for (int c = 0; c < 3; ++c) zsp[c][jf] = ((zsp[c][jf] * evf[jf]) * Z(1.0, 0.0)) * tsf;
+      }
+      for (int jf = nf1; jf <= nf2; ++jf) {
+        if (velocity) {
+          zc zom = Z(TWO_PI_F * (double)(jf - 1) * df, -sigma);
+          for (int c = 0; c < 3; ++c) zsp[c][jf] = (zsp[c][jf] * ci) * zom;
+        }
+        zc ur = zsp[0][jf], ul = zsp[1][jf], ut = zsp[2][jf];
+        zc ue = sa * ul + ca * ut;
+        zc un = (-ca) * ul + sa * ut;
+        zsp[0][jf] = ur; zsp[1][jf] = un; zsp[2][jf] = ue;
+      }
+      for (int c = 0; c < 3; ++c) {
+        rc = freqTime(nf1, nf2, df, sigma, zsp[c], nsamp, dt,
+                      traces + (((size_t)is * nmt + im) * 3 + c) * nsamp);
+        if (rc) return rc;
+      }
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"
