@@ -1,0 +1,419 @@
+// C ABI of the FK hot path (include/gemini_fk.h): context, model, nodes,
+// frequency grid and the batched FK run.
+//
+// The reference's driver loops (computeGreenFKSpectraForSynthetics.f90:361-501)
+// become one launch: all (omega, l) items of a frequency slab are queued,
+// most expensive frequencies first, and drained by a persistent grid.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gemini_fk.h"
+#include "fk_kernel.h"
+#include "fk_types.cuh"
+
+using namespace gem;
+
+struct gem_ctx {
+  int device = 0;
+  int backend = GEM_BACKEND_GPU_FP64;
+  int nsm = 148;
+  std::string err;
+  // model (1-based host copies)
+  bool have_model = false;
+  double fref = 1, rearth = 0, ric = 0, roc = 0;
+  int aniflag = 0, fsflag = 0, equidis = 0, nlay = 0, nk = 0, nic = 0, noc = 0;
+  std::vector<int> iflso, iktop, ikbot;
+  std::vector<double> rb, drk, rk, ro, vpv, vph, vsv, vsh, eta, qkinv, qminv;
+  // device copies of the knot arrays (1-based)
+  double* d_knots = nullptr;   // 11 arrays of nk+1
+  int* d_lay = nullptr;        // iktop, ikbot
+  // nodes
+  bool have_nodes = false;
+  int nnod = 0;
+  std::vector<double> rnod;
+  std::vector<int> state, layer;
+  // buffers grown on demand
+  double* d_spl = nullptr; size_t spl_cap = 0;
+  double2* d_scratch = nullptr; size_t scratch_cap = 0;
+  int2* d_items = nullptr; size_t items_cap = 0;
+  int* d_slots = nullptr; size_t slots_cap = 0;   // jf + koff
+  unsigned int* d_queue = nullptr;
+  unsigned long long* d_stats = nullptr;
+  int* d_err = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  gem_stats stats{};
+};
+
+namespace {
+
+int fail(gem_ctx* c, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return GEM_ERROR;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) return fail(ctx, "%s: %s", #call, cudaGetErrorString(e_));   \
+  } while (0)
+
+template <class T>
+int grow(gem_ctx* ctx, T*& p, size_t& cap, size_t n) {
+  if (n <= cap && p) return GEM_OK;
+  if (p) cudaFree(p);
+  p = nullptr; cap = 0;
+  size_t want = std::max(n, (size_t)1);
+  CK(cudaMalloc((void**)&p, want * sizeof(T)));
+  cap = want;
+  return GEM_OK;
+}
+
+int nint_(double x) { return x >= 0 ? (int)std::floor(x + 0.5) : -(int)std::floor(-x + 0.5); }
+
+struct Grid {
+  double df, sigma, dwn;
+  int nf1, nf2, nwnmax;
+  std::vector<int> nwn;   // [nf2+1], 1-based jf
+};
+
+// computeGreenFKSpectraForSynthetics.f90:186-236
+void make_grid(const gem_fk_params* p, double rearth, Grid& g) {
+  const double PIF = PI_F, TWOPIF = TWO_PI_F;
+  g.df = 1.0 / p->tlen;
+  g.nf2 = nint_(p->fmax / g.df) + 1;
+  g.nf1 = std::max(nint_(p->fmin / g.df), 2);
+  double ommax = TWOPIF * (double)(g.nf2 - 1) * g.df;
+  g.sigma = 5.0 * g.df;
+  g.dwn = TWOPIF / p->xlen;
+  double wnmax = 0.5 * ommax * (p->p1lim + p->p2lim) / (1.0 - p->frac);
+  g.nwnmax = (int)(wnmax / g.dwn) + 1;
+  if (p->global_ == 1) g.nwnmax = nint_(wnmax * rearth - 0.5) + 1;
+  g.nwn.assign(g.nf2 + 1, 0);
+  for (int jf = g.nf1; jf <= g.nf2; ++jf) {
+    double f = (double)(jf - 1) * g.df;
+    double omre = 2.0 * PIF * f;
+    double wn2;
+    if (f <= 0.5 * (double)(g.nf2 - 1) * g.df) wn2 = omre * p->p1lim + p->frac * wnmax;
+    else wn2 = 0.5 * ommax * (p->p1lim + p->p2lim) + (omre - ommax) * p->p2lim + p->frac * wnmax;
+    if (p->global_ == 1) g.nwn[jf] = nint_(wn2 * rearth - 0.5) + 1;
+    else g.nwn[jf] = (int)(wn2 / g.dwn) + 1;
+  }
+}
+
+int nsp_of(const gem_fk_params* p) {
+  int njsph = p->istyp == 0 ? 2 : 4, njtor = p->istyp == 0 ? 1 : 2;
+  return p->stressflag ? 4 * njsph + 2 * njtor : 2 * njsph + njtor;
+}
+
+int check_params(gem_ctx* ctx, const gem_fk_params* p) {
+  if (!ctx->have_model) return fail(ctx, "no earth model loaded");
+  if (!ctx->have_nodes) return fail(ctx, "no external nodes set");
+  if (!p) return fail(ctx, "null parameters");
+  if (!(p->tlen > 0) || !(p->fmax > 0) || !(p->eps > 0)) return fail(ctx, "invalid TLEN/FMAX/ACCURACY");
+  if (p->attmode < 0 || p->attmode > 3) return fail(ctx, "Invalid attenuation mode");
+  if (p->istyp != 0 && p->istyp != 1) return fail(ctx, "Invalid source type");
+  if (p->jre < 1 || p->jre > ctx->nnod) return fail(ctx, "Invalid index for receiver node");
+  if (p->global_ == 0 && !(p->xlen > 0)) return fail(ctx, "invalid XLEN");
+  if (ctx->state[p->jre] == 1) return fail(ctx, "receiver in an ocean layer is not supported");
+  if (ctx->rnod[1] < ctx->rb[1])
+    return fail(ctx, "External nodes within inner homogeneous sphere (halfspace) are not allowed.");
+  return GEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gem_ctx_create(int device, int backend, gem_ctx** out) {
+  if (!out) return GEM_ERROR;
+  *out = nullptr;
+  if (backend != GEM_BACKEND_GPU_FP64) return GEM_ERROR;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) return GEM_ERROR;
+  gem_ctx* ctx = new gem_ctx();
+  ctx->device = device;
+  ctx->backend = backend;
+  if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return GEM_ERROR; }
+  cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
+  if (cudaMalloc(&ctx->d_queue, sizeof(unsigned int)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_stats, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) {
+    gem_ctx_destroy(ctx);
+    return GEM_ERROR;
+  }
+  for (auto& e : ctx->ev) cudaEventCreate(&e);
+  *out = ctx;
+  return GEM_OK;
+}
+
+void gem_ctx_destroy(gem_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaFree(ctx->d_knots); cudaFree(ctx->d_lay); cudaFree(ctx->d_spl); cudaFree(ctx->d_scratch);
+  cudaFree(ctx->d_items); cudaFree(ctx->d_slots); cudaFree(ctx->d_queue); cudaFree(ctx->d_stats);
+  cudaFree(ctx->d_err);
+  for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+  delete ctx;
+}
+
+const char* gem_last_error(const gem_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int gem_model_load(gem_ctx* ctx, const gem_model_desc* m) {
+  if (!ctx || !m) return GEM_ERROR;
+  CK(cudaSetDevice(ctx->device));
+  if (m->nlay < 2 || m->nlay > MAXLAY) return fail(ctx, "number of layers %d outside 2..%d", m->nlay, MAXLAY);
+  if (m->nk < 2 || m->nk > MAXKNOT - 1) return fail(ctx, "number of knots %d outside 2..%d", m->nk, MAXKNOT - 1);
+  if (m->iflso[m->nlay - 1] == 1 && m->fsflag == 1) return fail(ctx, "Full space and ocean is not allowed!!");
+  int L = m->nlay, K = m->nk;
+  ctx->fref = m->fref; ctx->rearth = m->rearth; ctx->ric = m->ric; ctx->roc = m->roc;
+  ctx->aniflag = m->aniflag; ctx->fsflag = m->fsflag; ctx->equidis = m->equidis;
+  ctx->nlay = L; ctx->nk = K; ctx->nic = m->nic; ctx->noc = m->noc;
+  ctx->iflso.assign(L + 1, 0); ctx->iktop.assign(L + 1, 0); ctx->ikbot.assign(L + 1, 0);
+  ctx->rb.assign(L + 1, 0.0); ctx->drk.assign(L + 1, -1.0);
+  for (int i = 1; i <= L; ++i) { ctx->iflso[i] = m->iflso[i - 1]; ctx->iktop[i] = m->iktop[i - 1]; ctx->rb[i] = m->rb[i - 1]; }
+  for (int i = 2; i <= L; ++i) ctx->ikbot[i] = ctx->iktop[i - 1] + 1;
+  for (int i = 1; i <= L; ++i)
+    if (ctx->iktop[i] < 1 || ctx->iktop[i] > K || (i > 1 && ctx->iktop[i] - ctx->ikbot[i] + 1 > MAX_LAYER_KNOTS))
+      return fail(ctx, "invalid layer knot indices");
+  auto cp = [&](std::vector<double>& v, const double* s) { v.assign(K + 1, 0.0); for (int i = 1; i <= K; ++i) v[i] = s[i - 1]; };
+  ctx->rk.assign(K + 1, 0.0);
+  for (int i = 1; i <= K; ++i) ctx->rk[i] = m->rearth - m->depth[i - 1];             // nodeEarthmodel.f90:175
+  for (int i = 2; i < K + 1; ++i)
+    if (!(ctx->rk[i] >= ctx->rk[i - 1])) return fail(ctx, "knot radii must not decrease");
+  if (m->equidis == 1)
+    for (int nl = 2; nl <= L; ++nl)
+      ctx->drk[nl] = (ctx->rk[ctx->iktop[nl]] - ctx->rk[ctx->ikbot[nl]]) / (double)(ctx->iktop[nl] - ctx->ikbot[nl]);
+  cp(ctx->ro, m->ro);
+  ctx->qkinv.assign(K + 1, 0.0); ctx->qminv.assign(K + 1, 0.0);
+  for (int i = 1; i <= K; ++i) {
+    ctx->qkinv[i] = 1.0 / m->qk[i - 1];
+    ctx->qminv[i] = 1.0 / m->qm[i - 1];
+    if (ctx->qminv[i] < 0.0) ctx->qminv[i] = 0.0;
+  }
+  if (m->aniflag == 0) {
+    cp(ctx->vpv, m->vpv); cp(ctx->vph, m->vpv); cp(ctx->vsv, m->vsv); cp(ctx->vsh, m->vsv);
+    ctx->eta.assign(K + 1, 1.0);
+  } else {
+    cp(ctx->vpv, m->vpv); cp(ctx->vph, m->vph); cp(ctx->vsv, m->vsv); cp(ctx->vsh, m->vsh); cp(ctx->eta, m->eta);
+  }
+  for (int i = 1; i <= K; ++i)
+    if (!std::isfinite(ctx->ro[i]) || !std::isfinite(ctx->vpv[i]) || !std::isfinite(ctx->vsv[i]) ||
+        !std::isfinite(ctx->rk[i]))
+      return fail(ctx, "non-finite model value at knot %d", i);
+  // device knot arrays: ro vpv vph vsv vsh eta qkinv qminv rk
+  cudaFree(ctx->d_knots); ctx->d_knots = nullptr;
+  cudaFree(ctx->d_lay); ctx->d_lay = nullptr;
+  CK(cudaMalloc(&ctx->d_knots, 9 * (K + 1) * sizeof(double)));
+  CK(cudaMalloc(&ctx->d_lay, 2 * (L + 1) * sizeof(int)));
+  const std::vector<double>* arr[9] = {&ctx->ro, &ctx->vpv, &ctx->vph, &ctx->vsv, &ctx->vsh,
+                                       &ctx->eta, &ctx->qkinv, &ctx->qminv, &ctx->rk};
+  for (int a = 0; a < 9; ++a)
+    CK(cudaMemcpy(ctx->d_knots + a * (K + 1), arr[a]->data(), (K + 1) * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_lay, ctx->iktop.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_lay + (L + 1), ctx->ikbot.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  ctx->have_model = true;
+  ctx->have_nodes = false;
+  return GEM_OK;
+}
+
+int gem_nodes_set(gem_ctx* ctx, int nnod, const double* r, const int* state, const int* layer) {
+  if (!ctx) return GEM_ERROR;
+  if (!ctx->have_model) return fail(ctx, "load the earth model before the nodes");
+  if (nnod < 1 || nnod > MAXNOD) return fail(ctx, "number of nodes %d outside 1..%d", nnod, MAXNOD);
+  ctx->nnod = nnod;
+  ctx->rnod.assign(nnod + 1, 0.0); ctx->state.assign(nnod + 1, 0); ctx->layer.assign(nnod + 1, 0);
+  for (int i = 1; i <= nnod; ++i) {
+    ctx->rnod[i] = r[i - 1]; ctx->state[i] = state[i - 1]; ctx->layer[i] = layer[i - 1];
+    if (ctx->layer[i] < 1 || ctx->layer[i] > ctx->nlay) return fail(ctx, "node %d: layer out of range", i);
+    if (!(ctx->rnod[i] > 0) || (i > 1 && !(ctx->rnod[i] > ctx->rnod[i - 1])))
+      return fail(ctx, "node radii must be positive and ascending");
+  }
+  ctx->have_nodes = true;
+  return GEM_OK;
+}
+
+int gem_fk_grid(gem_ctx* ctx, const gem_fk_params* p, int* nf1, int* nf2, int* nwnmax, int* nsp, int* nwn, int cap) {
+  if (!ctx || !p) return GEM_ERROR;
+  if (!ctx->have_model) return fail(ctx, "no earth model loaded");
+  Grid g;
+  make_grid(p, ctx->rearth, g);
+  if (nf1) *nf1 = g.nf1;
+  if (nf2) *nf2 = g.nf2;
+  if (nwnmax) *nwnmax = g.nwnmax;
+  if (nsp) *nsp = nsp_of(p);
+  if (nwn) {
+    if (cap < g.nf2) return fail(ctx, "nwn capacity %d < nf2 %d", cap, g.nf2);
+    for (int jf = 1; jf <= g.nf2; ++jf) nwn[jf - 1] = g.nwn[jf];
+  }
+  return GEM_OK;
+}
+
+int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre, float* d_gfim,
+                      double* d_gf64, int32_t* d_status, void* stream) {
+  if (!ctx) return GEM_ERROR;
+  int rc = check_params(ctx, p);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  Grid g;
+  make_grid(p, ctx->rearth, g);
+  if (jf_first < g.nf1 || jf_last > g.nf2 || jf_first > jf_last)
+    return fail(ctx, "frequency range %d..%d outside %d..%d", jf_first, jf_last, g.nf1, g.nf2);
+  const int nslot = jf_last - jf_first + 1;
+  const int nsp = nsp_of(p);
+  // ---- parameter block
+  FKStatic P;
+  memset(&P, 0, sizeof P);
+  P.nlay = ctx->nlay; P.nk = ctx->nk; P.noc = ctx->noc; P.nic = ctx->nic; P.equidis = ctx->equidis;
+  P.fsflag = ctx->fsflag; P.nnod = ctx->nnod; P.jre = p->jre;
+  P.hascore = (ctx->noc > 0 && ctx->iflso[ctx->noc] == 1) ? 1 : 0;
+  P.hasocean = ctx->iflso[ctx->nlay] == 1 ? 1 : 0;
+  P.istyp = p->istyp; P.stressflag = p->stressflag; P.global_ = p->global_; P.nsp = nsp;
+  P.ncsph = 4; P.nctor = 2;
+  P.njsph = p->istyp == 0 ? 2 : 4; P.njtor = p->istyp == 0 ? 1 : 2;
+  P.dsvstep = p->stressflag ? 1 : 2;
+  P.rearth = ctx->rearth; P.ric = ctx->ric; P.roc = ctx->roc; P.rhs = ctx->rb[1];
+  P.ruc = P.hasocean ? ctx->rb[ctx->nlay - 1] : ctx->rearth;
+  P.eps = p->eps; P.sigma = g.sigma; P.df = g.df; P.dwn = g.dwn;
+  for (int i = 1; i <= ctx->nlay; ++i) {
+    P.rb[i] = ctx->rb[i]; P.drk[i] = ctx->drk[i]; P.iflso[i] = ctx->iflso[i]; P.iktop[i] = ctx->iktop[i];
+  }
+  for (int i = 1; i <= ctx->nk; ++i) P.rk[i] = ctx->rk[i];
+  for (int i = 1; i <= ctx->nnod; ++i) { P.rnod[i] = ctx->rnod[i]; P.state[i] = ctx->state[i]; P.layer[i] = ctx->layer[i]; }
+  // ---- frequency slots and the work queue (high frequencies first)
+  std::vector<int> slots(2 * nslot);
+  long long nkf = 0;
+  for (int s = 0; s < nslot; ++s) {
+    slots[s] = jf_first + s;
+    slots[nslot + s] = (int)nkf;
+    nkf += g.nwn[jf_first + s];
+  }
+  std::vector<int2> items;
+  items.reserve((size_t)nkf);
+  for (int s = nslot - 1; s >= 0; --s)
+    for (int iwn = 1; iwn <= g.nwn[jf_first + s]; ++iwn) items.push_back(make_int2(s, iwn));
+  const int nitems = (int)items.size();
+  if (grow(ctx, ctx->d_items, ctx->items_cap, items.size())) return GEM_ERROR;
+  if (grow(ctx, ctx->d_slots, ctx->slots_cap, slots.size())) return GEM_ERROR;
+  CK(cudaMemcpyAsync(ctx->d_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  // ---- K3: model preparation for all slots
+  size_t spl_n = (size_t)nslot * (ctx->nk + 1) * SPL_STRIDE;
+  if (grow(ctx, ctx->d_spl, ctx->spl_cap, spl_n)) return GEM_ERROR;
+  CK(cudaMemsetAsync(ctx->d_spl, 0, spl_n * sizeof(double), st));
+  CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  PrepArgs A;
+  const int K1 = ctx->nk + 1;
+  A.nslot = nslot; A.nk = ctx->nk; A.nlay = ctx->nlay; A.attmode = p->attmode; A.df = g.df; A.fref = ctx->fref;
+  A.jf = ctx->d_slots;
+  A.ro = ctx->d_knots; A.vpv = ctx->d_knots + K1; A.vph = ctx->d_knots + 2 * K1; A.vsv = ctx->d_knots + 3 * K1;
+  A.vsh = ctx->d_knots + 4 * K1; A.eta = ctx->d_knots + 5 * K1; A.qkinv = ctx->d_knots + 6 * K1;
+  A.qminv = ctx->d_knots + 7 * K1; A.rk = ctx->d_knots + 8 * K1;
+  A.iktop = ctx->d_lay; A.ikbot = ctx->d_lay + (ctx->nlay + 1);
+  A.spl = ctx->d_spl;
+  CK(cudaEventRecord(ctx->ev[0], st));
+  CK(launch_prep(A, ctx->d_err, st));
+  CK(cudaEventRecord(ctx->ev[1], st));
+  // ---- outputs zeroed (unreached nodes and skipped items stay zero)
+  size_t nout = (size_t)nkf * nsp * ctx->nnod;
+  if (d_gf64) CK(cudaMemsetAsync(d_gf64, 0, nout * 2 * sizeof(double), st));
+  if (d_gfre) CK(cudaMemsetAsync(d_gfre, 0, nout * sizeof(float), st));
+  if (d_gfim) CK(cudaMemsetAsync(d_gfim, 0, nout * sizeof(float), st));
+  // ---- K1/K2 persistent solver
+  int bps = fk_blocks_per_sm();
+  int grid = ctx->nsm * bps;
+  long long nthreads = (long long)grid * FK_BLOCK;
+  size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * Layout::PER_NODE;
+  if (grow(ctx, ctx->d_scratch, ctx->scratch_cap, scratch_n)) return GEM_ERROR;
+  CK(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(unsigned long long), st));
+  FKLaunch L;
+  L.spl = ctx->d_spl; L.jf = ctx->d_slots; L.koff = ctx->d_slots + nslot; L.items = ctx->d_items;
+  L.nitems = nitems; L.nkf = nkf; L.gf64 = (double2*)d_gf64; L.gfre = d_gfre; L.gfim = d_gfim;
+  L.status = d_status; L.scratch = ctx->d_scratch; L.nthreads = nthreads; L.queue = ctx->d_queue;
+  L.stats = ctx->d_stats;
+  CK(cudaEventRecord(ctx->ev[2], st));
+  CK(launch_fk(P, L, grid, st));
+  CK(cudaEventRecord(ctx->ev[3], st));
+  // ---- statistics (synchronises the stream)
+  unsigned long long hs[8];
+  int herr = 0;
+  CK(cudaMemcpyAsync(hs, ctx->d_stats, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (herr) return fail(ctx, "Cubic spline interpolation not successful (code %d)", herr);
+  float t_prep = 0, t_solve = 0;
+  cudaEventElapsedTime(&t_prep, ctx->ev[0], ctx->ev[1]);
+  cudaEventElapsedTime(&t_solve, ctx->ev[2], ctx->ev[3]);
+  ctx->stats.steps_ok = hs[0]; ctx->stats.steps_rej = hs[1]; ctx->stats.attempts = hs[2];
+  ctx->stats.sysmats = hs[3]; ctx->stats.matvecs = hs[4]; ctx->stats.flops = hs[5];
+  ctx->stats.items = nitems; ctx->stats.failed = 0;
+  ctx->stats.prep_ms = t_prep; ctx->stats.solve_ms = t_solve;
+  return GEM_OK;
+}
+
+int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* gfre, float* gfim,
+               double* gf64, int32_t* status) {
+  if (!ctx) return GEM_ERROR;
+  int rc = check_params(ctx, p);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  Grid g;
+  make_grid(p, ctx->rearth, g);
+  if (jf_first < g.nf1 || jf_last > g.nf2 || jf_first > jf_last)
+    return fail(ctx, "frequency range %d..%d outside %d..%d", jf_first, jf_last, g.nf1, g.nf2);
+  long long nkf = 0;
+  for (int jf = jf_first; jf <= jf_last; ++jf) nkf += g.nwn[jf];
+  size_t nout = (size_t)nkf * nsp_of(p) * ctx->nnod;
+  float *dre = nullptr, *dim = nullptr;
+  double* d64 = nullptr;
+  int32_t* dst = nullptr;
+  int ret = GEM_OK;
+  cudaStream_t st = nullptr;
+  auto cleanup = [&]() { cudaFree(dre); cudaFree(dim); cudaFree(d64); cudaFree(dst); };
+  if ((gfre && cudaMalloc(&dre, nout * sizeof(float)) != cudaSuccess) ||
+      (gfim && cudaMalloc(&dim, nout * sizeof(float)) != cudaSuccess) ||
+      (gf64 && cudaMalloc(&d64, nout * 2 * sizeof(double)) != cudaSuccess) ||
+      cudaMalloc(&dst, (size_t)nkf * sizeof(int32_t)) != cudaSuccess) {
+    cleanup();
+    return fail(ctx, "device allocation of %zu outputs failed", nout);
+  }
+  ret = gem_fk_run_device(ctx, p, jf_first, jf_last, dre, dim, d64, dst, st);
+  if (ret == GEM_OK) {
+    std::vector<int32_t> hst((size_t)nkf);
+    if ((gfre && cudaMemcpy(gfre, dre, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (gfim && cudaMemcpy(gfim, dim, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (gf64 && cudaMemcpy(gf64, d64, nout * 2 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        cudaMemcpy(hst.data(), dst, (size_t)nkf * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      ret = fail(ctx, "copy of FK spectra to the host failed");
+    } else {
+      long long nfail = 0;
+      for (auto v : hst) nfail += v != 0;
+      ctx->stats.failed = nfail;
+      if (status) memcpy(status, hst.data(), hst.size() * sizeof(int32_t));
+      if (nfail) ret = fail(ctx, "%lld (omega,l) items failed; see the per-item status", nfail);
+    }
+  }
+  cleanup();
+  return ret;
+}
+
+int gem_stats_get(const gem_ctx* ctx, gem_stats* out) {
+  if (!ctx || !out) return GEM_ERROR;
+  *out = ctx->stats;
+  return GEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+"""ctypes binding of libgemini_fk.so: FK spectra on the GPU.
+
+The host-side counterpart of computeGreenFKSpectraForSynthetics
+(f90/computeGreenFKSpectraForSynthetics.f90): load the earth model and the
+external nodes once, then compute the FK spectra gf(iwn, isp, node) of any
+frequency slab in one call.  There is no CPU path: without the CUDA library
+or a GPU every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+from .model import (ExternalRadialNodes, FKParams, GeminiError, NodeEarthModel, fk_params_c,
+                    frequency_grid, nsp_for)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libgemini_fk.so")
+
+GEM_BACKEND_GPU_FP64 = 1
+STATUS_TEXT = {0: "ok", 1: "step size smaller than minimum", 2: "maximum number of steps reached",
+               3: "continued fraction did not converge", 4: "node/discontinuity bookkeeping",
+               5: "non-finite value", 7: "ocean receiver or source not supported"}
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in
+                ("steps_ok", "steps_rej", "attempts", "sysmats", "matvecs", "flops", "items", "failed")] + \
+               [("solve_ms", ctypes.c_double), ("prep_ms", ctypes.c_double)]
+
+    def asdict(self):
+        return {n: (getattr(self, n)) for n, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the CUDA library; raise loudly when it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GeminiError("libgemini_fk.so is not built (python -m gemini_unified_b200.build)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p
+        L.gem_ctx_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+        L.gem_ctx_destroy.argtypes = [vp]
+        L.gem_ctx_destroy.restype = None
+        L.gem_last_error.argtypes = [vp]
+        L.gem_last_error.restype = ctypes.c_char_p
+        L.gem_model_load.argtypes = [vp, vp]
+        L.gem_nodes_set.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+        L.gem_fk_grid.argtypes = [vp, vp, ip, ip, ip, ip, vp, ctypes.c_int]
+        L.gem_fk_run.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
+        L.gem_fk_run_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
+        L.gem_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class GeminiFK:
+    """One GPU context with an earth model and external radial nodes loaded."""
+
+    def __init__(self, model: NodeEarthModel, nodes: ExternalRadialNodes, device: int = 0,
+                 backend: int = GEM_BACKEND_GPU_FP64):
+        self._h = ctypes.c_void_p()
+        rc = lib().gem_ctx_create(device, backend, ctypes.byref(self._h))
+        if rc != 0 or not self._h:
+            raise GeminiError("gem_ctx_create failed (no CUDA device %d or unsupported backend)" % device)
+        self.model, self.nodes = model, nodes
+        self._desc = model.desc()
+        self._check(lib().gem_model_load(self._h, ctypes.byref(self._desc)))
+        self._r = np.ascontiguousarray(nodes.r, np.float64)
+        self._s = np.ascontiguousarray(nodes.state, np.int32)
+        self._l = np.ascontiguousarray(nodes.layer, np.int32)
+        self._check(lib().gem_nodes_set(self._h, len(self._r), _ptr(self._r), _ptr(self._s), _ptr(self._l)))
+
+    def _check(self, rc: int):
+        if rc >= 2:
+            raise GeminiError(lib().gem_last_error(self._h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gem_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def grid(self, params: FKParams, jre: int):
+        pc = fk_params_c(params, jre)
+        nf1, nf2, nwnmax, nsp = (ctypes.c_int() for _ in range(4))
+        cap = 1 << 20
+        nwn = np.zeros(cap, np.int32)
+        self._check(lib().gem_fk_grid(self._h, ctypes.byref(pc), ctypes.byref(nf1), ctypes.byref(nf2),
+                                      ctypes.byref(nwnmax), ctypes.byref(nsp), _ptr(nwn), cap))
+        return nf1.value, nf2.value, nwnmax.value, nsp.value, nwn[: nf2.value].copy()
+
+    def run(self, params: FKParams, jre: int, jf_first: int, jf_last: int, f32: bool = True,
+            f64: bool = True, raise_on_failure: bool = True):
+        """FK spectra of frequencies jf_first..jf_last.
+
+        Returns (gfre, gfim, gf64, status) with gf arrays shaped
+        (nnod, nsp, nkf) -- the transpose view of the Fortran (nkf, nsp, nnod)
+        layout -- and status per wavenumber-frequency index k.
+        """
+        grid = frequency_grid(params, self.model.rearth)
+        nkf = int(grid.nwn[jf_first - 1: jf_last].sum())
+        nsp = nsp_for(params)
+        nnod = self.nodes.nnod
+        pc = fk_params_c(params, jre)
+        gre = np.zeros((nnod, nsp, nkf), np.float32) if f32 else None
+        gim = np.zeros((nnod, nsp, nkf), np.float32) if f32 else None
+        g64 = np.zeros((nnod, nsp, nkf), np.complex128) if f64 else None
+        status = np.zeros(nkf, np.int32)
+        rc = lib().gem_fk_run(self._h, ctypes.byref(pc), jf_first, jf_last, _ptr(gre), _ptr(gim), _ptr(g64),
+                              _ptr(status))
+        if rc >= 2 and (raise_on_failure or not np.any(status)):
+            raise GeminiError(lib().gem_last_error(self._h).decode())
+        return gre, gim, g64, status
+
+    def run_device(self, params: FKParams, jre: int, jf_first: int, jf_last: int, gfre=None, gfim=None,
+                   gf64=None, status=None, stream: int = 0):
+        """Same on caller-provided device buffers (integer device pointers)."""
+        pc = fk_params_c(params, jre)
+        self._check(lib().gem_fk_run_device(self._h, ctypes.byref(pc), jf_first, jf_last, gfre, gfim, gf64,
+                                            status, stream or None))
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(lib().gem_stats_get(self._h, ctypes.byref(s)))
+        return s.asdict()

@@ -1,0 +1,112 @@
+/*
+ * gemini_fk.h -- C ABI of the B200 GEMINI frequency-wavenumber hot path.
+ *
+ * Plain C types only; every array is caller-owned.  FK spectra use the
+ * reference's Fortran layout gf(iwn, isp, node), iwn fastest, i.e. element
+ * (k, isp, n) of a slab of frequencies is at  k + nkf*(isp + nsp*n)  where k
+ * runs over the wavenumbers of all frequencies of the slab
+ * (computeGreenFKSpectraForSynthetics.f90:508-519, HDF5 dataset
+ * (nkfmax, nsp, nnod)).
+ *
+ * Return codes follow the reference's error levels (errorMessage.f90:47):
+ * 0 ok, 1 warning, 2 error.  The library never exits or aborts; the text of
+ * the last error is available from gem_last_error.
+ *
+ * Per-item status codes (int32, one per wavenumber-frequency index k):
+ *   0 ok, 1 step size below minimum (integrationStep.f90:176-180),
+ *   2 maximum number of steps (integrationStep.f90:186),
+ *   3 continued fraction did not converge (initialValues.f90:490-574),
+ *   4 node/discontinuity bookkeeping (propagateOde.f90:177-186,319-324),
+ *   5 non-finite value, 7 receiver or source in an ocean layer (unsupported).
+ */
+#ifndef GEMINI_FK_H
+#define GEMINI_FK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GEM_OK 0
+#define GEM_WARNING 1
+#define GEM_ERROR 2
+
+#define GEM_BACKEND_GPU_FP64 1 /* faithful FP64 solver, the parity path */
+
+typedef struct gem_ctx gem_ctx;
+
+/* Node earth model: replaces createNodeEarthmodel (nodeEarthmodel.f90:98-257).
+ * Arrays are the JSON file's columns: 1-based semantics, 0-based storage. */
+typedef struct gem_model_desc {
+  double fref, rearth, ric, roc;
+  int aniflag, fsflag, equidis, nlay, nk, nic, noc;
+  const int* iflso;    /* [nlay] 1 fluid, 0 solid */
+  const int* iktop;    /* [nlay] 1-based knot index of each layer's top */
+  const double* rb;    /* [nlay] radius of each layer's top (m) */
+  const double* depth; /* [nk] knot depth (m) */
+  const double* ro;    /* [nk] density */
+  const double* vpv;
+  const double* vph;
+  const double* vsv;
+  const double* vsh;
+  const double* eta;
+  const double* qk;    /* Q kappa */
+  const double* qm;    /* Q mu */
+} gem_model_desc;
+
+/* Parfile keys of computeGreenFKSpectraForSynthetics on the hot path
+ * (computeGreenFKSpectraForSynthetics.f90:89-94,186-236). */
+typedef struct gem_fk_params {
+  double tlen, fmax, fmin, p1lim, p2lim, frac, xlen, eps;
+  int global_;     /* GLOBAL: 1 spherical harmonics, 0 wavenumbers */
+  int attmode;     /* 0 ELASTIC 1 ATTENUATION_ONLY 2 DISPERSION_ONLY 3 ATTENUATION_AND_DISPERSION */
+  int istyp;       /* 0 FORCE, 1 MOMENT */
+  int stressflag;  /* STRESSFLAG */
+  int jre;         /* receiver node, 1-based */
+} gem_fk_params;
+
+typedef struct gem_stats {
+  int64_t steps_ok, steps_rej, attempts, sysmats, matvecs, flops;
+  int64_t items, failed;
+  double solve_ms; /* device time of the last solver launch */
+  double prep_ms;  /* device time of the last model preparation */
+} gem_stats;
+
+/* Context holding the model, nodes and device buffers of one GPU.
+ * Replaces the module globals sec_* (splineEarthmodelCoefficients.f90:28-41);
+ * one host thread per context. */
+int gem_ctx_create(int device, int backend, gem_ctx** out);
+void gem_ctx_destroy(gem_ctx* ctx);
+const char* gem_last_error(const gem_ctx* ctx);
+
+/* Earth model (createNodeEarthmodel, nodeEarthmodel.f90:98). */
+int gem_model_load(gem_ctx* ctx, const gem_model_desc* model);
+
+/* External radial nodes after splitting at discontinuities
+ * (createExternalRadialNodes, externalRadialNodes.f90:82); radii ascending. */
+int gem_nodes_set(gem_ctx* ctx, int nnod, const double* rnod, const int* state, const int* layer);
+
+/* Frequency grid (computeGreenFKSpectraForSynthetics.f90:186-236): nf1, nf2,
+ * nwnmax and nwn[jf-1] for jf = 1..nf2 (nwn_cap >= nf2); *nsp = spectra per node. */
+int gem_fk_grid(gem_ctx* ctx, const gem_fk_params* p, int* nf1, int* nf2, int* nwnmax, int* nsp, int* nwn,
+                int nwn_cap);
+
+/* FK spectra of frequencies jf_first..jf_last (the wavenumber loop body
+ * computeGreenFKSpectraForSynthetics.f90:410-501 for all l, all frequencies in
+ * one launch).  Host buffers; any output pointer may be NULL.  Blocking.
+ * gfre/gfim: float32, gf64: interleaved complex128, status: int32 per k. */
+int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* gfre, float* gfim,
+               double* gf64, int32_t* status);
+
+/* Same with device buffers, ordered on `stream` (a cudaStream_t, may be NULL). */
+int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
+                      float* d_gfim, double* d_gf64, int32_t* d_status, void* stream);
+
+/* Counters of the last run (accepted/rejected steps, attempts, flops, ...). */
+int gem_stats_get(const gem_ctx* ctx, gem_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GEMINI_FK_H */
