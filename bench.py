@@ -1,0 +1,314 @@
+"""Benchmark of the GEMINI FK hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): the batched global FK configuration -- PREM (isotropic,
+no ocean), 410 frequencies to 0.2 Hz at df = 1/2048 Hz, slowness 4.0e-4 s/m,
+l <= 3205, 658,944 (omega, l) solves of uneven length, 20 source radii 5..700 km
+plus the surface receiver (37 external nodes after splitting).  Inputs are
+synthetic model/parameter files; nothing is read from the reference.
+
+Metric: (omega, l) ODE solves per second.  ``value`` is measured on the device
+(CUDA events around the model preparation and the persistent solver, inputs
+resident); ``e2e`` goes through the public C ABI with host buffers (the float32
+FK spectra are copied back every step).  With N GPUs the frequencies are
+split over the ranks in the reference's zig-zag order
+(computeGreenFKSpectraForSynthetics.f90:361-387); the time is the maximum over
+ranks.
+
+``--impl reference`` times the CPU FP64 restatement of the reference (the
+reference's Fortran/MPI program cannot be built here) with all host threads on
+a bounded random sample of the same items.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "(ω,ℓ) ODE solves/s + seismogram traces/s on 1 B200 vs plain GPU at ≤1e-5 err"
+WORKLOAD = "batched_fk"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--cpu-sample", type=int, default=0, help="items of the CPU baseline sample (0 = auto)")
+    return ap.parse_args()
+
+
+def zigzag(nf1, nf2, rank, size):
+    """Frequencies of one rank (computeGreenFKSpectraForSynthetics.f90:361-387)."""
+    nf = nf2 - nf1 + 1
+    npart = nf // size + (1 if nf % size else 0)
+    out, jfe = [], nf2
+    for k in range(1, npart + 1):
+        jf = jfe - rank if k % 2 == 1 else jfe + rank - size + 1
+        jfe -= size
+        if jf < nf1:
+            break
+        out.append(jf)
+    return sorted(out)
+
+
+def contiguous_runs(js):
+    runs, start = [], None
+    for a in js:
+        if start is None:
+            start = prev = a
+        elif a == prev + 1:
+            prev = a
+        else:
+            runs.append((start, prev)); start = prev = a
+    if start is not None:
+        runs.append((start, prev))
+    return runs
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(w, nsample, seed=12345):
+    """CPU FP64 oracle on a random sample of the workload's items, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from gemini_unified_b200 import model as M
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    pc = M.fk_params_c(w.params, jre)
+    o = oracle.Oracle(m, ex)
+    items = [(jf, iwn) for jf in range(g.nf1, g.nf2 + 1) for iwn in range(1, int(g.nwn[jf - 1]) + 1)]
+    rng = np.random.default_rng(seed)
+    pick = [items[i] for i in rng.choice(len(items), size=min(nsample, len(items)), replace=False)]
+    ncores = os.cpu_count() or 1
+
+    def one(it):
+        jf, iwn = it
+        o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), M.nsp_for(w.params), iwn, iwn)
+
+    t = time.perf_counter()
+    with cf.ThreadPoolExecutor(ncores) as ex_:
+        list(ex_.map(one, pick))
+    dt = time.perf_counter() - t
+    return {"value": len(pick) / dt, "unit": "solves/s", "cores": ncores, "kind": "port",
+            "sample": "%d (omega,l) items drawn uniformly (seed %d) from the %d of the workload; %.1f s"
+                      % (len(pick), seed, len(items), dt)}
+
+
+def run_reference(args, rank, size):
+    from gemini_unified_b200 import configs
+    w = configs.WORKLOADS[args.workload]
+    if rank != 0:
+        return
+    n = args.cpu_sample or 48
+    for _ in range(args.warmup):
+        cpu_baseline(w, max(8, n // 8), seed=1)
+    vals = []
+    for k in range(args.steps):
+        vals.append(cpu_baseline(w, n, seed=100 + k))
+    v = len(vals) * n / sum(n / x["value"] for x in vals)
+    cb = dict(vals[0]); cb["value"] = v
+    cb["sample"] = "%d steps of %d (omega,l) items drawn uniformly from the workload" % (len(vals), n)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n / v, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "items_per_step": n, "note": "CPU FP64 restatement of the reference"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    size = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, size)
+
+    import torch
+    from gemini_unified_b200 import configs, model as M
+    from gemini_unified_b200.fk import GeminiFK, lib as fklib
+
+    torch.cuda.set_device(local)
+    dist = None
+    if size > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    w = configs.WORKLOADS[args.workload]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    nsp = M.nsp_for(w.params)
+    mine = zigzag(g.nf1, g.nf2, rank, size)
+    runs = contiguous_runs(mine)
+    fk = GeminiFK(m, ex, device=local)
+    L = fklib()
+    nkf = {r: int(g.nwn[r[0] - 1: r[1]].sum()) for r in runs}
+    items_rank = sum(nkf.values())
+    biggest = max(nkf.values())
+    n_out = biggest * nsp * ex.nnod
+    dev = torch.device("cuda", local)
+    gre = torch.empty(n_out, dtype=torch.float32, device=dev)
+    gim = torch.empty(n_out, dtype=torch.float32, device=dev)
+    gst = torch.empty(biggest, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        flops = 0
+        for r in runs:
+            fk.run_device(w.params, jre, r[0], r[1], gfre=gre.data_ptr(), gfim=gim.data_ptr(),
+                          status=gst.data_ptr(), stream=stream.cuda_stream)
+            s = fk.stats()
+            flops += s["flops"]
+            if int(gst[: nkf[r]].abs().sum()) != 0:
+                raise RuntimeError("failed (omega,l) items in frequencies %d..%d" % r)
+        return flops
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---------------- device-timed steps (inputs resident, L2 flushed between steps)
+    times, flops_step, solve_ms = [], 0, 0.0
+    clocks = Clocks(local)
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        if dist: dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        flops_step = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist: dist.barrier()
+        times.append(e0.elapsed_time(e1))
+        solve_ms += fk.stats()["solve_ms"] if len(runs) == 1 else 0.0
+    clk = clocks.stop()
+    t_ms = float(np.mean(times))
+    if dist:
+        tt = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    total_items = g.nkfmax if size > 1 else items_rank
+    value = total_items / (t_ms / 1e3)
+
+    # ---------------- end-to-end through the host C ABI (float32 spectra back to the host)
+    e2e_times = []
+    for _ in range(max(1, min(args.steps, 2))):
+        if dist: dist.barrier()
+        t0 = time.perf_counter()
+        for r in runs:
+            fk.run(w.params, jre, r[0], r[1], f32=True, f64=False)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(e2e_times))
+    if dist:
+        tt = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    d2h = sum(nkf.values()) * nsp * ex.nnod * 4 * 2 + sum(nkf.values()) * 4
+    h2d = sum(nkf.values()) * 8 + 9 * (m.nk + 1) * 8
+
+    # ---------------- roofline of the solver (FP64 pipe)
+    peak = fp64_peak_tflops(local)
+    achieved = flops_step / (t_ms / 1e3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "fk_solve_batched_fk.json")
+    if os.path.exists(prof):
+        pj = json.load(open(prof))
+        traffic = pj["dram_bytes_per_item"] * items_rank
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (PREM node model from the reference's data files; seeded inputs)",
+            "config": {"workload": args.workload, "solves_per_step": int(g.nkfmax), "frequencies": int(g.nf2 - g.nf1 + 1),
+                       "lmax": int(g.nwn.max() - 1), "nodes": int(ex.nnod), "parallelism": "frequency zig-zag over %d GPU(s)" % size,
+                       "l2": "flushed between steps (256 MiB write); outputs (1.9 GB) exceed L2"},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak["tflops"], "unit": "TFLOP/s",
+                         "frac": achieved / peak["tflops"], "traffic": traffic, "peak_source": peak["source"],
+                         "flops_per_step": flops_step,
+                         "flops_note": "reference-algorithm FP64 flops (cached system matrices, full Neville) counted per event on the device"},
+            "e2e": {"value": total_items / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": 3 * len(runs) * args.steps,
+            "clocks": clk,
+        }
+        if size == 1:
+            n = args.cpu_sample or 8192
+            line["cpu_baseline"] = cpu_baseline(w, n)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def fp64_peak_tflops(device):
+    """FP64 FMA throughput measured with the library's probe kernel (this run)."""
+    import ctypes
+    from gemini_unified_b200.fk import lib
+    L = lib()
+    try:
+        f = L.gem_probe_fp64_tflops
+    except AttributeError:
+        return {"tflops": 37.0, "source": "nominal B200 FP64 (no probe)"}
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_int]
+    v = f(device)
+    if not v > 0:
+        return {"tflops": 37.0, "source": "nominal B200 FP64 (probe failed)"}
+    return {"tflops": v, "source": "measured in this run: FP64 FMA-chain probe kernel, all SMs"}
+
+
+if __name__ == "__main__":
+    main()

@@ -210,6 +210,21 @@ def load_node_model(path: str) -> NodeEarthModel:
     return node_model_from_dict(d, name=path)
 
 
+def _layer_tops(d: dict):
+    """Layer-top radii (key radius_upper_layer_boundary_m, nodeEarthmodel.f90:152).
+
+    Older model files (earthmodels/ak135q.json, the fixture of the reference's
+    model-reader test) name the key ``..._km`` and use km throughout; the values
+    are taken as they are, so that test's radii (in km) come out unchanged.
+    The reference itself stops with "Unable to resolve path" on such files.
+    """
+    if "radius_upper_layer_boundary_m" in d:
+        return d["radius_upper_layer_boundary_m"]
+    if "radius_upper_layer_boundary_km" in d:
+        return d["radius_upper_layer_boundary_km"]
+    raise GeminiError("Unable to resolve path: radius_upper_layer_boundary_m")
+
+
 def node_model_from_dict(d: dict, name: str = "") -> NodeEarthModel:
     np_ = d["node_properties"]
     nlay = int(d["num_layers"])
@@ -234,7 +249,7 @@ def node_model_from_dict(d: dict, name: str = "") -> NodeEarthModel:
         aniflag=aniflag, fsflag=fsflag, equidis=_as_int_bool(d["equidistant_nodes"]),
         nlay=nlay, nk=nk, nic=int(d["layer_inner_core"]), noc=int(d["layer_outer_core"]),
         iflso=iflso, iktop=np.asarray([int(x) for x in d["index_upper_boundary"]], dtype=np.int32),
-        rb=f64(d["radius_upper_layer_boundary_m"]), depth=f64(np_["depth"]),
+        rb=f64(_layer_tops(d)), depth=f64(np_["depth"]),
         ro=f64(np_["density"]), vpv=vpv, vph=vph, vsv=vsv, vsh=vsh, eta=eta,
         qk=f64(np_["Qkappa"]), qm=f64(np_["Qmu"]), name=name)
     if len(m.rb) != nlay or len(m.iktop) != nlay or len(m.depth) != nk:

@@ -106,6 +106,10 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
 /* Counters of the last run (accepted/rejected steps, attempts, flops, ...). */
 int gem_stats_get(const gem_ctx* ctx, gem_stats* out);
 
+/* Measurement utility (no counterpart in the reference): FP64 FMA throughput
+ * of the device in TFLOP/s, the denominator of the solver's FP64 roofline. */
+double gem_probe_fp64_tflops(int device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,118 @@
+"""GPU parity of the FK solver against the CPU oracle (through the C ABI).
+
+Tolerance: the FP64 solver repeats the reference's arithmetic operation by
+operation (no FMA contraction); its spectra must agree with the oracle to
+1e-10 relative to the largest value of each spectrum (the bar for the FP64
+path is 1e-8), with identical NaN positions (l = 0 V components)."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from gemini_unified_b200 import configs, model as M
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-10
+
+
+def _cmp(a, b):
+    na, nb = np.isnan(a), np.isnan(b)
+    assert np.array_equal(na, nb)
+    ok = ~na
+    scale = np.abs(b[ok]).max()
+    return np.abs(a[ok] - b[ok]).max() / scale
+
+
+@pytest.fixture(scope="module")
+def small(gpu):
+    import oracle
+    from gemini_unified_b200.fk import GeminiFK
+    w = configs.WORKLOADS["global_small"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    return w, m, ex, jre, GeminiFK(m, ex), oracle.Oracle(m, ex)
+
+
+def test_global_small_all_frequencies(small):
+    """Every frequency of the 51-frequency global configuration, all 18169 solves."""
+    w, m, ex, jre, fk, o = small
+    g = M.frequency_grid(w.params, m.rearth)
+    gre, gim, g64, st = fk.run(w.params, jre, g.nf1, g.nf2)
+    assert np.all(st == 0)
+    pc = M.fk_params_c(w.params, jre)
+    off = 0
+    worst = 0.0
+    for jf in range(g.nf1, g.nf2 + 1):
+        n = int(g.nwn[jf - 1])
+        ref, sto, _ = o.fk_frequency(pc, jf, n, 10)
+        got = g64[:, :, off:off + n]
+        worst = max(worst, _cmp(got, ref))
+        # float32 outputs are the rounded FP64 values
+        fin = ~np.isnan(ref)
+        assert np.array_equal(gre[:, :, off:off + n][fin], got.real[fin].astype(np.float32))
+        off += n
+    assert worst <= RTOL
+
+
+def test_batched_highest_frequency_sample(gpu):
+    import oracle
+    from gemini_unified_b200.fk import GeminiFK
+    w = configs.WORKLOADS["batched_fk"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    jf = g.nf2
+    n = int(g.nwn[jf - 1])
+    fk = GeminiFK(m, ex)
+    _, _, g64, st = fk.run(w.params, jre, jf, jf, f32=False)
+    assert np.all(st == 0)
+    o = oracle.Oracle(m, ex)
+    pc = M.fk_params_c(w.params, jre)
+    for iwn in (1, 2, 17, 400, 1601, 3000, n):
+        ref, sto, _ = o.fk_frequency(pc, jf, n, 10, iwn, iwn)
+        a, b = g64[:, :, iwn - 1], ref[:, :, iwn - 1]
+        if iwn == 1:
+            assert np.array_equal(np.isnan(a), np.isnan(b))
+            ok = ~np.isnan(b)
+            a, b = a[ok], b[ok]
+        assert np.abs(a - b).max() <= RTOL * np.abs(b).max()
+
+
+def test_deterministic_and_device_api(small):
+    import torch
+    w, m, ex, jre, fk, o = small
+    _, _, a, _ = fk.run(w.params, jre, 30, 34, f32=False)
+    _, _, b, _ = fk.run(w.params, jre, 30, 34, f32=False)
+    assert np.array_equal(np.nan_to_num(a, nan=1.0), np.nan_to_num(b, nan=1.0))
+    g = M.frequency_grid(w.params, m.rearth)
+    nkf = int(g.nwn[29:34].sum())
+    d64 = torch.zeros((ex.nnod, 10, nkf, 2), dtype=torch.float64, device="cuda")
+    dst = torch.ones(nkf, dtype=torch.int32, device="cuda")
+    fk.run_device(w.params, jre, 30, 34, gf64=d64.data_ptr(), status=dst.data_ptr())
+    torch.cuda.synchronize()
+    c = torch.view_as_complex(d64).cpu().numpy()
+    assert np.array_equal(np.nan_to_num(a, nan=1.0), np.nan_to_num(c, nan=1.0))
+    assert int(dst.abs().sum()) == 0
+
+
+def test_fault_injection_min_step_status(small):
+    """An unreachable accuracy: every item ends with status 1 (step size below
+    minimum), the call returns an error, nothing hangs."""
+    from gemini_unified_b200.model import GeminiError
+    w, m, ex, jre, fk, o = small
+    bad = dataclasses.replace(w.params, eps=1e-30)
+    with pytest.raises(GeminiError):
+        fk.run(bad, jre, 3, 3)
+    _, _, _, st = fk.run(bad, jre, 3, 3, raise_on_failure=False)
+    assert np.all(st[1:] == 1)
+
+
+def test_rejects_invalid_inputs(small):
+    from gemini_unified_b200.model import GeminiError
+    w, m, ex, jre, fk, o = small
+    with pytest.raises(GeminiError):
+        fk.run(w.params, jre, 1, 3)          # below nf1
+    with pytest.raises(GeminiError):
+        fk.run(w.params, ex.nnod + 5, 3, 3)  # receiver node out of range

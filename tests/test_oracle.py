@@ -1,0 +1,125 @@
+"""Self-consistency checks of the CPU oracle (no reference golden data exists
+for the FK hot path: the reference's regression data refseis/ is not shipped)."""
+import numpy as np
+import pytest
+
+import oracle
+from gemini_unified_b200 import configs, model as M
+
+
+def test_legendre_against_scipy():
+    sp = pytest.importorskip("scipy.special")
+    lmax = 60
+    for theta in (0.3, 1.2, 2.9):
+        t = oracle.legendre(lmax, theta)
+        ls = np.arange(lmax + 1)
+        x = np.cos(theta)
+        for m in range(3):
+            ref = sp.lpmv(m, ls, x) * (-1) ** m          # reference omits the Condon-Shortley sign
+            got = t[0, m]
+            mask = ls >= m
+            assert np.allclose(got[mask], ref[mask], rtol=1e-10, atol=1e-12 * np.abs(ref[mask]).max())
+        # dP/dtheta by central differences
+        eps = 1e-6
+        tp, tm = oracle.legendre(lmax, theta + eps), oracle.legendre(lmax, theta - eps)
+        fd = (tp[0] - tm[0]) / (2 * eps)
+        assert np.allclose(t[1], fd, rtol=1e-5, atol=1e-6 * np.abs(fd).max())
+        # P/sin(theta) for m >= 1
+        assert np.allclose(t[2, 1:, 1:], t[0, 1:, 1:] / np.sin(theta), rtol=1e-13)
+
+
+def test_legendre_poles():
+    t = oracle.legendre(10, 0.0)
+    ls = np.arange(11)
+    assert np.allclose(t[0, 0], 1.0)                         # P_l(1) = 1
+    assert np.allclose(t[1, 1], 0.5 * ls * (ls + 1))         # legendreFunctions.f90:113
+
+
+def test_fft_against_numpy():
+    n = 8
+    N = 1 << n
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(N); y = rng.standard_normal(N)
+    ox, oy = oracle.fft(x, y, n, +1)
+    ref = np.fft.ifft(x + 1j * y) * N                         # sum x_k exp(+2 pi i nk/N)
+    got = ox + 1j * oy
+    # twiddles use pi rounded to single precision (fourierTransform.f90:128)
+    assert np.max(np.abs(got - ref)) < 1e-4 * np.max(np.abs(ref))
+    dx, dy = oracle.fft(np.eye(1, N, 0)[0], np.zeros(N), n, +1)
+    assert np.all(dx == 1.0) and np.all(dy == 0.0)
+
+
+def test_degree_sums_against_direct_formula():
+    """harmonicDegreeSums.f90:231-351 evaluated independently in numpy."""
+    rng = np.random.default_rng(7)
+    nf1, nf2 = 2, 4
+    nwn = np.array([0, 30, 41, 52], np.int32)
+    nkf = int(nwn.sum())
+    gr = rng.standard_normal((10, nkf)).astype(np.float32)
+    gi = rng.standard_normal((10, nkf)).astype(np.float32)
+    theta = np.array([0.4, 2.0])
+    hd = oracle.degree_sums(nf1, nf2, nwn, 52, gr, gi, theta)
+    PI_F = M.PI_F
+    defs = [(0, 0, 0, 0.0, 0), (0, 0, 0, 0.0, 1), (0, 1, 1, 2.0, 2), (0, 2, 2, 2.0, 3), (1, 0, 1, 0.0, 4),
+            (1, 0, 1, 0.0, 5), (1, 1, 1, 2.0, 6), (1, 2, 2, 2.0, 7), (2, 1, 1, 2.0, 8), (2, 2, 2, 4.0, 9),
+            (1, 1, 1, 2.0, 8), (1, 2, 2, -2.0, 9), (2, 1, 1, 2.0, 6), (2, 2, 2, -4.0, 7)]
+    for it, th in enumerate(theta):
+        tab = oracle.legendre(51, th)
+        off = 0
+        for jf in range(nf1, nf2 + 1):
+            n = int(nwn[jf - 1]); lmax = n - 1
+            l = np.arange(n)
+            jt = max(1, min(int(np.floor(lmax * 0.8 + 0.5)), lmax))
+            c1 = lmax * 0.2 * 2.0 / PI_F; c2 = 0.8 / 0.2 * 0.5 * PI_F
+            tap = np.where(l < jt, 1.0, np.cos(l / c1 - c2) ** 2)
+            for k, (kind, m, l0, fac, col) in enumerate(defs):
+                g = gr[col, off:off + n].astype(np.float64) + 1j * gi[col, off:off + n]
+                T = tab[kind, m, :n]
+                w = np.ones(n) if fac == 0.0 else fac / np.maximum(l * (l + 1), 1)
+                terms = T * w * g * (2 * l + 1) / (4 * PI_F) * tap
+                ref = terms[l0:].sum()
+                assert abs(hd[it, jf - 1, k] - ref) <= 1e-12 * max(1.0, np.abs(terms).sum())
+            off += n
+
+
+@pytest.fixture(scope="module")
+def small():
+    w = configs.WORKLOADS["global_small"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    return w, m, ex, jre, oracle.Oracle(m, ex)
+
+
+def test_fk_deterministic_and_status(small):
+    w, m, ex, jre, o = small
+    pc = M.fk_params_c(w.params, jre)
+    g1, s1, st1 = o.fk_frequency(pc, 6, 71, 10)
+    g2, s2, st2 = o.fk_frequency(pc, 6, 71, 10)
+    assert np.array_equal(s1, np.zeros_like(s1))
+    assert np.array_equal(np.nan_to_num(g1, nan=7.0), np.nan_to_num(g2, nan=7.0)) and st1 == st2
+    # l = 0 V-components are NaN in the reference too: bgout(3,1) = -f*bgin(2,4)/elp1 with elp1 = 0
+    assert np.all(np.isnan(g1[:, 4:8, 0])) and not np.any(np.isnan(g1[:, :4, :]))
+
+
+def test_fk_accuracy_convergence(small):
+    """Spectra at ACCURACY 1e-5 and 1e-7 agree to O(1e-5) (the integrator's own error)."""
+    w, m, ex, jre, o = small
+    import dataclasses
+    p_lo = M.fk_params_c(w.params, jre)
+    p_hi = M.fk_params_c(dataclasses.replace(w.params, eps=1e-7), jre)
+    a, _, _ = o.fk_frequency(p_lo, 12, 161, 10, 2, 161)
+    b, _, _ = o.fk_frequency(p_hi, 12, 161, 10, 2, 161)
+    u, v = a[jre - 1, :, 1:], b[jre - 1, :, 1:]
+    rel = np.linalg.norm(u - v) / np.linalg.norm(v)
+    assert rel < 1e-3
+
+
+def test_fk_fault_injection_min_step(small):
+    """An unreachable accuracy makes every step fail down to the minimum step size
+    (integrationStep.f90:176-180): status 1, no hang."""
+    w, m, ex, jre, o = small
+    import dataclasses
+    pc = M.fk_params_c(dataclasses.replace(w.params, eps=1e-30), jre)
+    g, st, _ = o.fk_frequency(pc, 3, 23, 10, 3, 5)
+    assert np.all(st[2:5] == 1)
