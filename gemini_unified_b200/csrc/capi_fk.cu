@@ -43,11 +43,23 @@ struct gem_ctx {
   double* d_spl = nullptr; size_t spl_cap = 0;
   double2* d_scratch = nullptr; size_t scratch_cap = 0;
   int2* d_items = nullptr; size_t items_cap = 0;
+  int* d_order = nullptr; size_t order_cap = 0;
+  int32_t* d_status = nullptr; size_t status_cap = 0;
+  double* d_rstart = nullptr; size_t rstart_cap = 0;
+  double2* d_um = nullptr; size_t um_cap = 0;
+  double2* d_dm = nullptr; size_t dm_cap = 0;
+  double2* d_dets = nullptr; size_t dets_cap = 0;
+  cudaEvent_t ev_ph[3] = {nullptr, nullptr, nullptr};
+  float phase_ms[3] = {0, 0, 0};
   int* d_slots = nullptr; size_t slots_cap = 0;   // jf + koff
   unsigned int* d_queue = nullptr;
   unsigned long long* d_stats = nullptr;
   int* d_err = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // optional instrumentation (enabled by gem_instrument)
+  unsigned long long* d_prof = nullptr;
+  unsigned long long* d_warp_ns = nullptr;
+  int last_grid = 0;
   gem_stats stats{};
 };
 
@@ -147,13 +159,14 @@ int gem_ctx_create(int device, int backend, gem_ctx** out) {
   ctx->backend = backend;
   if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return GEM_ERROR; }
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
-  if (cudaMalloc(&ctx->d_queue, sizeof(unsigned int)) != cudaSuccess ||
+  if (cudaMalloc(&ctx->d_queue, 4 * sizeof(unsigned int)) != cudaSuccess ||
       cudaMalloc(&ctx->d_stats, 8 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) {
     gem_ctx_destroy(ctx);
     return GEM_ERROR;
   }
   for (auto& e : ctx->ev) cudaEventCreate(&e);
+  for (auto& e : ctx->ev_ph) cudaEventCreate(&e);
   *out = ctx;
   return GEM_OK;
 }
@@ -163,8 +176,11 @@ void gem_ctx_destroy(gem_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaFree(ctx->d_knots); cudaFree(ctx->d_lay); cudaFree(ctx->d_spl); cudaFree(ctx->d_scratch);
   cudaFree(ctx->d_items); cudaFree(ctx->d_slots); cudaFree(ctx->d_queue); cudaFree(ctx->d_stats);
-  cudaFree(ctx->d_err);
+  cudaFree(ctx->d_err); cudaFree(ctx->d_prof); cudaFree(ctx->d_warp_ns);
+  cudaFree(ctx->d_order); cudaFree(ctx->d_status); cudaFree(ctx->d_rstart); cudaFree(ctx->d_um);
+  cudaFree(ctx->d_dm); cudaFree(ctx->d_dets);
   for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->ev_ph) if (e) cudaEventDestroy(e);
   delete ctx;
 }
 
@@ -292,7 +308,7 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   }
   for (int i = 1; i <= ctx->nk; ++i) P.rk[i] = ctx->rk[i];
   for (int i = 1; i <= ctx->nnod; ++i) { P.rnod[i] = ctx->rnod[i]; P.state[i] = ctx->state[i]; P.layer[i] = ctx->layer[i]; }
-  // ---- frequency slots and the work queue (high frequencies first)
+  // ---- frequency slots; output index k = koff[slot] + iwn - 1
   std::vector<int> slots(2 * nslot);
   long long nkf = 0;
   for (int s = 0; s < nslot; ++s) {
@@ -300,14 +316,20 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
     slots[nslot + s] = (int)nkf;
     nkf += g.nwn[jf_first + s];
   }
-  std::vector<int2> items;
-  items.reserve((size_t)nkf);
+  std::vector<int2> items((size_t)nkf);
+  for (int s = 0; s < nslot; ++s)
+    for (int iwn = 1; iwn <= g.nwn[jf_first + s]; ++iwn) items[slots[nslot + s] + iwn - 1] = make_int2(s, iwn);
+  // work queue: high frequencies first, low degrees (long paths) first within a frequency
+  std::vector<int> order;
+  order.reserve((size_t)nkf);
   for (int s = nslot - 1; s >= 0; --s)
-    for (int iwn = 1; iwn <= g.nwn[jf_first + s]; ++iwn) items.push_back(make_int2(s, iwn));
-  const int nitems = (int)items.size();
+    for (int iwn = 1; iwn <= g.nwn[jf_first + s]; ++iwn) order.push_back(slots[nslot + s] + iwn - 1);
+  const int nitems = (int)nkf;
   if (grow(ctx, ctx->d_items, ctx->items_cap, items.size())) return GEM_ERROR;
+  if (grow(ctx, ctx->d_order, ctx->order_cap, order.size())) return GEM_ERROR;
   if (grow(ctx, ctx->d_slots, ctx->slots_cap, slots.size())) return GEM_ERROR;
   CK(cudaMemcpyAsync(ctx->d_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   // ---- K3: model preparation for all slots
   size_t spl_n = (size_t)nslot * (ctx->nk + 1) * SPL_STRIDE;
@@ -326,26 +348,57 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   CK(cudaEventRecord(ctx->ev[0], st));
   CK(launch_prep(A, ctx->d_err, st));
   CK(cudaEventRecord(ctx->ev[1], st));
-  // ---- outputs zeroed (unreached nodes and skipped items stay zero)
+  // ---- outputs and per-item storage zeroed (unreached nodes and skipped items stay zero)
   size_t nout = (size_t)nkf * nsp * ctx->nnod;
   if (d_gf64) CK(cudaMemsetAsync(d_gf64, 0, nout * 2 * sizeof(double), st));
   if (d_gfre) CK(cudaMemsetAsync(d_gfre, 0, nout * sizeof(float), st));
   if (d_gfim) CK(cudaMemsetAsync(d_gfim, 0, nout * sizeof(float), st));
-  // ---- K1/K2 persistent solver
-  int bps = fk_blocks_per_sm();
-  int grid = ctx->nsm * bps;
-  long long nthreads = (long long)grid * FK_BLOCK;
-  size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * Layout::PER_NODE;
+  int32_t* status = d_status;
+  if (!status) {
+    if (grow(ctx, ctx->d_status, ctx->status_cap, (size_t)nkf)) return GEM_ERROR;
+    status = ctx->d_status;
+  }
+  CK(cudaMemsetAsync(status, 0, (size_t)nkf * sizeof(int32_t), st));
+  const int jre = p->jre;
+  size_t nu = (size_t)jre * 6 * nkf, nd = (size_t)(ctx->nnod - jre + 1) * 6 * nkf;
+  if (grow(ctx, ctx->d_um, ctx->um_cap, nu)) return GEM_ERROR;
+  if (grow(ctx, ctx->d_dm, ctx->dm_cap, nd)) return GEM_ERROR;
+  if (grow(ctx, ctx->d_rstart, ctx->rstart_cap, 2 * (size_t)nkf)) return GEM_ERROR;
+  if (grow(ctx, ctx->d_dets, ctx->dets_cap, (size_t)nkf)) return GEM_ERROR;
+  CK(cudaMemsetAsync(ctx->d_um, 0, nu * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_dm, 0, nd * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_dets, 0, (size_t)nkf * sizeof(double2), st));
+  // ---- grid: the largest of the three phases sets the per-lane scratch
+  int grid[3];
+  long long nthreads = 0;
+  for (int ph = 0; ph < 3; ++ph) {
+    grid[ph] = ctx->nsm * fk_phase_blocks_per_sm(ph);
+    nthreads = std::max(nthreads, (long long)grid[ph] * FK_BLOCK);
+  }
+  size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * fk_lane_slot_per_node();
   if (grow(ctx, ctx->d_scratch, ctx->scratch_cap, scratch_n)) return GEM_ERROR;
-  CK(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned int), st));
   CK(cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(unsigned long long), st));
   FKLaunch L;
   L.spl = ctx->d_spl; L.jf = ctx->d_slots; L.koff = ctx->d_slots + nslot; L.items = ctx->d_items;
+  L.order = ctx->d_order;
   L.nitems = nitems; L.nkf = nkf; L.gf64 = (double2*)d_gf64; L.gfre = d_gfre; L.gfim = d_gfim;
-  L.status = d_status; L.scratch = ctx->d_scratch; L.nthreads = nthreads; L.queue = ctx->d_queue;
+  L.status = status; L.scratch = ctx->d_scratch; L.nthreads = nthreads; L.queue = ctx->d_queue;
   L.stats = ctx->d_stats;
+  L.rstart = ctx->d_rstart; L.um = (double2*)ctx->d_um; L.dm = (double2*)ctx->d_dm; L.dets = (double2*)ctx->d_dets;
+  L.prof = nullptr;
+  L.warp_ns = nullptr;
+  if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
+  ctx->last_grid = grid[1];
   CK(cudaEventRecord(ctx->ev[2], st));
-  CK(launch_fk(P, L, grid, st));
+  CK(launch_fk_phase(-1, P, L, ctx->nsm * 8, st));
+  for (int ph = 0; ph < 3; ++ph) {
+    FKLaunch Lp = L;
+    if (ctx->d_prof) Lp.prof = ctx->d_prof + 8 * ph;
+    if (ctx->d_warp_ns && ph == 1) Lp.warp_ns = ctx->d_warp_ns;
+    CK(launch_fk_phase(ph, P, Lp, grid[ph], st));
+    CK(cudaEventRecord(ctx->ev_ph[ph], st));
+  }
   CK(cudaEventRecord(ctx->ev[3], st));
   // ---- statistics (synchronises the stream)
   unsigned long long hs[8];
@@ -354,9 +407,15 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   if (herr) return fail(ctx, "Cubic spline interpolation not successful (code %d)", herr);
-  float t_prep = 0, t_solve = 0;
+  float t_prep = 0, t_solve = 0, t0 = 0;
   cudaEventElapsedTime(&t_prep, ctx->ev[0], ctx->ev[1]);
   cudaEventElapsedTime(&t_solve, ctx->ev[2], ctx->ev[3]);
+  for (int ph = 0; ph < 3; ++ph) {
+    float t = 0;
+    cudaEventElapsedTime(&t, ctx->ev[2], ctx->ev_ph[ph]);
+    ctx->phase_ms[ph] = t - t0;
+    t0 = t;
+  }
   ctx->stats.steps_ok = hs[0]; ctx->stats.steps_rej = hs[1]; ctx->stats.attempts = hs[2];
   ctx->stats.sysmats = hs[3]; ctx->stats.matvecs = hs[4]; ctx->stats.flops = hs[5];
   ctx->stats.items = nitems; ctx->stats.failed = 0;
@@ -408,6 +467,31 @@ int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   }
   cleanup();
   return ret;
+}
+
+// Instrumentation of the solver (not part of the reference interface):
+// enable = 1 allocates lockstep counters and per-warp timestamps for the
+// following runs; gem_instrument_read copies them out.
+int gem_instrument(gem_ctx* ctx, int enable) {
+  if (!ctx) return GEM_ERROR;
+  CK(cudaSetDevice(ctx->device));
+  cudaFree(ctx->d_prof); cudaFree(ctx->d_warp_ns);
+  ctx->d_prof = nullptr; ctx->d_warp_ns = nullptr;
+  if (enable) {
+    CK(cudaMalloc(&ctx->d_prof, 32 * sizeof(unsigned long long)));
+    CK(cudaMalloc(&ctx->d_warp_ns, (size_t)2 * ctx->nsm * 64 * sizeof(unsigned long long)));
+  }
+  return GEM_OK;
+}
+
+int gem_instrument_read(gem_ctx* ctx, unsigned long long* prof8, unsigned long long* warp_ns, int* nwarps) {
+  if (!ctx || !ctx->d_prof) return fail(ctx, "instrumentation not enabled");
+  CK(cudaMemcpy(prof8, ctx->d_prof, 24 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  for (int ph = 0; ph < 3; ++ph) prof8[24 + ph] = (unsigned long long)(ctx->phase_ms[ph] * 1000.0);
+  int nw = ctx->last_grid * (FK_BLOCK / 32);
+  if (nwarps) *nwarps = nw;
+  if (warp_ns) CK(cudaMemcpy(warp_ns, ctx->d_warp_ns, (size_t)2 * nw * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return GEM_OK;
 }
 
 int gem_stats_get(const gem_ctx* ctx, gem_stats* out) {

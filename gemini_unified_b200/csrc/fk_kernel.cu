@@ -143,7 +143,7 @@ __global__ void spline_kernel(PrepArgs A, int* err) {
 
 }  // namespace gem
 
-#include "fk_lockstep.cuh"
+#include "fk_phases.cuh"
 
 // =========================================================================
 //  Host-side launch wrappers
@@ -160,28 +160,54 @@ cudaError_t launch_prep(const PrepArgs& A, int* d_err, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-static const size_t FK_SMEM = (size_t)FK_WARPS * DIAG_PER_WARP * sizeof(double2);
+template <int PH>
+static size_t phase_smem() { return (size_t)(FK_BLOCK / 32) * DIAG_LEVELS * PhaseNV<PH>::NV * 32 * sizeof(double2); }
 
-static cudaError_t fk_attr() {
+template <int PH>
+static cudaError_t phase_attr() {
   static bool done = false;
   if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(fk_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FK_SMEM);
+  cudaError_t e = cudaFuncSetAttribute(fk_phase_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)phase_smem<PH>());
   if (e == cudaSuccess) done = true;
   return e;
 }
 
-cudaError_t launch_fk(const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
-  cudaError_t e = fk_attr();
+template <int PH>
+static cudaError_t launch_ph(const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
+  cudaError_t e = phase_attr<PH>();
   if (e != cudaSuccess) return e;
-  fk_solve_kernel<<<grid, FK_BLOCK, FK_SMEM, st>>>(P, L);
+  fk_phase_kernel<PH><<<grid, FK_BLOCK, phase_smem<PH>(), st>>>(P, L);
   return cudaGetLastError();
 }
 
-int fk_blocks_per_sm() {
-  if (fk_attr() != cudaSuccess) return 1;
+cudaError_t launch_fk_phase(int phase, const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
+  switch (phase) {
+    case PH_TOR: return launch_ph<PH_TOR>(P, L, grid, st);
+    case PH_SPH: return launch_ph<PH_SPH>(P, L, grid, st);
+    case PH_ADJ: return launch_ph<PH_ADJ>(P, L, grid, st);
+    default:
+      fk_setup_kernel<<<grid, 128, 0, st>>>(P, L);
+      return cudaGetLastError();
+  }
+}
+
+template <int PH>
+static int bps() {
+  if (phase_attr<PH>() != cudaSuccess) return 1;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk_solve_kernel, FK_BLOCK, FK_SMEM) != cudaSuccess) return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk_phase_kernel<PH>, FK_BLOCK, phase_smem<PH>()) != cudaSuccess) return 1;
   return nb < 1 ? 1 : nb;
 }
+
+int fk_phase_blocks_per_sm(int phase) {
+  switch (phase) {
+    case PH_TOR: return bps<PH_TOR>();
+    case PH_SPH: return bps<PH_SPH>();
+    case PH_ADJ: return bps<PH_ADJ>();
+    default: return 8;
+  }
+}
+
+int fk_lane_slot_per_node() { return LaneLayout::PER_NODE; }
 
 }  // namespace gem

@@ -6,7 +6,7 @@
 
 namespace gem {
 
-constexpr int FK_BLOCK = 256;          // threads per block of the solver
+constexpr int FK_BLOCK = 384;          // threads per block of the solver (12 warps, 1 block per SM)
 constexpr int MAX_LAYER_KNOTS = 64;    // knots per layer handled by the spline kernel
 
 struct PrepArgs {
@@ -31,7 +31,8 @@ struct FKLaunch {
   const double* spl;    // spline tables [nslot][nk+1][SPL_STRIDE]
   const int* jf;        // [nslot]
   const int* koff;      // [nslot] output index of (slot, iwn = 1)
-  const int2* items;    // (slot, iwn), most expensive first
+  const int2* items;    // (slot, iwn) of each output index k
+  const int* order;     // queue position -> k, most expensive first
   int nitems;
   long long nkf;        // extent of the wavenumber-frequency index in the outputs
   double2* gf64;        // optional FP64 output (nkf, nsp, nnod)
@@ -40,8 +41,14 @@ struct FKLaunch {
   int* status;          // optional per-k status
   double2* scratch;     // per-thread node storage, element-major
   long long nthreads;   // scratch stride
-  unsigned int* queue;  // work-queue counter (zeroed before launch)
+  unsigned int* queue;  // work-queue counters, one per phase (zeroed before launch)
+  double* rstart;       // [2][nkf] start radius, toroidal then spheroidal
+  double2* um;          // [jre*6][nkf] upward minors at nodes 1..jre
+  double2* dm;          // [(nnod-jre+1)*6][nkf] downward minors at nodes jre..nnod
+  double2* dets;        // [nkf] spheroidal determinant at the receiver
   unsigned long long* stats;   // 6 counters
+  unsigned long long* prof;    // optional lockstep counters [8]
+  unsigned long long* warp_ns; // optional per-warp (start, end) globaltimer stamps
 };
 
 struct FKStatic;
@@ -50,6 +57,8 @@ struct FKStatic;
 #include <cuda_runtime.h>
 namespace gem {
 cudaError_t launch_prep(const PrepArgs& A, int* d_err, cudaStream_t st);
-cudaError_t launch_fk(const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st);
-int fk_blocks_per_sm();
+// phase < 0: start radii; 0 toroidal, 1 spheroidal minors, 2 adjoint + spheroidal spectra
+cudaError_t launch_fk_phase(int phase, const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st);
+int fk_phase_blocks_per_sm(int phase);
+int fk_lane_slot_per_node();
 }  // namespace gem

@@ -46,8 +46,10 @@ __device__ __forceinline__ void layer_index(const FKStatic& P, double r, int& nl
 //  MASK selects the elastic constants (bit c -> constant c of A,C,F,L,N,K,M).
 // ------------------------------------------------------------------------
 template <unsigned MASK>
-__device__ __forceinline__ void eval_spline(const FKStatic& P, const double* __restrict__ spl, double r, int nl,
-                                            double& ro, dz* el) {
+__device__ __forceinline__ void eval_spline(const FKStatic& P, const Env& e, double r, int nl, double& ro,
+                                            dz* el) {
+  const Tab* __restrict__ T = e.tab;
+  const double* __restrict__ spl = e.spl;
   // One code path for every layer, so lanes of a warp stay converged:
   //  * layer 1 (homogeneous sphere) reads knot iktop(1) with weights (1,0,0,0);
   //  * two-knot layers use the cubic formula with their zero second
@@ -55,26 +57,26 @@ __device__ __forceinline__ void eval_spline(const FKStatic& P, const double* __r
   int j;
   double a, b, cc, dd;
   if (nl == 1) {
-    j = P.iktop[1];
+    j = T->iktop[1];
     a = 1.0; b = 0.0; cc = 0.0; dd = 0.0;
   } else {
-    int j1 = P.iktop[nl - 1] + 1, j2 = P.iktop[nl];
+    int j1 = T->iktop[nl - 1] + 1, j2 = T->iktop[nl];
     if (j2 - j1 == 1) {
       j = j1;
     } else if (P.equidis == 1) {
-      j = (int)((r - P.rk[j1]) / P.drk[nl]) + j1;
+      j = (int)((r - T->rk[j1]) / T->drk[nl]) + j1;
       if (j == j2) j = j2 - 1;
     } else {
       j = j1 - 1;
       int jr = j2 + 1;
       while (jr - j > 1) {
         int m = (j + jr) >> 1;
-        if (r > P.rk[m]) j = m; else jr = m;
+        if (r > T->rk[m]) j = m; else jr = m;
       }
       if (j == j1 - 1) j = j1;
     }
     j = j < 1 ? 1 : (j > P.nk - 1 ? P.nk - 1 : j);   // memory guard (in-range inputs unaffected)
-    double x1 = P.rk[j], x2 = P.rk[j + 1], h = x2 - x1;
+    double x1 = T->rk[j], x2 = T->rk[j + 1], h = x2 - x1;
     a = (x2 - r) / h;
     b = 1.0 - a;
     cc = h * h * a * (a * a - 1.0) / 6.0;
@@ -112,7 +114,7 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
   dz zom{e.omre, e.omim};
   double dll1 = e.dll1;
   if (SYS == SYS_MINORS) {          // minorsOdeSystem.f90:77-126
-    eval_spline<0x1Fu>(P, e.spl, x, e.nl, ro, el);
+    eval_spline<0x1Fu>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
     double rr = 1.0 / x, rr2 = rr * rr;
     dz zrpc = 1.0 / el[1];
@@ -138,14 +140,14 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
     y[3] = m41 * z[0] + m42 * z[1] + (-m22) * z[3] + m23 * z[4];
     y[4] = z3 * z[0] + m42 * z[2] + m32 * z[3] + m55 * z[4];
   } else if (SYS == SYS_FLUID) {    // fluidOdeSystem.f90:78-95
-    eval_spline<0x02u>(P, e.spl, x, e.nl, ro, el);
+    eval_spline<0x02u>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
     double m11 = -2.0 / x;
     dz m12 = 1.0 / el[1] - dll1 / ((zomro * x) * x);
     y[0] = m11 * z[0] + m12 * z[1];
     y[1] = (-zomro) * z[0];
   } else if (SYS == SYS_RADIAL) {   // radialOdeSystem.f90:78-99
-    eval_spline<0x17u>(P, e.spl, x, e.nl, ro, el);
+    eval_spline<0x17u>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
     double rr = 1.0 / x, rr2 = rr * rr;
     dz m11 = ((-2.0 * el[2]) * rr) / el[1];
@@ -155,7 +157,7 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
     y[0] = m11 * z[0] + m12 * z[1];
     y[1] = m21 * z[0] + m22 * z[1];
   } else if (SYS == SYS_TOROIDAL) { // toroidalOdeSystem.f90:81-102
-    eval_spline<0x18u>(P, e.spl, x, e.nl, ro, el);
+    eval_spline<0x18u>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
     double rr = 1.0 / x, rr2 = rr * rr;
     dz m12 = 1.0 / el[3];
@@ -163,7 +165,7 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
     y[0] = rr * z[0] + m12 * z[1];
     y[1] = m21 * z[0] + (-3.0 * rr) * z[1];
   } else {                          // solidtOdeSystem.f90:77-114
-    eval_spline<0x1Fu>(P, e.spl, x, e.nl, ro, el);
+    eval_spline<0x1Fu>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
     double rr = 1.0 / x, rr2 = rr * rr;
     dz zrpc = 1.0 / el[1];
@@ -251,7 +253,7 @@ __device__ __forceinline__ void node_range(const FKStatic& P, double x1, double 
 // ------------------------------------------------------------------------
 __device__ __forceinline__ double velocity_at(const FKStatic& P, const Env& e, double r, int nl) {
   double ro; dz el[7];
-  eval_spline<0x60u>(P, e.spl, r, nl, ro, el);
+  eval_spline<0x60u>(P, e, r, nl, ro, el);
   double v = sqrt(el[6].re / ro);
   if (P.iflso[nl] == 1) v = sqrt(el[5].re / ro);
   return v;
@@ -373,7 +375,7 @@ __device__ __forceinline__ void minors_from_ratios(bool liquid, double el, doubl
 // minorsBottomInitialValues (initialValues.f90:202-275)
 __device__ int minors_bottom_iv(const FKStatic& P, const Env& e, double rstart, dz* ys, double& htry) {
   double ro; dz el7[7];
-  eval_spline<0x7Fu>(P, e.spl, rstart, e.nl, ro, el7);
+  eval_spline<0x7Fu>(P, e, rstart, e.nl, ro, el7);
   bool liquid = P.iflso[e.nl] == 1;
   double el = -0.5 + sqrt(0.25 + e.dll1);
   double elp1 = e.dll1;
@@ -411,7 +413,7 @@ __device__ int minors_surface_iv(const FKStatic& P, const Env& e, dz* ys, double
   dz zom{e.omre, e.omim};
   bool liquid = P.iflso[nlay] == 1;
   double ro; dz el7[7];
-  eval_spline<0x7Fu>(P, e.spl, rearth, nlay, ro, el7);
+  eval_spline<0x7Fu>(P, e, rearth, nlay, ro, el7);
   double v = sqrt(el7[6].re / ro);
   if (liquid) v = sqrt(el7[5].re / ro);
   htry = ((0.25 * v) * TWO_PI_F) / e.omre;
@@ -435,7 +437,7 @@ __device__ int minors_surface_iv(const FKStatic& P, const Env& e, dz* ys, double
 // toroidalBottomInitialValues (initialValues.f90:376-418)
 __device__ int toroidal_bottom_iv(const FKStatic& P, const Env& e, double rstart, dz* ys, double& htry) {
   double ro; dz el7[7];
-  eval_spline<0x40u>(P, e.spl, rstart, e.nl, ro, el7);
+  eval_spline<0x40u>(P, e, rstart, e.nl, ro, el7);
   double el = -0.5 + sqrt(0.25 + e.dll1);
   double elp1 = e.dll1;
   dz zom{e.omre, e.omim};
@@ -464,7 +466,7 @@ __device__ int toroidal_surface_iv(const FKStatic& P, const Env& e, dz* ys, doub
   double el = -0.5 + sqrt(0.25 + e.dll1);
   dz zom{e.omre, e.omim};
   double ro; dz el7[7];
-  eval_spline<0x40u>(P, e.spl, rsurf, nl, ro, el7);
+  eval_spline<0x40u>(P, e, rsurf, nl, ro, el7);
   double v = sqrt(el7[6].re / ro);
   htry = ((0.25 * v) * TWO_PI_F) / e.omre;
   if (P.fsflag == 1) {

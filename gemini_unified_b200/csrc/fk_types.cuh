@@ -24,9 +24,19 @@ struct FKStatic {
 
 struct Counters {
   long long steps_ok, steps_rej, attempts, sysmats, matvecs, flops;
+  long long warp_attempts, lane_attempts;   // lockstep utilisation (instrumentation)
+};
+
+// knot and layer tables used at every spline evaluation, copied to shared
+// memory (lanes index them divergently)
+struct Tab {
+  double rk[MAXKNOT + 1];
+  double drk[MAXLAY + 1];
+  int iktop[MAXLAY + 1];
 };
 
 struct Env {
+  const Tab* tab;                   // shared-memory copy of the knot tables
   const double* __restrict__ spl;   // spline table of this frequency, [knot][SPL_STRIDE]
   int nl;
   double omre, omim, dll1;

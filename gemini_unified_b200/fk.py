@@ -57,6 +57,8 @@ def lib() -> ctypes.CDLL:
         L.gem_fk_run.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
         L.gem_fk_run_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
         L.gem_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.gem_instrument.argtypes = [vp, ctypes.c_int]
+        L.gem_instrument_read.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_int)]
         _lib = L
     return _lib
 
@@ -139,6 +141,16 @@ class GeminiFK:
         pc = fk_params_c(params, jre)
         self._check(lib().gem_fk_run_device(self._h, ctypes.byref(pc), jf_first, jf_last, gfre, gfim, gf64,
                                             status, stream or None))
+
+    def instrument(self, enable: bool = True):
+        self._check(lib().gem_instrument(self._h, 1 if enable else 0))
+
+    def instrument_read(self):
+        prof = np.zeros(32, np.uint64)
+        ns = np.zeros(2 * 148 * 64, np.uint64)
+        nw = ctypes.c_int()
+        self._check(lib().gem_instrument_read(self._h, _ptr(prof), _ptr(ns), ctypes.byref(nw)))
+        return prof, ns[: 2 * nw.value].reshape(-1, 2)
 
     def stats(self) -> dict:
         s = Stats()

@@ -106,6 +106,15 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
 /* Counters of the last run (accepted/rejected steps, attempts, flops, ...). */
 int gem_stats_get(const gem_ctx* ctx, gem_stats* out);
 
+/* Instrumentation (no counterpart in the reference): enable = 1 makes the
+ * following runs record, per phase ph = 0 toroidal, 1 spheroidal, 2 adjoint,
+ * lockstep counters prof[8*ph + 0..3] = {warp trips, integrating lanes summed
+ * over trips, attempt iterations, lanes computing an attempt summed over
+ * iterations}, phase times prof[24 + ph] in microseconds (prof holds 32
+ * entries), and per-warp (start, end) timestamps in ns of the spheroidal phase. */
+int gem_instrument(gem_ctx* ctx, int enable);
+int gem_instrument_read(gem_ctx* ctx, unsigned long long* prof8, unsigned long long* warp_ns, int* nwarps);
+
 /* Measurement utility (no counterpart in the reference): FP64 FMA throughput
  * of the device in TFLOP/s, the denominator of the solver's FP64 roofline. */
 double gem_probe_fp64_tflops(int device);
