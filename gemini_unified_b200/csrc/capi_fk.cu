@@ -17,6 +17,7 @@
 #include "../../include/gemini_fk.h"
 #include "fk_kernel.h"
 #include "fk_types.cuh"
+#include "synth.h"
 
 using namespace gem;
 
@@ -145,6 +146,9 @@ int check_params(gem_ctx* ctx, const gem_fk_params* p) {
 }
 
 }  // namespace
+
+int gem_set_error(gem_ctx* ctx, const char* msg) { return fail(ctx, "%s", msg); }
+void gem_note_synth_ms(gem_ctx* ctx, float ms) { if (ctx) ctx->stats.synth_ms = ms; }
 
 extern "C" {
 

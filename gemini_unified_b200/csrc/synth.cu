@@ -1,0 +1,485 @@
+// Synthetic seismograms from FK spectra (phase 2 of the hot path).
+//
+// Reference: computeSyntheticSeismograms.f90:311-414 (station loop),
+// displacementSpectra.f90:49-113, harmonicDegreeSums.f90:231-369,
+// legendreFunctions.f90:48-157, singleFrequencyDisplacement.f90:108-125,
+// eventFilter.f90:40-83, butterworthFilter.f90:49-96, axesRotation.f90:560-568,
+// frequencyTime.f90:55-113, fourierTransform.f90:118-192.
+//
+// The station loop of the reference evaluates, per station and frequency, 14
+// dot products of length nwn(f).  Here all stations are batched: for each of
+// the 8 Legendre table kinds the sums form one matrix product
+//     C[(f, sum, re/im), station] = sum_l A[(f, sum, re/im), l] * T[l, station]
+// with A holding the FK coefficients times (2l+1)/4pi, the degree factor and
+// the cos^2 taper (zero beyond nwn(f)), and T the Legendre table.  The
+// products run as tiled FP64 kernels; ZRT assembly, filters, rotation and the
+// inverse FFT follow per trace.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/gemini_fk.h"
+#include "gem_device.cuh"
+#include "synth.h"
+
+namespace gem {
+
+// table kinds: 0 plm0 1 plm1 2 plm2 3 dpdt0 4 dpdt1 5 dpdt2 6 pdst1 7 pdst2
+// moment sums k = 1..14 (harmonicDegreeSums.f90:297-351): kind, first l, factor,
+// FK column (0-based offset of (component, jump), greenFKSpectra.f90:204-212)
+__constant__ int c_sum_kind[14] = {0, 0, 1, 2, 3, 3, 4, 5, 6, 7, 4, 5, 6, 7};
+__constant__ int c_sum_l0[14] = {0, 0, 1, 2, 1, 1, 1, 2, 1, 2, 1, 2, 1, 2};
+__constant__ double c_sum_fac[14] = {0, 0, 2, 2, 0, 0, 2, 2, 2, 4, 2, -2, 2, -4};
+__constant__ int c_sum_col[14] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 8, 9, 6, 7};
+
+// ---------------------------------------------------------------------------
+//  Legendre tables (legendreFunctions.f90:48-157), one thread per (station, m)
+//  tab[(kind * lcap + l) * nsta + sta]
+// ---------------------------------------------------------------------------
+__global__ void legendre_kernel(int nsta, int lmax, int lcap, const double* __restrict__ theta, double* tab) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nsta * 3) return;
+  int sta = idx % nsta, m = idx / nsta;
+  double ct = cos(theta[sta]), st = sin(theta[sta]);
+  bool atpoles = !(st > 0.0);
+  auto T = [&](int kind, int l) -> double& { return tab[((long long)kind * lcap + l) * nsta + sta]; };
+  const int kp = m, kd = 3 + m, ks = m >= 1 ? 5 + m : -1;   // plm, dpdt, pdst kinds of this m
+  double pmm = 1.0, fact = 1.0;
+  for (int j = 1; j <= m; ++j) { pmm = pmm * fact * st; fact = fact + 2.0; }
+  double rst = 1.0 / st;
+  int isct = ct >= 0.0 ? 1 : -1;
+  double pl2 = 0.0, pl1 = 0.0;
+  for (int l = 0; l <= lmax; ++l) {
+    double p;
+    if (l < m) p = 0.0;
+    else if (l == m) p = pmm;
+    else if (l == m + 1) p = ct * (double)(2 * m + 1) * pmm;
+    else p = (ct * (double)(2 * l - 1) * pl1 - (double)(l + m - 1) * pl2) / (double)(l - m);
+    double dp = 0.0, ps = 0.0;
+    if (!atpoles) {
+      if (l == m) dp = (double)m * ct * p * rst;
+      else if (l > m) dp = ((double)l * ct * p - (double)(l + m) * pl1) * rst;
+      if (m >= 1 && l >= m) ps = p * rst;
+    } else {
+      long long sg = 1;
+      if (m == 1) { for (int i = 0; i < l; ++i) sg *= isct; dp = 0.5 * (double)((long long)l * (l + 1) * sg); }
+      if (m == 1 && l >= 1) { long long s2 = sg * isct; ps = 0.5 * (double)((long long)l * (l + 1) * s2); }
+    }
+    T(kp, l) = p;
+    T(kd, l) = dp;
+    if (ks >= 0) T(ks, l) = ps;
+    pl2 = pl1;
+    pl1 = p;
+  }
+}
+
+// ---------------------------------------------------------------------------
+//  Coefficient matrices A_kind[row][l], row = 2*(slot*nsk + s) + re/im where s
+//  runs over the sums of that kind (harmonicDegreeSums.f90:238-351,356-369).
+//  A layout: A[kind][row][lcap]; rowoff[kind], nsk[kind] describe the rows.
+// ---------------------------------------------------------------------------
+__global__ void coef_kernel(SynthDev S, const float* __restrict__ gr, const float* __restrict__ gi, double* A) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = S.nf2 - S.nf1 + 1;
+  if (idx >= (long long)nf * 14 * S.lcap) return;
+  int l = (int)(idx % S.lcap);
+  int k = (int)((idx / S.lcap) % 14);
+  int slot = (int)(idx / ((long long)S.lcap * 14));
+  const int jf = S.nf1 + slot;
+  const int nwn = S.nwn[jf - 1];
+  const int kind = c_sum_kind[k];
+  // rank of sum k among the sums of its kind
+  int s = 0;
+  for (int q = 0; q < k; ++q) s += c_sum_kind[q] == kind;
+  long long row = 2LL * ((long long)slot * S.nsk[kind] + s);
+  double* Ar = A + (long long)S.aoff[kind] + row * S.lcap;
+  double* Ai = Ar + S.lcap;
+  double vr = 0.0, vi = 0.0;
+  const int lmaxf = nwn - 1;
+  if (l >= c_sum_l0[k] && l <= lmaxf) {
+    // cos^2 taper of this frequency (harmonicDegreeSums.f90:356-369), TAPFRAC = 0.2
+    const double tapfrac = 0.2;
+    int jt = (int)floor((double)lmaxf * (1.0 - tapfrac) + 0.5);
+    jt = jt < lmaxf ? jt : lmaxf;
+    jt = jt > 1 ? jt : 1;
+    double tap = 1.0;
+    if (l >= jt) {
+      double c1 = (double)lmaxf * tapfrac * 2.0 / PI_F;
+      double c2 = (1.0 - tapfrac) / tapfrac * 0.5 * PI_F;
+      double c = cos((double)(float)l / c1 - c2);
+      tap = c * c;
+    }
+    const long long o = (long long)S.col_off[c_sum_col[k]] * S.nkf + S.koff[slot] + l;
+    double g_r = (double)gr[o], g_i = (double)gi[o];
+    double w = 1.0;
+    double fac = c_sum_fac[k];
+    if (fac != 0.0) w = fac / (double)(float)(l * (l + 1));
+    double sc = w * (2.0 * (double)l + 1.0) / (4.0 * PI_F) * tap;
+    vr = sc * g_r;
+    vi = sc * g_i;
+  }
+  Ar[l] = vr;
+  Ai[l] = vi;
+}
+
+// ---------------------------------------------------------------------------
+//  FP64 tiled product C[kind][row][sta] = sum_l A[kind][row][l] * T[kind][l][sta]
+//  64x64 output tile per block of 256 threads, 4x4 per thread, K step 16.
+// ---------------------------------------------------------------------------
+constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
+
+__global__ void __launch_bounds__(256) sums_gemm_kernel(SynthDev S, const double* __restrict__ A,
+                                                        const double* __restrict__ T, double* C) {
+  const int kind = blockIdx.z;
+  const int M = 2 * (S.nf2 - S.nf1 + 1) * S.nsk[kind];
+  const int N = S.nsta, K = S.lmax + 1;
+  const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
+  if (m0 >= M) return;
+  const double* Ak = A + S.aoff[kind];
+  const double* Tk = T + (long long)kind * S.lcap * N;
+  double* Ck = C + S.coff[kind];
+  __shared__ double As[GT_K][GT_M + 1];
+  __shared__ double Bs[GT_K][GT_N];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < K; k0 += GT_K) {
+    for (int i = threadIdx.x; i < GT_M * GT_K; i += 256) {
+      int mm = i / GT_K, kk = i % GT_K;
+      int gm = m0 + mm, gk = k0 + kk;
+      As[kk][mm] = (gm < M && gk < K) ? Ak[(long long)gm * S.lcap + gk] : 0.0;
+    }
+    for (int i = threadIdx.x; i < GT_K * GT_N; i += 256) {
+      int kk = i / GT_N, nn = i % GT_N;
+      int gk = k0 + kk, gn = n0 + nn;
+      Bs[kk][nn] = (gk < K && gn < N) ? Tk[(long long)gk * N + gn] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GT_K; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int gm = m0 + ty * 4 + i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int gn = n0 + tx * 4 + j;
+      if (gn < N) Ck[(long long)gm * N + gn] = acc[i][j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+//  ZRT spectra from the sums, filters, velocity, rotation; writes the FFT
+//  input of every trace (sta, mt, comp) at bins nf1..nf2 (1-based), the rest 0.
+//  X[trace][ns] complex (double2).
+// ---------------------------------------------------------------------------
+__global__ void spectra_kernel(SynthDev S, const double* __restrict__ C, const double2* __restrict__ evf,
+                               const double* __restrict__ phi, const double* __restrict__ propdir,
+                               const double* __restrict__ mt, double2* X) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = S.nf2 - S.nf1 + 1;
+  if (idx >= (long long)S.nsta * nf) return;
+  const int sta = (int)(idx % S.nsta);
+  const int slot = (int)(idx / S.nsta);
+  const int jf = S.nf1 + slot;
+  dz w[15];
+  for (int k = 0; k < 14; ++k) {
+    int kind = c_sum_kind[k];
+    int s = 0;
+    for (int q = 0; q < k; ++q) s += c_sum_kind[q] == kind;
+    long long row = 2LL * ((long long)slot * S.nsk[kind] + s);
+    const double* Ck = C + S.coff[kind];
+    w[k + 1] = dz{Ck[row * S.nsta + sta], Ck[(row + 1) * S.nsta + sta]};
+  }
+  const double ph = phi[sta];
+  const double sphi = sin(ph), cphi = cos(ph);
+  const double s2phi = sin(2.0 * ph), c2phi = cos(2.0 * ph);
+  const double ca = cos(propdir[sta]), sa = sin(propdir[sta]);
+  const dz ci{0.0, 1.0};
+  const dz ef = dz{evf[jf].x, evf[jf].y};
+  dz tsf = zexp_dev(((ci * TWO_PI_F) * (double)(jf - 1)) * S.df * S.tred) * exp(S.sigma * S.tred);
+  for (int im = 0; im < S.nmt; ++im) {
+    const double* m = mt + im * 6;
+    double t1 = m[3] * cphi + m[4] * sphi;
+    double t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
+    double t3 = m[4] * cphi - m[3] * sphi;
+    double t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
+    dz z[3];
+    z[0] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
+    z[1] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
+    z[2] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+    for (int c = 0; c < 3; ++c) z[c] = ((z[c] * ef) * dz{1.0, 0.0}) * tsf;
+    if (S.velocity) {
+      dz zom{TWO_PI_F * (double)(jf - 1) * S.df, -S.sigma};
+      for (int c = 0; c < 3; ++c) z[c] = (z[c] * ci) * zom;
+    }
+    dz ue = sa * z[1] + ca * z[2];
+    dz un = (-ca) * z[1] + sa * z[2];
+    dz out[3] = {z[0], un, ue};
+    for (int c = 0; c < 3; ++c) {
+      long long tr = ((long long)sta * S.nmt + im) * 3 + c;
+      X[tr * S.ns + (jf - 1)] = make_double2(out[c].re, out[c].im);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+//  Inverse FFT of one trace per block (frequencyTime.f90:55-113,
+//  fourierTransform.f90:118-192): Hermitian fill, radix-2 decimation in
+//  frequency with the reference's twiddles (host table), bit reversal,
+//  ts = Re * df * exp(sigma t).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) ifft_kernel(SynthDev S, const double2* __restrict__ X,
+                                                   const double2* __restrict__ tw, const double* __restrict__ fac,
+                                                   float* traces) {
+  extern __shared__ double2 buf[];
+  const int ns = S.ns, nslog = S.nslog;
+  const long long tr = blockIdx.x;
+  const double2* x = X + tr * ns;
+  // bins 1..nf2 (1-based index i <-> frequency (i-1) df); zero below nf1 and above nf2
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+    int i1 = i + 1;   // 1-based
+    double2 v = make_double2(0.0, 0.0);
+    if (i1 <= ns / 2 + 1) {
+      if (i1 >= S.nf1 && i1 <= S.nf2) v = x[i];
+    } else {
+      int j1 = ns - i1 + 2;
+      if (j1 >= S.nf1 && j1 <= S.nf2) { double2 u = x[j1 - 1]; v = make_double2(u.x, -u.y); }
+    }
+    buf[i] = v;
+  }
+  __syncthreads();
+  // stages m = 1..nslog: nar = 2^(m-1) groups of length lar = ns/nar
+  int twoff = 0;
+  for (int m = 1; m <= nslog; ++m) {
+    const int nar = 1 << (m - 1), lar = ns / nar, larh = lar / 2;
+    for (int t = threadIdx.x; t < ns / 2; t += blockDim.x) {
+      const int jr = t % larh, nr = t / larh;   // jr 0-based (reference jr-1)
+      const int ja = nr * lar + jr, jb = ja + larh;
+      const double2 c = tw[twoff + jr];
+      double2 a = buf[ja], b = buf[jb];
+      double zx = a.x - b.x, zy = a.y - b.y;
+      buf[ja] = make_double2(a.x + b.x, a.y + b.y);
+      buf[jb] = make_double2(zx * c.x - zy * c.y, zx * c.y + zy * c.x);
+    }
+    twoff += larh;
+    __syncthreads();
+  }
+  // bit reversal is a permutation: read element rev(i) for output i
+  for (int i = threadIdx.x; i < S.nsamp; i += blockDim.x) {
+    int src = (int)(__brev((unsigned)(S.ndec * i)) >> (32 - nslog));
+    traces[tr * S.nsamp + i] = (float)(buf[src].x * S.df * fac[i]);
+  }
+}
+
+}  // namespace gem
+
+// ===========================================================================
+//  Host side
+// ===========================================================================
+using namespace gem;
+
+namespace {
+
+struct SynthBuffers {
+  double* tab = nullptr;
+  double* A = nullptr;
+  double* C = nullptr;
+  double2* X = nullptr;
+  double2* evf = nullptr;
+  double2* tw = nullptr;
+  double* fac = nullptr;
+  int* nwn = nullptr;
+  int* koff = nullptr;
+  double *theta = nullptr, *phi = nullptr, *propdir = nullptr, *mt = nullptr;
+};
+
+void free_all(SynthBuffers& b) {
+  cudaFree(b.tab); cudaFree(b.A); cudaFree(b.C); cudaFree(b.X); cudaFree(b.evf); cudaFree(b.tw); cudaFree(b.fac);
+  cudaFree(b.nwn); cudaFree(b.koff); cudaFree(b.theta); cudaFree(b.phi); cudaFree(b.propdir); cudaFree(b.mt);
+}
+
+int nint_(double x) { return x >= 0 ? (int)std::floor(x + 0.5) : -(int)std::floor(-x + 0.5); }
+
+// complex Butterworth band-pass at f - i sigma/2pi (butterworthFilter.f90:49-96)
+void event_filter(const gem_synth_params* p, std::vector<double2>& h) {
+  const int nf1 = p->nf1, nf2 = p->nf2, nf = nf2 - nf1 + 1;
+  const double PIF = PI_F, TPF = TWO_PI_F;
+  std::vector<dz> hh(nf, dz{1, 0}), hl(nf, dz{1, 0});
+  const double fmin = (double)(nf1 - 1) * p->df;
+  const dz ci{0.0, 1.0};
+  auto cexp_ = [](dz z) { double e = std::exp(z.re); return dz{e * std::cos(z.im), e * std::sin(z.im)}; };
+  dz zfna = (fmin - (ci * p->sigma) / TPF) / p->fc_highpass;
+  for (int j = 1; j <= p->order_highpass; ++j) {
+    dz zfn = zfna;
+    dz ep = cexp_(((ci * PIF) * ((double)j - 0.5)) / (double)p->order_highpass);
+    for (int i = 0; i < nf; ++i) { hh[i] = (hh[i] * zfn) / (zfn - ep); zfn = zfn + p->df / p->fc_highpass; }
+  }
+  zfna = (fmin - (ci * p->sigma) / TPF) / p->fc_lowpass;
+  for (int j = 1; j <= p->order_lowpass; ++j) {
+    dz zfn = zfna;
+    dz ep = cexp_(((ci * PIF) * ((double)j - 0.5)) / (double)p->order_lowpass);
+    for (int i = 0; i < nf; ++i) { hl[i] = (hl[i] * (-ci)) / (zfn - ep); zfn = zfn + p->df / p->fc_lowpass; }
+  }
+  h.assign(nf2 + 1, make_double2(0, 0));
+  for (int i = 0; i < nf; ++i) { dz v = hh[i] * hl[i]; h[nf1 + i] = make_double2(v.re, v.im); }
+}
+
+}  // namespace
+
+extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gr,
+                                    const float* d_gi, int nsta, const double* theta, const double* phi,
+                                    const double* propdir, int nmt, const double* mt, float* d_traces,
+                                    void* stream);
+
+// Phase-2 run on device FK spectra (d_gr/d_gi: float32 (nkfmax, nsp)), host station/moment arrays.
+extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gr,
+                                    const float* d_gi, int nsta, const double* theta, const double* phi,
+                                    const double* propdir, int nmt, const double* mt, float* d_traces,
+                                    void* stream) {
+  if (!ctx || !p || !nwn || !theta || !phi || !propdir || !mt) return GEM_ERROR;
+  if (p->istyp != 1) return gem_set_error(ctx, "synthetics: only moment-tensor sources are supported");
+  if (p->global_ != 1) return gem_set_error(ctx, "synthetics: only the spherical-harmonics (global) mode is supported");
+  if (p->nsp < 10) return gem_set_error(ctx, "synthetics: expected the 10 moment spectra U,V (4 jumps) and W (2 jumps)");
+  if (nsta < 1 || nmt < 1 || p->nf1 < 2 || p->nf2 < p->nf1 || p->nwnmax < 3) return gem_set_error(ctx, "synthetics: invalid sizes");
+  cudaStream_t st = (cudaStream_t)stream;
+  // ---- time axis (frequencyTime.f90:55-80)
+  int nslog = (int)std::ceil((double)std::log((float)p->nf2) / std::log(2.0)) + 1;
+  int ns = 1 << nslog;
+  double dts;
+  int ndec;
+  if (ns <= p->nsamp) {
+    ns = p->nsamp;
+    nslog = (int)std::ceil(-std::log(p->df * p->dt) / std::log(2.0));
+    dts = p->dt; ndec = 1;
+  } else {
+    dts = 1.0 / (p->df * ns);
+    ndec = nint_(p->dt / dts);
+    if (std::fabs(p->dt - ndec * dts) > 1.e-5) return gem_set_error(ctx, "Non-integer ratio of desired dt and dt defined from frequency spectrum");
+  }
+  if ((1 << nslog) != ns || ns > 16384) return gem_set_error(ctx, "synthetics: nsamp must be a power of two <= 16384 consistent with df*dt");
+  // ---- layout
+  SynthDev S{};
+  S.nf1 = p->nf1; S.nf2 = p->nf2; S.nsta = nsta; S.nmt = nmt; S.lmax = p->nwnmax - 1; S.lcap = p->nwnmax;
+  S.nkf = p->nkfmax; S.df = p->df; S.sigma = p->sigma; S.tred = p->tred; S.velocity = p->velocity;
+  S.ns = ns; S.nslog = nslog; S.nsamp = p->nsamp; S.ndec = ndec;
+  const int nsk_h[8] = {2, 1, 1, 2, 2, 2, 2, 2};
+  const int nf = p->nf2 - p->nf1 + 1;
+  long long ao = 0, co = 0;
+  for (int k = 0; k < 8; ++k) {
+    S.nsk[k] = nsk_h[k];
+    S.aoff[k] = ao; S.coff[k] = co;
+    ao += 2LL * nf * nsk_h[k] * S.lcap;
+    co += 2LL * nf * nsk_h[k] * nsta;
+  }
+  for (int c = 0; c < 10; ++c) S.col_off[c] = c;
+  // frequency offsets in the FK slab
+  std::vector<int> koff(nf);
+  long long kk = 0;
+  for (int jf = 1; jf < p->nf1; ++jf) kk += 0;   // the FK file starts at nf1 (nwn(jf < nf1) = 0)
+  for (int s = 0; s < nf; ++s) { koff[s] = (int)kk; kk += nwn[p->nf1 + s - 1]; }
+  if (kk > p->nkfmax) return gem_set_error(ctx, "synthetics: nwn does not fit nkfmax");
+  for (int s = 0; s < nf; ++s) if (nwn[p->nf1 + s - 1] > p->nwnmax) return gem_set_error(ctx, "synthetics: nwn > nwnmax");
+  // ---- host tables: event filter, twiddles, exp(sigma t)
+  std::vector<double2> evf;
+  event_filter(p, evf);
+  std::vector<double2> tw;
+  const double piz = 2.0 * PI_F;
+  for (int m = 1; m <= nslog; ++m) {
+    int nar = 1 << (m - 1), lar = ns / nar, larh = lar / 2;
+    double alpha = piz / (double)lar;
+    for (int jr = 1; jr <= larh; ++jr) {
+      double beta = alpha * (double)(jr - 1);
+      tw.push_back(make_double2(std::cos(beta), std::sin(beta)));
+    }
+  }
+  std::vector<double> fac(p->nsamp);
+  double f = 1.0, expo = std::exp(p->sigma * dts);
+  for (int i = 0; i < p->nsamp; ++i) { fac[i] = f; f = f * expo; }
+  // ---- device buffers
+  SynthBuffers b;
+  const long long ntr = (long long)nsta * nmt * 3;
+  auto alloc = [&](void** q, size_t n) { return cudaMalloc(q, n) == cudaSuccess; };
+  bool ok = alloc((void**)&b.tab, (size_t)8 * S.lcap * nsta * sizeof(double)) &&
+            alloc((void**)&b.A, (size_t)ao * sizeof(double)) && alloc((void**)&b.C, (size_t)co * sizeof(double)) &&
+            alloc((void**)&b.X, (size_t)ntr * ns * sizeof(double2)) &&
+            alloc((void**)&b.evf, evf.size() * sizeof(double2)) && alloc((void**)&b.tw, tw.size() * sizeof(double2)) &&
+            alloc((void**)&b.fac, fac.size() * sizeof(double)) && alloc((void**)&b.nwn, (size_t)p->nf2 * sizeof(int)) &&
+            alloc((void**)&b.koff, (size_t)nf * sizeof(int)) && alloc((void**)&b.theta, nsta * sizeof(double)) &&
+            alloc((void**)&b.phi, nsta * sizeof(double)) && alloc((void**)&b.propdir, nsta * sizeof(double)) &&
+            alloc((void**)&b.mt, (size_t)nmt * 6 * sizeof(double));
+  if (!ok) { free_all(b); return gem_set_error(ctx, "synthetics: device allocation failed"); }
+  cudaMemcpyAsync(b.evf, evf.data(), evf.size() * sizeof(double2), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.nwn, nwn, (size_t)p->nf2 * sizeof(int), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.koff, koff.data(), nf * sizeof(int), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.theta, theta, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.phi, phi, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.propdir, propdir, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.mt, mt, (size_t)nmt * 6 * sizeof(double), cudaMemcpyHostToDevice, st);
+  S.nwn = b.nwn; S.koff = b.koff;
+  cudaMemsetAsync(b.X, 0, (size_t)ntr * ns * sizeof(double2), st);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0); cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  legendre_kernel<<<(nsta * 3 + 127) / 128, 128, 0, st>>>(nsta, S.lmax, S.lcap, b.theta, b.tab);
+  long long ncoef = (long long)nf * 14 * S.lcap;
+  coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
+  int mmax = 2 * nf * 2;
+  dim3 g((nsta + GT_N - 1) / GT_N, (mmax + GT_M - 1) / GT_M, 8);
+  sums_gemm_kernel<<<g, 256, 0, st>>>(S, b.A, b.tab, b.C);
+  long long nsp_ = (long long)nsta * nf;
+  spectra_kernel<<<(unsigned)((nsp_ + 127) / 128), 128, 0, st>>>(S, b.C, b.evf, b.phi, b.propdir, b.mt, b.X);
+  size_t smem = (size_t)ns * sizeof(double2);
+  cudaFuncSetAttribute(ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  ifft_kernel<<<(unsigned)ntr, 512, smem, st>>>(S, b.X, b.tw, b.fac, d_traces);
+  cudaEventRecord(e1, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  gem_note_synth_ms(ctx, ms);
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  free_all(b);
+  if (e != cudaSuccess) return gem_set_error(ctx, cudaGetErrorString(e));
+  return GEM_OK;
+}
+
+extern "C" int gem_synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* gr, const float* gi,
+                             int nsta, const double* theta, const double* phi, const double* propdir, int nmt,
+                             const double* mt, float* traces) {
+  if (!ctx || !p || !gr || !gi || !traces) return GEM_ERROR;
+  size_t nin = (size_t)p->nkfmax * p->nsp;
+  size_t nout = (size_t)nsta * nmt * 3 * p->nsamp;
+  float *dgr = nullptr, *dgi = nullptr, *dtr = nullptr;
+  if (cudaMalloc(&dgr, nin * sizeof(float)) != cudaSuccess || cudaMalloc(&dgi, nin * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&dtr, nout * sizeof(float)) != cudaSuccess) {
+    cudaFree(dgr); cudaFree(dgi); cudaFree(dtr);
+    return gem_set_error(ctx, "synthetics: device allocation failed");
+  }
+  int rc = GEM_OK;
+  if (cudaMemcpy(dgr, gr, nin * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(dgi, gi, nin * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+    rc = gem_set_error(ctx, "synthetics: copy of the FK spectra failed");
+  }
+  if (rc == GEM_OK) rc = gem_synth_run_device(ctx, p, nwn, dgr, dgi, nsta, theta, phi, propdir, nmt, mt, dtr, nullptr);
+  if (rc == GEM_OK && cudaMemcpy(traces, dtr, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = gem_set_error(ctx, "synthetics: copy of the traces failed");
+  cudaFree(dgr); cudaFree(dgi); cudaFree(dtr);
+  return rc;
+}

@@ -29,7 +29,7 @@ STATUS_TEXT = {0: "ok", 1: "step size smaller than minimum", 2: "maximum number 
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in
                 ("steps_ok", "steps_rej", "attempts", "sysmats", "matvecs", "flops", "items", "failed")] + \
-               [("solve_ms", ctypes.c_double), ("prep_ms", ctypes.c_double)]
+               [("solve_ms", ctypes.c_double), ("prep_ms", ctypes.c_double), ("synth_ms", ctypes.c_double)]
 
     def asdict(self):
         return {n: (getattr(self, n)) for n, _ in self._fields_}
@@ -57,10 +57,32 @@ def lib() -> ctypes.CDLL:
         L.gem_fk_run.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
         L.gem_fk_run_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
         L.gem_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.gem_synth_run.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp]
+        L.gem_synth_run_device.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp]
         L.gem_instrument.argtypes = [vp, ctypes.c_int]
         L.gem_instrument_read.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_int)]
         _lib = L
     return _lib
+
+
+class SynthParams(ctypes.Structure):
+    """C layout of ``gem_synth_params`` (include/gemini_fk.h)."""
+
+    _fields_ = [("nf1", ctypes.c_int), ("nf2", ctypes.c_int), ("nwnmax", ctypes.c_int),
+                ("nkfmax", ctypes.c_longlong), ("nsp", ctypes.c_int), ("istyp", ctypes.c_int),
+                ("global_", ctypes.c_int), ("df", ctypes.c_double), ("sigma", ctypes.c_double),
+                ("nsamp", ctypes.c_int), ("dt", ctypes.c_double), ("velocity", ctypes.c_int),
+                ("tred", ctypes.c_double), ("order_highpass", ctypes.c_int), ("fc_highpass", ctypes.c_double),
+                ("order_lowpass", ctypes.c_int), ("fc_lowpass", ctypes.c_double)]
+
+
+def synth_params(grid, nsp, nsamp, dt, filspecs, velocity=False, tred=0.0) -> SynthParams:
+    """Parameters as computeSyntheticSeismograms reads them back from the FK file:
+    df and sigma are stored as float32 (computeGreenFKSpectraForSynthetics.f90:261-263)."""
+    f32 = lambda v: float(np.float32(v))
+    return SynthParams(grid.nf1, grid.nf2, int(grid.nwnmax), int(grid.nkfmax), nsp, 1, 1, f32(grid.df),
+                       f32(grid.sigma), int(nsamp), float(dt), 1 if velocity else 0, float(tred),
+                       int(round(filspecs[0])), float(filspecs[1]), int(round(filspecs[2])), float(filspecs[3]))
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -141,6 +163,20 @@ class GeminiFK:
         pc = fk_params_c(params, jre)
         self._check(lib().gem_fk_run_device(self._h, ctypes.byref(pc), jf_first, jf_last, gfre, gfim, gf64,
                                             status, stream or None))
+
+    def synthetics(self, sp: SynthParams, nwn, gfkr, gfki, theta, phi, propdir, mt):
+        """Seismograms of all stations x moment tensors: float32 [nsta, nmt, 3 (Z,N,E), nsamp].
+
+        gfkr/gfki: float32 FK spectra of the source node, shaped (nsp, nkfmax)."""
+        gr = np.ascontiguousarray(gfkr, np.float32); gi = np.ascontiguousarray(gfki, np.float32)
+        nwn = np.ascontiguousarray(nwn, np.int32)
+        th = np.ascontiguousarray(theta, np.float64); ph = np.ascontiguousarray(phi, np.float64)
+        pd = np.ascontiguousarray(propdir, np.float64)
+        mt = np.ascontiguousarray(mt, np.float64).reshape(-1, 6)
+        out = np.zeros((len(th), len(mt), 3, sp.nsamp), np.float32)
+        self._check(lib().gem_synth_run(self._h, ctypes.byref(sp), _ptr(nwn), _ptr(gr), _ptr(gi), len(th), _ptr(th),
+                                        _ptr(ph), _ptr(pd), len(mt), _ptr(mt), _ptr(out)))
+        return out
 
     def instrument(self, enable: bool = True):
         self._check(lib().gem_instrument(self._h, 1 if enable else 0))

@@ -71,7 +71,28 @@ typedef struct gem_stats {
   int64_t items, failed;
   double solve_ms; /* device time of the last solver launch */
   double prep_ms;  /* device time of the last model preparation */
+  double synth_ms; /* device time of the last synthetics run */
 } gem_stats;
+
+/* Synthetics parameters (computeSyntheticSeismograms.f90:136-240); df and
+ * sigma are the values stored with the FK spectra (float32 in the reference's
+ * file), the filter is EVENT_FILTER_TYPE = BUTTERWORTH_BANDPASS. */
+typedef struct gem_synth_params {
+  int nf1, nf2, nwnmax;   /* frequency range and largest number of degrees */
+  long long nkfmax;       /* wavenumber-frequency extent of the FK spectra */
+  int nsp;                /* spectra per node (10: U, V x 4 jumps, W x 2 jumps) */
+  int istyp;              /* 1 MOMENT (only moment tensors are supported) */
+  int global_;            /* 1: spherical harmonics (Legendre) */
+  double df, sigma;
+  int nsamp;              /* power of two */
+  double dt;              /* nsamp * dt * df = 1 */
+  int velocity;           /* SEISMO_TYPE velocity (1) or displacement (0) */
+  double tred;            /* reduction time */
+  int order_highpass;
+  double fc_highpass;
+  int order_lowpass;
+  double fc_lowpass;
+} gem_synth_params;
 
 /* Context holding the model, nodes and device buffers of one GPU.
  * Replaces the module globals sec_* (splineEarthmodelCoefficients.f90:28-41);
@@ -102,6 +123,25 @@ int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
 /* Same with device buffers, ordered on `stream` (a cudaStream_t, may be NULL). */
 int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
                       float* d_gfim, double* d_gf64, int32_t* d_status, void* stream);
+
+/* Synthetic seismograms of all stations and moment tensors of one source
+ * node: replaces, for every station, computeLegendreFunctions +
+ * sphericalHarmonicsDisplacementSpectra (displacementSpectra.f90:49) + event
+ * filter + ZNE rotation + transformFrequencyTime (frequencyTime.f90:55)
+ * (computeSyntheticSeismograms.f90:311-388).  gfkr/gfki: float32 FK spectra
+ * of the node in the file layout (nkfmax, nsp); nwn[jf-1] for jf = 1..nf2;
+ * theta = epicentral distance (rad), phi = azimuth at the source, propdir =
+ * propagation direction at the receiver (rad); mt[nmt][6] = (Mrr, Mtt, Mff,
+ * Mrt, Mrf, Mtf).  traces[((sta*nmt + imt)*3 + comp)*nsamp + i], comp Z, N, E.
+ * Host buffers, blocking. */
+int gem_synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* gfkr, const float* gfki,
+                  int nsta, const double* theta, const double* phi, const double* propdir, int nmt,
+                  const double* mt, float* traces);
+
+/* Same with the FK spectra and the traces in device memory. */
+int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gfkr,
+                         const float* d_gfki, int nsta, const double* theta, const double* phi,
+                         const double* propdir, int nmt, const double* mt, float* d_traces, void* stream);
 
 /* Counters of the last run (accepted/rejected steps, attempts, flops, ...). */
 int gem_stats_get(const gem_ctx* ctx, gem_stats* out);

@@ -28,7 +28,7 @@ def lib():
 
 def test_header_declares_entry_points():
     names = declared_functions()
-    for n in ("gem_ctx_create", "gem_fk_run", "gem_fk_run_device", "gem_last_error"):
+    for n in ("gem_ctx_create", "gem_fk_run", "gem_fk_run_device", "gem_synth_run", "gem_last_error"):
         assert n in names, n
 
 
