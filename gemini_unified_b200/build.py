@@ -3,9 +3,10 @@
     python -m gemini_unified_b200.build          # compile if sources changed
     python -m gemini_unified_b200.build --force  # always compile
 
-The FK solver is compiled with --fmad=false so its arithmetic repeats the
-reference's operation by operation (the reference is built without FMA
-contraction); the other kernels are not affected by the flag.
+The parity build of the FK solver (and every other file) is compiled with
+--fmad=false so its arithmetic repeats the reference's operation by operation
+(the reference is built without FMA contraction); the fast build of the solver
+(fk_solver_fast.cu) uses FMA contraction.
 """
 from __future__ import annotations
 
@@ -21,8 +22,10 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libgemini_fk.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
          "-I" + os.path.join(ROOT, "include")]
+# files compiled with FMA contraction; all others repeat the reference's rounding (--fmad=false)
+FMAD_TRUE = {"fk_solver_fast.cu"}
 
 
 def sources():
@@ -46,7 +49,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     logs = []
     for src in sources():
         obj = os.path.join(OUT_DIR, os.path.basename(src)[:-3] + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+        fmad = "--fmad=true" if os.path.basename(src) in FMAD_TRUE else "--fmad=false"
+        cmd = [NVCC, *ARCH, *FLAGS, fmad, "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         logs.append(r.stdout + r.stderr)
         if r.returncode != 0:

@@ -42,6 +42,7 @@ struct gem_ctx {
   std::vector<int> state, layer;
   // buffers grown on demand
   double* d_spl = nullptr; size_t spl_cap = 0;
+  double* d_poly = nullptr; size_t poly_cap = 0;
   double2* d_scratch = nullptr; size_t scratch_cap = 0;
   int2* d_items = nullptr; size_t items_cap = 0;
   int* d_order = nullptr; size_t order_cap = 0;
@@ -155,7 +156,7 @@ extern "C" {
 int gem_ctx_create(int device, int backend, gem_ctx** out) {
   if (!out) return GEM_ERROR;
   *out = nullptr;
-  if (backend != GEM_BACKEND_GPU_FP64) return GEM_ERROR;
+  if (backend != GEM_BACKEND_GPU_FP64 && backend != GEM_BACKEND_GPU_FAST) return GEM_ERROR;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) return GEM_ERROR;
   gem_ctx* ctx = new gem_ctx();
@@ -178,7 +179,7 @@ int gem_ctx_create(int device, int backend, gem_ctx** out) {
 void gem_ctx_destroy(gem_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
-  cudaFree(ctx->d_knots); cudaFree(ctx->d_lay); cudaFree(ctx->d_spl); cudaFree(ctx->d_scratch);
+  cudaFree(ctx->d_knots); cudaFree(ctx->d_lay); cudaFree(ctx->d_spl); cudaFree(ctx->d_scratch); cudaFree(ctx->d_poly);
   cudaFree(ctx->d_items); cudaFree(ctx->d_slots); cudaFree(ctx->d_queue); cudaFree(ctx->d_stats);
   cudaFree(ctx->d_err); cudaFree(ctx->d_prof); cudaFree(ctx->d_warp_ns);
   cudaFree(ctx->d_order); cudaFree(ctx->d_status); cudaFree(ctx->d_rstart); cudaFree(ctx->d_um);
@@ -349,8 +350,14 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   A.qminv = ctx->d_knots + 7 * K1; A.rk = ctx->d_knots + 8 * K1;
   A.iktop = ctx->d_lay; A.ikbot = ctx->d_lay + (ctx->nlay + 1);
   A.spl = ctx->d_spl;
+  const bool fast = ctx->backend == GEM_BACKEND_GPU_FAST;
   CK(cudaEventRecord(ctx->ev[0], st));
   CK(launch_prep(A, ctx->d_err, st));
+  if (fast) {
+    size_t poly_n = (size_t)nslot * (ctx->nk + 1) * POLY_STRIDE;
+    if (grow(ctx, ctx->d_poly, ctx->poly_cap, poly_n)) return GEM_ERROR;
+    CK(launch_poly(A, ctx->d_poly, st));
+  }
   CK(cudaEventRecord(ctx->ev[1], st));
   // ---- outputs and per-item storage zeroed (unreached nodes and skipped items stay zero)
   size_t nout = (size_t)nkf * nsp * ctx->nnod;
@@ -376,15 +383,15 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   int grid[3];
   long long nthreads = 0;
   for (int ph = 0; ph < 3; ++ph) {
-    grid[ph] = ctx->nsm * fk_phase_blocks_per_sm(ph);
+    grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph) : gem_plain::fk_phase_blocks_per_sm(ph));
     nthreads = std::max(nthreads, (long long)grid[ph] * FK_BLOCK);
   }
-  size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * fk_lane_slot_per_node();
+  size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * gem_plain::fk_lane_slot_per_node();
   if (grow(ctx, ctx->d_scratch, ctx->scratch_cap, scratch_n)) return GEM_ERROR;
   CK(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned int), st));
   CK(cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(unsigned long long), st));
   FKLaunch L;
-  L.spl = ctx->d_spl; L.jf = ctx->d_slots; L.koff = ctx->d_slots + nslot; L.items = ctx->d_items;
+  L.spl = ctx->d_spl; L.poly = fast ? ctx->d_poly : nullptr; L.jf = ctx->d_slots; L.koff = ctx->d_slots + nslot; L.items = ctx->d_items;
   L.order = ctx->d_order;
   L.nitems = nitems; L.nkf = nkf; L.gf64 = (double2*)d_gf64; L.gfre = d_gfre; L.gfim = d_gfim;
   L.status = status; L.scratch = ctx->d_scratch; L.nthreads = nthreads; L.queue = ctx->d_queue;
@@ -395,12 +402,15 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
   ctx->last_grid = grid[1];
   CK(cudaEventRecord(ctx->ev[2], st));
-  CK(launch_fk_phase(-1, P, L, ctx->nsm * 8, st));
+  auto launch = [&](int ph, const FKLaunch& LX, int g) {
+    return fast ? gem_fast::launch_fk_phase(ph, P, LX, g, st) : gem_plain::launch_fk_phase(ph, P, LX, g, st);
+  };
+  CK(launch(-1, L, ctx->nsm * 8));
   for (int ph = 0; ph < 3; ++ph) {
     FKLaunch Lp = L;
     if (ctx->d_prof) Lp.prof = ctx->d_prof + 8 * ph;
     if (ctx->d_warp_ns && ph == 1) Lp.warp_ns = ctx->d_warp_ns;
-    CK(launch_fk_phase(ph, P, Lp, grid[ph], st));
+    CK(launch(ph, Lp, grid[ph]));
     CK(cudaEventRecord(ctx->ev_ph[ph], st));
   }
   CK(cudaEventRecord(ctx->ev[3], st));

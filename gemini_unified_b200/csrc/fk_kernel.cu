@@ -7,7 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "fk_kernel.h"
-#include "fk_solver.cuh"
+#include "fk_types.cuh"
 
 namespace gem {
 
@@ -141,14 +141,40 @@ __global__ void spline_kernel(PrepArgs A, int* err) {
   for (int i = 1; i <= n; ++i) base[(j1 - 1 + i) * SPL_STRIDE + cout] = y2[i];
 }
 
-}  // namespace gem
 
-#include "fk_phases.cuh"
-
-// =========================================================================
-//  Host-side launch wrappers
-// =========================================================================
-namespace gem {
+// cubic coefficients per knot interval in t = r - rk(j) (fast variant): from
+// y = a y1 + b y2 + cc s1 + dd s2 with b = t/h, a = 1 - b,
+// cc = h^2 a (a^2 - 1)/6, dd = h^2 b (b^2 - 1)/6 (splineEarthmodelCoefficients.f90:143-160).
+// Layer 1 (homogeneous) keeps the constant of knot iktop(1) in c0.
+__global__ void poly_kernel(PrepArgs A, double* poly) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  int nk = A.nk;
+  if (idx >= A.nslot * nk) return;
+  int slot = idx / nk, j = idx % nk + 1;   // interval [rk(j), rk(j+1)]
+  const double* base = A.spl + (long long)slot * (nk + 1) * SPL_STRIDE;
+  double* q = poly + ((long long)slot * (nk + 1) + j) * POLY_STRIDE;
+  // interval inside a layer: ikbot(nl) <= j < iktop(nl) for some layer nl >= 2;
+  // otherwise (homogeneous layer 1, the top knot of a layer) the value is constant
+  bool inside = false;
+  for (int nl = 2; nl <= A.nlay; ++nl) inside |= (j >= A.ikbot[nl] && j < A.iktop[nl]);
+  const bool last = !inside;
+  double h = last ? 1.0 : A.rk[j + 1] - A.rk[j];
+  for (int v = 0; v < 15; ++v) {
+    int ci = v == 0 ? 0 : 2 + (v - 1);
+    int c2i = v == 0 ? 1 : 16 + (v - 1);
+    double y1 = base[j * SPL_STRIDE + ci];
+    double s1 = base[j * SPL_STRIDE + c2i];
+    double c0 = y1, c1 = 0, c2 = 0, c3 = 0;
+    if (!last) {
+      double y2 = base[(j + 1) * SPL_STRIDE + ci];
+      double s2 = base[(j + 1) * SPL_STRIDE + c2i];
+      c1 = ((y2 - y1) - h * h * (2.0 * s1 + s2) / 6.0) / h;
+      c2 = 0.5 * s1;
+      c3 = (s2 - s1) / (6.0 * h);
+    }
+    q[4 * v + 0] = c3; q[4 * v + 1] = c2; q[4 * v + 2] = c1; q[4 * v + 3] = c0;
+  }
+}
 
 cudaError_t launch_prep(const PrepArgs& A, int* d_err, cudaStream_t st) {
   int n1 = A.nslot * A.nk;
@@ -160,54 +186,10 @@ cudaError_t launch_prep(const PrepArgs& A, int* d_err, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <int PH>
-static size_t phase_smem() { return (size_t)(FK_BLOCK / 32) * DIAG_LEVELS * PhaseNV<PH>::NV * 32 * sizeof(double2); }
-
-template <int PH>
-static cudaError_t phase_attr() {
-  static bool done = false;
-  if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(fk_phase_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)phase_smem<PH>());
-  if (e == cudaSuccess) done = true;
-  return e;
-}
-
-template <int PH>
-static cudaError_t launch_ph(const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
-  cudaError_t e = phase_attr<PH>();
-  if (e != cudaSuccess) return e;
-  fk_phase_kernel<PH><<<grid, FK_BLOCK, phase_smem<PH>(), st>>>(P, L);
+cudaError_t launch_poly(const PrepArgs& A, double* poly, cudaStream_t st) {
+  int n = A.nslot * A.nk;
+  poly_kernel<<<(n + 127) / 128, 128, 0, st>>>(A, poly);
   return cudaGetLastError();
 }
-
-cudaError_t launch_fk_phase(int phase, const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
-  switch (phase) {
-    case PH_TOR: return launch_ph<PH_TOR>(P, L, grid, st);
-    case PH_SPH: return launch_ph<PH_SPH>(P, L, grid, st);
-    case PH_ADJ: return launch_ph<PH_ADJ>(P, L, grid, st);
-    default:
-      fk_setup_kernel<<<grid, 128, 0, st>>>(P, L);
-      return cudaGetLastError();
-  }
-}
-
-template <int PH>
-static int bps() {
-  if (phase_attr<PH>() != cudaSuccess) return 1;
-  int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk_phase_kernel<PH>, FK_BLOCK, phase_smem<PH>()) != cudaSuccess) return 1;
-  return nb < 1 ? 1 : nb;
-}
-
-int fk_phase_blocks_per_sm(int phase) {
-  switch (phase) {
-    case PH_TOR: return bps<PH_TOR>();
-    case PH_SPH: return bps<PH_SPH>();
-    case PH_ADJ: return bps<PH_ADJ>();
-    default: return 8;
-  }
-}
-
-int fk_lane_slot_per_node() { return LaneLayout::PER_NODE; }
 
 }  // namespace gem

@@ -29,6 +29,7 @@ struct PrepArgs {
 
 struct FKLaunch {
   const double* spl;    // spline tables [nslot][nk+1][SPL_STRIDE]
+  const double* poly;   // cubic coefficients per knot interval [nslot][nk+1][POLY_STRIDE] (fast variant)
   const int* jf;        // [nslot]
   const int* koff;      // [nslot] output index of (slot, iwn = 1)
   const int2* items;    // (slot, iwn) of each output index k
@@ -57,8 +58,19 @@ struct FKStatic;
 #include <cuda_runtime.h>
 namespace gem {
 cudaError_t launch_prep(const PrepArgs& A, int* d_err, cudaStream_t st);
-// phase < 0: start radii; 0 toroidal, 1 spheroidal minors, 2 adjoint + spheroidal spectra
-cudaError_t launch_fk_phase(int phase, const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st);
-int fk_phase_blocks_per_sm(int phase);
-int fk_lane_slot_per_node();
+cudaError_t launch_poly(const PrepArgs& A, double* poly, cudaStream_t st);
+}  // namespace gem
+
+// Two builds of the solver: gem_plain (parity path, no FMA contraction) and
+// gem_fast (FMA, division-free spline, reciprocal complex inverses).
+#define GEM_DECLARE_SOLVER(NS)                                                                          \
+  namespace NS {                                                                                     \
+  /* phase < 0: start radii; 0 toroidal, 1 spheroidal minors, 2 adjoint + spheroidal spectra */      \
+  cudaError_t launch_fk_phase(int phase, const gem::FKStatic& P, const gem::FKLaunch& L, int grid, cudaStream_t st); \
+  int fk_phase_blocks_per_sm(int phase);                                                             \
+  int fk_lane_slot_per_node();                                                                       \
+  }
+GEM_DECLARE_SOLVER(gem_plain)
+GEM_DECLARE_SOLVER(gem_fast)
+namespace gem {
 }  // namespace gem

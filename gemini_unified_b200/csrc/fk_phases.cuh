@@ -27,7 +27,7 @@
 #include "fk_kernel.h"
 #include "fk_solver.cuh"
 
-namespace gem {
+namespace GEM_NS {
 
 enum : int { PH_TOR = 0, PH_SPH = 1, PH_ADJ = 2 };
 template <int PH> struct PhaseNV { static constexpr int NV = PH == PH_TOR ? 2 : (PH == PH_SPH ? 5 : 4); };
@@ -128,11 +128,18 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e, bool activ
     for (int m = 1; m <= p; ++m) {
       const double xi = h / (double)SEQDIV[p - m];
       const double hh = xi - xp;
+#if GEM_FAST
+      const double rhh = __drcp_rn(hh);
+#endif
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         double2* slot = D + ((m - 1) * NVD + v) * 32 + lane;
         double2 pv = *slot;
+#if GEM_FAST
+        dz u = (c[v] - dz{pv.x, pv.y}) * rhh;
+#else
         dz u = (c[v] - dz{pv.x, pv.y}) / hh;
+#endif
         c[v] = xi * u;
         dz nd = xp * u;
         *slot = make_double2(pend[v].re, pend[v].im);   // level m-1 of the new diagonal
@@ -148,12 +155,21 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e, bool activ
     if (j >= 3) {
       cnt.flops += (long long)(j * (j - 1) / 2) * 8 * NV + (long long)(j - 1) * 2 * NV + 8 * NV + 3;
       double s1 = 0.0, s2 = 0.0;
+#if GEM_FAST
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s1 += dy[v].re * dy[v].re + dy[v].im * dy[v].im;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s2 += yy[v].re * yy[v].re + yy[v].im * yy[v].im;
+      const bool conv = s1 < (P.eps * P.eps) * s2;
+#else
 #pragma unroll
       for (int v = 0; v < NV; ++v) { double a = zabs(dy[v]); s1 += a * a; }
 #pragma unroll
       for (int v = 0; v < NV; ++v) { double a = zabs(yy[v]); s2 += a * a; }
       double errmax = sqrt(s1 / s2);
-      if (errmax / P.eps < 1.0) {
+      const bool conv = errmax / P.eps < 1.0;
+#endif
+      if (conv) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) yext[v] = yy[v];
         result = j;
@@ -208,6 +224,7 @@ __device__ __forceinline__ void set_env(const FKStatic& P, const FKLaunch& LL, i
   const int jf = LL.jf[slot];
   const double f = (double)(jf - 1) * P.df;
   e.spl = LL.spl + (long long)slot * (P.nk + 1) * SPL_STRIDE;
+  e.poly = LL.poly + (long long)slot * (P.nk + 1) * POLY_STRIDE;
   e.nl = 1;
   e.omre = 2.0 * PI_F * f;
   e.omim = -P.sigma;
@@ -733,7 +750,9 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
 __global__ void __launch_bounds__(128) fk_setup_kernel(const __grid_constant__ FKStatic P, FKLaunch LL) {
   __shared__ Tab tab;
   for (int i = threadIdx.x; i <= MAXKNOT; i += blockDim.x) tab.rk[i] = P.rk[i];
-  for (int i = threadIdx.x; i <= MAXLAY; i += blockDim.x) { tab.drk[i] = P.drk[i]; tab.iktop[i] = P.iktop[i]; }
+  for (int i = threadIdx.x; i <= MAXLAY; i += blockDim.x) {
+    tab.drk[i] = P.drk[i]; tab.iktop[i] = P.iktop[i]; tab.rdrk[i] = 1.0 / P.drk[i];
+  }
   __syncthreads();
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < LL.nitems; k += (long long)gridDim.x * blockDim.x) {
     int2 w = LL.items[k];
@@ -754,7 +773,9 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
   extern __shared__ double2 smem_diag[];
   __shared__ Tab tab;
   for (int i = threadIdx.x; i <= MAXKNOT; i += blockDim.x) tab.rk[i] = P.rk[i];
-  for (int i = threadIdx.x; i <= MAXLAY; i += blockDim.x) { tab.drk[i] = P.drk[i]; tab.iktop[i] = P.iktop[i]; }
+  for (int i = threadIdx.x; i <= MAXLAY; i += blockDim.x) {
+    tab.drk[i] = P.drk[i]; tab.iktop[i] = P.iktop[i]; tab.rdrk[i] = 1.0 / P.drk[i];
+  }
   __syncthreads();
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -769,7 +790,9 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
   Lane L;
   L.e.tab = &tab;
   L.st = S_FETCH;
+  unsigned long long cyc_adv = 0, cyc_step = 0;
   for (;;) {
+    unsigned long long c0 = clock64();
     for (int round = 0; round < 64; ++round) {
       unsigned fm = __ballot_sync(FULL, L.st == S_FETCH);
       if (fm) {
@@ -787,6 +810,8 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
       if (!__any_sync(FULL, L.st == S_FETCH)) break;
     }
     const bool integ = L.st == S_INTEG;
+    unsigned long long c1 = clock64();
+    cyc_adv += c1 - c0;
     ++trips;
     integ_lanes += __popc(__ballot_sync(FULL, integ));
     if (!__any_sync(FULL, integ)) {
@@ -816,6 +841,7 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
         if (integ && L.sys == SYS_RADIAL) result = r;
       }
     }
+    cyc_step += clock64() - c1;
     // step-size control (integrationStep.f90:140-185)
     if (integ) {
       L.nstep++;
@@ -843,6 +869,8 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
     atomicAdd(LL.prof + 1, integ_lanes);
     atomicAdd(LL.prof + 2, (unsigned long long)cnt.warp_attempts);
     atomicAdd(LL.prof + 3, (unsigned long long)cnt.lane_attempts);
+    atomicAdd(LL.prof + 4, cyc_adv);
+    atomicAdd(LL.prof + 5, cyc_step);
   }
   if (LL.warp_ns && lane == 0) {
     unsigned long long t_end;
@@ -859,4 +887,4 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
   }
 }
 
-}  // namespace gem
+}  // namespace GEM_NS

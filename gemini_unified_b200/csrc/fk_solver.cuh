@@ -17,7 +17,25 @@
 #include "gem_device.cuh"
 #include "fk_types.cuh"
 
-namespace gem {
+// Compiled twice: GEM_NS = gem_plain (GEM_FAST 0, built with --fmad=false, the
+// parity path) and GEM_NS = gem_fast (GEM_FAST 1, FMA contraction, division-free
+// spline evaluation, reciprocal-based complex inverses).
+#ifndef GEM_NS
+#error "define GEM_NS and GEM_FAST before including fk_solver.cuh"
+#endif
+
+namespace GEM_NS {
+using namespace gem;
+
+// Bulirsch-Stoer subdivision scheme (parametersBulirschStep.f90:28-48)
+__device__ __constant__ const int SEQDIV[7] = {2, 4, 6, 8, 12, 16, 24};
+__device__ __constant__ const int NXDIV[7] = {3, 2, 4, 4, 4, 8, 8};
+// flop weights of one system-matrix evaluation (incl. spline) and of one
+// midpoint matrix-vector update, per ODE system (minors, fluid, radial,
+// toroidal, adjoint); identical to the oracle's accounting.
+__device__ __constant__ const int FLOP_SYSMAT[5] = {230, 150, 175, 140, 215};
+__device__ __constant__ const int FLOP_MV[5] = {8 * 19 + 4 * 5, 8 * 3 + 4 * 2, 8 * 4 + 4 * 2,
+                                               8 * 4 + 4 * 2, 8 * 14 + 4 * 4};
 
 // ------------------------------------------------------------------------
 //  locate (locatePoint.f90:72-101), 1-based x in the parameter block
@@ -49,6 +67,46 @@ template <unsigned MASK>
 __device__ __forceinline__ void eval_spline(const FKStatic& P, const Env& e, double r, int nl, double& ro,
                                             dz* el) {
   const Tab* __restrict__ T = e.tab;
+#if GEM_FAST
+  {
+    // cubic in t = r - rk(j) per knot interval, Horner form (no divisions)
+    int j;
+    double t;
+    if (nl == 1) {
+      j = T->iktop[1];
+      t = 0.0;
+    } else {
+      int j1 = T->iktop[nl - 1] + 1, j2 = T->iktop[nl];
+      if (j2 - j1 == 1) {
+        j = j1;
+      } else if (P.equidis == 1) {
+        j = (int)((r - T->rk[j1]) * T->rdrk[nl]) + j1;
+        j = j < j1 ? j1 : (j > j2 - 1 ? j2 - 1 : j);
+      } else {
+        j = j1 - 1;
+        int jr = j2 + 1;
+        while (jr - j > 1) {
+          int m = (j + jr) >> 1;
+          if (r > T->rk[m]) j = m; else jr = m;
+        }
+        if (j == j1 - 1) j = j1;
+      }
+      j = j < 1 ? 1 : (j > P.nk - 1 ? P.nk - 1 : j);
+      t = r - T->rk[j];
+    }
+    const double* __restrict__ q = e.poly + (long long)j * POLY_STRIDE;
+    auto horner = [&](int v) {
+      double2 c32 = __ldg(reinterpret_cast<const double2*>(q + 4 * v));
+      double2 c10 = __ldg(reinterpret_cast<const double2*>(q + 4 * v + 2));
+      return fma(fma(fma(c32.x, t, c32.y), t, c10.x), t, c10.y);
+    };
+    ro = horner(0);
+#pragma unroll
+    for (int c = 0; c < 7; ++c)
+      if (MASK & (1u << c)) el[c] = dz{horner(1 + 2 * c), horner(2 + 2 * c)};
+    return;
+  }
+#endif
   const double* __restrict__ spl = e.spl;
   // One code path for every layer, so lanes of a warp stay converged:
   //  * layer 1 (homogeneous sphere) reads knot iktop(1) with weights (1,0,0,0);
@@ -107,6 +165,22 @@ template <> struct SysNV<SYS_RADIAL> { static constexpr int NV = 2; };
 template <> struct SysNV<SYS_TOROIDAL> { static constexpr int NV = 2; };
 template <> struct SysNV<SYS_SOLIDT> { static constexpr int NV = 4; };
 
+// 1/z: Smith's division on the parity path, one reciprocal on the fast path
+__device__ __forceinline__ dz zinv(dz z) {
+#if GEM_FAST
+  return zinv_fast(z);
+#else
+  return 1.0 / z;
+#endif
+}
+__device__ __forceinline__ double rinv(double x) {
+#if GEM_FAST
+  return __drcp_rn(x);
+#else
+  return 1.0 / x;
+#endif
+}
+
 template <int SYS>
 __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, double x, const dz* z, dz* y) {
   double ro;
@@ -116,8 +190,8 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
   if (SYS == SYS_MINORS) {          // minorsOdeSystem.f90:77-126
     eval_spline<0x1Fu>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
-    double rr = 1.0 / x, rr2 = rr * rr;
-    dz zrpc = 1.0 / el[1];
+    double rr = rinv(x), rr2 = rr * rr;
+    dz zrpc = zinv(el[1]);
     dz z1 = el[0] - (el[2] * el[2]) * zrpc - el[4];
     dz z2 = (2.0 * el[2]) * zrpc;
     dz z3 = (4.0 * z1) * rr2;
@@ -126,7 +200,7 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
     double m13 = dll1 * rr;
     dz m14 = (((-dll1) * el[2]) * zrpc) * rr;
     dz m22 = (1.0 - z2) * rr;
-    dz m23 = 1.0 / el[3];
+    dz m23 = zinv(el[3]);
     dz m24 = zrpc;
     dz m31 = (-z2) * rr;
     dz m32 = (-zomro) + ((dll1 * (z1 + el[4])) - 2.0 * el[4]) * rr2;
@@ -143,32 +217,44 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
     eval_spline<0x02u>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
     double m11 = -2.0 / x;
+#if GEM_FAST
+    dz m12 = zinv(el[1]) - dll1 * zinv((zomro * x) * x);
+#else
     dz m12 = 1.0 / el[1] - dll1 / ((zomro * x) * x);
+#endif
     y[0] = m11 * z[0] + m12 * z[1];
     y[1] = (-zomro) * z[0];
   } else if (SYS == SYS_RADIAL) {   // radialOdeSystem.f90:78-99
     eval_spline<0x17u>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
-    double rr = 1.0 / x, rr2 = rr * rr;
+    double rr = rinv(x), rr2 = rr * rr;
+#if GEM_FAST
+    dz rc = zinv(el[1]);
+    dz m11 = ((-2.0 * el[2]) * rr) * rc;
+    dz m12 = rc;
+    dz m21 = (-zomro) + (4.0 * rr2) * ((el[0] - (el[2] * el[2]) * rc) - el[4]);
+    dz m22 = (2.0 * rr) * (el[2] * rc - 1.0);
+#else
     dz m11 = ((-2.0 * el[2]) * rr) / el[1];
     dz m12 = 1.0 / el[1];
     dz m21 = (-zomro) + (4.0 * rr2) * ((el[0] - (el[2] * el[2]) / el[1]) - el[4]);
     dz m22 = (2.0 * rr) * (el[2] / el[1] - 1.0);
+#endif
     y[0] = m11 * z[0] + m12 * z[1];
     y[1] = m21 * z[0] + m22 * z[1];
   } else if (SYS == SYS_TOROIDAL) { // toroidalOdeSystem.f90:81-102
     eval_spline<0x18u>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
-    double rr = 1.0 / x, rr2 = rr * rr;
-    dz m12 = 1.0 / el[3];
+    double rr = rinv(x), rr2 = rr * rr;
+    dz m12 = zinv(el[3]);
     dz m21 = (-zomro) - (el[4] * rr2) * (2.0 - dll1);
     y[0] = rr * z[0] + m12 * z[1];
     y[1] = m21 * z[0] + (-3.0 * rr) * z[1];
   } else {                          // solidtOdeSystem.f90:77-114
     eval_spline<0x1Fu>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
-    double rr = 1.0 / x, rr2 = rr * rr;
-    dz zrpc = 1.0 / el[1];
+    double rr = rinv(x), rr2 = rr * rr;
+    dz zrpc = zinv(el[1]);
     dz z1 = el[0] - (el[2] * el[2]) * zrpc - el[4];
     dz z2 = (el[2] * rr) * zrpc;
     dz zdlz1 = dll1 * z1;
@@ -179,7 +265,7 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
     dz a22 = (-a11) + 2.0 * rr;
     dz a32 = (2.0 * rr2) * zdlz1;
     double a42 = (-dll1) * rr;
-    dz a43 = -(1.0 / el[3]);
+    dz a43 = -zinv(el[3]);
     dz a14 = (2.0 * z1) * rr2;
     dz a34 = zomro - (zdlz1 + (dll1 - 2.0) * el[4]) * rr2;
     y[0] = a11 * z[0] + a12 * z[1] + rr * z[2] + a14 * z[3];
@@ -481,4 +567,4 @@ __device__ int toroidal_surface_iv(const FKStatic& P, const Env& e, dz* ys, doub
   return ST_OK;
 }
 
-}  // namespace gem
+}  // namespace GEM_NS

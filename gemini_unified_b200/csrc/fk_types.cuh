@@ -32,12 +32,16 @@ struct Counters {
 struct Tab {
   double rk[MAXKNOT + 1];
   double drk[MAXLAY + 1];
+  double rdrk[MAXLAY + 1];   // 1/drk (fast variant)
   int iktop[MAXLAY + 1];
 };
+
+constexpr int POLY_STRIDE = 64;   // doubles per knot interval in the polynomial table
 
 struct Env {
   const Tab* tab;                   // shared-memory copy of the knot tables
   const double* __restrict__ spl;   // spline table of this frequency, [knot][SPL_STRIDE]
+  const double* __restrict__ poly;  // cubic coefficients per knot interval (fast variant), [knot][POLY_STRIDE]
   int nl;
   double omre, omim, dll1;
 };

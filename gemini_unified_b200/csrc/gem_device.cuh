@@ -41,6 +41,11 @@ __host__ __device__ __forceinline__ dz operator/(dz a, dz b) {
 }
 __host__ __device__ __forceinline__ dz operator/(double a, dz b) { return dz{a, 0.0} / b; }
 __device__ __forceinline__ double zabs(dz a) { return hypot(a.re, a.im); }
+// 1/z = conj(z) / |z|^2 (one reciprocal; used by the fast variant only)
+__device__ __forceinline__ dz zinv_fast(dz z) {
+  double r = __drcp_rn(z.re * z.re + z.im * z.im);
+  return {z.re * r, -z.im * r};
+}
 
 // principal square root (Kahan's formulation, branch cut on the negative axis)
 __device__ __forceinline__ dz zsqrt(dz z) {
@@ -65,9 +70,6 @@ constexpr double MINSIZE_IS = 1.0e-12;
 constexpr int MAXNUM_IS = 200000;
 constexpr double MAXY_PROP = 1.0e10;
 
-// Bulirsch-Stoer subdivision scheme (parametersBulirschStep.f90:28-48)
-__device__ __constant__ const int SEQDIV[7] = {2, 4, 6, 8, 12, 16, 24};
-__device__ __constant__ const int NXDIV[7] = {3, 2, 4, 4, 4, 8, 8};
 
 // Limits of the fixed-size parameter block
 constexpr int MAXLAY = 32;
@@ -86,11 +88,5 @@ enum : int {
   ST_UNSUPPORTED = 7,  // receiver or source in an ocean layer
 };
 
-// flop weights of one system-matrix evaluation (incl. spline) and of one
-// midpoint matrix-vector update, per ODE system (minors, fluid, radial,
-// toroidal, adjoint); identical to the oracle's accounting.
-__device__ __constant__ const int FLOP_SYSMAT[5] = {230, 150, 175, 140, 215};
-__device__ __constant__ const int FLOP_MV[5] = {8 * 19 + 4 * 5, 8 * 3 + 4 * 2, 8 * 4 + 4 * 2,
-                                               8 * 4 + 4 * 2, 8 * 14 + 4 * 4};
 
 }  // namespace gem

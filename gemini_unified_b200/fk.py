@@ -21,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libgemini_fk.so")
 
 GEM_BACKEND_GPU_FP64 = 1
+GEM_BACKEND_GPU_FAST = 2
 STATUS_TEXT = {0: "ok", 1: "step size smaller than minimum", 2: "maximum number of steps reached",
                3: "continued fraction did not converge", 4: "node/discontinuity bookkeeping",
                5: "non-finite value", 7: "ocean receiver or source not supported"}

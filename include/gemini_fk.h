@@ -32,7 +32,8 @@ extern "C" {
 #define GEM_WARNING 1
 #define GEM_ERROR 2
 
-#define GEM_BACKEND_GPU_FP64 1 /* faithful FP64 solver, the parity path */
+#define GEM_BACKEND_GPU_FP64 1 /* FP64 solver in the reference's operation order (parity path) */
+#define GEM_BACKEND_GPU_FAST 2 /* FP64 solver with FMA, division-free spline, reciprocal inverses */
 
 typedef struct gem_ctx gem_ctx;
 

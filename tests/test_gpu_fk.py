@@ -116,3 +116,48 @@ def test_rejects_invalid_inputs(small):
         fk.run(w.params, jre, 1, 3)          # below nf1
     with pytest.raises(GeminiError):
         fk.run(w.params, ex.nnod + 5, 3, 3)  # receiver node out of range
+
+
+# The fast build contracts products into FMAs, evaluates the splines from a
+# per-interval Horner table and replaces divisions by reciprocals: rounding
+# differs from the reference's, so its bar is the FP64 spectral bar itself,
+# 1e-8 relative to the largest value of each spectrum (node, component).
+RTOL_FAST = 1e-8
+
+
+def _cmp_per_spectrum(a, b):
+    na, nb = np.isnan(a), np.isnan(b)
+    assert np.array_equal(na, nb)
+    err = np.where(na, 0.0, np.abs(a - b))
+    scale = np.nanmax(np.where(na, 0.0, np.abs(b)), axis=-1, keepdims=True)
+    return float((err / np.maximum(scale, 1e-300)).max())
+
+
+def test_fast_backend_global_small(small):
+    """Fast build against the oracle on every solve of the global configuration."""
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST
+    w, m, ex, jre, _, o = small
+    g = M.frequency_grid(w.params, m.rearth)
+    fast = GeminiFK(m, ex, backend=GEM_BACKEND_GPU_FAST)
+    _, _, g64, st = fast.run(w.params, jre, g.nf1, g.nf2, f32=False)
+    assert np.all(st == 0)
+    pc = M.fk_params_c(w.params, jre)
+    ref = np.concatenate([o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), 10)[0]
+                          for jf in range(g.nf1, g.nf2 + 1)], axis=2)
+    assert _cmp_per_spectrum(g64, ref) <= RTOL_FAST
+
+
+def test_fast_backend_batched_slab(gpu):
+    """Fast against plain on a slab of the batched configuration's top frequencies."""
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST
+    w = configs.WORKLOADS["batched_fk"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    plain = GeminiFK(m, ex)
+    fast = GeminiFK(m, ex, backend=GEM_BACKEND_GPU_FAST)
+    _, _, a, sa = plain.run(w.params, jre, g.nf2 - 3, g.nf2, f32=False)
+    _, _, b, sb = fast.run(w.params, jre, g.nf2 - 3, g.nf2, f32=False)
+    assert np.all(sa == 0) and np.all(sb == 0)
+    assert _cmp_per_spectrum(b, a) <= RTOL_FAST
