@@ -164,6 +164,14 @@ def run_reference(args, rank, size):
     print(json.dumps(line), flush=True)
 
 
+def fk_launches_per_run(backend):
+    """Kernels one gem_fk_run_device call launches: knots, splines, (Horner table,) setup, 3 phases."""
+    return 6 + (1 if backend == 2 else 0)
+
+
+SYNTH_LAUNCHES = 5   # Legendre tables, coefficients, degree-sum products, spectra, inverse FFT
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -172,9 +180,10 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, size)
 
+    import ctypes
     import torch
     from gemini_unified_b200 import configs, model as M
-    from gemini_unified_b200.fk import GeminiFK, lib as fklib
+    from gemini_unified_b200.fk import GeminiFK, synth_params, lib as fklib
 
     torch.cuda.set_device(local)
     dist = None
@@ -182,6 +191,13 @@ def main():
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
     w = configs.WORKLOADS[args.workload]
     m = w.model()
@@ -191,57 +207,63 @@ def main():
     nsp = M.nsp_for(w.params)
     mine = zigzag(g.nf1, g.nf2, rank, size)
     runs = contiguous_runs(mine)
-    fk = GeminiFK(m, ex, device=local)
-    L = fklib()
+    dev = torch.device("cuda", local)
     nkf = {r: int(g.nwn[r[0] - 1: r[1]].sum()) for r in runs}
     items_rank = sum(nkf.values())
     biggest = max(nkf.values())
     n_out = biggest * nsp * ex.nnod
-    dev = torch.device("cuda", local)
     gre = torch.empty(n_out, dtype=torch.float32, device=dev)
     gim = torch.empty(n_out, dtype=torch.float32, device=dev)
     gst = torch.empty(biggest, dtype=torch.int32, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    total_items = int(g.nkfmax)
 
-    def step():
+    def fk_step(fk, keep=None):
         flops = 0
         for r in runs:
             fk.run_device(w.params, jre, r[0], r[1], gfre=gre.data_ptr(), gfim=gim.data_ptr(),
                           status=gst.data_ptr(), stream=stream.cuda_stream)
-            s = fk.stats()
-            flops += s["flops"]
+            flops += fk.stats()["flops"]
             if int(gst[: nkf[r]].abs().sum()) != 0:
                 raise RuntimeError("failed (omega,l) items in frequencies %d..%d" % r)
+            if keep is not None:
+                keep(r)
         return flops
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
+    def timed(fn, steps, clocks=None):
+        times, out = [], None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            if dist: dist.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if dist: dist.barrier()
+            times.append(e0.elapsed_time(e1))
+        return max_over_ranks(float(np.mean(times))), out
 
-    # ---------------- device-timed steps (inputs resident, L2 flushed between steps)
-    times, flops_step, solve_ms = [], 0, 0.0
+    # ---------------- batched + mixed-precision form (fast FP64 build): the headline
+    fast = GeminiFK(m, ex, device=local, backend=2)
+    for _ in range(args.warmup):
+        fk_step(fast)
+    torch.cuda.synchronize()
     clocks = Clocks(local)
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        if dist: dist.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        flops_step = step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        if dist: dist.barrier()
-        times.append(e0.elapsed_time(e1))
-        solve_ms += fk.stats()["solve_ms"] if len(runs) == 1 else 0.0
+    t_ms, flops_step = timed(lambda: fk_step(fast), args.steps)
     clk = clocks.stop()
-    t_ms = float(np.mean(times))
-    if dist:
-        tt = torch.tensor([t_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
-    total_items = g.nkfmax if size > 1 else items_rank
     value = total_items / (t_ms / 1e3)
+    sph_ms = fast.stats()["solve_ms"]
+
+    # ---------------- plain FP64 form (reference rounding, one operation at a time)
+    plain = GeminiFK(m, ex, device=local, backend=1)
+    fk_step(plain)
+    plain_steps = max(1, min(args.steps, 2))
+    t_plain, _ = timed(lambda: fk_step(plain), plain_steps)
+    plain_value = total_items / (t_plain / 1e3)
+    del plain
 
     # ---------------- end-to-end through the host C ABI (float32 spectra back to the host)
     e2e_times = []
@@ -249,15 +271,15 @@ def main():
         if dist: dist.barrier()
         t0 = time.perf_counter()
         for r in runs:
-            fk.run(w.params, jre, r[0], r[1], f32=True, f64=False)
+            fast.run(w.params, jre, r[0], r[1], f32=True, f64=False)
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = float(np.mean(e2e_times))
-    if dist:
-        tt = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    d2h = sum(nkf.values()) * nsp * ex.nnod * 4 * 2 + sum(nkf.values()) * 4
-    h2d = sum(nkf.values()) * 8 + 9 * (m.nk + 1) * 8
+    e2e_s = max_over_ranks(float(np.mean(e2e_times)))
+    d2h = items_rank * nsp * ex.nnod * 4 * 2 + items_rank * 4
+    h2d = items_rank * 8 + 9 * (m.nk + 1) * 8
+
+    # ---------------- seismogram traces: FK spectra of one source node -> traces at all stations
+    traces = time_traces(args, w, m, ex, g, nsp, fast, runs, nkf, gre, gim, dev, stream, dist, rank, size,
+                         timed, synth_params, fklib, fk_step)
 
     # ---------------- roofline of the solver (FP64 pipe)
     peak = fp64_peak_tflops(local)
@@ -273,24 +295,96 @@ def main():
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (PREM node model from the reference's data files; seeded inputs)",
-            "config": {"workload": args.workload, "solves_per_step": int(g.nkfmax), "frequencies": int(g.nf2 - g.nf1 + 1),
+            "config": {"workload": args.workload, "solves_per_step": total_items, "frequencies": int(g.nf2 - g.nf1 + 1),
                        "lmax": int(g.nwn.max() - 1), "nodes": int(ex.nnod), "parallelism": "frequency zig-zag over %d GPU(s)" % size,
+                       "form": "fast FP64 build (FMA, Horner spline table, reciprocals); batched phase kernels",
                        "l2": "flushed between steps (256 MiB write); outputs (1.9 GB) exceed L2"},
+            "plain_fp64": {"value": plain_value, "unit": "solves/s", "ms_per_step": t_plain, "steps": plain_steps,
+                           "speedup_of_value": value / plain_value},
+            "traces": traces,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak["tflops"], "unit": "TFLOP/s",
                          "frac": achieved / peak["tflops"], "traffic": traffic, "peak_source": peak["source"],
                          "flops_per_step": flops_step,
                          "flops_note": "reference-algorithm FP64 flops (cached system matrices, full Neville) counted per event on the device"},
             "e2e": {"value": total_items / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": 3 * len(runs) * args.steps,
+            "gpu_launches": fk_launches_per_run(2) * len(runs) * args.steps,
             "clocks": clk,
         }
         if size == 1:
-            n = args.cpu_sample or 8192
+            n = args.cpu_sample or 16384
             line["cpu_baseline"] = cpu_baseline(w, n)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def time_traces(args, w, m, ex, g, nsp, fk, runs, nkf, gre, gim, dev, stream, dist, rank, size, timed,
+                synth_params, fklib, fk_step):
+    """Seismogram traces (station x moment tensor, 3 components) of the source
+    node nearest 5 km depth from the FK spectra left on the device.  With N
+    ranks the spectra are summed into a full (nsp, nkfmax) slab on every rank
+    and the stations are split over the ranks."""
+    import ctypes
+    import torch
+    from gemini_unified_b200 import configs
+    src = ex.node_index(m.rearth - 5000.0)
+    nkfmax = int(g.nkfmax)
+    full_r = torch.zeros((nsp, nkfmax), dtype=torch.float32, device=dev)
+    full_i = torch.zeros((nsp, nkfmax), dtype=torch.float32, device=dev)
+    koff = np.concatenate([[0], np.cumsum(g.nwn[g.nf1 - 1: g.nf2])])
+
+    def keep(r):
+        n = nkf[r]
+        a = koff[r[0] - g.nf1]
+        vr = gre[: ex.nnod * nsp * n].view(ex.nnod, nsp, n)[src - 1]
+        vi = gim[: ex.nnod * nsp * n].view(ex.nnod, nsp, n)[src - 1]
+        full_r[:, a: a + n].copy_(vr)
+        full_i[:, a: a + n].copy_(vi)
+
+    fk_step(fk, keep)
+    if dist:
+        dist.all_reduce(full_r)
+        dist.all_reduce(full_i)
+    torch.cuda.synchronize()
+    theta, phi, propdir = w.stations()
+    sel = slice(rank, None, size)
+    theta, phi, propdir = [np.ascontiguousarray(a[sel]) for a in (theta, phi, propdir)]
+    mt = np.ascontiguousarray(configs.unit_moment_tensors(), np.float64)
+    nsta, nmt = len(theta), len(mt)
+    sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs)
+    nwn = np.ascontiguousarray(g.nwn, np.int32)
+    out = torch.empty((nsta, nmt, 3, w.nsamp), dtype=torch.float32, device=dev)
+    L = fklib()
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+
+    def one():
+        rc = L.gem_synth_run_device(fk._h, ctypes.byref(sp), p(nwn), full_r.data_ptr(), full_i.data_ptr(), nsta,
+                                    p(theta), p(phi), p(propdir), nmt, p(mt), out.data_ptr(),
+                                    ctypes.c_void_p(stream.cuda_stream))
+        if rc >= 2:
+            raise RuntimeError(L.gem_last_error(fk._h).decode())
+
+    for _ in range(max(1, args.warmup - 1)):
+        one()
+    t_ms, _ = timed(one, max(1, min(args.steps, 3)))
+    ntr = w.ndist * nmt
+    ok = bool(torch.isfinite(out).all().item())
+    # end to end: FK spectra of the node from the host, traces back to the host
+    gr_h = full_r.cpu().numpy(); gi_h = full_i.cpu().numpy()
+    t0 = time.perf_counter()
+    fk.synthetics(sp, g.nwn, gr_h, gi_h, theta, phi, propdir, mt)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    return {"value": ntr / (t_ms / 1e3), "unit": "traces/s", "ms_per_step": t_ms,
+            "traces_per_step": ntr, "samples": w.nsamp, "components": 3, "stations": w.ndist, "moment_tensors": nmt,
+            "form": "FP64 tiled degree-sum products (CUDA cores) + radix-2 FP64 inverse FFT", "finite": ok,
+            "launches_per_step": SYNTH_LAUNCHES,
+            "e2e": {"value": ntr / e2e_s, "unit": "traces/s", "h2d_bytes_per_step": int(gr_h.nbytes * 2),
+                    "d2h_bytes_per_step": int(nsta * nmt * 3 * w.nsamp * 4)}}
 
 
 def fp64_peak_tflops(device):

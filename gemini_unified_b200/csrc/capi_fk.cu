@@ -63,6 +63,9 @@ struct gem_ctx {
   unsigned long long* d_warp_ns = nullptr;
   int last_grid = 0;
   gem_stats stats{};
+  // device buffers of the other entry points, grown on demand
+  void* d_aux[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t aux_cap[4] = {0, 0, 0, 0};
 };
 
 namespace {
@@ -150,6 +153,20 @@ int check_params(gem_ctx* ctx, const gem_fk_params* p) {
 
 int gem_set_error(gem_ctx* ctx, const char* msg) { return fail(ctx, "%s", msg); }
 void gem_note_synth_ms(gem_ctx* ctx, float ms) { if (ctx) ctx->stats.synth_ms = ms; }
+int gem_ctx_device(const gem_ctx* ctx) { return ctx->device; }
+void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes) {
+  if (slot < 0 || slot >= 4) return nullptr;
+  if (ctx->d_aux[slot] && ctx->aux_cap[slot] >= bytes) return ctx->d_aux[slot];
+  cudaFree(ctx->d_aux[slot]);
+  ctx->d_aux[slot] = nullptr; ctx->aux_cap[slot] = 0;
+  if (cudaMalloc(&ctx->d_aux[slot], std::max(bytes, (size_t)256)) != cudaSuccess) {
+    ctx->d_aux[slot] = nullptr;
+    fail(ctx, "device allocation of %zu bytes failed", bytes);
+    return nullptr;
+  }
+  ctx->aux_cap[slot] = std::max(bytes, (size_t)256);
+  return ctx->d_aux[slot];
+}
 
 extern "C" {
 
@@ -184,6 +201,7 @@ void gem_ctx_destroy(gem_ctx* ctx) {
   cudaFree(ctx->d_err); cudaFree(ctx->d_prof); cudaFree(ctx->d_warp_ns);
   cudaFree(ctx->d_order); cudaFree(ctx->d_status); cudaFree(ctx->d_rstart); cudaFree(ctx->d_um);
   cudaFree(ctx->d_dm); cudaFree(ctx->d_dets);
+  for (auto* a : ctx->d_aux) cudaFree(a);
   for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto& e : ctx->ev_ph) if (e) cudaEventDestroy(e);
   delete ctx;

@@ -232,7 +232,7 @@ __global__ void spectra_kernel(SynthDev S, const double* __restrict__ C, const d
     dz out[3] = {z[0], un, ue};
     for (int c = 0; c < 3; ++c) {
       long long tr = ((long long)sta * S.nmt + im) * 3 + c;
-      X[tr * S.ns + (jf - 1)] = make_double2(out[c].re, out[c].im);
+      X[tr * S.ldx + (jf - 1)] = make_double2(out[c].re, out[c].im);
     }
   }
 }
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(512) ifft_kernel(SynthDev S, const double2* __
   extern __shared__ double2 buf[];
   const int ns = S.ns, nslog = S.nslog;
   const long long tr = blockIdx.x;
-  const double2* x = X + tr * ns;
+  const double2* x = X + tr * S.ldx;
   // bins 1..nf2 (1-based index i <-> frequency (i-1) df); zero below nf1 and above nf2
   for (int i = threadIdx.x; i < ns; i += blockDim.x) {
     int i1 = i + 1;   // 1-based
@@ -283,6 +283,30 @@ __global__ void __launch_bounds__(512) ifft_kernel(SynthDev S, const double2* __
   for (int i = threadIdx.x; i < S.nsamp; i += blockDim.x) {
     int src = (int)(__brev((unsigned)(S.ndec * i)) >> (32 - nslog));
     traces[tr * S.nsamp + i] = (float)(buf[src].x * S.df * fac[i]);
+  }
+}
+
+// Twiddles (cos beta, sin beta), beta = (2 pi_f32 / lar) (jr - 1), of every
+// radix-2 stage in the order ifft_kernel reads them (fourierTransform.f90:
+// 139-147, is = +1), and fac[i] = expo^i as the reference's running product
+// fac = fac*expo (frequencyTime.f90:105-110): one thread keeps that product
+// sequential, so its rounding is the reference's.
+__global__ void ifft_tables_kernel(int ns, int nslog, int nsamp, double expo, double2* tw, double* fac) {
+  const double piz = 2.0 * PI_F;
+  int off = 0;
+  for (int m = 1; m <= nslog; ++m) {
+    const int lar = ns >> (m - 1), larh = lar / 2;
+    const double alpha = piz / (double)lar;
+    for (int jr = threadIdx.x + blockIdx.x * blockDim.x; jr < larh; jr += blockDim.x * gridDim.x) {
+      double sn, cs;
+      sincos(alpha * (double)jr, &sn, &cs);
+      tw[off + jr] = make_double2(cs, sn);
+    }
+    off += larh;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double f = 1.0;
+    for (int i = 0; i < nsamp; ++i) { fac[i] = f; f = f * expo; }
   }
 }
 
@@ -341,6 +365,34 @@ void event_filter(const gem_synth_params* p, std::vector<double2>& h) {
 
 }  // namespace
 
+namespace gem {
+const char* fft_geometry(int nf1, int nf2, double df, int nsamp, double dt, FftGeometry& g) {
+  if (nf1 < 1 || nf2 < nf1 || nsamp < 1 || !(df > 0) || !(dt > 0)) return "ifft: invalid frequency range or sampling";
+  if (nf2 > IFFT_MAX_NS / 2 || nsamp > IFFT_MAX_NS) return "ifft: FFT length above 8192 (2*nf2 and nsamp must be <= 8192)";
+  g.nslog = (int)std::ceil((double)std::log((float)nf2) / std::log(2.0)) + 1;
+  g.ns = 1 << g.nslog;
+  g.decimated = false;
+  if (g.ns <= nsamp) {
+    g.ns = nsamp;
+    double lb = std::ceil(-std::log(df * dt) / std::log(2.0));
+    if (!(lb >= 1.0 && lb <= 13.0)) return "ifft: nsamp * dt * df must be 1 with nsamp a power of two <= 8192";
+    g.nslog = (int)lb;
+    g.dts = dt;
+    g.ndec = 1;
+  } else {
+    g.decimated = true;
+    g.dts = 1.0 / (df * g.ns);
+    double r = dt / g.dts;
+    if (!(r >= 0.5 && r < 1e6)) return "Non-integer ratio of desired dt and dt defined from frequency spectrum";
+    g.ndec = (int)std::floor(r + 0.5);
+    if (std::fabs(dt - g.ndec * g.dts) > 1.e-5) return "Non-integer ratio of desired dt and dt defined from frequency spectrum";
+  }
+  if ((1 << g.nslog) != g.ns) return "ifft: nsamp * dt * df must be 1 with nsamp a power of two <= 8192";
+  if ((long long)g.ndec * (nsamp - 1) >= g.ns) return "ifft: nsamp * dt exceeds the period 1/df of the spectrum";
+  return nullptr;
+}
+}  // namespace gem
+
 extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gr,
                                     const float* d_gi, int nsta, const double* theta, const double* phi,
                                     const double* propdir, int nmt, const double* mt, float* d_traces,
@@ -357,26 +409,16 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   if (p->nsp < 10) return gem_set_error(ctx, "synthetics: expected the 10 moment spectra U,V (4 jumps) and W (2 jumps)");
   if (nsta < 1 || nmt < 1 || p->nf1 < 2 || p->nf2 < p->nf1 || p->nwnmax < 3) return gem_set_error(ctx, "synthetics: invalid sizes");
   cudaStream_t st = (cudaStream_t)stream;
-  // ---- time axis (frequencyTime.f90:55-80)
-  int nslog = (int)std::ceil((double)std::log((float)p->nf2) / std::log(2.0)) + 1;
-  int ns = 1 << nslog;
-  double dts;
-  int ndec;
-  if (ns <= p->nsamp) {
-    ns = p->nsamp;
-    nslog = (int)std::ceil(-std::log(p->df * p->dt) / std::log(2.0));
-    dts = p->dt; ndec = 1;
-  } else {
-    dts = 1.0 / (p->df * ns);
-    ndec = nint_(p->dt / dts);
-    if (std::fabs(p->dt - ndec * dts) > 1.e-5) return gem_set_error(ctx, "Non-integer ratio of desired dt and dt defined from frequency spectrum");
-  }
-  if ((1 << nslog) != ns || ns > 16384) return gem_set_error(ctx, "synthetics: nsamp must be a power of two <= 16384 consistent with df*dt");
+  // ---- time axis (frequencyTime.f90:55-84)
+  FftGeometry fg;
+  if (const char* why = fft_geometry(p->nf1, p->nf2, p->df, p->nsamp, p->dt, fg)) return gem_set_error(ctx, why);
+  int nslog = fg.nslog, ns = fg.ns, ndec = fg.ndec;
+  double dts = fg.dts;
   // ---- layout
   SynthDev S{};
   S.nf1 = p->nf1; S.nf2 = p->nf2; S.nsta = nsta; S.nmt = nmt; S.lmax = p->nwnmax - 1; S.lcap = p->nwnmax;
   S.nkf = p->nkfmax; S.df = p->df; S.sigma = p->sigma; S.tred = p->tred; S.velocity = p->velocity;
-  S.ns = ns; S.nslog = nslog; S.nsamp = p->nsamp; S.ndec = ndec;
+  S.ns = ns; S.nslog = nslog; S.nsamp = p->nsamp; S.ndec = ndec; S.ldx = p->nf2;
   const int nsk_h[8] = {2, 1, 1, 2, 2, 2, 2, 2};
   const int nf = p->nf2 - p->nf1 + 1;
   long long ao = 0, co = 0;
@@ -416,7 +458,7 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   auto alloc = [&](void** q, size_t n) { return cudaMalloc(q, n) == cudaSuccess; };
   bool ok = alloc((void**)&b.tab, (size_t)8 * S.lcap * nsta * sizeof(double)) &&
             alloc((void**)&b.A, (size_t)ao * sizeof(double)) && alloc((void**)&b.C, (size_t)co * sizeof(double)) &&
-            alloc((void**)&b.X, (size_t)ntr * ns * sizeof(double2)) &&
+            alloc((void**)&b.X, (size_t)ntr * S.ldx * sizeof(double2)) &&
             alloc((void**)&b.evf, evf.size() * sizeof(double2)) && alloc((void**)&b.tw, tw.size() * sizeof(double2)) &&
             alloc((void**)&b.fac, fac.size() * sizeof(double)) && alloc((void**)&b.nwn, (size_t)p->nf2 * sizeof(int)) &&
             alloc((void**)&b.koff, (size_t)nf * sizeof(int)) && alloc((void**)&b.theta, nsta * sizeof(double)) &&
@@ -433,7 +475,6 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   cudaMemcpyAsync(b.propdir, propdir, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b.mt, mt, (size_t)nmt * 6 * sizeof(double), cudaMemcpyHostToDevice, st);
   S.nwn = b.nwn; S.koff = b.koff;
-  cudaMemsetAsync(b.X, 0, (size_t)ntr * ns * sizeof(double2), st);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
@@ -481,5 +522,60 @@ extern "C" int gem_synth_run(gem_ctx* ctx, const gem_synth_params* p, const int*
   if (rc == GEM_OK && cudaMemcpy(traces, dtr, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
     rc = gem_set_error(ctx, "synthetics: copy of the traces failed");
   cudaFree(dgr); cudaFree(dgi); cudaFree(dtr);
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+//  Batched transformFrequencyTime on device buffers (frequencyTime.f90:55-113)
+// ---------------------------------------------------------------------------
+extern "C" int gem_ifft_run_device(gem_ctx* ctx, int nf1, int nf2, double df, double sigma, int ntr,
+                                   const double* d_sp, long long ldsp, int nsamp, double dt, float* d_ts,
+                                   void* stream) {
+  if (!ctx) return GEM_ERROR;
+  if (!d_sp || !d_ts) return gem_set_error(ctx, "ifft: null spectrum or time-series buffer");
+  if (ntr < 1 || ldsp < nf2) return gem_set_error(ctx, "ifft: need ntr >= 1 and ldsp >= nf2");
+  FftGeometry g;
+  if (const char* why = fft_geometry(nf1, nf2, df, nsamp, dt, g)) return gem_set_error(ctx, why);
+  if (cudaSetDevice(gem_ctx_device(ctx)) != cudaSuccess) return gem_set_error(ctx, "ifft: cudaSetDevice failed");
+  char* tab = (char*)gem_ctx_aux(ctx, 0, ifft_table_bytes(g.ns, nsamp));
+  if (!tab) return GEM_ERROR;
+  double2* tw = (double2*)tab;
+  double* fac = (double*)(tab + (size_t)g.ns * sizeof(double2));
+  cudaStream_t st = (cudaStream_t)stream;
+  SynthDev S{};
+  S.nf1 = nf1; S.nf2 = nf2; S.ns = g.ns; S.nslog = g.nslog; S.nsamp = nsamp; S.ndec = g.ndec; S.df = df;
+  S.sigma = sigma; S.ldx = ldsp;
+  const double expo = std::exp(sigma * g.dts);
+  ifft_tables_kernel<<<8, 256, 0, st>>>(g.ns, g.nslog, nsamp, expo, tw, fac);
+  const size_t smem = (size_t)g.ns * sizeof(double2);
+  cudaFuncSetAttribute(ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  ifft_kernel<<<(unsigned)ntr, IFFT_THREADS, smem, st>>>(S, (const double2*)d_sp, tw, fac, d_ts);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return gem_set_error(ctx, cudaGetErrorString(e));
+  if (g.decimated) {
+    gem_set_error(ctx, "Downsampling to less than 1./(2*fny) requested");
+    return GEM_WARNING;
+  }
+  return GEM_OK;
+}
+
+extern "C" int gem_ifft_run(gem_ctx* ctx, int nf1, int nf2, double df, double sigma, int ntr, const double* sp,
+                            long long ldsp, int nsamp, double dt, float* ts) {
+  if (!ctx) return GEM_ERROR;
+  if (!sp || !ts) return gem_set_error(ctx, "ifft: null spectrum or time-series buffer");
+  if (ntr < 1 || ldsp < nf2 || nsamp < 1) return gem_set_error(ctx, "ifft: need ntr >= 1, ldsp >= nf2, nsamp >= 1");
+  if (cudaSetDevice(gem_ctx_device(ctx)) != cudaSuccess) return gem_set_error(ctx, "ifft: cudaSetDevice failed");
+  const size_t nin = (size_t)ntr * ldsp * 2 * sizeof(double), nout = (size_t)ntr * nsamp * sizeof(float);
+  void* din = gem_ctx_aux(ctx, 1, nin);
+  if (!din) return GEM_ERROR;
+  void* dout = gem_ctx_aux(ctx, 2, nout);
+  if (!dout) return GEM_ERROR;
+  if (cudaMemcpy(din, sp, nin, cudaMemcpyHostToDevice) != cudaSuccess)
+    return gem_set_error(ctx, "ifft: copy of the spectra failed");
+  int rc = gem_ifft_run_device(ctx, nf1, nf2, df, sigma, ntr, (const double*)din, ldsp, nsamp, dt, (float*)dout, nullptr);
+  if (rc >= GEM_ERROR) return rc;
+  if (cudaMemcpy(ts, dout, nout, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return gem_set_error(ctx, "ifft: copy of the time series failed");
   return rc;
 }

@@ -8,6 +8,7 @@ namespace gem {
 struct SynthDev {
   int nf1, nf2, nsta, nmt, lmax, lcap, ns, nslog, nsamp, ndec, velocity;
   long long nkf;
+  long long ldx;            // complex elements between consecutive spectra of the FFT input
   double df, sigma, tred;
   int nsk[8];               // sums per Legendre table kind
   long long aoff[8], coff[8];   // offsets of each kind's coefficient and result matrices
@@ -23,6 +24,30 @@ __device__ __forceinline__ dz zexp_dev(dz z) {
 
 }  // namespace gem
 
-// error / timing hooks of the context (defined with gem_ctx)
+namespace gem {
+
+// Length and decimation of the inverse FFT (frequencyTime.f90:65-84).
+struct FftGeometry {
+  int ns, nslog, ndec;
+  double dts;
+  bool decimated;   // the reference's warning 'Downsampling to less than 1./(2*fny) requested'
+};
+// Fills g; returns nullptr or the reason the sizes are rejected.
+const char* fft_geometry(int nf1, int nf2, double df, int nsamp, double dt, FftGeometry& g);
+constexpr int IFFT_MAX_NS = 8192;   // one series in shared memory: 8192 * 16 B
+constexpr int IFFT_THREADS = 512;
+
+// twiddles of the radix-2 stages (fourierTransform.f90:139-147) and
+// fac[i] = expo^i by the reference's sequential product (frequencyTime.f90:105-110)
+__global__ void ifft_tables_kernel(int ns, int nslog, int nsamp, double expo, double2* tw, double* fac);
+__global__ void __launch_bounds__(512) ifft_kernel(SynthDev S, const double2* __restrict__ X, const double2* __restrict__ tw,
+                            const double* __restrict__ fac, float* traces);
+inline size_t ifft_table_bytes(int ns, int nsamp) { return (size_t)ns * sizeof(double2) + (size_t)nsamp * sizeof(double); }
+
+}  // namespace gem
+
+// error / timing / buffer hooks of the context (defined with gem_ctx)
 int gem_set_error(gem_ctx* ctx, const char* msg);
 void gem_note_synth_ms(gem_ctx* ctx, float ms);
+int gem_ctx_device(const gem_ctx* ctx);
+void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes);

@@ -60,6 +60,10 @@ def lib() -> ctypes.CDLL:
         L.gem_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
         L.gem_synth_run.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp]
         L.gem_synth_run_device.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp]
+        L.gem_ifft_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                   vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, vp]
+        L.gem_ifft_run_device.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int, vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, vp, vp]
         L.gem_instrument.argtypes = [vp, ctypes.c_int]
         L.gem_instrument_read.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_int)]
         _lib = L
@@ -88,6 +92,44 @@ def synth_params(grid, nsp, nsamp, dt, filspecs, velocity=False, tred=0.0) -> Sy
 
 def _ptr(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class FrequencyTime:
+    """Batched transformFrequencyTime (f90/frequencyTime.f90:55-113) on one GPU."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        rc = lib().gem_ctx_create(device, GEM_BACKEND_GPU_FP64, ctypes.byref(self._h))
+        if rc != 0 or not self._h:
+            raise GeminiError("gem_ctx_create failed (no CUDA device %d)" % device)
+        self.warning = None
+
+    def _check(self, rc: int):
+        self.warning = lib().gem_last_error(self._h).decode() if rc == 1 else None
+        if rc >= 2:
+            raise GeminiError(lib().gem_last_error(self._h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gem_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def run(self, nf1: int, nf2: int, df: float, sigma: float, sp: np.ndarray, nsamp: int, dt: float) -> np.ndarray:
+        """sp: complex [ntr, ldsp >= nf2] (column j is frequency j*df) -> float32 [ntr, nsamp]."""
+        sp = np.ascontiguousarray(sp, np.complex128)
+        ntr, ld = sp.shape
+        ts = np.zeros((ntr, nsamp), np.float32)
+        self._check(lib().gem_ifft_run(self._h, nf1, nf2, df, sigma, ntr, _ptr(sp), ld, nsamp, dt, _ptr(ts)))
+        return ts
+
+    def run_device(self, nf1, nf2, df, sigma, ntr, d_sp: int, ldsp: int, nsamp, dt, d_ts: int, stream: int = 0):
+        """Same on device buffers (integer device pointers)."""
+        return self._check(lib().gem_ifft_run_device(self._h, nf1, nf2, df, sigma, ntr, d_sp, ldsp, nsamp, dt,
+                                                     d_ts, stream or None))
 
 
 class GeminiFK:

@@ -144,6 +144,23 @@ int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, const int* nwn
                          const float* d_gfki, int nsta, const double* theta, const double* phi,
                          const double* propdir, int nmt, const double* mt, float* d_traces, void* stream);
 
+/* Batched transformFrequencyTime (frequencyTime.f90:55-113): ntr complex
+ * spectra to ntr float32 time series.  Spectrum t is interleaved complex128
+ * at sp + 2*t*ldsp; element j (0-based) is frequency j*df; elements
+ * nf1-1..nf2-1 are read (ldsp >= nf2), the others are taken as zero.  Series t
+ * is written to ts + t*nsamp.  The FFT length is the reference's (nsamp, or
+ * the next power of two above 2*nf2 followed by decimation to dt, which
+ * returns GEM_WARNING as the reference does); at most 8192.
+ * ts(i) = Re(FFT(+1) of the Hermitian-completed spectrum)(ndec*(i-1)+1)
+ *         * df * exp(sigma*dts)^(i-1).
+ * Host buffers, blocking. */
+int gem_ifft_run(gem_ctx* ctx, int nf1, int nf2, double df, double sigma, int ntr, const double* sp,
+                 long long ldsp, int nsamp, double dt, float* ts);
+
+/* Same with sp and ts in device memory, ordered on stream. */
+int gem_ifft_run_device(gem_ctx* ctx, int nf1, int nf2, double df, double sigma, int ntr, const double* d_sp,
+                        long long ldsp, int nsamp, double dt, float* d_ts, void* stream);
+
 /* Counters of the last run (accepted/rejected steps, attempts, flops, ...). */
 int gem_stats_get(const gem_ctx* ctx, gem_stats* out);
 

@@ -54,6 +54,9 @@ def lib():
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.oracle_legendre.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
         L.oracle_fft.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_freq_time.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_void_p]
         L.oracle_degree_sums.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_void_p]
@@ -153,6 +156,18 @@ def fft(x, y, n, is_):
     x = np.ascontiguousarray(x, np.float64).copy(); y = np.ascontiguousarray(y, np.float64).copy()
     lib().oracle_fft(n, is_, _p(x), _p(y))
     return x, y
+
+
+def freq_time(nf1, nf2, df, sigma, sp, nsamp, dt):
+    """transformFrequencyTime of each row of sp (complex [ntr, ldsp >= nf2]).
+    Returns (float32 [ntr, nsamp], level 0 ok / 1 decimation warning)."""
+    sp = np.ascontiguousarray(sp, np.complex128)
+    ntr, ld = sp.shape
+    ts = np.zeros((ntr, nsamp), np.float32)
+    rc = lib().oracle_freq_time(nf1, nf2, df, sigma, ntr, _p(sp), ld, nsamp, dt, _p(ts))
+    if rc >= 2:
+        raise RuntimeError("oracle_freq_time: invalid sizes")
+    return ts, rc
 
 
 def degree_sums(nf1, nf2, nwn, nwnmax, gr, gi, theta):

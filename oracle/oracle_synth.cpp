@@ -176,7 +176,7 @@ void fft(std::vector<double>& x, std::vector<double>& y, int n, int is) {
 
 // transformFrequencyTime (frequencyTime.f90:55-113); sp 1-based [1..nf2]
 int freqTime(int nf1, int nf2, double df, double sigma, const std::vector<zc>& sp, int nsamp,
-             double dt, float* ts) {
+             double dt, float* ts, int* warning = nullptr) {
   int nslog = (int)std::ceil((double)std::log((float)nf2) / std::log(2.0)) + 1;
   int ns = 1 << nslog;
   double dts; int ndec;
@@ -188,8 +188,10 @@ int freqTime(int nf1, int nf2, double df, double sigma, const std::vector<zc>& s
     dts = 1.0 / (df * ns);
     ndec = (int)std::lround(dt / dts);
     if (std::fabs(dt - ndec * dts) > 1.e-5) return 2;
+    if (warning) *warning = 1;   // 'Downsampling to less than 1./(2*fny) requested'
   }
   if ((1 << nslog) != ns) return 2;   // inconsistent nsamp / dt
+  if ((long long)ndec * (nsamp - 1) >= ns) return 2;   // beyond the period 1/df
   std::vector<double> x(ns + 1, 0.0), y(ns + 1, 0.0);
   for (int i = nf1; i <= nf2; ++i) { x[i] = sp[i].re; y[i] = sp[i].im; }
   for (int i = ns / 2 + 2; i <= ns; ++i) { x[i] = x[ns - i + 2]; y[i] = -y[ns - i + 2]; }
@@ -243,6 +245,22 @@ void oracle_legendre(int lmax, double theta, double* out) {
       out[3 * 3 * L + m * L + l] = a.d2pdt2[m][l];
       out[4 * 3 * L + m * L + l] = a.dtpdst[m][l];
     }
+}
+
+// transformFrequencyTime of ntr spectra: spectrum t at sp + 2*t*ldsp (interleaved
+// complex, element j is frequency j*df), series t at ts + t*nsamp.  Returns 0, 1
+// (decimation warning) or 2 (error), the reference's levels.
+int oracle_freq_time(int nf1, int nf2, double df, double sigma, int ntr, const double* sp, long long ldsp,
+                     int nsamp, double dt, float* ts) {
+  int warning = 0;
+  std::vector<zc> z(nf2 + 1);
+  for (int t = 0; t < ntr; ++t) {
+    const double* s = sp + 2 * (long long)t * ldsp;
+    for (int j = 1; j <= nf2; ++j) z[j] = zc{s[2 * (j - 1)], s[2 * (j - 1) + 1]};
+    int rc = freqTime(nf1, nf2, df, sigma, z, nsamp, dt, ts + (long long)t * nsamp, &warning);
+    if (rc) return rc;
+  }
+  return warning;
 }
 
 void oracle_fft(int n, int is, double* x, double* y) {

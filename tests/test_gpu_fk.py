@@ -34,18 +34,30 @@ def small(gpu):
     return w, m, ex, jre, GeminiFK(m, ex), oracle.Oracle(m, ex)
 
 
-def test_global_small_all_frequencies(small):
-    """Every frequency of the 51-frequency global configuration, all 18169 solves."""
+@pytest.fixture(scope="module")
+def small_ref(small):
+    """Oracle spectra of every frequency of the global configuration (threads over frequencies)."""
+    import concurrent.futures as cf
+    import os
     w, m, ex, jre, fk, o = small
     g = M.frequency_grid(w.params, m.rearth)
+    pc = M.fk_params_c(w.params, jre)
+    with cf.ThreadPoolExecutor(os.cpu_count() or 1) as pool:
+        refs = list(pool.map(lambda jf: o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), 10)[0], range(g.nf1, g.nf2 + 1)))
+    return g, refs
+
+
+def test_global_small_all_frequencies(small, small_ref):
+    """Every frequency of the 51-frequency global configuration, all 18169 solves."""
+    w, m, ex, jre, fk, o = small
+    g, refs = small_ref
     gre, gim, g64, st = fk.run(w.params, jre, g.nf1, g.nf2)
     assert np.all(st == 0)
-    pc = M.fk_params_c(w.params, jre)
     off = 0
     worst = 0.0
     for jf in range(g.nf1, g.nf2 + 1):
         n = int(g.nwn[jf - 1])
-        ref, sto, _ = o.fk_frequency(pc, jf, n, 10)
+        ref = refs[jf - g.nf1]
         got = g64[:, :, off:off + n]
         worst = max(worst, _cmp(got, ref))
         # float32 outputs are the rounded FP64 values
@@ -133,17 +145,15 @@ def _cmp_per_spectrum(a, b):
     return float((err / np.maximum(scale, 1e-300)).max())
 
 
-def test_fast_backend_global_small(small):
+def test_fast_backend_global_small(small, small_ref):
     """Fast build against the oracle on every solve of the global configuration."""
     from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST
     w, m, ex, jre, _, o = small
-    g = M.frequency_grid(w.params, m.rearth)
+    g, refs = small_ref
     fast = GeminiFK(m, ex, backend=GEM_BACKEND_GPU_FAST)
     _, _, g64, st = fast.run(w.params, jre, g.nf1, g.nf2, f32=False)
     assert np.all(st == 0)
-    pc = M.fk_params_c(w.params, jre)
-    ref = np.concatenate([o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), 10)[0]
-                          for jf in range(g.nf1, g.nf2 + 1)], axis=2)
+    ref = np.concatenate(refs, axis=2)
     assert _cmp_per_spectrum(g64, ref) <= RTOL_FAST
 
 

@@ -49,6 +49,41 @@ def test_fft_against_numpy():
     assert np.all(dx == 1.0) and np.all(dy == 0.0)
 
 
+def _spectra(ntr, ld, nf1, nf2, seed):
+    rng = np.random.default_rng(seed)
+    sp = rng.standard_normal((ntr, ld)) + 1j * rng.standard_normal((ntr, ld))
+    sp[:, :nf1 - 1] = 7.0    # outside nf1..nf2: must be ignored
+    sp[:, nf2:] = -3.0
+    return sp
+
+
+def test_freq_time_against_numpy():
+    """transformFrequencyTime: Hermitian completion of bins nf1..nf2, inverse
+    DFT, times df * exp(sigma t); with and without decimation."""
+    df = 1.0 / 1024
+    sigma = 5 * df
+    for nf1, nf2, nsamp, dt, ndec in ((2, 52, 2048, 0.5, 1), (3, 300, 256, 4.0, 4)):
+        sp = _spectra(3, nf2 + 5, nf1, nf2, nf2)
+        ts, level = oracle.freq_time(nf1, nf2, df, sigma, sp, nsamp, dt)
+        ns = max(nsamp, 2 ** (int(np.ceil(np.log2(nf2))) + 1))
+        X = np.zeros((3, ns), complex)
+        X[:, nf1 - 1:nf2] = sp[:, nf1 - 1:nf2]
+        full = np.fft.irfft(X[:, : ns // 2 + 1], n=ns) * ns    # Re of the Hermitian sum
+        t = np.arange(nsamp) * (dt / ndec)                      # the reference's exp(sigma*dts) per output sample
+        ref = full[:, ::ndec][:, :nsamp] * df * np.exp(sigma * t)
+        err = np.linalg.norm(ts - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert err.max() < 1e-5                                 # twiddles use single-precision pi
+        assert level == (1 if ndec > 1 else 0)
+
+
+def test_freq_time_rejects_inconsistent_sampling():
+    sp = _spectra(1, 60, 2, 52, 0)
+    with pytest.raises(RuntimeError):
+        oracle.freq_time(2, 52, 1.0 / 1024, 0.0, sp, 2048, 0.3)     # nsamp*dt*df != 1
+    with pytest.raises(RuntimeError):
+        oracle.freq_time(2, 52, 1.0 / 1024, 0.0, sp, 4096, 0.5)     # nsamp*dt beyond 1/df
+
+
 def test_degree_sums_against_direct_formula():
     """harmonicDegreeSums.f90:231-351 evaluated independently in numpy."""
     rng = np.random.default_rng(7)
