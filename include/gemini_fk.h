@@ -161,6 +161,23 @@ int gem_ifft_run(gem_ctx* ctx, int nf1, int nf2, double df, double sigma, int nt
 int gem_ifft_run_device(gem_ctx* ctx, int nf1, int nf2, double df, double sigma, int ntr, const double* d_sp,
                         long long ldsp, int nsamp, double dt, float* d_ts, void* stream);
 
+/* gem_ifft_run_noalloc -- no counterpart in the reference.  The transform of
+ * gem_ifft_run_device for callers that cannot allocate device memory when they
+ * call it: codes whose device memory is already handed out by their own pool
+ * allocator, or that must not let cudaMalloc/cudaFree synchronise the device
+ * while other streams run.  It takes no context and allocates nothing (no
+ * cudaMalloc, no cudaFree, no host heap); its tables live in one static 256 KiB
+ * device array that every GPU loading this library holds until exit.  Same
+ * arguments and limits as gem_ifft_run_device (FFT length <= 8192; larger sizes
+ * are rejected with GEM_ERROR and a message); the device is the caller's
+ * current one; errors and the decimation warning are written to errbuf
+ * (errlen bytes, may be NULL).  Returns after queuing its kernels on stream.
+ * All calls on a device share the array: calls that overlap on the GPU race and
+ * must be ordered on one stream.  The first call on each device looks up the
+ * array's address and should come before any stream capture. */
+int gem_ifft_run_noalloc(int nf1, int nf2, double df, double sigma, int ntr, const double* d_sp, long long ldsp,
+                         int nsamp, double dt, float* d_ts, void* stream, char* errbuf, int errlen);
+
 /* Counters of the last run (accepted/rejected steps, attempts, flops, ...). */
 int gem_stats_get(const gem_ctx* ctx, gem_stats* out);
 
