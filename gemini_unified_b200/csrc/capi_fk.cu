@@ -182,7 +182,7 @@ int gem_ctx_create(int device, int backend, gem_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return GEM_ERROR; }
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   if (cudaMalloc(&ctx->d_queue, 4 * sizeof(unsigned int)) != cudaSuccess ||
-      cudaMalloc(&ctx->d_stats, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_stats, 32 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) {
     gem_ctx_destroy(ctx);
     return GEM_ERROR;
@@ -430,12 +430,15 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
     if (ctx->d_warp_ns && ph == 1) Lp.warp_ns = ctx->d_warp_ns;
     CK(launch(ph, Lp, grid[ph]));
     CK(cudaEventRecord(ctx->ev_ph[ph], st));
+    // running counters after this phase (stream-ordered snapshot)
+    CK(cudaMemcpyAsync(ctx->d_stats + 8 * (ph + 1), ctx->d_stats, 8 * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToDevice, st));
   }
   CK(cudaEventRecord(ctx->ev[3], st));
   // ---- statistics (synchronises the stream)
-  unsigned long long hs[8];
+  unsigned long long hs[32];
   int herr = 0;
-  CK(cudaMemcpyAsync(hs, ctx->d_stats, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(hs, ctx->d_stats, 32 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   if (herr) return fail(ctx, "Cubic spline interpolation not successful (code %d)", herr);
@@ -446,6 +449,8 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
     float t = 0;
     cudaEventElapsedTime(&t, ctx->ev[2], ctx->ev_ph[ph]);
     ctx->phase_ms[ph] = t - t0;
+    ctx->stats.phase_ms[ph] = t - t0;
+    ctx->stats.phase_flops[ph] = (int64_t)(hs[8 * (ph + 1) + 5] - (ph ? hs[8 * ph + 5] : 0ULL));
     t0 = t;
   }
   ctx->stats.steps_ok = hs[0]; ctx->stats.steps_rej = hs[1]; ctx->stats.attempts = hs[2];

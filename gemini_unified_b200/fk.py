@@ -30,10 +30,11 @@ STATUS_TEXT = {0: "ok", 1: "step size smaller than minimum", 2: "maximum number 
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in
                 ("steps_ok", "steps_rej", "attempts", "sysmats", "matvecs", "flops", "items", "failed")] + \
-               [("solve_ms", ctypes.c_double), ("prep_ms", ctypes.c_double), ("synth_ms", ctypes.c_double)]
+               [("solve_ms", ctypes.c_double), ("prep_ms", ctypes.c_double), ("synth_ms", ctypes.c_double),
+                ("phase_flops", ctypes.c_int64 * 3), ("phase_ms", ctypes.c_double * 3)]
 
     def asdict(self):
-        return {n: (getattr(self, n)) for n, _ in self._fields_}
+        return {n: (list(getattr(self, n)) if n.startswith("phase") else getattr(self, n)) for n, _ in self._fields_}
 
 
 _lib = None

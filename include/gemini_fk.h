@@ -73,6 +73,8 @@ typedef struct gem_stats {
   double solve_ms; /* device time of the last solver launch */
   double prep_ms;  /* device time of the last model preparation */
   double synth_ms; /* device time of the last synthetics run */
+  int64_t phase_flops[3]; /* FP64 flops of the toroidal, spheroidal and adjoint phase kernels */
+  double phase_ms[3];     /* device time of each phase (the first includes the start-radius kernel) */
 } gem_stats;
 
 /* Synthetics parameters (computeSyntheticSeismograms.f90:136-240); df and

@@ -171,3 +171,23 @@ def test_fast_backend_batched_slab(gpu):
     _, _, b, sb = fast.run(w.params, jre, g.nf2 - 3, g.nf2, f32=False)
     assert np.all(sa == 0) and np.all(sb == 0)
     assert _cmp_per_spectrum(b, a) <= RTOL_FAST
+
+
+@pytest.mark.parametrize("istyp,stress", [(0, 0), (1, 1), (0, 1)])
+@pytest.mark.parametrize("backend", [1, 2])
+def test_force_source_and_stress_outputs(small, istyp, stress, backend):
+    """Force sources (nsp 5, or 10 with stresses) and moment sources with
+    stresses (nsp 20) against the oracle, on three frequencies of the global
+    configuration; plain build to the parity bar, fast build to the FP64 bar."""
+    from gemini_unified_b200.fk import GeminiFK
+    w, m, ex, jre, _, o = small
+    params = dataclasses.replace(w.params, source_type="FORCE" if istyp == 0 else "MOMENT", stressflag=bool(stress))
+    nsp = M.nsp_for(params)
+    assert nsp == {(0, 0): 5, (1, 1): 20, (0, 1): 10}[(istyp, stress)]
+    g = M.frequency_grid(params, m.rearth)
+    fk = GeminiFK(m, ex, backend=backend)
+    _, _, g64, st = fk.run(params, jre, 20, 22, f32=False)
+    assert np.all(st == 0) and g64.shape[1] == nsp
+    pc = M.fk_params_c(params, jre)
+    ref = np.concatenate([o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), nsp)[0] for jf in (20, 21, 22)], axis=2)
+    assert _cmp_per_spectrum(g64, ref) <= (RTOL if backend == 1 else RTOL_FAST)
