@@ -264,7 +264,6 @@ def main():
     sph_flops, sph_ms = phase["flops"][1], max_over_ranks(phase["ms"][1])
     phase_ms_fast = list(phase["ms"])
     value = total_items / (t_ms / 1e3)
-    sph_ms = fast.stats()["solve_ms"]
 
     # ---------------- plain FP64 form (reference rounding, one operation at a time)
     plain = GeminiFK(m, ex, device=local, backend=1)

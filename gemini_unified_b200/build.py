@@ -6,7 +6,7 @@
 The parity build of the FK solver (and every other file) is compiled with
 --fmad=false so its arithmetic repeats the reference's operation by operation
 (the reference is built without FMA contraction); the fast build of the solver
-(fk_solver_fast.cu) uses FMA contraction.
+(fk_solver_fast.cu) and the fast inverse FFT (ifft_fast.cu) use FMA contraction.
 """
 from __future__ import annotations
 
@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
          "-I" + os.path.join(ROOT, "include")]
 # files compiled with FMA contraction; all others repeat the reference's rounding (--fmad=false)
-FMAD_TRUE = {"fk_solver_fast.cu"}
+FMAD_TRUE = {"fk_solver_fast.cu", "ifft_fast.cu"}
 
 
 def sources():

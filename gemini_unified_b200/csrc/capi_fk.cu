@@ -154,6 +154,7 @@ int check_params(gem_ctx* ctx, const gem_fk_params* p) {
 int gem_set_error(gem_ctx* ctx, const char* msg) { return fail(ctx, "%s", msg); }
 void gem_note_synth_ms(gem_ctx* ctx, float ms) { if (ctx) ctx->stats.synth_ms = ms; }
 int gem_ctx_device(const gem_ctx* ctx) { return ctx->device; }
+int gem_ctx_backend(const gem_ctx* ctx) { return ctx->backend; }
 void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes) {
   if (slot < 0 || slot >= 4) return nullptr;
   if (ctx->d_aux[slot] && ctx->aux_cap[slot] >= bytes) return ctx->d_aux[slot];

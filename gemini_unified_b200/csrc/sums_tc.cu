@@ -1,0 +1,521 @@
+// Degree sums on the 5th-generation tensor cores with sliced integer operands.
+//
+// The degree sums of harmonicDegreeSums.f90:95-351 are, for every Legendre
+// table kind, the product C[row, station] = sum_l A[row, l] * T[l, station]
+// (rows: frequency x sum x re/im; see synth.cu).  The FP64 form runs it on
+// CUDA cores.  Here the Legendre recurrences and the coefficient weights stay
+// FP64 and the product runs on tcgen05 as an exact integer computation:
+//
+//   T[l, n] = s_l c_n t,    s_l, c_n powers of two, |t| < 1
+//   A[m, l] s_l = r_m a,    r_m a power of two,      |a| < 1
+//   a = sum_i a_i 128^-(i+1), t = sum_j t_j 128^-(j+1), a_i, t_j in [-127, 127]
+//   C[m, n] = r_m c_n sum_{w=0}^{S-1} 128^-(w+2) sum_{i+j=w} (sum_l a_i t_j)
+//
+// with S = 7 slices of 7 bits (49 bits of each operand relative to its row or
+// column scale; terms with i + j >= S are dropped).  The slice products are
+// accumulated exactly in INT32 by tcgen05.mma kind::i8 and combined in FP64,
+// so the result keeps FP64-level accuracy even where the degree sum cancels by
+// five orders of magnitude (near-antipodal stations), which FP16 operands with
+// FP32 accumulation cannot.
+//
+// GEMM kernel: one CTA per 128 x 64 output tile.  Per k-block of 64 degrees,
+// warp 0 issues TMA loads (64-byte swizzle) of the 7 slices of A and of T into
+// a 2-stage shared-memory ring; warp 1 issues the 28 slice products (2 MMAs of
+// K 32 each) into 7 TMEM accumulators of 64 columns, one per weight w = i + j;
+// warps 2-5 combine the accumulators in FP64 and write C.  All mbarrier waits
+// are bounded by a 1 s timer: a wait that runs out records an error flag, the
+// CTA stops issuing work, waits (bounded) for its own copies and products,
+// frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "synth.h"
+
+namespace gem {
+
+constexpr int TC_S = 7;                                  // slices per operand
+constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 64;      // tile; BK int8 = 64 bytes = one swizzle row
+constexpr int TC_STAGES = 2;
+constexpr int TC_A_BYTES = TC_BM * TC_BK;               // 8 KiB per slice
+constexpr int TC_B_BYTES = TC_BN * TC_BK;               // 4 KiB per slice
+constexpr int TC_STAGE_BYTES = TC_S * (TC_A_BYTES + TC_B_BYTES);   // 84 KiB
+constexpr int TC_THREADS = 192;
+constexpr int TC_TMEM_COLS = 512;                       // 7 accumulators of 64 columns
+constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
+constexpr unsigned long long TC_WAIT_NS = 1000000000ull;
+
+// ---------------------------------------------------------------------------
+//  Operand preparation (FP64 in, INT8 slices out)
+// ---------------------------------------------------------------------------
+
+// smallest power of two strictly above |x| (1 for 0 or non-finite)
+__device__ __forceinline__ double pow2_above(double x) {
+  if (!(x > 0.0) || !isfinite(x)) return 1.0;
+  int e;
+  frexp(x, &e);   // x = f 2^e, f in [0.5, 1)
+  return ldexp(1.0, e);
+}
+
+// the 7-bit slices of x, |x| < 1: x = sum_i q_i 128^-(i+1) + O(128^-S)
+__device__ __forceinline__ void slices_of(double x, signed char q[TC_S]) {
+#pragma unroll
+  for (int i = 0; i < TC_S; ++i) {
+    x *= 128.0;
+    const double a = trunc(x);
+    x -= a;
+    q[i] = (signed char)(int)a;
+  }
+}
+
+__device__ __forceinline__ double block_max(double m) {
+  __shared__ double red[256];
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// s[kind][l] = power of two above max over stations of |T[kind][l][sta]| (one block per (l, kind))
+__global__ void tab_scale_kernel(int nsta, int lcap, int K, const double* __restrict__ tab, double* lscale, int Kp) {
+  const int l = blockIdx.x, kind = blockIdx.y;
+  double m = 0.0;
+  if (l < K) {
+    const double* row = tab + ((long long)kind * lcap + l) * nsta;
+    for (int i = threadIdx.x; i < nsta; i += blockDim.x) m = fmax(m, fabs(row[i]));
+  }
+  m = block_max(m);
+  if (threadIdx.x == 0) lscale[(long long)kind * Kp + l] = pow2_above(m);
+}
+
+// c[kind][sta] = power of two above max over l of |T[kind][l][sta] / s_l| (one thread per station)
+__global__ void tab_colscale_kernel(int nsta, int lcap, int K, int Kp, const double* __restrict__ tab,
+                                    const double* __restrict__ lscale, double* cscale) {
+  const int sta = blockIdx.x * blockDim.x + threadIdx.x, kind = blockIdx.y;
+  if (sta >= nsta) return;
+  double m = 0.0;
+  for (int l = 0; l < K; ++l)
+    m = fmax(m, fabs(tab[((long long)kind * lcap + l) * nsta + sta] / lscale[(long long)kind * Kp + l]));
+  cscale[(long long)kind * nsta + sta] = pow2_above(m);
+}
+
+// T8[j][kind*nsta + sta][l] = slice j of T / (s_l c_sta), through a 64 x 64 shared-memory transpose
+__global__ void tab_slice_kernel(int nsta, int lcap, int K, int Kp, const double* __restrict__ tab,
+                                 const double* __restrict__ lscale, const double* __restrict__ cscale,
+                                 signed char* T8) {
+  __shared__ double tile[64][65];
+  const int kind = blockIdx.z;
+  const int l0 = blockIdx.x * 64, s0 = blockIdx.y * 64;
+  const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;   // 256 threads: 64 x 4
+  for (int r = ty; r < 64; r += 4) {
+    const int l = l0 + r, sta = s0 + tx;
+    double v = 0.0;
+    if (l < K && sta < nsta)
+      v = tab[((long long)kind * lcap + l) * nsta + sta] / lscale[(long long)kind * Kp + l] /
+          cscale[(long long)kind * nsta + sta];
+    tile[r][tx] = v;
+  }
+  __syncthreads();
+  const long long plane = 8LL * nsta * Kp;
+  for (int r = ty; r < 64; r += 4) {
+    const int sta = s0 + r, l = l0 + tx;
+    if (sta >= nsta) continue;
+    signed char q[TC_S];
+    slices_of(tile[tx][r], q);
+    const long long o = ((long long)kind * nsta + sta) * Kp + l;
+#pragma unroll
+    for (int j = 0; j < TC_S; ++j) T8[j * plane + o] = q[j];
+  }
+}
+
+// A8[i][row][l] = slice i of A[row][l] s_l / r_row; one block per row of every kind
+__global__ void coef_slice_kernel(SynthDev S, long long mtot, int K, int Kp, const double* __restrict__ A,
+                                  const double* __restrict__ lscale, const int* __restrict__ row_kind,
+                                  signed char* A8, double* rscale) {
+  const long long row = blockIdx.x;
+  const int kind = row_kind[row];
+  const double* a = A + row * S.lcap;
+  const double* sl = lscale + (long long)kind * Kp;
+  double m = 0.0;
+  for (int l = threadIdx.x; l < K; l += blockDim.x) m = fmax(m, fabs(a[l] * sl[l]));
+  const double r = pow2_above(block_max(m));
+  if (threadIdx.x == 0) rscale[row] = r;
+  const long long plane = mtot * Kp;
+  for (int l = threadIdx.x; l < Kp; l += blockDim.x) {
+    signed char q[TC_S];
+    slices_of(l < K ? a[l] * sl[l] / r : 0.0, q);
+#pragma unroll
+    for (int i = 0; i < TC_S; ++i) A8[i * plane + row * Kp + l] = q[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+//  tcgen05 integer GEMM
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: true when the phase completed, false after the time limit or
+// when another role of this CTA has already given up (abort flag).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (true) {
+    if (mbar_try(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (global_ns() - t0 > TC_WAIT_NS) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+}
+
+// wait that ignores the abort flag (used to drain this CTA's own copies before exit)
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity) {
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try(bar, parity) && global_ns() - t0 < TC_WAIT_NS) {
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"((unsigned long long)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// K-major operand, 64-byte swizzle: rows of 64 bytes, 8-row groups 512 bytes apart
+__device__ __forceinline__ uint64_t smem_desc_sw64(const void* p) {
+  const uint64_t addr = smem_u32(p);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;          // start address
+  d |= (uint64_t)1 << 16;                // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;       // stride byte offset: 8 rows x 64 B
+  d |= (uint64_t)1 << 46;                // descriptor version (tcgen05)
+  d |= (uint64_t)4 << 61;                // SWIZZLE_64B
+  return d;
+}
+
+// kind::i8 instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = 64, M = 128
+constexpr uint32_t TC_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+                              ((uint32_t)(TC_BM >> 4) << 24);
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    sums_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                   const int2* __restrict__ tiles, const int* __restrict__ kind_rows,
+                   const long long* __restrict__ kind_rowoff, const long long* __restrict__ coff, int nsta,
+                   long long mtot, int nkb, const double* __restrict__ rscale, const double* __restrict__ cscale,
+                   double* C, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = (uint64_t*)(smem + TC_STAGES * TC_STAGE_BYTES);
+  uint64_t* empty = full + TC_STAGES;
+  uint64_t* acc_full = empty + TC_STAGES;
+  uint32_t* tmem_slot = (uint32_t*)(acc_full + 1);
+  volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int2 t = tiles[blockIdx.y];      // (kind, first row of the tile within the kind)
+  const int kind = t.x, m0 = t.y;
+  const int n0 = blockIdx.x * TC_BN;
+  const int Mk = kind_rows[kind];
+  const long long rowA = kind_rowoff[kind] + m0;
+  const long long rowB = (long long)kind * nsta + n0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TC_STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(acc_full, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- producer: the 7 slices of A and of T per k-block
+    int issued = 0;
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % TC_STAGES;
+      if (kb >= TC_STAGES && !mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1, abort_flag)) break;
+      unsigned char* st = smem + s * TC_STAGE_BYTES;
+      mbar_expect_tx(&full[s], TC_STAGE_BYTES);
+#pragma unroll 1
+      for (int i = 0; i < TC_S; ++i)
+        tma_load_2d(st + i * TC_A_BYTES, &mapA, &full[s], kb * TC_BK, (int)(i * mtot + rowA));
+#pragma unroll 1
+      for (int j = 0; j < TC_S; ++j)
+        tma_load_2d(st + TC_S * TC_A_BYTES + j * TC_B_BYTES, &mapB, &full[s], kb * TC_BK,
+                    (int)(j * 8LL * nsta + rowB));
+      ++issued;
+    }
+    for (int kb = (issued > TC_STAGES ? issued - TC_STAGES : 0); kb < issued; ++kb)
+      mbar_drain(&full[kb % TC_STAGES], (kb / TC_STAGES) & 1);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer: accumulator w = i + j at TMEM columns 64 w
+    bool ok = true;
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % TC_STAGES;
+      if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1, abort_flag)) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const unsigned char* st = smem + s * TC_STAGE_BYTES;
+#pragma unroll 1
+      for (int i = 0; i < TC_S; ++i) {
+        const uint64_t da = smem_desc_sw64(st + i * TC_A_BYTES);
+#pragma unroll 1
+        for (int j = 0; j + i < TC_S; ++j) {
+          const uint64_t db = smem_desc_sw64(st + TC_S * TC_A_BYTES + j * TC_B_BYTES);
+          const uint32_t dtm = tmem + (uint32_t)((i + j) * TC_BN);
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 32; ++kk) {
+            const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 32 int8 = 32 bytes along K
+            const uint32_t acc = (kb > 0 || kk > 0 || i > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtm),
+                "l"(da + adv), "l"(db + adv), "r"(TC_IDESC), "r"(acc));
+          }
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&empty[s]))
+                   : "memory");
+    }
+    // signals the epilogue once every product issued above has completed
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(acc_full))
+                 : "memory");
+    if (!ok) *abort_flag = 1;
+  } else if (warp >= 2) {
+    // ---- epilogue: TMEM lanes 32*(warp % 4) .. +31 hold rows of the tile
+    const int q = warp & 3;
+    const bool done = mbar_wait(acc_full, 0, abort_flag);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const int r = m0 + q * 32 + lane;   // row within the kind
+    const bool row_ok = done && !*abort_flag && r < Mk;
+    const double rs = row_ok ? rscale[kind_rowoff[kind] + r] : 0.0;
+    double* crow = C + coff[kind] + (long long)r * nsta;
+    const double* cs = cscale + (long long)kind * nsta;
+#pragma unroll 1
+    for (int c = 0; c < TC_BN / 32; ++c) {
+      double sum[32];
+#pragma unroll
+      for (int jj = 0; jj < 32; ++jj) sum[jj] = 0.0;
+#pragma unroll 1
+      for (int w = TC_S - 1; w >= 0; --w) {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * TC_BN + c * 32);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+              "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+              "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+              "=r"(v[30]), "=r"(v[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const double wgt = ldexp(1.0, -7 * (w + 2));
+#pragma unroll
+        for (int jj = 0; jj < 32; ++jj) sum[jj] += (double)(int)v[jj] * wgt;   // smallest weights first
+      }
+      if (row_ok) {
+        const int nb = n0 + c * 32;
+#pragma unroll
+        for (int jj = 0; jj < 32; ++jj)
+          if (nb + jj < nsta) crow[nb + jj] = sum[jj] * rs * cs[nb + jj];
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+  }
+  if (threadIdx.x == 0 && *abort_flag) atomicExch(err, 1);
+}
+
+}  // namespace gem
+
+// ===========================================================================
+//  Host side
+// ===========================================================================
+using namespace gem;
+
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// 2D map over int8 rows of Kp bytes, box 64 bytes x box_rows, 64-byte swizzle
+bool make_map(CUtensorMap* map, const signed char* base, long long rows, long long kp, int box_rows) {
+  EncodeTiledFn f = encode_fn();
+  if (!f) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kp};
+  cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return f(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+struct TcLayout {
+  int Kp;
+  size_t off[9], total;
+};
+
+TcLayout tc_layout(const SynthDev& S, long long mtot) {
+  TcLayout L{};
+  const int K = S.lmax + 1;
+  L.Kp = (K + TC_BK - 1) / TC_BK * TC_BK;
+  const size_t sz[9] = {(size_t)TC_S * 8 * S.nsta * L.Kp,            // T8
+                        (size_t)TC_S * mtot * L.Kp,                   // A8
+                        (size_t)8 * L.Kp * sizeof(double),            // lscale
+                        (size_t)8 * S.nsta * sizeof(double),          // cscale
+                        (size_t)mtot * sizeof(double),                // rscale
+                        (size_t)mtot * sizeof(int),                   // row kind
+                        (size_t)(mtot / TC_BM + 16) * sizeof(int2),   // tiles
+                        (size_t)24 * sizeof(long long),               // per-kind tables
+                        (size_t)16 * sizeof(int)};                    // kind rows + error flag
+  size_t b = 0;
+  for (int i = 0; i < 9; ++i) {
+    L.off[i] = b;
+    b += (sz[i] + 1023) / 1024 * 1024;
+  }
+  L.total = b + 1024;
+  return L;
+}
+
+}  // namespace
+
+namespace gem {
+
+size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out) {
+  TcLayout L = tc_layout(S, mtot);
+  if (Kp_out) *Kp_out = L.Kp;
+  return L.total;
+}
+
+// Sliced-integer sums: from the FP64 tables tab[kind][l][sta] and coefficients
+// A[kind rows][lcap], write C[kind][row][sta] in FP64.  ws: device workspace of
+// sums_tc_workspace bytes.  Blocking (synchronises the stream).
+const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, const double* A, double* C, void* ws,
+                        size_t ws_bytes, cudaStream_t st) {
+  TcLayout L = tc_layout(S, mtot);
+  if (ws_bytes < L.total) return "sums_tc: workspace too small";
+  if (7LL * mtot >= (1LL << 31) || 7LL * 8 * S.nsta >= (1LL << 31)) return "sums_tc: operand rows exceed 2^31";
+  if ((long long)L.Kp * TC_S * 127 * 127 >= (1LL << 31)) return "sums_tc: degree range too large for INT32 accumulation";
+  const int K = S.lmax + 1, Kp = L.Kp;
+  const int nf = S.nf2 - S.nf1 + 1;
+  char* base = (char*)(((uintptr_t)ws + 1023) & ~(uintptr_t)1023);
+  signed char* T8 = (signed char*)(base + L.off[0]);
+  signed char* A8 = (signed char*)(base + L.off[1]);
+  double* lscale = (double*)(base + L.off[2]);
+  double* cscale = (double*)(base + L.off[3]);
+  double* rscale = (double*)(base + L.off[4]);
+  int* row_kind = (int*)(base + L.off[5]);
+  int2* tiles = (int2*)(base + L.off[6]);
+  long long* tabs = (long long*)(base + L.off[7]);
+  int* ints = (int*)(base + L.off[8]);   // [0..7] rows per kind, [8] error flag
+  int krows[16] = {0};
+  long long htabs[24];
+  std::vector<int2> htiles;
+  std::vector<int> hrk((size_t)mtot);
+  long long ro = 0;
+  for (int k = 0; k < 8; ++k) {
+    krows[k] = 2 * nf * S.nsk[k];
+    htabs[k] = 0;
+    htabs[8 + k] = ro;
+    htabs[16 + k] = S.coff[k];
+    for (int m = 0; m < krows[k]; m += TC_BM) htiles.push_back(make_int2(k, m));
+    for (int m = 0; m < krows[k]; ++m) hrk[(size_t)(ro + m)] = k;
+    ro += krows[k];
+  }
+  if (ro != mtot) return "sums_tc: row count mismatch";
+  if (cudaMemcpyAsync(tiles, htiles.data(), htiles.size() * sizeof(int2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(row_kind, hrk.data(), hrk.size() * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(tabs, htabs, sizeof htabs, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(ints, krows, sizeof krows, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return "sums_tc: upload failed";
+  // operands
+  tab_scale_kernel<<<dim3(Kp, 8), 256, 0, st>>>(S.nsta, S.lcap, K, tab, lscale, Kp);
+  tab_colscale_kernel<<<dim3((S.nsta + 127) / 128, 8), 128, 0, st>>>(S.nsta, S.lcap, K, Kp, tab, lscale, cscale);
+  tab_slice_kernel<<<dim3(Kp / 64, (S.nsta + 63) / 64, 8), 256, 0, st>>>(S.nsta, S.lcap, K, Kp, tab, lscale, cscale,
+                                                                         T8);
+  coef_slice_kernel<<<(unsigned)mtot, 256, 0, st>>>(S, mtot, K, Kp, A, lscale, row_kind, A8, rscale);
+  // tensor maps over A8 [7 mtot][Kp] and T8 [7 * 8 nsta][Kp]
+  CUtensorMap mA, mB;
+  if (!make_map(&mA, A8, TC_S * mtot, Kp, TC_BM) || !make_map(&mB, T8, TC_S * 8LL * S.nsta, Kp, TC_BN))
+    return "sums_tc: cuTensorMapEncodeTiled failed";
+  if (cudaFuncSetAttribute(sums_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) != cudaSuccess)
+    return "sums_tc: shared-memory attribute";
+  if (cudaMemsetAsync(ints + 8, 0, sizeof(int), st) != cudaSuccess) return "sums_tc: upload failed";
+  dim3 grid((S.nsta + TC_BN - 1) / TC_BN, (unsigned)htiles.size());
+  sums_tc_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(mA, mB, tiles, ints, tabs + 8, tabs + 16, S.nsta, mtot,
+                                                    Kp / TC_BK, rscale, cscale, C, ints + 8);
+  if (cudaGetLastError() != cudaSuccess) return "sums_tc: launch failed";
+  int herr = 0;
+  if (cudaMemcpyAsync(&herr, ints + 8, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return "sums_tc: execution failed";
+  if (herr) return "sums_tc: a pipeline wait timed out";
+  return nullptr;
+}
+
+}  // namespace gem

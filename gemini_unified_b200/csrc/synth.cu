@@ -326,6 +326,7 @@ struct SynthBuffers {
   double2* X = nullptr;
   double2* evf = nullptr;
   double2* tw = nullptr;
+  double2* twx = nullptr;   // e^{2 pi i m/ns} of the fast-form transform
   double* fac = nullptr;
   int* nwn = nullptr;
   int* koff = nullptr;
@@ -334,6 +335,7 @@ struct SynthBuffers {
 
 void free_all(SynthBuffers& b) {
   cudaFree(b.tab); cudaFree(b.A); cudaFree(b.C); cudaFree(b.X); cudaFree(b.evf); cudaFree(b.tw); cudaFree(b.fac);
+  cudaFree(b.twx);
   cudaFree(b.nwn); cudaFree(b.koff); cudaFree(b.theta); cudaFree(b.phi); cudaFree(b.propdir); cudaFree(b.mt);
 }
 
@@ -481,14 +483,36 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   legendre_kernel<<<(nsta * 3 + 127) / 128, 128, 0, st>>>(nsta, S.lmax, S.lcap, b.theta, b.tab);
   long long ncoef = (long long)nf * 14 * S.lcap;
   coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
-  int mmax = 2 * nf * 2;
-  dim3 g((nsta + GT_N - 1) / GT_N, (mmax + GT_M - 1) / GT_M, 8);
-  sums_gemm_kernel<<<g, 256, 0, st>>>(S, b.A, b.tab, b.C);
+  if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST) {
+    // split-precision products on the tensor cores (FP16 hi/lo operands, FP32 accumulation)
+    const long long mtot = 2LL * nf * 14;
+    const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
+    void* ws = gem_ctx_aux(ctx, 3, wsb);
+    if (!ws) { free_all(b); return GEM_ERROR; }
+    if (const char* why = sums_tc_run(S, mtot, b.tab, b.A, b.C, ws, wsb, st)) {
+      free_all(b);
+      return gem_set_error(ctx, why);
+    }
+  } else {
+    int mmax = 2 * nf * 2;
+    dim3 g((nsta + GT_N - 1) / GT_N, (mmax + GT_M - 1) / GT_M, 8);
+    sums_gemm_kernel<<<g, 256, 0, st>>>(S, b.A, b.tab, b.C);
+  }
   long long nsp_ = (long long)nsta * nf;
   spectra_kernel<<<(unsigned)((nsp_ + 127) / 128), 128, 0, st>>>(S, b.C, b.evf, b.phi, b.propdir, b.mt, b.X);
-  size_t smem = (size_t)ns * sizeof(double2);
-  cudaFuncSetAttribute(ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  ifft_kernel<<<(unsigned)ntr, 512, smem, st>>>(S, b.X, b.tw, b.fac, d_traces);
+  const bool fast_fft = gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST && ifft_fast_supported(ns);
+  if (fast_fft) {
+    if (cudaMalloc((void**)&b.twx, (size_t)ns * sizeof(double2)) != cudaSuccess) {
+      free_all(b);
+      return gem_set_error(ctx, "synthetics: device allocation failed");
+    }
+    ifft_fast_twiddles_launch(ns, b.twx, st);
+    ifft_fast_launch(S, ntr, b.X, b.twx, b.fac, d_traces, st);
+  } else {
+    size_t smem = (size_t)ns * sizeof(double2);
+    cudaFuncSetAttribute(ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ifft_kernel<<<(unsigned)ntr, 512, smem, st>>>(S, b.X, b.tw, b.fac, d_traces);
+  }
   cudaEventRecord(e1, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -537,7 +561,9 @@ extern "C" int gem_ifft_run_device(gem_ctx* ctx, int nf1, int nf2, double df, do
   FftGeometry g;
   if (const char* why = fft_geometry(nf1, nf2, df, nsamp, dt, g)) return gem_set_error(ctx, why);
   if (cudaSetDevice(gem_ctx_device(ctx)) != cudaSuccess) return gem_set_error(ctx, "ifft: cudaSetDevice failed");
-  char* tab = (char*)gem_ctx_aux(ctx, 0, ifft_table_bytes(g.ns, nsamp));
+  const bool fast = gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST && ifft_fast_supported(g.ns);
+  const size_t tbytes = ifft_table_bytes(g.ns, nsamp);
+  char* tab = (char*)gem_ctx_aux(ctx, 0, tbytes + (fast ? (size_t)g.ns * sizeof(double2) + 16 : 0));
   if (!tab) return GEM_ERROR;
   double2* tw = (double2*)tab;
   double* fac = (double*)(tab + (size_t)g.ns * sizeof(double2));
@@ -547,9 +573,15 @@ extern "C" int gem_ifft_run_device(gem_ctx* ctx, int nf1, int nf2, double df, do
   S.sigma = sigma; S.ldx = ldsp;
   const double expo = std::exp(sigma * g.dts);
   ifft_tables_kernel<<<8, 256, 0, st>>>(g.ns, g.nslog, nsamp, expo, tw, fac);
-  const size_t smem = (size_t)g.ns * sizeof(double2);
-  cudaFuncSetAttribute(ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  ifft_kernel<<<(unsigned)ntr, IFFT_THREADS, smem, st>>>(S, (const double2*)d_sp, tw, fac, d_ts);
+  if (fast) {
+    double2* twx = (double2*)(tab + (tbytes + 15) / 16 * 16);
+    ifft_fast_twiddles_launch(g.ns, twx, st);
+    ifft_fast_launch(S, ntr, (const double2*)d_sp, twx, fac, d_ts, st);
+  } else {
+    const size_t smem = (size_t)g.ns * sizeof(double2);
+    cudaFuncSetAttribute(ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ifft_kernel<<<(unsigned)ntr, IFFT_THREADS, smem, st>>>(S, (const double2*)d_sp, tw, fac, d_ts);
+  }
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return gem_set_error(ctx, cudaGetErrorString(e));

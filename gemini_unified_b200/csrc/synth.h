@@ -44,10 +44,23 @@ __global__ void __launch_bounds__(512) ifft_kernel(SynthDev S, const double2* __
                             const double* __restrict__ fac, float* traces);
 inline size_t ifft_table_bytes(int ns, int nsamp) { return (size_t)ns * sizeof(double2) + (size_t)nsamp * sizeof(double); }
 
+// fast-form inverse FFT (ifft_fast.cu): real output from a half-length radix-16
+// transform; ns in 512..8192; tw = e^{2 pi i m/ns}, m < ns
+cudaError_t ifft_fast_launch(const SynthDev& S, long long ntr, const double2* X, const double2* tw, const double* fac,
+                             float* traces, cudaStream_t st);
+cudaError_t ifft_fast_twiddles_launch(int N, double2* tw, cudaStream_t st);
+inline bool ifft_fast_supported(int ns) { return ns >= 512 && ns <= IFFT_MAX_NS; }
+
+// sliced-integer tensor-core degree sums (sums_tc.cu): workspace size and run
+size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out);
+const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, const double* A, double* C, void* ws,
+                        size_t ws_bytes, cudaStream_t st);
+
 }  // namespace gem
 
 // error / timing / buffer hooks of the context (defined with gem_ctx)
 int gem_set_error(gem_ctx* ctx, const char* msg);
 void gem_note_synth_ms(gem_ctx* ctx, float ms);
 int gem_ctx_device(const gem_ctx* ctx);
+int gem_ctx_backend(const gem_ctx* ctx);
 void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes);

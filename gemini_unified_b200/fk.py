@@ -98,9 +98,9 @@ def _ptr(a: Optional[np.ndarray]):
 class FrequencyTime:
     """Batched transformFrequencyTime (f90/frequencyTime.f90:55-113) on one GPU."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, backend: int = GEM_BACKEND_GPU_FP64):
         self._h = ctypes.c_void_p()
-        rc = lib().gem_ctx_create(device, GEM_BACKEND_GPU_FP64, ctypes.byref(self._h))
+        rc = lib().gem_ctx_create(device, backend, ctypes.byref(self._h))
         if rc != 0 or not self._h:
             raise GeminiError("gem_ctx_create failed (no CUDA device %d)" % device)
         self.warning = None

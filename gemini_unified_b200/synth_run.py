@@ -35,6 +35,9 @@ def main(argv=None):
     ap.add_argument("--workload", default="batched_fk", choices=sorted(configs.WORKLOADS))
     ap.add_argument("--repeat", type=int, default=2)
     ap.add_argument("--stations", type=int, default=0, help="first N stations only (0 = all)")
+    ap.add_argument("--backend", type=int, default=2, choices=[1, 2],
+                    help="1 FP64 degree sums, 2 sliced-integer tensor-core degree sums")
+    ap.add_argument("--check", action="store_true", help="also run the FP64 form and report the relative error")
     a = ap.parse_args(argv)
     w = configs.WORKLOADS[a.workload]
     m = w.model()
@@ -48,27 +51,51 @@ def main(argv=None):
     mt = np.ascontiguousarray(configs.unit_moment_tensors(), np.float64)
     sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs)
     nwn = np.ascontiguousarray(g.nwn, np.int32)
-    ctx = FrequencyTime()
     d_gr = torch.from_numpy(gr).cuda()
     d_gi = torch.from_numpy(gi).cuda()
-    out = torch.empty((len(theta), len(mt), 3, w.nsamp), dtype=torch.float32, device="cuda")
     L = lib()
     p = lambda x: x.ctypes.data_as(ctypes.c_void_p)
-    ms = []
-    for _ in range(a.repeat):
-        rc = L.gem_synth_run_device(ctx._h, ctypes.byref(sp), p(nwn), d_gr.data_ptr(), d_gi.data_ptr(), len(theta),
-                                    p(theta), p(phi), p(propdir), len(mt), p(mt), out.data_ptr(), None)
-        if rc >= 2:
-            raise SystemExit(L.gem_last_error(ctx._h).decode())
+
+    def run(backend, repeat):
         from .fk import Stats
-        s = Stats()
-        L.gem_stats_get(ctx._h, ctypes.byref(s))
-        ms.append(s.synth_ms)
+        ctx = FrequencyTime(backend=backend)
+        out = torch.empty((len(theta), len(mt), 3, w.nsamp), dtype=torch.float32, device="cuda")
+        ms = []
+        for _ in range(repeat):
+            rc = L.gem_synth_run_device(ctx._h, ctypes.byref(sp), p(nwn), d_gr.data_ptr(), d_gi.data_ptr(),
+                                        len(theta), p(theta), p(phi), p(propdir), len(mt), p(mt), out.data_ptr(), None)
+            if rc >= 2:
+                raise SystemExit(L.gem_last_error(ctx._h).decode())
+            s = Stats()
+            L.gem_stats_get(ctx._h, ctypes.byref(s))
+            ms.append(s.synth_ms)
+        return out, ms
+
+    out, ms = run(a.backend, a.repeat)
     ntr = len(theta) * len(mt)
-    print(json.dumps({"workload": a.workload, "stations": len(theta), "moment_tensors": len(mt), "traces": ntr,
-                      "nsamp": w.nsamp, "synth_ms": ms, "traces_per_s": ntr / (min(ms) / 1e3),
-                      "finite": bool(torch.isfinite(out).all().item())}))
+    res = {"workload": a.workload, "backend": a.backend, "stations": len(theta), "moment_tensors": len(mt),
+           "traces": ntr, "nsamp": w.nsamp, "synth_ms": ms, "traces_per_s": ntr / (min(ms) / 1e3),
+           "finite": bool(torch.isfinite(out).all().item())}
+    if a.check:
+        ref, ms_ref = run(1, 1)
+        res.update(trace_errors(out, ref))
+        res["fp64_synth_ms"] = ms_ref[0]
+    print(json.dumps(res))
     return 0
+
+
+def trace_errors(got, ref) -> dict:
+    """Relative L2 error of every 1-component trace (float64 norms) and of the whole set."""
+    import torch
+    g = got.double().reshape(-1, got.shape[-1])
+    r = ref.double().reshape(-1, ref.shape[-1])
+    scale = 1.0 / r.abs().max()
+    g, r = g * scale, r * scale
+    num = torch.linalg.vector_norm(g - r, dim=1)
+    den = torch.linalg.vector_norm(r, dim=1)
+    rel = (num / den).cpu().numpy()
+    return {"rel_l2_trace_max": float(rel.max()), "rel_l2_trace_median": float(np.median(rel)),
+            "rel_l2_all": float((torch.linalg.vector_norm(g - r) / torch.linalg.vector_norm(r)).item())}
 
 
 if __name__ == "__main__":

@@ -11,10 +11,11 @@ RTOL_L2 = 1e-7
 
 CASES = [
     # nf1, nf2, df, nsamp, dt: the global configuration's series, a decimated
-    # series, and the 8192-sample series of the batched configuration
+    # series, the 8192-sample series of the batched configuration, a 512-sample one
     (2, 52, 1.0 / 1024, 2048, 0.5),
     (3, 300, 1.0 / 1024, 256, 4.0),
     (2, 411, 1.0 / 2048, 8192, 0.25),
+    (2, 200, 1.0 / 512, 512, 1.0),
 ]
 
 
@@ -66,3 +67,32 @@ def test_ifft_rejects_invalid_sizes(ft):
         ft.run(2, 52, 1.0 / 1024, 0.0, sp, 16384, 1.0 / 16)  # FFT length above 8192
     with pytest.raises(GeminiError):
         ft.run(2, 61, 1.0 / 1024, 0.0, sp, 2048, 0.5)       # nf2 beyond the leading dimension
+
+
+def _exact(nf1, nf2, df, sigma, sp, nsamp, dt):
+    """transformFrequencyTime with an exact inverse DFT (numpy, FP64)."""
+    ns = max(nsamp, 2 ** (int(np.ceil(np.log2(np.float32(nf2)))) + 1))
+    ndec = 1 if ns == nsamp else int(round(dt / (1.0 / (df * ns))))
+    X = np.zeros((sp.shape[0], ns // 2 + 1), complex)
+    X[:, nf1 - 1:nf2] = sp[:, nf1 - 1:nf2]
+    x = np.fft.irfft(X, n=ns) * ns
+    dts = dt / ndec
+    return x[:, ::ndec][:, :nsamp] * df * np.exp(sigma * dts * np.arange(nsamp))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fast_ifft_exact_and_reference(case):
+    """Fast form (real output from a half-length radix-16 transform): within
+    float32 rounding of the exact inverse DFT, and within the 1e-5 seismogram
+    bar of the reference's transform (whose twiddles use single-precision pi)."""
+    import oracle
+    from gemini_unified_b200.fk import FrequencyTime, GEM_BACKEND_GPU_FAST
+    nf1, nf2, df, nsamp, dt = case
+    sigma = 5 * df
+    sp = _spectra(29, nf2 + 2, nf2 + 7)
+    got = FrequencyTime(backend=GEM_BACKEND_GPU_FAST).run(nf1, nf2, df, sigma, sp, nsamp, dt).astype(np.float64)
+    ex = _exact(nf1, nf2, df, sigma, sp, nsamp, dt)
+    assert (np.linalg.norm(got - ex, axis=1) / np.linalg.norm(ex, axis=1)).max() <= RTOL_L2
+    ref, _ = oracle.freq_time(nf1, nf2, df, sigma, sp, nsamp, dt)
+    ref = ref.astype(np.float64)
+    assert (np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)).max() <= 1e-5

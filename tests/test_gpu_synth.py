@@ -64,3 +64,48 @@ def test_synthetics_velocity_and_shift(fkdata):
     num, den = _rel(got, ref, w.nsamp)
     assert np.all(den > 0)
     assert np.max(num / den) <= 1e-7
+
+
+# The mixed-precision form (fast backend) computes the degree sums on the
+# tensor cores from FP16 hi/lo operands with FP32 accumulation; its seismograms
+# must agree with the FP64 form to 1e-5 relative L2 per trace.
+RTOL_MIXED = 1e-5
+
+
+def test_mixed_precision_synthetics_against_fp64(fkdata):
+    import oracle
+    from gemini_unified_b200.fk import FrequencyTime, GEM_BACKEND_GPU_FAST, GeminiFK, synth_params
+    w, m, ex, g, fk, gr, gi = fkdata
+    theta, phi, propdir = w.stations()
+    mt = configs.unit_moment_tensors()
+    sp = synth_params(g, 10, w.nsamp, w.dt, w.filspecs)
+    fast = GeminiFK(m, ex, backend=GEM_BACKEND_GPU_FAST)
+    got = fast.synthetics(sp, g.nwn, gr, gi, theta, phi, propdir, mt)
+    ref = oracle.synthetics(g.nf1, g.nf2, g.nwn, g.nwnmax, sp.df, sp.sigma, gr, gi, theta, phi, propdir, mt,
+                            w.filspecs, False, 0.0, w.nsamp, w.dt)
+    assert np.all(np.isfinite(got))
+    num, den = _rel(got, ref, w.nsamp)
+    assert np.max(num / den) <= RTOL_MIXED
+
+
+def test_mixed_precision_synthetics_many_stations(gpu):
+    """Seeded log-normal FK coefficients of the batched configuration's shape
+    (10 spectra x 658,944 wavenumber-frequency samples, l <= 3205) at 600
+    stations: several tiles in every dimension of the tensor-core products."""
+    from gemini_unified_b200.fk import GEM_BACKEND_GPU_FAST, GEM_BACKEND_GPU_FP64, GeminiFK, synth_params
+    from gemini_unified_b200.synth_run import fk_coefficients
+    w = configs.WORKLOADS["batched_fk"]
+    m = w.model()
+    ex = w.nodes(m)
+    g = M.frequency_grid(w.params, m.rearth)
+    gr, gi = fk_coefficients(10, int(g.nkfmax))
+    theta, phi, propdir = w.stations()
+    sel = slice(0, 4000, 7)   # 572 stations over 0.5..179.5 deg
+    theta, phi, propdir = theta[sel], phi[sel], propdir[sel]
+    mt = configs.unit_moment_tensors()[[0, 3, 5]]
+    sp = synth_params(g, 10, w.nsamp, w.dt, w.filspecs)
+    ref = GeminiFK(m, ex, backend=GEM_BACKEND_GPU_FP64).synthetics(sp, g.nwn, gr, gi, theta, phi, propdir, mt)
+    got = GeminiFK(m, ex, backend=GEM_BACKEND_GPU_FAST).synthetics(sp, g.nwn, gr, gi, theta, phi, propdir, mt)
+    assert np.all(np.isfinite(got))
+    num, den = _rel(got, ref, w.nsamp)
+    assert np.max(num / den) <= RTOL_MIXED
