@@ -16,6 +16,12 @@ split over the ranks in the reference's zig-zag order
 (computeGreenFKSpectraForSynthetics.f90:361-387); the time is the maximum over
 ranks.
 
+Traces leg (``traces``): seismograms of the tensor-core degree-sum configuration
+(seeded log-normal FK coefficients of the batched grid's shape, 4000 stations
+x 6 moment tensors x 3 components x 8192 samples), the mixed-precision form
+(sliced-integer tensor-core sums, radix-16 FFT) against the plain FP64 form,
+with the relative error between the two.
+
 ``--impl reference`` times the CPU FP64 restatement of the reference (the
 reference's Fortran/MPI program cannot be built here) with all host threads on
 a bounded random sample of the same items.
@@ -169,7 +175,9 @@ def fk_launches_per_run(backend):
     return 6 + (1 if backend == 2 else 0)
 
 
-SYNTH_LAUNCHES = 5   # Legendre tables, coefficients, degree-sum products, spectra, inverse FFT
+# mixed-precision synthetics: Legendre tables, coefficients, 5 operand-slicing kernels, tensor-core sums,
+# spectra, FFT twiddles, inverse FFT
+SYNTH_LAUNCHES = 11
 
 
 def main():
@@ -286,8 +294,7 @@ def main():
     h2d = items_rank * 8 + 9 * (m.nk + 1) * 8
 
     # ---------------- seismogram traces: FK spectra of one source node -> traces at all stations
-    traces = time_traces(args, w, m, ex, g, nsp, fast, runs, nkf, gre, gim, dev, stream, dist, rank, size,
-                         timed, synth_params, fklib, fk_step)
+    traces = time_traces(args, w, m, g, nsp, dev, stream, dist, rank, size, timed)
 
     # ---------------- roofline of the dominant kernel: the spheroidal phase (FP64 pipe)
     peak = fp64_peak_tflops(local)
@@ -318,6 +325,7 @@ def main():
                          "flops_note": "reference-algorithm FP64 flops (cached system matrices, full Neville) counted per event on the device; traffic scaled from an ncu capture of the 8 highest frequencies"},
             "e2e": {"value": total_items / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": fk_launches_per_run(2) * len(runs) * args.steps,
+            "gpu_launches_traces": SYNTH_LAUNCHES * traces.pop("steps_timed", max(1, min(args.steps, 3))),
             "clocks": clk,
         }
         if size == 1:
@@ -329,34 +337,21 @@ def main():
         dist.destroy_process_group()
 
 
-def time_traces(args, w, m, ex, g, nsp, fk, runs, nkf, gre, gim, dev, stream, dist, rank, size, timed,
-                synth_params, fklib, fk_step):
-    """Seismogram traces (station x moment tensor, 3 components) of the source
-    node nearest 5 km depth from the FK spectra left on the device.  With N
-    ranks the spectra are summed into a full (nsp, nkfmax) slab on every rank
-    and the stations are split over the ranks."""
+def time_traces(args, w, m, g, nsp, dev, stream, dist, rank, size, timed):
+    """Seismogram traces of the tensor-core degree-sum configuration: seeded
+    log-normal FK coefficients of the batched grid's shape (nsp x 658,944,
+    l <= 3205), 4000 stations 0.5..179.5 deg x 6 unit moment tensors, 3
+    components of 8192 samples.  The mixed-precision form (sliced-integer
+    tensor-core sums, radix-16 inverse FFT) against the plain FP64 form.  With
+    N ranks the stations are split over the ranks."""
     import ctypes
     import torch
     from gemini_unified_b200 import configs
-    src = ex.node_index(m.rearth - 5000.0)
-    nkfmax = int(g.nkfmax)
-    full_r = torch.zeros((nsp, nkfmax), dtype=torch.float32, device=dev)
-    full_i = torch.zeros((nsp, nkfmax), dtype=torch.float32, device=dev)
-    koff = np.concatenate([[0], np.cumsum(g.nwn[g.nf1 - 1: g.nf2])])
-
-    def keep(r):
-        n = nkf[r]
-        a = koff[r[0] - g.nf1]
-        vr = gre[: ex.nnod * nsp * n].view(ex.nnod, nsp, n)[src - 1]
-        vi = gim[: ex.nnod * nsp * n].view(ex.nnod, nsp, n)[src - 1]
-        full_r[:, a: a + n].copy_(vr)
-        full_i[:, a: a + n].copy_(vi)
-
-    fk_step(fk, keep)
-    if dist:
-        dist.all_reduce(full_r)
-        dist.all_reduce(full_i)
-    torch.cuda.synchronize()
+    from gemini_unified_b200.fk import FrequencyTime, lib as fklib, synth_params
+    from gemini_unified_b200.synth_run import fk_coefficients, trace_errors
+    gr_h, gi_h = fk_coefficients(nsp, int(g.nkfmax))
+    d_gr = torch.from_numpy(gr_h).to(dev)
+    d_gi = torch.from_numpy(gi_h).to(dev)
     theta, phi, propdir = w.stations()
     sel = slice(rank, None, size)
     theta, phi, propdir = [np.ascontiguousarray(a[sel]) for a in (theta, phi, propdir)]
@@ -364,37 +359,52 @@ def time_traces(args, w, m, ex, g, nsp, fk, runs, nkf, gre, gim, dev, stream, di
     nsta, nmt = len(theta), len(mt)
     sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs)
     nwn = np.ascontiguousarray(g.nwn, np.int32)
-    out = torch.empty((nsta, nmt, 3, w.nsamp), dtype=torch.float32, device=dev)
     L = fklib()
     p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
-
-    def one():
-        rc = L.gem_synth_run_device(fk._h, ctypes.byref(sp), p(nwn), full_r.data_ptr(), full_i.data_ptr(), nsta,
-                                    p(theta), p(phi), p(propdir), nmt, p(mt), out.data_ptr(),
-                                    ctypes.c_void_p(stream.cuda_stream))
-        if rc >= 2:
-            raise RuntimeError(L.gem_last_error(fk._h).decode())
-
-    for _ in range(max(1, args.warmup - 1)):
-        one()
-    t_ms, _ = timed(one, max(1, min(args.steps, 3)))
     ntr = w.ndist * nmt
-    ok = bool(torch.isfinite(out).all().item())
-    # end to end: FK spectra of the node from the host, traces back to the host
-    gr_h = full_r.cpu().numpy(); gi_h = full_i.cpu().numpy()
+
+    def form(backend, steps):
+        ctx = FrequencyTime(device=dev.index, backend=backend)
+        out = torch.empty((nsta, nmt, 3, w.nsamp), dtype=torch.float32, device=dev)
+
+        def one():
+            rc = L.gem_synth_run_device(ctx._h, ctypes.byref(sp), p(nwn), d_gr.data_ptr(), d_gi.data_ptr(), nsta,
+                                        p(theta), p(phi), p(propdir), nmt, p(mt), out.data_ptr(),
+                                        ctypes.c_void_p(stream.cuda_stream))
+            if rc >= 2:
+                raise RuntimeError(L.gem_last_error(ctx._h).decode())
+
+        for _ in range(max(1, args.warmup - 1)):
+            one()
+        t_ms, _ = timed(one, steps)
+        return ctx, out, t_ms
+
+    fast_ctx, out_fast, t_fast = form(2, max(1, min(args.steps, 3)))
+    _, out_plain, t_plain = form(1, 1)
+    err = trace_errors(out_fast, out_plain)
+    # end to end through the host C ABI: FK coefficients from the host, traces back to the host
+    tr_h = np.empty((nsta, nmt, 3, w.nsamp), np.float32)
+    if dist: dist.barrier()
     t0 = time.perf_counter()
-    fk.synthetics(sp, g.nwn, gr_h, gi_h, theta, phi, propdir, mt)
+    rc = L.gem_synth_run(fast_ctx._h, ctypes.byref(sp), p(nwn), p(gr_h), p(gi_h), nsta, p(theta), p(phi),
+                         p(propdir), nmt, p(mt), p(tr_h))
     e2e_s = time.perf_counter() - t0
+    if rc >= 2:
+        raise RuntimeError(L.gem_last_error(fast_ctx._h).decode())
     if dist:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    return {"value": ntr / (t_ms / 1e3), "unit": "traces/s", "ms_per_step": t_ms,
-            "traces_per_step": ntr, "samples": w.nsamp, "components": 3, "stations": w.ndist, "moment_tensors": nmt,
-            "form": "FP64 tiled degree-sum products (CUDA cores) + radix-2 FP64 inverse FFT", "finite": ok,
-            "launches_per_step": SYNTH_LAUNCHES,
+    return {"value": ntr / (t_fast / 1e3), "unit": "traces/s", "ms_per_step": t_fast, "traces_per_step": ntr,
+            "samples": w.nsamp, "components": 3, "stations": w.ndist, "moment_tensors": nmt,
+            "data": "seeded log-normal FK coefficients, log10|c| ~ N(-3, 1) clipped to [-6, 0], uniform phase",
+            "form": "sliced-INT8 degree sums on tcgen05 (exact INT32 accumulation) + real-output radix-16 FP64 inverse FFT",
+            "plain_fp64": {"value": ntr / (t_plain / 1e3), "unit": "traces/s", "ms_per_step": t_plain,
+                           "form": "FP64 tiled degree-sum products (CUDA cores) + reference radix-2 inverse FFT",
+                           "speedup_of_value": t_plain / t_fast},
+            "error_vs_plain_fp64": err,
             "e2e": {"value": ntr / e2e_s, "unit": "traces/s", "h2d_bytes_per_step": int(gr_h.nbytes * 2),
-                    "d2h_bytes_per_step": int(nsta * nmt * 3 * w.nsamp * 4)}}
+                    "d2h_bytes_per_step": int(tr_h.nbytes)}}
 
 
 def fp64_peak_tflops(device):

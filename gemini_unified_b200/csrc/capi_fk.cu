@@ -64,8 +64,12 @@ struct gem_ctx {
   int last_grid = 0;
   gem_stats stats{};
   // device buffers of the other entry points, grown on demand
-  void* d_aux[4] = {nullptr, nullptr, nullptr, nullptr};
-  size_t aux_cap[4] = {0, 0, 0, 0};
+  void* d_aux[8] = {};
+  size_t aux_cap[8] = {};
+  // optional step log (gem_steplog)
+  StepRec* d_steplog = nullptr;
+  unsigned long long steplog_cap = 0;
+  unsigned long long* d_steplog_n = nullptr;
 };
 
 namespace {
@@ -156,7 +160,7 @@ void gem_note_synth_ms(gem_ctx* ctx, float ms) { if (ctx) ctx->stats.synth_ms = 
 int gem_ctx_device(const gem_ctx* ctx) { return ctx->device; }
 int gem_ctx_backend(const gem_ctx* ctx) { return ctx->backend; }
 void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes) {
-  if (slot < 0 || slot >= 4) return nullptr;
+  if (slot < 0 || slot >= 8) return nullptr;
   if (ctx->d_aux[slot] && ctx->aux_cap[slot] >= bytes) return ctx->d_aux[slot];
   cudaFree(ctx->d_aux[slot]);
   ctx->d_aux[slot] = nullptr; ctx->aux_cap[slot] = 0;
@@ -203,6 +207,7 @@ void gem_ctx_destroy(gem_ctx* ctx) {
   cudaFree(ctx->d_order); cudaFree(ctx->d_status); cudaFree(ctx->d_rstart); cudaFree(ctx->d_um);
   cudaFree(ctx->d_dm); cudaFree(ctx->d_dets);
   for (auto* a : ctx->d_aux) cudaFree(a);
+  cudaFree(ctx->d_steplog); cudaFree(ctx->d_steplog_n);
   for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto& e : ctx->ev_ph) if (e) cudaEventDestroy(e);
   delete ctx;
@@ -418,6 +423,8 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   L.rstart = ctx->d_rstart; L.um = (double2*)ctx->d_um; L.dm = (double2*)ctx->d_dm; L.dets = (double2*)ctx->d_dets;
   L.prof = nullptr;
   L.warp_ns = nullptr;
+  L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
+  if (ctx->d_steplog_n) CK(cudaMemsetAsync(ctx->d_steplog_n, 0, sizeof(unsigned long long), st));
   if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
   ctx->last_grid = grid[1];
   CK(cudaEventRecord(ctx->ev[2], st));
@@ -529,6 +536,35 @@ int gem_instrument_read(gem_ctx* ctx, unsigned long long* prof8, unsigned long l
   int nw = ctx->last_grid * (FK_BLOCK / 32);
   if (nwarps) *nwarps = nw;
   if (warp_ns) CK(cudaMemcpy(warp_ns, ctx->d_warp_ns, (size_t)2 * nw * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return GEM_OK;
+}
+
+// Step log (instrumentation, no counterpart in the reference): capacity > 0
+// makes the following runs record every Bulirsch-Stoer step attempt of every
+// lane (StepRec, 32 bytes) up to capacity records; 0 switches it off.
+int gem_steplog(gem_ctx* ctx, long long capacity) {
+  if (!ctx) return GEM_ERROR;
+  CK(cudaSetDevice(ctx->device));
+  cudaFree(ctx->d_steplog); cudaFree(ctx->d_steplog_n);
+  ctx->d_steplog = nullptr; ctx->d_steplog_n = nullptr; ctx->steplog_cap = 0;
+  if (capacity > 0) {
+    CK(cudaMalloc(&ctx->d_steplog, (size_t)capacity * sizeof(StepRec)));
+    CK(cudaMalloc(&ctx->d_steplog_n, sizeof(unsigned long long)));
+    CK(cudaMemset(ctx->d_steplog_n, 0, sizeof(unsigned long long)));
+    ctx->steplog_cap = (unsigned long long)capacity;
+  }
+  return GEM_OK;
+}
+
+// Copies up to cap records of the last run into out (32 bytes each); *n = records
+// the run produced (may exceed the capacity, then only the first were kept).
+int gem_steplog_read(gem_ctx* ctx, void* out, long long cap, long long* n) {
+  if (!ctx || !ctx->d_steplog) return fail(ctx, "step log not enabled");
+  unsigned long long hn = 0;
+  CK(cudaMemcpy(&hn, ctx->d_steplog_n, sizeof hn, cudaMemcpyDeviceToHost));
+  if (n) *n = (long long)hn;
+  unsigned long long m = std::min<unsigned long long>(hn, std::min<unsigned long long>(ctx->steplog_cap, (unsigned long long)cap));
+  if (out && m) CK(cudaMemcpy(out, ctx->d_steplog, m * sizeof(StepRec), cudaMemcpyDeviceToHost));
   return GEM_OK;
 }
 

@@ -50,6 +50,22 @@ struct FKLaunch {
   unsigned long long* stats;   // 6 counters
   unsigned long long* prof;    // optional lockstep counters [8]
   unsigned long long* warp_ns; // optional per-warp (start, end) globaltimer stamps
+  struct StepRec* steplog;     // optional record of every step attempt
+  unsigned long long steplog_cap;
+  unsigned long long* steplog_n;
+};
+
+// One Bulirsch-Stoer step attempt as the step log records it (32 bytes).
+struct StepRec {
+  double x;             // radius at the start of the step
+  double h;             // step tried (signed)
+  int k;                // item (wavenumber-frequency index of the run)
+  float lgy;            // log10 of the mean |y| of the solution, including the renormalisation
+  short nl;             // layer
+  signed char sys;      // system (toroidal, minors, fluid, radial, adjoint)
+  signed char result;   // attempt at which the step converged (3..7); 0: rejected
+  short phase;          // phase kernel (0 toroidal, 1 spheroidal, 2 adjoint)
+  short nstep;          // step number within the sub-interval
 };
 
 struct FKStatic;

@@ -842,6 +842,25 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
       }
     }
     cyc_step += clock64() - c1;
+    if (LL.steplog) {
+      // one warp-aggregated slot reservation per lockstep step
+      const unsigned lm = __ballot_sync(FULL, integ);
+      const int first = __ffs(lm) - 1;
+      unsigned long long base = 0;
+      if (lane == first) base = atomicAdd(LL.steplog_n, (unsigned long long)__popc(lm));
+      base = __shfl_sync(FULL, base, first);
+      const unsigned long long slot = base + __popc(lm & ((1u << lane) - 1u));
+      if (integ && slot < LL.steplog_cap) {
+        double sm = 0.0;
+        for (int v = 0; v < L.nv; ++v) sm += fabs(L.y[v].re) + fabs(L.y[v].im);
+        StepRec rec;
+        rec.x = L.x; rec.h = L.h; rec.k = L.k;
+        rec.lgy = (float)(log10(sm / L.nv + 1e-300) + L.lgnorm);
+        rec.nl = (short)L.e.nl; rec.sys = (signed char)L.sys; rec.result = (signed char)(result > 0 ? result : 0);
+        rec.phase = (short)PH; rec.nstep = (short)(L.nstep < 32767 ? L.nstep : 32767);
+        LL.steplog[slot] = rec;
+      }
+    }
     // step-size control (integrationStep.f90:140-185)
     if (integ) {
       L.nstep++;

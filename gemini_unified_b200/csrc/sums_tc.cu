@@ -95,15 +95,24 @@ __global__ void tab_scale_kernel(int nsta, int lcap, int K, const double* __rest
   if (threadIdx.x == 0) lscale[(long long)kind * Kp + l] = pow2_above(m);
 }
 
-// c[kind][sta] = power of two above max over l of |T[kind][l][sta] / s_l| (one thread per station)
-__global__ void tab_colscale_kernel(int nsta, int lcap, int K, int Kp, const double* __restrict__ tab,
-                                    const double* __restrict__ lscale, double* cscale) {
-  const int sta = blockIdx.x * blockDim.x + threadIdx.x, kind = blockIdx.y;
+// per (kind, station) max over l of |T[kind][l][sta] / s_l|, as the bits of a
+// non-negative double (whose order is the unsigned integer order): blocks of
+// 128 stations x 64 degrees
+__global__ void tab_colmax_kernel(int nsta, int lcap, int K, int Kp, const double* __restrict__ tab,
+                                  const double* __restrict__ lscale, unsigned long long* colmax) {
+  const int sta = blockIdx.x * blockDim.x + threadIdx.x, kind = blockIdx.z;
   if (sta >= nsta) return;
+  const int l0 = blockIdx.y * 64, l1 = min(l0 + 64, K);
   double m = 0.0;
-  for (int l = 0; l < K; ++l)
+  for (int l = l0; l < l1; ++l)
     m = fmax(m, fabs(tab[((long long)kind * lcap + l) * nsta + sta] / lscale[(long long)kind * Kp + l]));
-  cscale[(long long)kind * nsta + sta] = pow2_above(m);
+  atomicMax(colmax + (long long)kind * nsta + sta, (unsigned long long)__double_as_longlong(m));
+}
+
+// c[kind][sta] = power of two above that maximum
+__global__ void tab_colscale_kernel(int n, const unsigned long long* __restrict__ colmax, double* cscale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) cscale[i] = pow2_above(__longlong_as_double((long long)colmax[i]));
 }
 
 // T8[j][kind*nsta + sta][l] = slice j of T / (s_l c_sta), through a 64 x 64 shared-memory transpose
@@ -417,14 +426,14 @@ bool make_map(CUtensorMap* map, const signed char* base, long long rows, long lo
 
 struct TcLayout {
   int Kp;
-  size_t off[9], total;
+  size_t off[10], total;
 };
 
 TcLayout tc_layout(const SynthDev& S, long long mtot) {
   TcLayout L{};
   const int K = S.lmax + 1;
   L.Kp = (K + TC_BK - 1) / TC_BK * TC_BK;
-  const size_t sz[9] = {(size_t)TC_S * 8 * S.nsta * L.Kp,            // T8
+  const size_t sz[10] = {(size_t)TC_S * 8 * S.nsta * L.Kp,            // T8
                         (size_t)TC_S * mtot * L.Kp,                   // A8
                         (size_t)8 * L.Kp * sizeof(double),            // lscale
                         (size_t)8 * S.nsta * sizeof(double),          // cscale
@@ -432,9 +441,10 @@ TcLayout tc_layout(const SynthDev& S, long long mtot) {
                         (size_t)mtot * sizeof(int),                   // row kind
                         (size_t)(mtot / TC_BM + 16) * sizeof(int2),   // tiles
                         (size_t)24 * sizeof(long long),               // per-kind tables
-                        (size_t)16 * sizeof(int)};                    // kind rows + error flag
+                        (size_t)16 * sizeof(int),                     // kind rows + error flag
+                        (size_t)8 * S.nsta * sizeof(unsigned long long)};   // column maxima
   size_t b = 0;
-  for (int i = 0; i < 9; ++i) {
+  for (int i = 0; i < 10; ++i) {
     L.off[i] = b;
     b += (sz[i] + 1023) / 1024 * 1024;
   }
@@ -473,6 +483,7 @@ const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, co
   int2* tiles = (int2*)(base + L.off[6]);
   long long* tabs = (long long*)(base + L.off[7]);
   int* ints = (int*)(base + L.off[8]);   // [0..7] rows per kind, [8] error flag
+  unsigned long long* colmax = (unsigned long long*)(base + L.off[9]);
   int krows[16] = {0};
   long long htabs[24];
   std::vector<int2> htiles;
@@ -495,7 +506,11 @@ const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, co
     return "sums_tc: upload failed";
   // operands
   tab_scale_kernel<<<dim3(Kp, 8), 256, 0, st>>>(S.nsta, S.lcap, K, tab, lscale, Kp);
-  tab_colscale_kernel<<<dim3((S.nsta + 127) / 128, 8), 128, 0, st>>>(S.nsta, S.lcap, K, Kp, tab, lscale, cscale);
+  if (cudaMemsetAsync(colmax, 0, (size_t)8 * S.nsta * sizeof(unsigned long long), st) != cudaSuccess)
+    return "sums_tc: upload failed";
+  tab_colmax_kernel<<<dim3((S.nsta + 127) / 128, (K + 63) / 64, 8), 128, 0, st>>>(S.nsta, S.lcap, K, Kp, tab, lscale,
+                                                                                 colmax);
+  tab_colscale_kernel<<<(8 * S.nsta + 255) / 256, 256, 0, st>>>(8 * S.nsta, colmax, cscale);
   tab_slice_kernel<<<dim3(Kp / 64, (S.nsta + 63) / 64, 8), 256, 0, st>>>(S.nsta, S.lcap, K, Kp, tab, lscale, cscale,
                                                                          T8);
   coef_slice_kernel<<<(unsigned)mtot, 256, 0, st>>>(S, mtot, K, Kp, A, lscale, row_kind, A8, rscale);

@@ -333,12 +333,6 @@ struct SynthBuffers {
   double *theta = nullptr, *phi = nullptr, *propdir = nullptr, *mt = nullptr;
 };
 
-void free_all(SynthBuffers& b) {
-  cudaFree(b.tab); cudaFree(b.A); cudaFree(b.C); cudaFree(b.X); cudaFree(b.evf); cudaFree(b.tw); cudaFree(b.fac);
-  cudaFree(b.twx);
-  cudaFree(b.nwn); cudaFree(b.koff); cudaFree(b.theta); cudaFree(b.phi); cudaFree(b.propdir); cudaFree(b.mt);
-}
-
 int nint_(double x) { return x >= 0 ? (int)std::floor(x + 0.5) : -(int)std::floor(-x + 0.5); }
 
 // complex Butterworth band-pass at f - i sigma/2pi (butterworthFilter.f90:49-96)
@@ -457,16 +451,26 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   // ---- device buffers
   SynthBuffers b;
   const long long ntr = (long long)nsta * nmt * 3;
-  auto alloc = [&](void** q, size_t n) { return cudaMalloc(q, n) == cudaSuccess; };
-  bool ok = alloc((void**)&b.tab, (size_t)8 * S.lcap * nsta * sizeof(double)) &&
-            alloc((void**)&b.A, (size_t)ao * sizeof(double)) && alloc((void**)&b.C, (size_t)co * sizeof(double)) &&
-            alloc((void**)&b.X, (size_t)ntr * S.ldx * sizeof(double2)) &&
-            alloc((void**)&b.evf, evf.size() * sizeof(double2)) && alloc((void**)&b.tw, tw.size() * sizeof(double2)) &&
-            alloc((void**)&b.fac, fac.size() * sizeof(double)) && alloc((void**)&b.nwn, (size_t)p->nf2 * sizeof(int)) &&
-            alloc((void**)&b.koff, (size_t)nf * sizeof(int)) && alloc((void**)&b.theta, nsta * sizeof(double)) &&
-            alloc((void**)&b.phi, nsta * sizeof(double)) && alloc((void**)&b.propdir, nsta * sizeof(double)) &&
-            alloc((void**)&b.mt, (size_t)nmt * 6 * sizeof(double));
-  if (!ok) { free_all(b); return gem_set_error(ctx, "synthetics: device allocation failed"); }
+  // all buffers of one run in one context-owned allocation, grown on demand
+  const bool fast_fft = gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST && ifft_fast_supported(ns);
+  const size_t sizes[14] = {(size_t)8 * S.lcap * nsta * sizeof(double), (size_t)ao * sizeof(double),
+                            (size_t)co * sizeof(double), (size_t)ntr * S.ldx * sizeof(double2),
+                            evf.size() * sizeof(double2), tw.size() * sizeof(double2), fac.size() * sizeof(double),
+                            (size_t)p->nf2 * sizeof(int), (size_t)nf * sizeof(int), nsta * sizeof(double),
+                            nsta * sizeof(double), nsta * sizeof(double), (size_t)nmt * 6 * sizeof(double),
+                            fast_fft ? (size_t)ns * sizeof(double2) : 0};
+  size_t total = 0;
+  for (size_t z : sizes) total += (z + 255) / 256 * 256;
+  char* pool = (char*)gem_ctx_aux(ctx, 4, total);
+  if (!pool) return GEM_ERROR;
+  void* parts[14];
+  for (int i = 0; i < 14; ++i) { parts[i] = sizes[i] ? pool : nullptr; pool += (sizes[i] + 255) / 256 * 256; }
+  b.tab = (double*)parts[0]; b.A = (double*)parts[1]; b.C = (double*)parts[2]; b.X = (double2*)parts[3];
+  b.evf = (double2*)parts[4]; b.tw = (double2*)parts[5]; b.fac = (double*)parts[6]; b.nwn = (int*)parts[7];
+  b.koff = (int*)parts[8]; b.theta = (double*)parts[9]; b.phi = (double*)parts[10]; b.propdir = (double*)parts[11];
+  b.mt = (double*)parts[12]; b.twx = (double2*)parts[13];
+  const bool ok = true;
+  (void)ok;
   cudaMemcpyAsync(b.evf, evf.data(), evf.size() * sizeof(double2), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b.tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b.fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice, st);
@@ -488,11 +492,8 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
     const long long mtot = 2LL * nf * 14;
     const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
     void* ws = gem_ctx_aux(ctx, 3, wsb);
-    if (!ws) { free_all(b); return GEM_ERROR; }
-    if (const char* why = sums_tc_run(S, mtot, b.tab, b.A, b.C, ws, wsb, st)) {
-      free_all(b);
-      return gem_set_error(ctx, why);
-    }
+    if (!ws) return GEM_ERROR;
+    if (const char* why = sums_tc_run(S, mtot, b.tab, b.A, b.C, ws, wsb, st)) return gem_set_error(ctx, why);
   } else {
     int mmax = 2 * nf * 2;
     dim3 g((nsta + GT_N - 1) / GT_N, (mmax + GT_M - 1) / GT_M, 8);
@@ -500,12 +501,7 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   }
   long long nsp_ = (long long)nsta * nf;
   spectra_kernel<<<(unsigned)((nsp_ + 127) / 128), 128, 0, st>>>(S, b.C, b.evf, b.phi, b.propdir, b.mt, b.X);
-  const bool fast_fft = gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST && ifft_fast_supported(ns);
   if (fast_fft) {
-    if (cudaMalloc((void**)&b.twx, (size_t)ns * sizeof(double2)) != cudaSuccess) {
-      free_all(b);
-      return gem_set_error(ctx, "synthetics: device allocation failed");
-    }
     ifft_fast_twiddles_launch(ns, b.twx, st);
     ifft_fast_launch(S, ntr, b.X, b.twx, b.fac, d_traces, st);
   } else {
@@ -520,7 +516,6 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   cudaEventElapsedTime(&ms, e0, e1);
   gem_note_synth_ms(ctx, ms);
   cudaEventDestroy(e0); cudaEventDestroy(e1);
-  free_all(b);
   if (e != cudaSuccess) return gem_set_error(ctx, cudaGetErrorString(e));
   return GEM_OK;
 }
@@ -531,12 +526,11 @@ extern "C" int gem_synth_run(gem_ctx* ctx, const gem_synth_params* p, const int*
   if (!ctx || !p || !gr || !gi || !traces) return GEM_ERROR;
   size_t nin = (size_t)p->nkfmax * p->nsp;
   size_t nout = (size_t)nsta * nmt * 3 * p->nsamp;
-  float *dgr = nullptr, *dgi = nullptr, *dtr = nullptr;
-  if (cudaMalloc(&dgr, nin * sizeof(float)) != cudaSuccess || cudaMalloc(&dgi, nin * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&dtr, nout * sizeof(float)) != cudaSuccess) {
-    cudaFree(dgr); cudaFree(dgi); cudaFree(dtr);
-    return gem_set_error(ctx, "synthetics: device allocation failed");
-  }
+  if (cudaSetDevice(gem_ctx_device(ctx)) != cudaSuccess) return gem_set_error(ctx, "synthetics: cudaSetDevice failed");
+  float* dgr = (float*)gem_ctx_aux(ctx, 5, nin * sizeof(float));
+  float* dgi = dgr ? (float*)gem_ctx_aux(ctx, 6, nin * sizeof(float)) : nullptr;
+  float* dtr = dgi ? (float*)gem_ctx_aux(ctx, 7, nout * sizeof(float)) : nullptr;
+  if (!dtr) return GEM_ERROR;
   int rc = GEM_OK;
   if (cudaMemcpy(dgr, gr, nin * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(dgi, gi, nin * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -545,7 +539,6 @@ extern "C" int gem_synth_run(gem_ctx* ctx, const gem_synth_params* p, const int*
   if (rc == GEM_OK) rc = gem_synth_run_device(ctx, p, nwn, dgr, dgi, nsta, theta, phi, propdir, nmt, mt, dtr, nullptr);
   if (rc == GEM_OK && cudaMemcpy(traces, dtr, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
     rc = gem_set_error(ctx, "synthetics: copy of the traces failed");
-  cudaFree(dgr); cudaFree(dgi); cudaFree(dtr);
   return rc;
 }
 

@@ -192,6 +192,15 @@ int gem_stats_get(const gem_ctx* ctx, gem_stats* out);
 int gem_instrument(gem_ctx* ctx, int enable);
 int gem_instrument_read(gem_ctx* ctx, unsigned long long* prof8, unsigned long long* warp_ns, int* nwarps);
 
+/* Step log (instrumentation, no counterpart in the reference): capacity > 0
+ * makes the following FK runs record every Bulirsch-Stoer step attempt (32-byte
+ * records: double x, double h, int32 item, float log10|y|, int16 layer, int8
+ * system, int8 converged attempt or 0 when rejected, int16 phase, int16 step
+ * number) up to capacity records; 0 switches it off.  gem_steplog_read copies
+ * up to cap records of the last run and returns the number produced in *n. */
+int gem_steplog(gem_ctx* ctx, long long capacity);
+int gem_steplog_read(gem_ctx* ctx, void* out, long long cap, long long* n);
+
 /* Measurement utility (no counterpart in the reference): FP64 FMA throughput
  * of the device in TFLOP/s, the denominator of the solver's FP64 roofline. */
 double gem_probe_fp64_tflops(int device);
