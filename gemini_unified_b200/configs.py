@@ -12,6 +12,10 @@ model (no ocean, SI units) made isotropic (PV -> P, SV -> S, eta = 1).
 * ``batched_fk``    -- 410 frequencies to 0.2 Hz (df = 1/2048), slowness
   4.0e-4 s/m (l <= ~3205, ~658k solves), 20 source depths 5..700 km plus the
   surface receiver.
+* ``body_waves``    -- global body waves to 0.5 Hz (df = 1/2048, 1024
+  frequencies), slowness 4.0e-4 s/m (l <= ~8006, ~4.1M solves), source at
+  10 km depth, receiver at the surface: the evaluation workload of the learned
+  step/order proposer.
 """
 from __future__ import annotations
 
@@ -86,4 +90,10 @@ BATCHED_FK = Workload(
     nnod_blocks=[1, 19], dr_blocks=[5000.0, 695000.0 / 19.0], shift=0.0, rec_radius=6371000.0,
     ndist=4000, dist_deg=(0.5, 179.5), nsamp=8192, dt=0.25)
 
-WORKLOADS = {w.name: w for w in (GLOBAL_SMALL, BATCHED_FK)}
+BODY_WAVES = Workload(
+    name="body_waves",
+    params=FKParams(tlen=2048.0, fmax=0.5, p1lim=4.0e-4, p2lim=4.0e-4, frac=0.0, eps=1.0e-5),
+    nnod_blocks=[1], dr_blocks=[10000.0], shift=0.0, rec_radius=6371000.0,
+    ndist=50, nsamp=4096, dt=0.25)
+
+WORKLOADS = {w.name: w for w in (GLOBAL_SMALL, BATCHED_FK, BODY_WAVES)}

@@ -17,6 +17,7 @@
 #include "../../include/gemini_fk.h"
 #include "fk_kernel.h"
 #include "fk_types.cuh"
+#include "proposer.h"
 #include "synth.h"
 
 using namespace gem;
@@ -66,6 +67,17 @@ struct gem_ctx {
   // device buffers of the other entry points, grown on demand
   void* d_aux[8] = {};
   size_t aux_cap[8] = {};
+  int kopt = 6;   // order target of the step-size control (gem_order_target; fast backend)
+  // learned proposer (fast backend): FP16 weights, feature normalisation, proposals per (phase, item)
+  __half* d_propw = nullptr;
+  float* d_propnorm = nullptr;
+  int prop_use = 0;
+  float prop_margin = 0.1f;
+  signed char* d_prop_kopt = nullptr; size_t prop_kopt_cap = 0;
+  float* d_prop_hs = nullptr; size_t prop_hs_cap = 0;
+  float* d_feat = nullptr; size_t feat_cap = 0;
+  bool dump_feat = false;
+  long long feat_n = 0;
   // optional step log (gem_steplog)
   StepRec* d_steplog = nullptr;
   unsigned long long steplog_cap = 0;
@@ -208,6 +220,8 @@ void gem_ctx_destroy(gem_ctx* ctx) {
   cudaFree(ctx->d_dm); cudaFree(ctx->d_dets);
   for (auto* a : ctx->d_aux) cudaFree(a);
   cudaFree(ctx->d_steplog); cudaFree(ctx->d_steplog_n);
+  cudaFree(ctx->d_propw); cudaFree(ctx->d_propnorm); cudaFree(ctx->d_prop_kopt); cudaFree(ctx->d_prop_hs);
+  cudaFree(ctx->d_feat);
   for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto& e : ctx->ev_ph) if (e) cudaEventDestroy(e);
   delete ctx;
@@ -332,6 +346,7 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   P.rearth = ctx->rearth; P.ric = ctx->ric; P.roc = ctx->roc; P.rhs = ctx->rb[1];
   P.ruc = P.hasocean ? ctx->rb[ctx->nlay - 1] : ctx->rearth;
   P.eps = p->eps; P.sigma = g.sigma; P.df = g.df; P.dwn = g.dwn;
+  P.kopt = ctx->backend == GEM_BACKEND_GPU_FAST ? ctx->kopt : 6;
   for (int i = 1; i <= ctx->nlay; ++i) {
     P.rb[i] = ctx->rb[i]; P.drk[i] = ctx->drk[i]; P.iflso[i] = ctx->iflso[i]; P.iktop[i] = ctx->iktop[i];
   }
@@ -424,6 +439,7 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   L.prof = nullptr;
   L.warp_ns = nullptr;
   L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
+  L.prop_kopt = nullptr; L.prop_hs = nullptr;
   if (ctx->d_steplog_n) CK(cudaMemsetAsync(ctx->d_steplog_n, 0, sizeof(unsigned long long), st));
   if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
   ctx->last_grid = grid[1];
@@ -432,6 +448,33 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
     return fast ? gem_fast::launch_fk_phase(ph, P, LX, g, st) : gem_plain::launch_fk_phase(ph, P, LX, g, st);
   };
   CK(launch(-1, L, ctx->nsm * 8));
+  // learned proposer: features / proposals per (phase, item) from the start radii
+  const bool propose = fast && ctx->prop_use != 0 && ctx->d_propw;
+  if (ctx->dump_feat || propose) {
+    PropArgs A{};
+    A.items = ctx->d_items; A.jf = ctx->d_slots; A.rstart = ctx->d_rstart; A.nkf = nkf; A.nitems = nitems;
+    A.nk = ctx->nk; A.nlay = ctx->nlay; A.use = ctx->prop_use; A.margin = ctx->prop_margin;
+    A.df = P.df; A.rearth = ctx->rearth;
+    for (int i = 0; i <= ctx->nk; ++i) {
+      A.rk[i] = ctx->rk[i];
+      A.knot_feat[3 * i + 0] = (float)(ctx->vpv[i] / 1e4);
+      A.knot_feat[3 * i + 1] = (float)(ctx->vsv[i] / 1e4);
+      A.knot_feat[3 * i + 2] = (float)(ctx->ro[i] / 1e4);
+    }
+    for (int i = 0; i <= ctx->nlay; ++i) A.rb[i] = ctx->rb[i];
+    if (ctx->dump_feat) {
+      if (grow(ctx, ctx->d_feat, ctx->feat_cap, (size_t)3 * nitems * PROP_NF)) return GEM_ERROR;
+      CK(prop_features_launch(A, ctx->d_feat, st));
+      ctx->feat_n = 3LL * nitems * PROP_NF;
+    }
+    if (propose) {
+      if (grow(ctx, ctx->d_prop_kopt, ctx->prop_kopt_cap, (size_t)3 * nkf)) return GEM_ERROR;
+      if (grow(ctx, ctx->d_prop_hs, ctx->prop_hs_cap, (size_t)3 * nkf)) return GEM_ERROR;
+      CK(prop_infer_launch(A, ctx->d_propw, ctx->d_propnorm, ctx->d_prop_kopt, ctx->d_prop_hs, st));
+      L.prop_kopt = ctx->d_prop_kopt;
+      L.prop_hs = ctx->d_prop_hs;
+    }
+  }
   for (int ph = 0; ph < 3; ++ph) {
     FKLaunch Lp = L;
     if (ctx->d_prof) Lp.prof = ctx->d_prof + 8 * ph;
@@ -565,6 +608,63 @@ int gem_steplog_read(gem_ctx* ctx, void* out, long long cap, long long* n) {
   if (n) *n = (long long)hn;
   unsigned long long m = std::min<unsigned long long>(hn, std::min<unsigned long long>(ctx->steplog_cap, (unsigned long long)cap));
   if (out && m) CK(cudaMemcpy(out, ctx->d_steplog, m * sizeof(StepRec), cudaMemcpyDeviceToHost));
+  return GEM_OK;
+}
+
+// Learned proposer (no counterpart in the reference): w = PROP_NPARAM FP32
+// weights (kept as FP16 on the device), norm = feature mean and deviation
+// (2 * PROP_NF), use = PROP_USE_ORDER | PROP_USE_STEP, margin = least predicted
+// log work saving that moves the order target off 6.  use = 0 or w = NULL
+// switches it off.  Fast backend only.
+int gem_proposer_set(gem_ctx* ctx, const float* w, const float* norm, int use, float margin) {
+  if (!ctx) return GEM_ERROR;
+  CK(cudaSetDevice(ctx->device));
+  ctx->prop_use = 0;
+  if (!w || use == 0) return GEM_OK;
+  if (!norm) return fail(ctx, "proposer: feature normalisation missing");
+  if (use & ~(PROP_USE_ORDER | PROP_USE_STEP)) return fail(ctx, "proposer: unknown use flags %d", use);
+  if (!(margin >= 0.f)) return fail(ctx, "proposer: margin must be >= 0");
+  for (int i = 0; i < PROP_NF; ++i)
+    if (!(norm[PROP_NF + i] > 0.f)) return fail(ctx, "proposer: feature deviation must be positive");
+  std::vector<__half> hw(PROP_NPARAM);
+  for (int i = 0; i < PROP_NPARAM; ++i) {
+    if (!std::isfinite(w[i])) return fail(ctx, "proposer: non-finite weight %d", i);
+    hw[i] = __float2half_rn(w[i]);
+  }
+  if (!ctx->d_propw) CK(cudaMalloc(&ctx->d_propw, PROP_NPARAM * sizeof(__half)));
+  if (!ctx->d_propnorm) CK(cudaMalloc(&ctx->d_propnorm, PROP_NNORM * sizeof(float)));
+  CK(cudaMemcpy(ctx->d_propw, hw.data(), PROP_NPARAM * sizeof(__half), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_propnorm, norm, PROP_NNORM * sizeof(float), cudaMemcpyHostToDevice));
+  ctx->prop_use = use;
+  ctx->prop_margin = margin;
+  return GEM_OK;
+}
+
+// Training data of the proposer: enable = 1 makes the following runs keep the
+// raw features of every (phase, item), [3][nitems][PROP_NF].
+int gem_proposer_dump(gem_ctx* ctx, int enable) {
+  if (!ctx) return GEM_ERROR;
+  ctx->dump_feat = enable != 0;
+  ctx->feat_n = 0;
+  return GEM_OK;
+}
+
+int gem_proposer_dump_read(gem_ctx* ctx, float* out, long long cap, long long* n) {
+  if (!ctx || !ctx->d_feat) return fail(ctx, "proposer feature dump not enabled");
+  if (n) *n = ctx->feat_n;
+  const long long m = std::min(cap, ctx->feat_n);
+  if (out && m > 0) CK(cudaMemcpy(out, ctx->d_feat, (size_t)m * sizeof(float), cudaMemcpyDeviceToHost));
+  return GEM_OK;
+}
+
+// Order target of the step-size control (fast backend; no counterpart in the
+// reference, which fixes it at 6, parametersBulirschStep.f90:28-48): k in 3..7;
+// 0 restores 6.
+int gem_order_target(gem_ctx* ctx, int k) {
+  if (!ctx) return GEM_ERROR;
+  if (k == 0) k = 6;
+  if (k < 3 || k > 7) return fail(ctx, "order target must be 3..7");
+  ctx->kopt = k;
   return GEM_OK;
 }
 

@@ -50,6 +50,8 @@ struct FKLaunch {
   unsigned long long* stats;   // 6 counters
   unsigned long long* prof;    // optional lockstep counters [8]
   unsigned long long* warp_ns; // optional per-warp (start, end) globaltimer stamps
+  const signed char* prop_kopt;   // optional proposed order target per (phase, k): [3][nkf]
+  const float* prop_hs;           // optional proposed multiplier of the initial step per (phase, k): [3][nkf]
   struct StepRec* steplog;     // optional record of every step attempt
   unsigned long long steplog_cap;
   unsigned long long* steplog_n;

@@ -70,6 +70,8 @@ struct Lane {
   int sys, nv, sink, after, do_norm;
   int jl, jr, dl, dr, nnodp, ndp, jnod, jd, kmin, nstep;
   double x1, x2, xa, xe, x, h, hdid, lgnorm, s0, s1, idir;
+  int kopt;   // target attempt of the step-size control
+  double hs;  // multiplier of the initial steps given by the initial-value formulas
   dz y[5];
 };
 
@@ -440,6 +442,8 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
         set_env(P, LL, w.x, w.y, L.e);
         L.iwn = w.y;
         L.status = ST_OK;
+        L.kopt = LL.prop_kopt ? (int)LL.prop_kopt[(long long)PH * LL.nkf + L.k] : P.kopt;
+        L.hs = LL.prop_hs ? (double)LL.prop_hs[(long long)PH * LL.nkf + L.k] : 1.0;
         L.det = dz{0, 0};
         if (LL.status && LL.status[L.k] != ST_OK) { L.st = S_FETCH; break; }   // failed in an earlier phase
         if (P.global_ == 0 && L.iwn == 1) { L.st = S_FETCH; break; }           // wn = 0 stays zero
@@ -457,7 +461,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
           if (rsurf < rmin) { L.st = S_ITEM_END; break; }
           L.e.nl = nl;
           L.rend = rsurf;
-          prop_begin<PH>(P, LL, s, lay, L, SYS_TOROIDAL, rsurf, rmin, htry, ys, false, 0.0, K_DT, S_TOR_UP);
+          prop_begin<PH>(P, LL, s, lay, L, SYS_TOROIDAL, rsurf, rmin, htry * L.hs, ys, false, 0.0, K_DT, S_TOR_UP);
         } else if (PH == PH_SPH) {   // spheroidalMinors.f90:155-182
           for (int el = 0; el < lay.NN; ++el) s.put(lay.lg(el), dz{0.0, 0.0});
           if (L.rstart_s >= P.rnod[jre]) { L.st = S_ITEM_END; break; }
@@ -487,7 +491,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
           double re_ic = fmax(L.rstart_s, P.rnod[1]);
           if (re_ic < P.ric) {   // inner-core propagator P_4m (:227-238)
             dz ys[5] = {{0, 0}, {0, 0}, {0, 0}, {1.0, 0}, {0, 0}};
-            double htry = adjoint_htry(P, L.e, P.ric, re_ic);
+            double htry = adjoint_htry(P, L.e, P.ric, re_ic) * L.hs;
             prop_begin<PH>(P, LL, s, lay, L, SYS_SOLIDT, P.ric, re_ic, htry, ys, false, 0.0, K_ADJIC, S_ADJ_PLAN);
             L.up = 1;
           } else {
@@ -509,7 +513,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
         dz ys[5]; double htry;
         int rc = toroidal_bottom_iv(P, L.e, L.rstart_t, ys, htry);
         if (rc) { FAIL(rc); break; }
-        prop_begin<PH>(P, LL, s, lay, L, SYS_TOROIDAL, L.rstart_t, rmax, htry, ys, false, 0.0, K_UT, S_TOR_DONE);
+        prop_begin<PH>(P, LL, s, lay, L, SYS_TOROIDAL, L.rstart_t, rmax, htry * L.hs, ys, false, 0.0, K_UT, S_TOR_DONE);
         L.up = 1;
         break;
       }
@@ -581,6 +585,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
         if (L.rbeg == (up ? L.rstart_s : P.rearth)) {
           int rc = up ? minors_bottom_iv(P, L.e, L.rbeg, ys, L.htry_g) : minors_surface_iv(P, L.e, ys, L.htry_g);
           if (rc) { FAIL(rc); break; }
+          L.htry_g *= L.hs;
         } else if (L.liq && !L.liq_old) {
           if (l0) { ys[0] = L.yend[0]; ys[1] = L.yend[1]; } else { ys[0] = L.yend[2]; ys[1] = L.yend[4]; }
         } else if (!L.liq && L.liq_old) {
@@ -643,7 +648,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
         ys[4] = dz{0, 0};
         const double ra = P.rnod[jre];
         const double xe = upd ? (L.ocean_above ? P.ruc : P.rnod[L.highest]) : (L.core_below ? L.re_dn : P.rnod[L.lowest]);
-        double htry = adjoint_htry(P, L.e, ra, upd ? P.ruc : L.re_dn);
+        double htry = adjoint_htry(P, L.e, ra, upd ? P.ruc : L.re_dn) * L.hs;
         prop_begin<PH>(P, LL, s, lay, L, SYS_SOLIDT, ra, xe, htry, ys, false, 0.0, upd ? K_ADJ_UP : K_ADJ_DN, S_ADJ_END);
         break;
       }
@@ -871,8 +876,8 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
         if (fabs(L.x - L.xe) < MINSIZE_IS) {
           L.st = S_SUB_END;
         } else {
-          if (result > 6) L.h = L.h * SHRINK_BS;
-          else if (result < 6) L.h = L.h * GROW_BS;
+          if (result > L.kopt) L.h = L.h * SHRINK_BS;
+          else if (result < L.kopt) L.h = L.h * GROW_BS;
           L.hdid = L.h;
         }
       } else {

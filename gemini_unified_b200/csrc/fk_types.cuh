@@ -12,6 +12,7 @@ struct FKStatic {
   int hascore, hasocean, istyp, stressflag, global_, nsp;
   int ncsph, nctor, njsph, njtor, dsvstep;
   double rearth, ric, roc, rhs, ruc, eps, sigma, df, dwn;
+  int kopt;   // attempt the step-size control aims at (opttry, parametersBulirschStep.f90:28-48: 6)
   double rb[MAXLAY + 1];
   double drk[MAXLAY + 1];
   int iflso[MAXLAY + 1];

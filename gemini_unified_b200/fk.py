@@ -65,10 +65,19 @@ def lib() -> ctypes.CDLL:
                                    vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, vp]
         L.gem_ifft_run_device.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_int, vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, vp, vp]
+        L.gem_steplog.argtypes = [vp, ctypes.c_longlong]
+        L.gem_steplog_read.argtypes = [vp, vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+        L.gem_order_target.argtypes = [vp, ctypes.c_int]
         L.gem_instrument.argtypes = [vp, ctypes.c_int]
         L.gem_instrument_read.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_int)]
         _lib = L
     return _lib
+
+
+# one Bulirsch-Stoer step attempt of the step log (StepRec, 32 bytes)
+STEP_DTYPE = np.dtype([("x", "<f8"), ("h", "<f8"), ("k", "<i4"), ("lgy", "<f4"), ("nl", "<i2"), ("sys", "i1"),
+                       ("result", "i1"), ("phase", "<i2"), ("nstep", "<i2")])
+assert STEP_DTYPE.itemsize == 32
 
 
 class SynthParams(ctypes.Structure):
@@ -221,6 +230,20 @@ class GeminiFK:
         self._check(lib().gem_synth_run(self._h, ctypes.byref(sp), _ptr(nwn), _ptr(gr), _ptr(gi), len(th), _ptr(th),
                                         _ptr(ph), _ptr(pd), len(mt), _ptr(mt), _ptr(out)))
         return out
+
+    def order_target(self, k: int):
+        """Attempt the step-size control aims at (fast backend; 3..7, 0 restores the reference's 6)."""
+        self._check(lib().gem_order_target(self._h, int(k)))
+
+    def steplog(self, capacity: int):
+        """Record every step attempt of the following runs (capacity records; 0 = off)."""
+        self._check(lib().gem_steplog(self._h, int(capacity)))
+
+    def steplog_read(self, capacity: int) -> np.ndarray:
+        out = np.zeros(capacity, STEP_DTYPE)
+        n = ctypes.c_longlong()
+        self._check(lib().gem_steplog_read(self._h, _ptr(out), capacity, ctypes.byref(n)))
+        return out[: min(n.value, capacity)]
 
     def instrument(self, enable: bool = True):
         self._check(lib().gem_instrument(self._h, 1 if enable else 0))

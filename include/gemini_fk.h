@@ -201,6 +201,40 @@ int gem_instrument_read(gem_ctx* ctx, unsigned long long* prof8, unsigned long l
 int gem_steplog(gem_ctx* ctx, long long capacity);
 int gem_steplog_read(gem_ctx* ctx, void* out, long long cap, long long* n);
 
+/* Order target of the step-size control (fast backend; no counterpart in the
+ * reference, which fixes it at 6, parametersBulirschStep.f90:28-48): the step
+ * grows when a step converges before attempt k and shrinks when after; k in
+ * 3..7, 0 restores 6.  Acceptance and rejection are unchanged. */
+int gem_order_target(gem_ctx* ctx, int k);
+
+/* Learned step/order proposer (no counterpart in the reference).  A 3-layer
+ * MLP of width 64 maps 11 features of each (item, phase) to the predicted work
+ * with the step-size control aiming at attempt 5 and 7 (relative to 6) and to
+ * a factor for the initial steps of the initial-value formulas; the fast
+ * backend sets each lane's order target (use & GEM_PROP_USE_ORDER; 5 or 7
+ * only when the predicted log saving exceeds margin) and initial steps (use &
+ * GEM_PROP_USE_STEP) from it.  The error control still accepts or rejects
+ * every step.  w: GEM_PROP_NPARAM FP32 weights (W1 [64][11], b1, W2 [64][64],
+ * b2, W3 [3][64], b3), used as FP16; norm: feature mean [11] then deviation
+ * [11].  use = 0 or w = NULL switches it off. */
+#define GEM_PROP_NF 11
+#define GEM_PROP_NPARAM 5123
+#define GEM_PROP_USE_ORDER 1
+#define GEM_PROP_USE_STEP 2
+int gem_proposer_set(gem_ctx* ctx, const float* w, const float* norm, int use, float margin);
+/* Training data: enable = 1 makes the following runs keep the raw features of
+ * every (phase, item), [3][nitems][11]; read them with gem_proposer_dump_read. */
+int gem_proposer_dump(gem_ctx* ctx, int enable);
+int gem_proposer_dump_read(gem_ctx* ctx, float* out, long long cap, long long* n);
+/* Training kernels of the proposer: gradient of the masked mean-squared error
+ * on n standardised samples (x [n][11], y and mask [n][3], host buffers), and
+ * Adam training in place of the FP32 weights (epochs over n samples in batches,
+ * order from seed; loss_hist[epochs] may be NULL).  They allocate their own
+ * device buffers on the current device. */
+int gem_prop_grad(const float* w, const float* x, const float* y, const float* mask, int n, float* grad, float* loss);
+int gem_prop_train(float* w, const float* x, const float* y, const float* mask, int n, int epochs, int batch,
+                   float lr, unsigned seed, float* loss_hist);
+
 /* Measurement utility (no counterpart in the reference): FP64 FMA throughput
  * of the device in TFLOP/s, the denominator of the solver's FP64 roofline. */
 double gem_probe_fp64_tflops(int device);

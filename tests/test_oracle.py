@@ -158,3 +158,19 @@ def test_fk_fault_injection_min_step(small):
     pc = M.fk_params_c(dataclasses.replace(w.params, eps=1e-30), jre)
     g, st, _ = o.fk_frequency(pc, 3, 23, 10, 3, 5)
     assert np.all(st[2:5] == 1)
+
+
+def test_proposer_mlp_gradient_against_finite_differences():
+    """The FP64 restatement of the proposer network: its reverse-mode gradient
+    agrees with central differences of its loss."""
+    import proposer_mlp
+    rng = np.random.default_rng(11)
+    w = rng.normal(0, 0.3, proposer_mlp.NPARAM)
+    x = rng.normal(0, 1, (40, proposer_mlp.NF))
+    y = rng.normal(0, 1, (40, proposer_mlp.NO))
+    mask = (rng.random((40, proposer_mlp.NO)) > 0.3).astype(float)
+    _, g = proposer_mlp.loss_and_grad(w, x, y, mask)
+    for i in rng.choice(proposer_mlp.NPARAM, 25, replace=False):
+        e = np.zeros_like(w); e[i] = 1e-6
+        fd = (proposer_mlp.loss_and_grad(w + e, x, y, mask)[0] - proposer_mlp.loss_and_grad(w - e, x, y, mask)[0]) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(g[i])
