@@ -101,11 +101,15 @@ struct ItemStore {
 //  (complexBulirschStep.f90:111-170,180-238,297-340)
 // ------------------------------------------------------------------------
 template <int SYS, int NVD>
-__device__ __noinline__ void bs_step(const FKStatic& P, const Env& e, bool active, double h, double x,
-                                     const dz* y0, dz* yext, int& result, double2* D, int lane, Counters& cnt) {
+__device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool active, double h, double x,
+                                     const dz* y0, dz* yext, int& result, double2* D, int lane, Counters& cnt_out) {
   constexpr int NV = SysNV<SYS>::NV;
+  // the lane state lives in local memory: work on register copies of the
+  // environment and the counters for the whole step
+  const Env e = e_in;
+  Counters cnt{};
   bool need = active;
-  result = 0;   // 0: failed; > 0: number of attempts of a successful step
+  int res = 0;   // 0: failed; > 0: number of attempts of a successful step
   dz ys[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) ys[v] = y0[v];
@@ -174,13 +178,20 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e, bool activ
       if (conv) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) yext[v] = yy[v];
-        result = j;
+        res = j;
         need = false;
       } else if (j == 7) {
         need = false;
       }
     }
   }
+  result = res;
+  cnt_out.lane_attempts += cnt.lane_attempts;
+  cnt_out.warp_attempts += cnt.warp_attempts;
+  cnt_out.attempts += cnt.attempts;
+  cnt_out.matvecs += cnt.matvecs;
+  cnt_out.sysmats += cnt.sysmats;
+  cnt_out.flops += cnt.flops;
 }
 
 // ------------------------------------------------------------------------
