@@ -124,6 +124,152 @@ __global__ void coef_kernel(SynthDev S, const float* __restrict__ gr, const floa
   Ai[l] = vi;
 }
 
+
+// ---------------------------------------------------------------------------
+//  Regional mode: wavenumber integrals (wavenumberIntegrals.f90:320-491)
+//
+//  Integral k of frequency f at distance x is a sum over the wavenumbers j of
+//  G_f(j) taper_f(j) kern_k(wn_j, J(wn_j x)) w(j, x) with the weights of the
+//  reference's rule: dk for 2 <= j < j3 (trapezoid, kx < 3), dk/2 + F at j3 and
+//  2F beyond (Filon, F = (1 - cos x dk)/(x dk x)), times R^2/(2 pi).  The
+//  products run as the degree sums do: T[kind][j][sta] holds kern x weight x
+//  R^2/(2 pi) for the 8 kernel kinds, the coefficient rows hold G taper sign.
+//  What depends on both f and x -- the end of the frequency's wavenumber range
+//  and the Neumann (Y) end terms -- is added afterwards per (f, x).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double wn_kernel(int kind, double wn, double b0, double b1, double b2, double re,
+                                            double x) {
+  switch (kind) {
+    case 0: return wn * b0;                                         // integrals 1, 2
+    case 1: return 2.0 / re * b1;                                   // 3
+    case 2: return wn * 2.0 * b2;                                   // 4
+    case 3: return wn * (-wn * re) * b1;                            // 5, 6
+    case 4: return wn * 2.0 * (b0 - b1 / (wn * x));                 // 7, 11
+    case 5: return wn * 2.0 * wn * re * (b1 - 2.0 * b2 / (wn * x)); // 8, -12
+    case 6: return wn * 2.0 * b1 / (wn * x);                        // 9, 13
+    default: return wn * 4.0 * wn * re * b2 / (wn * x);             // 10, -14
+  }
+}
+__constant__ double c_wn_sign[14] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, -1, 1, -1};
+
+struct WnGeom {   // the rule's geometry at distance xx (wavenumberIntegrals.f90:337-348)
+  double x, xdk, F;
+  int j3;
+};
+__device__ __forceinline__ WnGeom wn_geom(double xx, double dwn) {
+  WnGeom g;
+  g.x = xx < 3.0 / (dwn * 1.e9) ? 3.0 / (dwn * 1.e9) : xx;
+  g.j3 = (int)(3.0 / g.x / dwn) + 2;
+  g.xdk = g.x * dwn;
+  g.F = (1.0 - cos(g.xdk)) / g.xdk / g.x;
+  return g;
+}
+__device__ __forceinline__ double wn_kernel_at(int kind, double wn, double x, double re, bool neumann) {
+  const double a = wn * x;
+  const double b0 = neumann ? y0(a) : j0(a), b1 = neumann ? y1(a) : j1(a);
+  const double b2 = -b0 + 2.0 / a * b1;
+  return wn_kernel(kind, wn, b0, b1, b2, re, x);
+}
+
+// tab[(kind * lcap + j-1) * nsta + sta], j = 1..lcap (1-based wavenumber index)
+__global__ void bessel_tab_kernel(SynthDev S, const double* __restrict__ theta, double* tab) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)S.lcap * S.nsta) return;
+  const int sta = (int)(idx % S.nsta);
+  const int j = (int)(idx / S.nsta) + 1;
+  const WnGeom g = wn_geom(theta[sta] * S.rearth, S.dwn);
+  double w = 0.0;
+  if (j >= 2 && j < g.j3) w = S.dwn;
+  else if (j >= 2 && j == g.j3) w = 0.5 * S.dwn + g.F;
+  else if (j > g.j3) w = 2.0 * g.F;
+  const double scale = S.rearth * S.rearth / (2.0 * PI_F);
+  const double wn = (double)(j - 1) * S.dwn;
+  double b0 = 0, b1 = 0, b2 = 0;
+  if (w != 0.0) { const double a = wn * g.x; b0 = j0(a); b1 = j1(a); b2 = -b0 + 2.0 / a * b1; }
+  for (int kind = 0; kind < 8; ++kind) {
+    const double v = w != 0.0 ? wn_kernel(kind, wn, b0, b1, b2, S.rearth, g.x) * w * scale : 0.0;
+    tab[((long long)kind * S.lcap + (j - 1)) * S.nsta + sta] = v;
+  }
+}
+
+// cos^2 taper of the wavenumber integrals (wavenumberIntegrals.f90:480-491), 1-based j
+__device__ __forceinline__ double wn_taper(int nwn, double dwn, int j) {
+  const double tapfrac = 0.2;
+  int jt = (int)floor((double)nwn * (1.0 - tapfrac) + 0.5);
+  jt = jt < nwn ? jt : nwn;
+  jt = jt > 1 ? jt : 1;
+  if (j < jt) return 1.0;
+  const double c1 = (double)(nwn - 1) * dwn * tapfrac * 2.0 / PI_F;
+  const double c2 = (1.0 - tapfrac) / tapfrac * 0.5 * PI_F;
+  const double c = cos((double)(j - 1) * dwn / c1 - c2);
+  return c * c;
+}
+
+// coefficient rows of the integrals, the layout of coef_kernel: sign G taper
+__global__ void bessel_coef_kernel(SynthDev S, const float* __restrict__ gr, const float* __restrict__ gi, double* A) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = S.nf2 - S.nf1 + 1;
+  if (idx >= (long long)nf * 14 * S.lcap) return;
+  const int jj = (int)(idx % S.lcap);   // j - 1
+  const int k = (int)((idx / S.lcap) % 14);
+  const int slot = (int)(idx / ((long long)S.lcap * 14));
+  const int nwn = S.nwn[S.nf1 + slot - 1];
+  const int kind = c_sum_kind[k];
+  int s = 0;
+  for (int q = 0; q < k; ++q) s += c_sum_kind[q] == kind;
+  const long long row = 2LL * ((long long)slot * S.nsk[kind] + s);
+  double* Ar = A + (long long)S.aoff[kind] + row * S.lcap;
+  double vr = 0.0, vi = 0.0;
+  if (jj < nwn) {
+    const long long o = (long long)S.col_off[c_sum_col[k]] * S.nkf + S.koff[slot] + jj;
+    const double t = wn_taper(nwn, S.dwn, jj + 1) * c_wn_sign[k];
+    vr = (double)gr[o] * t;
+    vi = (double)gi[o] * t;
+  }
+  Ar[jj] = vr;
+  Ar[S.lcap + jj] = vi;
+}
+
+// end terms per (frequency, integral, station) added to the products C
+__global__ void bessel_corr_kernel(SynthDev S, const float* __restrict__ gr, const float* __restrict__ gi,
+                                   const double* __restrict__ theta, double* C) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = S.nf2 - S.nf1 + 1;
+  if (idx >= (long long)nf * 14 * S.nsta) return;
+  const int sta = (int)(idx % S.nsta);
+  const int k = (int)((idx / S.nsta) % 14);
+  const int slot = (int)(idx / ((long long)S.nsta * 14));
+  const int nwn = S.nwn[S.nf1 + slot - 1];
+  if (nwn < 2) return;
+  const int kind = c_sum_kind[k];
+  const double re = S.rearth, dwn = S.dwn;
+  const WnGeom g = wn_geom(theta[sta] * re, dwn);
+  const long long o = (long long)S.col_off[c_sum_col[k]] * S.nkf + S.koff[slot];
+  const double sg = c_wn_sign[k];
+  auto G = [&](int j) { return dz{(double)gr[o + j - 1], (double)gi[o + j - 1]}; };
+  auto kern = [&](int j) { return sg * wn_kernel_at(kind, (double)(j - 1) * dwn, g.x, re, false); };
+  dz corr{0.0, 0.0};
+  if (nwn > g.j3) {
+    // Filon end at nwn has weight F (the table holds 2F); Neumann terms at both ends
+    const double tn = wn_taper(nwn, dwn, nwn), t3 = wn_taper(nwn, dwn, g.j3);
+    const double wne = (double)(nwn - 1) * dwn, wn3 = (double)(g.j3 - 1) * dwn;
+    const double ybn = sg * wn_kernel_at(kind, wne, g.x, re, true), yb3 = sg * wn_kernel_at(kind, wn3, g.x, re, true);
+    corr = corr - (G(nwn) * kern(nwn)) * (tn * g.F);
+    corr = corr + ((G(nwn) * ybn) * tn - (G(g.j3) * yb3) * t3) / g.x * (1.0 - sin(g.xdk) / g.xdk);
+  } else if (nwn == g.j3) {
+    corr = corr - (G(nwn) * kern(nwn)) * (wn_taper(nwn, dwn, nwn) * g.F);   // no Filon part
+  } else {
+    corr = corr - (G(nwn) * kern(nwn)) * (wn_taper(nwn, dwn, nwn) * 0.5 * dwn);   // trapezoid end
+  }
+  corr = corr * (re * re / (2.0 * PI_F));
+  int s = 0;
+  for (int q = 0; q < k; ++q) s += c_sum_kind[q] == kind;
+  const long long row = 2LL * ((long long)slot * S.nsk[kind] + s);
+  double* Ck = C + S.coff[kind];
+  Ck[row * S.nsta + sta] += corr.re;
+  Ck[(row + 1) * S.nsta + sta] += corr.im;
+}
+
 // ---------------------------------------------------------------------------
 //  FP64 tiled product C[kind][row][sta] = sum_l A[kind][row][l] * T[kind][l][sta]
 //  64x64 output tile per block of 256 threads, 4x4 per thread, K step 16.
@@ -401,7 +547,9 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
                                     void* stream) {
   if (!ctx || !p || !nwn || !theta || !phi || !propdir || !mt) return GEM_ERROR;
   if (p->istyp != 1) return gem_set_error(ctx, "synthetics: only moment-tensor sources are supported");
-  if (p->global_ != 1) return gem_set_error(ctx, "synthetics: only the spherical-harmonics (global) mode is supported");
+  if (p->global_ != 1 && p->global_ != 0) return gem_set_error(ctx, "synthetics: GLOBAL must be 0 or 1");
+  if (p->global_ == 0 && (!(p->dwn > 0) || !(p->rearth > 0)))
+    return gem_set_error(ctx, "synthetics: the regional mode needs the wavenumber spacing and the earth radius");
   if (p->nsp < 10) return gem_set_error(ctx, "synthetics: expected the 10 moment spectra U,V (4 jumps) and W (2 jumps)");
   if (nsta < 1 || nmt < 1 || p->nf1 < 2 || p->nf2 < p->nf1 || p->nwnmax < 3) return gem_set_error(ctx, "synthetics: invalid sizes");
   cudaStream_t st = (cudaStream_t)stream;
@@ -414,6 +562,7 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   SynthDev S{};
   S.nf1 = p->nf1; S.nf2 = p->nf2; S.nsta = nsta; S.nmt = nmt; S.lmax = p->nwnmax - 1; S.lcap = p->nwnmax;
   S.nkf = p->nkfmax; S.df = p->df; S.sigma = p->sigma; S.tred = p->tred; S.velocity = p->velocity;
+  S.dwn = p->dwn; S.rearth = p->rearth;
   S.ns = ns; S.nslog = nslog; S.nsamp = p->nsamp; S.ndec = ndec; S.ldx = p->nf2;
   const int nsk_h[8] = {2, 1, 1, 2, 2, 2, 2, 2};
   const int nf = p->nf2 - p->nf1 + 1;
@@ -484,9 +633,15 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
-  legendre_kernel<<<(nsta * 3 + 127) / 128, 128, 0, st>>>(nsta, S.lmax, S.lcap, b.theta, b.tab);
   long long ncoef = (long long)nf * 14 * S.lcap;
-  coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
+  if (p->global_ == 1) {
+    legendre_kernel<<<(nsta * 3 + 127) / 128, 128, 0, st>>>(nsta, S.lmax, S.lcap, b.theta, b.tab);
+    coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
+  } else {
+    const long long ntab = (long long)S.lcap * nsta;
+    bessel_tab_kernel<<<(unsigned)((ntab + 255) / 256), 256, 0, st>>>(S, b.theta, b.tab);
+    bessel_coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
+  }
   if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST) {
     // split-precision products on the tensor cores (FP16 hi/lo operands, FP32 accumulation)
     const long long mtot = 2LL * nf * 14;
@@ -498,6 +653,10 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
     int mmax = 2 * nf * 2;
     dim3 g((nsta + GT_N - 1) / GT_N, (mmax + GT_M - 1) / GT_M, 8);
     sums_gemm_kernel<<<g, 256, 0, st>>>(S, b.A, b.tab, b.C);
+  }
+  if (p->global_ == 0) {
+    const long long ncorr = (long long)nf * 14 * nsta;
+    bessel_corr_kernel<<<(unsigned)((ncorr + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.theta, b.C);
   }
   long long nsp_ = (long long)nsta * nf;
   spectra_kernel<<<(unsigned)((nsp_ + 127) / 128), 128, 0, st>>>(S, b.C, b.evf, b.phi, b.propdir, b.mt, b.X);

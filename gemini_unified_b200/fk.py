@@ -88,16 +88,20 @@ class SynthParams(ctypes.Structure):
                 ("global_", ctypes.c_int), ("df", ctypes.c_double), ("sigma", ctypes.c_double),
                 ("nsamp", ctypes.c_int), ("dt", ctypes.c_double), ("velocity", ctypes.c_int),
                 ("tred", ctypes.c_double), ("order_highpass", ctypes.c_int), ("fc_highpass", ctypes.c_double),
-                ("order_lowpass", ctypes.c_int), ("fc_lowpass", ctypes.c_double)]
+                ("order_lowpass", ctypes.c_int), ("fc_lowpass", ctypes.c_double), ("dwn", ctypes.c_double),
+                ("rearth", ctypes.c_double)]
 
 
-def synth_params(grid, nsp, nsamp, dt, filspecs, velocity=False, tred=0.0) -> SynthParams:
+def synth_params(grid, nsp, nsamp, dt, filspecs, velocity=False, tred=0.0, global_=1,
+                 rearth=6371000.0) -> SynthParams:
     """Parameters as computeSyntheticSeismograms reads them back from the FK file:
-    df and sigma are stored as float32 (computeGreenFKSpectraForSynthetics.f90:261-263)."""
+    df, sigma, dwn and the earth radius are stored as float32
+    (computeGreenFKSpectraForSynthetics.f90:261-263)."""
     f32 = lambda v: float(np.float32(v))
-    return SynthParams(grid.nf1, grid.nf2, int(grid.nwnmax), int(grid.nkfmax), nsp, 1, 1, f32(grid.df),
+    return SynthParams(grid.nf1, grid.nf2, int(grid.nwnmax), int(grid.nkfmax), nsp, 1, int(global_), f32(grid.df),
                        f32(grid.sigma), int(nsamp), float(dt), 1 if velocity else 0, float(tred),
-                       int(round(filspecs[0])), float(filspecs[1]), int(round(filspecs[2])), float(filspecs[3]))
+                       int(round(filspecs[0])), float(filspecs[1]), int(round(filspecs[2])), float(filspecs[3]),
+                       f32(grid.dwn), f32(rearth))
 
 
 def _ptr(a: Optional[np.ndarray]):

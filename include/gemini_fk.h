@@ -85,7 +85,7 @@ typedef struct gem_synth_params {
   long long nkfmax;       /* wavenumber-frequency extent of the FK spectra */
   int nsp;                /* spectra per node (10: U, V x 4 jumps, W x 2 jumps) */
   int istyp;              /* 1 MOMENT (only moment tensors are supported) */
-  int global_;            /* 1: spherical harmonics (Legendre) */
+  int global_;            /* 1: spherical harmonics (Legendre), 0: wavenumber integrals (Bessel) */
   double df, sigma;
   int nsamp;              /* power of two */
   double dt;              /* nsamp * dt * df = 1 */
@@ -95,6 +95,8 @@ typedef struct gem_synth_params {
   double fc_highpass;
   int order_lowpass;
   double fc_lowpass;
+  double dwn;             /* wavenumber spacing (regional mode; float32 in the reference's FK file) */
+  double rearth;          /* earth radius of the FK file (regional mode; float32 there) */
 } gem_synth_params;
 
 /* Context holding the model, nodes and device buffers of one GPU.

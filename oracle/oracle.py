@@ -54,6 +54,16 @@ def lib():
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.oracle_legendre.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
         L.oracle_fft.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_wavenumber_integrals.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+                                                  ctypes.c_void_p]
+        L.oracle_synthetics_bessel.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
         L.oracle_freq_time.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                        ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_double,
                                        ctypes.c_void_p]
@@ -168,6 +178,38 @@ def freq_time(nf1, nf2, df, sigma, sp, nsamp, dt):
     if rc >= 2:
         raise RuntimeError("oracle_freq_time: invalid sizes")
     return ts, rc
+
+
+def wavenumber_integrals(nf1, nf2, nwn, nwnmax, gr, gi, dwn, rearth, x):
+    """The 14 moment wavenumber integrals (regional mode): complex [nsta, nf2, 14]; x in m."""
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkf = gr.shape
+    x = np.ascontiguousarray(x, np.float64)
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    hd = np.zeros(len(x) * nf2 * 14 * 2)
+    rc = lib().oracle_wavenumber_integrals(nf1, nf2, _p(nwn), nwnmax, nkf, nsp, _p(gr), _p(gi), dwn, rearth, len(x),
+                                           _p(x), _p(hd))
+    if rc:
+        raise RuntimeError("oracle_wavenumber_integrals failed")
+    return hd.view(np.complex128).reshape(len(x), nf2, 14)
+
+
+def synthetics_bessel(nf1, nf2, nwn, nwnmax, df, sigma, dwn, rearth, gr, gi, theta, phi, propdir, mt, filspecs,
+                      velocity, tred, nsamp, dt):
+    """Synthetics of the regional mode; theta = distance / rearth.  float32 [nsta, nmt, 3, nsamp]."""
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkf = gr.shape
+    th = np.ascontiguousarray(theta, np.float64); ph = np.ascontiguousarray(phi, np.float64)
+    pd = np.ascontiguousarray(propdir, np.float64); mt = np.ascontiguousarray(mt, np.float64).reshape(-1, 6)
+    fs = np.ascontiguousarray(filspecs, np.float64)
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    out = np.zeros((len(th), len(mt), 3, nsamp), np.float32)
+    rc = lib().oracle_synthetics_bessel(nf1, nf2, _p(nwn), nwnmax, df, sigma, dwn, rearth, nkf, nsp, _p(gr), _p(gi),
+                                        len(th), _p(th), _p(ph), _p(pd), len(mt), _p(mt), _p(fs), int(velocity),
+                                        tred, nsamp, dt, _p(out))
+    if rc:
+        raise RuntimeError("oracle_synthetics_bessel failed (%d)" % rc)
+    return out
 
 
 def degree_sums(nf1, nf2, nwn, nwnmax, gr, gi, theta):

@@ -229,7 +229,126 @@ void eventFilter(int nordh, double fch, int nordl, double fcl, int nf1, int nf2,
 
 }  // namespace
 
+
+namespace {
+// ---------------------------------------------------------------------------
+//  Regional (Bessel) mode: wavenumber integrals
+// ---------------------------------------------------------------------------
+// Bessel functions at the wavenumber points (besselFunctions.f90:33-51): J[3*(j-1) + n]
+// for j = 1..nwn, wn accumulated as wn = wn + dwn.  J0 and J1 come from the C
+// library (the reference evaluates Cody's rational approximations CALJY0/CALJY1,
+// accurate to double precision).
+void besselTable(int nwn, double dwn, double x, std::vector<double>& J) {
+  J.assign(3 * (size_t)nwn, 0.0);
+  J[0] = 1.0;
+  double wn = dwn;
+  for (int j = 2; j <= nwn; ++j) {
+    double j0v = ::j0(wn * x), j1v = ::j1(wn * x);
+    J[3 * (j - 1)] = j0v;
+    J[3 * (j - 1) + 1] = j1v;
+    J[3 * (j - 1) + 2] = -j0v + 2.0 / (wn * x) * j1v;
+    wn = wn + dwn;
+  }
+}
+
+// integrand factor of moment integral kint (1..14) at wavenumber wn from the
+// Bessel values b0, b1, b2 at wn*x (wavenumberIntegrals.f90:352-366, 372-386)
+double wnKernel(int kint, double wn, double b0, double b1, double b2, double re, double x) {
+  switch (kint) {
+    case 1: case 2: return wn * b0;
+    case 3: return 2.0 / re * b1;
+    case 4: return wn * 2.0 * b2;
+    case 5: case 6: return wn * (-wn * re) * b1;
+    case 7: case 11: return wn * 2.0 * (b0 - b1 / (wn * x));
+    case 8: return wn * 2.0 * wn * re * (b1 - 2.0 * b2 / (wn * x));
+    case 9: case 13: return wn * 2.0 * b1 / (wn * x);
+    case 10: return wn * 4.0 * wn * re * b2 / (wn * x);
+    case 12: return -(wn * 2.0 * wn * re * (b1 - 2.0 * b2 / (wn * x)));
+    default: return -(wn * 4.0 * wn * re * b2 / (wn * x));   // 14
+  }
+}
+
+// cos^2 taper of the wavenumber integrals (wavenumberIntegrals.f90:480-491), 1-based g[j]
+void taperWn(int nwn, double dwn, double tapfrac, std::vector<double>& g) {
+  int jt = std::min((int)std::lround((double)nwn * (1.0 - tapfrac)), nwn);
+  jt = std::max(1, jt);
+  double c1 = (double)(nwn - 1) * dwn * tapfrac * 2.0 / PI_F;
+  double c2 = (1.0 - tapfrac) / tapfrac * 0.5 * PI_F;
+  g.assign(nwn + 1, 1.0);
+  for (int j = jt; j <= nwn; ++j) { double c = std::cos((double)(j - 1) * dwn / c1 - c2); g[j] = c * c; }
+}
+
+// momentWavenumberIntegrals (wavenumberIntegrals.f90:320-475) for one frequency:
+// G 1-based [1..nwn] of the integral's FK column, J the Bessel table of distance xx
+zc momentWavenumberIntegral(int kint, const std::vector<zc>& G, int nwn, double dwn, double re, double xx,
+                            const std::vector<double>& J, const std::vector<double>& tap) {
+  double x = xx < 3.0 / (dwn * 1.e9) ? 3.0 / (dwn * 1.e9) : xx;
+  double wn3 = 3.0 / x;
+  int j3 = (int)(wn3 / dwn) + 2;
+  wn3 = (double)(j3 - 1) * dwn;
+  auto wnb = [&](int j) {
+    double wn = (double)(j - 1) * dwn;
+    return wnKernel(kint, wn, J[3 * (j - 1)], J[3 * (j - 1) + 1], J[3 * (j - 1) + 2], re, x);
+  };
+  auto ybes = [&](double w) {
+    double y0v = ::y0(w * x), y1v = ::y1(w * x);
+    double y2v = -y0v + 2.0 / (w * x) * y1v;
+    return wnKernel(kint, w, y0v, y1v, y2v, re, x);
+  };
+  double wn3besy = ybes(wn3);
+  int j33 = std::min(j3, nwn);
+  zc zdis = Z(0.0);
+  for (int j = 2; j <= j33 - 1; ++j) zdis = zdis + (G[j] * wnb(j)) * tap[j];
+  zdis = zdis + ((0.5 * G[j33]) * wnb(j33)) * tap[j33];
+  zdis = zdis * dwn;
+  if (j33 != nwn) {
+    double wne = (double)(nwn - 1) * dwn;
+    double wnbesy = ybes(wne);
+    double xdk = x * dwn;
+    zc zsum = (G[j3] * wnb(j3)) * tap[j3];
+    for (int j = j3 + 1; j <= nwn - 1; ++j) zsum = zsum + ((2.0 * G[j]) * wnb(j)) * tap[j];
+    zsum = zsum + (G[nwn] * wnb(nwn)) * tap[nwn];
+    zdis = zdis + ((zsum / x) * (1.0 - std::cos(xdk))) / xdk;
+    zdis = zdis + (((G[nwn] * wnbesy) * tap[nwn] - (G[j3] * wn3besy) * tap[j3]) / x) * (1.0 - std::sin(xdk) / xdk);
+  }
+  return zdis * (re * re / (2.0 * PI_F));
+}
+
+}  // namespace
+
 extern "C" {
+
+// Wavenumber integrals of the regional mode: hd[(sta*nf2 + jf-1)*14 + k] complex
+// interleaved for the 14 moment integrals; x: distances in m.
+int oracle_wavenumber_integrals(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp,
+                                const float* gr, const float* gi, double dwn, double rearth, int nsta,
+                                const double* x, double* hd) {
+  static const int col[14] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 8, 9, 6, 7};   // FK column of each integral
+  if (nsp < 10) return 2;
+  std::vector<int> koff(nf2 + 1, 0);
+  long long k = 0;
+  for (int jf = nf1; jf <= nf2; ++jf) { koff[jf] = (int)k; k += nwn[jf - 1]; }
+  if (k > nkfmax) return 2;
+  std::vector<double> J, tap;
+  std::vector<zc> G;
+  for (int is = 0; is < nsta; ++is) {
+    besselTable(nwnmax, dwn, x[is], J);
+    for (int jf = nf1; jf <= nf2; ++jf) {
+      const int n = nwn[jf - 1];
+      taperWn(n, dwn, 0.2, tap);
+      for (int kk = 1; kk <= 14; ++kk) {
+        G.assign(n + 1, Z(0.0));
+        const long long o = (long long)col[kk - 1] * nkfmax + koff[jf];
+        for (int j = 1; j <= n; ++j) G[j] = Z((double)gr[o + j - 1], (double)gi[o + j - 1]);
+        zc z = momentWavenumberIntegral(kk, G, n, dwn, rearth, x[is], J, tap);
+        double* h = hd + (((size_t)is * nf2 + (jf - 1)) * 14 + (kk - 1)) * 2;
+        h[0] = z.re; h[1] = z.im;
+      }
+    }
+  }
+  return 0;
+}
+
 
 // Legendre tables for the unit tests: out[kind*3*(lmax+1) + m*(lmax+1) + l], kinds
 // plm, dpdt, pdst, d2pdt2, dtpdst.
@@ -302,14 +421,15 @@ int oracle_degree_sums(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax,
 
 // Full phase 2 for moment tensor sources: traces[((sta*nmt + imt)*3 + comp)*nsamp + i]
 // comp order Z, N, E.  filspecs = {nord_hp, fc_hp, nord_lp, fc_lp}.
-int oracle_synthetics(int nf1, int nf2, const int* nwn, int nwnmax, double df, double sigma,
-                      int nkfmax, int nsp, const float* gr, const float* gi, int nsta,
-                      const double* theta, const double* phi, const double* propdir, int nmt,
-                      const double* mt, const double* filspecs, int velocity, double tred,
-                      int nsamp, double dt, float* traces) {
-  std::vector<double> hd((size_t)nsta * nf2 * 14 * 2, 0.0);
-  int rc = oracle_degree_sums(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, nsta, theta, hd.data());
-  if (rc) return rc;
+}  // extern "C"
+
+namespace {
+// displacement spectra from the 14 sums or integrals hd, filters, rotation and
+// inverse FFT of every station and moment tensor (computeSyntheticSeismograms.f90:336-390)
+int synth_from_sums(const std::vector<double>& hd, int nf1, int nf2, double df, double sigma, int nsta,
+                    const double* phi, const double* propdir, int nmt, const double* mt, const double* filspecs,
+                    int velocity, double tred, int nsamp, double dt, float* traces) {
+  int rc = 0;
   std::vector<zc> evf;
   eventFilter((int)std::lround(filspecs[0]), filspecs[1], (int)std::lround(filspecs[2]), filspecs[3],
               nf1, nf2, df, sigma, evf);
@@ -357,6 +477,39 @@ int oracle_synthetics(int nf1, int nf2, const int* nwn, int nwnmax, double df, d
     }
   }
   return 0;
+}
+}  // namespace
+
+extern "C" {
+
+// Synthetics of the global mode (harmonic degree sums at colatitudes theta).
+int oracle_synthetics(int nf1, int nf2, const int* nwn, int nwnmax, double df, double sigma,
+                      int nkfmax, int nsp, const float* gr, const float* gi, int nsta,
+                      const double* theta, const double* phi, const double* propdir, int nmt,
+                      const double* mt, const double* filspecs, int velocity, double tred,
+                      int nsamp, double dt, float* traces) {
+  std::vector<double> hd((size_t)nsta * nf2 * 14 * 2, 0.0);
+  int rc = oracle_degree_sums(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, nsta, theta, hd.data());
+  if (rc) return rc;
+  return synth_from_sums(hd, nf1, nf2, df, sigma, nsta, phi, propdir, nmt, mt, filspecs, velocity, tred, nsamp, dt,
+                         traces);
+}
+
+// Synthetics of the regional mode (wavenumber integrals at distances theta * rearth,
+// besselDisplacementSpectra, displacementSpectra.f90:125-188).
+int oracle_synthetics_bessel(int nf1, int nf2, const int* nwn, int nwnmax, double df, double sigma, double dwn,
+                             double rearth, int nkfmax, int nsp, const float* gr, const float* gi, int nsta,
+                             const double* theta, const double* phi, const double* propdir, int nmt,
+                             const double* mt, const double* filspecs, int velocity, double tred, int nsamp,
+                             double dt, float* traces) {
+  std::vector<double> x(nsta);
+  for (int i = 0; i < nsta; ++i) x[i] = theta[i] * rearth;
+  std::vector<double> hd((size_t)nsta * nf2 * 14 * 2, 0.0);
+  int rc = oracle_wavenumber_integrals(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, dwn, rearth, nsta, x.data(),
+                                       hd.data());
+  if (rc) return rc;
+  return synth_from_sums(hd, nf1, nf2, df, sigma, nsta, phi, propdir, nmt, mt, filspecs, velocity, tred, nsamp, dt,
+                         traces);
 }
 
 }  // extern "C"

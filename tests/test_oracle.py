@@ -174,3 +174,41 @@ def test_proposer_mlp_gradient_against_finite_differences():
         e = np.zeros_like(w); e[i] = 1e-6
         fd = (proposer_mlp.loss_and_grad(w + e, x, y, mask)[0] - proposer_mlp.loss_and_grad(w - e, x, y, mask)[0]) / 2e-6
         assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(g[i])
+
+
+def test_wavenumber_integral_of_an_analytic_spectrum():
+    """Trapezoid + Filon + Neumann end terms of momentWavenumberIntegrals on
+    G(k) = exp(-a k): int k exp(-a k) J0(k x) dk = a / (a^2 + x^2)^(3/2).  The
+    rule is second order in x dk: its error falls 4x when dk halves."""
+    a, re = 20000.0, 6371000.0
+
+    def rel_err(n, x):
+        dwn = 40.0 / a / n
+        gr = np.zeros((10, n), np.float32)
+        gr[0] = np.exp(-a * np.arange(n) * dwn)
+        hd = oracle.wavenumber_integrals(2, 2, np.array([0, n], np.int32), n, gr, np.zeros_like(gr), dwn, re, [x])
+        got = hd[0, 1, 0].real / (re * re / (2 * np.float32(np.pi)))
+        return got / (a / (a * a + x * x) ** 1.5) - 1.0, x * dwn
+
+    for x in (5000.0, 50000.0, 200000.0):
+        e1, xdk = rel_err(8000, x)
+        e2, _ = rel_err(16000, x)
+        assert abs(e1) < 2.0 * xdk * xdk
+        if abs(e1) > 1e-5:
+            assert 3.5 < e1 / e2 < 4.5
+
+
+def test_bessel_functions_of_the_oracle_against_scipy():
+    sp = pytest.importorskip("scipy.special")
+    # the oracle's integral of a single wavenumber sample isolates J at that point
+    n, dwn, x, re = 64, 1e-5, 123456.0, 6371000.0
+    for j in (5, 20, 40):
+        gr = np.zeros((10, n), np.float32); gi = np.zeros_like(gr)
+        gr[:, j - 1] = 1.0
+        hd = oracle.wavenumber_integrals(2, 2, np.array([0, n], np.int32), n, gr, gi, dwn, re, [x])
+        k = (j - 1) * dwn
+        taper_w = hd[0, 1, 0].real / (re * re / (2 * np.float32(np.pi))) / (k * sp.j0(k * x))
+        # integral 1 (k J0) and integral 3 (2/re J1) share the sample's weight
+        ratio = hd[0, 1, 2].real / hd[0, 1, 0].real
+        assert abs(ratio - (2.0 / re * sp.j1(k * x)) / (k * sp.j0(k * x))) < 1e-9 * abs(ratio) + 1e-12
+        assert np.isfinite(taper_w)
