@@ -68,6 +68,11 @@ struct gem_ctx {
   void* d_aux[8] = {};
   size_t aux_cap[8] = {};
   int kopt = 6;   // order target of the step-size control (gem_order_target; fast backend)
+  // captured launch sequence of one slab (gem_fk_graph_build)
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  bool graph_valid = false;
+  long long graph_items = 0;
   // learned proposer (fast backend): FP16 weights, feature normalisation, proposals per (phase, item)
   __half* d_propw = nullptr;
   float* d_propnorm = nullptr;
@@ -222,6 +227,8 @@ void gem_ctx_destroy(gem_ctx* ctx) {
   cudaFree(ctx->d_steplog); cudaFree(ctx->d_steplog_n);
   cudaFree(ctx->d_propw); cudaFree(ctx->d_propnorm); cudaFree(ctx->d_prop_kopt); cudaFree(ctx->d_prop_hs);
   cudaFree(ctx->d_feat);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph_stream) cudaStreamDestroy(ctx->graph_stream);
   for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto& e : ctx->ev_ph) if (e) cudaEventDestroy(e);
   delete ctx;
@@ -231,6 +238,7 @@ const char* gem_last_error(const gem_ctx* ctx) { return ctx ? ctx->err.c_str() :
 
 int gem_model_load(gem_ctx* ctx, const gem_model_desc* m) {
   if (!ctx || !m) return GEM_ERROR;
+  ctx->graph_valid = false;
   CK(cudaSetDevice(ctx->device));
   if (m->nlay < 2 || m->nlay > MAXLAY) return fail(ctx, "number of layers %d outside 2..%d", m->nlay, MAXLAY);
   if (m->nk < 2 || m->nk > MAXKNOT - 1) return fail(ctx, "number of knots %d outside 2..%d", m->nk, MAXKNOT - 1);
@@ -288,6 +296,7 @@ int gem_model_load(gem_ctx* ctx, const gem_model_desc* m) {
 }
 
 int gem_nodes_set(gem_ctx* ctx, int nnod, const double* r, const int* state, const int* layer) {
+  if (ctx) ctx->graph_valid = false;
   if (!ctx) return GEM_ERROR;
   if (!ctx->have_model) return fail(ctx, "load the earth model before the nodes");
   if (nnod < 1 || nnod > MAXNOD) return fail(ctx, "number of nodes %d outside 1..%d", nnod, MAXNOD);
@@ -319,21 +328,45 @@ int gem_fk_grid(gem_ctx* ctx, const gem_fk_params* p, int* nf1, int* nf2, int* n
   return GEM_OK;
 }
 
-int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre, float* d_gfim,
-                      double* d_gf64, int32_t* d_status, void* stream) {
-  if (!ctx) return GEM_ERROR;
+}  // extern "C"
+
+namespace {
+
+// Everything one FK slab run needs on the device, prepared on the host: the
+// parameter block, the item and queue tables (uploaded), the kernel arguments
+// and the grids.  fk_enqueue then issues only device work, so that the same
+// sequence can be run directly or captured into a CUDA graph.
+struct SlabPlan {
+  FKStatic P;
+  PrepArgs A;
+  PropArgs PA;
+  FKLaunch L;
+  int grid[3];
+  int nslot, nitems, nsp;
+  long long nkf;
+  size_t spl_n, nout, nu, nd;
+  bool fast, propose;
+  float* gfre;
+  float* gfim;
+  double* gf64;
+  int32_t* status;
+};
+
+int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre, float* d_gfim,
+               double* d_gf64, int32_t* d_status, SlabPlan& S) {
   int rc = check_params(ctx, p);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
-  cudaStream_t st = (cudaStream_t)stream;
+  ctx->graph_valid = false;   // the tables below are rewritten: a captured graph no longer matches them
   Grid g;
   make_grid(p, ctx->rearth, g);
   if (jf_first < g.nf1 || jf_last > g.nf2 || jf_first > jf_last)
     return fail(ctx, "frequency range %d..%d outside %d..%d", jf_first, jf_last, g.nf1, g.nf2);
   const int nslot = jf_last - jf_first + 1;
   const int nsp = nsp_of(p);
+  S.nslot = nslot; S.nsp = nsp;
   // ---- parameter block
-  FKStatic P;
+  FKStatic& P = S.P;
   memset(&P, 0, sizeof P);
   P.nlay = ctx->nlay; P.nk = ctx->nk; P.noc = ctx->noc; P.nic = ctx->nic; P.equidis = ctx->equidis;
   P.fsflag = ctx->fsflag; P.nnod = ctx->nnod; P.jre = p->jre;
@@ -369,18 +402,17 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   for (int s = nslot - 1; s >= 0; --s)
     for (int iwn = 1; iwn <= g.nwn[jf_first + s]; ++iwn) order.push_back(slots[nslot + s] + iwn - 1);
   const int nitems = (int)nkf;
+  S.nkf = nkf; S.nitems = nitems;
   if (grow(ctx, ctx->d_items, ctx->items_cap, items.size())) return GEM_ERROR;
   if (grow(ctx, ctx->d_order, ctx->order_cap, order.size())) return GEM_ERROR;
   if (grow(ctx, ctx->d_slots, ctx->slots_cap, slots.size())) return GEM_ERROR;
-  CK(cudaMemcpyAsync(ctx->d_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(ctx->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(ctx->d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-  // ---- K3: model preparation for all slots
-  size_t spl_n = (size_t)nslot * (ctx->nk + 1) * SPL_STRIDE;
-  if (grow(ctx, ctx->d_spl, ctx->spl_cap, spl_n)) return GEM_ERROR;
-  CK(cudaMemsetAsync(ctx->d_spl, 0, spl_n * sizeof(double), st));
-  CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
-  PrepArgs A;
+  CK(cudaMemcpy(ctx->d_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice));
+  // ---- model preparation for all slots
+  S.spl_n = (size_t)nslot * (ctx->nk + 1) * SPL_STRIDE;
+  if (grow(ctx, ctx->d_spl, ctx->spl_cap, S.spl_n)) return GEM_ERROR;
+  PrepArgs& A = S.A;
   const int K1 = ctx->nk + 1;
   A.nslot = nslot; A.nk = ctx->nk; A.nlay = ctx->nlay; A.attmode = p->attmode; A.df = g.df; A.fref = ctx->fref;
   A.jf = ctx->d_slots;
@@ -390,46 +422,36 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   A.iktop = ctx->d_lay; A.ikbot = ctx->d_lay + (ctx->nlay + 1);
   A.spl = ctx->d_spl;
   const bool fast = ctx->backend == GEM_BACKEND_GPU_FAST;
-  CK(cudaEventRecord(ctx->ev[0], st));
-  CK(launch_prep(A, ctx->d_err, st));
+  S.fast = fast;
   if (fast) {
     size_t poly_n = (size_t)nslot * (ctx->nk + 1) * POLY_STRIDE;
     if (grow(ctx, ctx->d_poly, ctx->poly_cap, poly_n)) return GEM_ERROR;
-    CK(launch_poly(A, ctx->d_poly, st));
   }
-  CK(cudaEventRecord(ctx->ev[1], st));
-  // ---- outputs and per-item storage zeroed (unreached nodes and skipped items stay zero)
-  size_t nout = (size_t)nkf * nsp * ctx->nnod;
-  if (d_gf64) CK(cudaMemsetAsync(d_gf64, 0, nout * 2 * sizeof(double), st));
-  if (d_gfre) CK(cudaMemsetAsync(d_gfre, 0, nout * sizeof(float), st));
-  if (d_gfim) CK(cudaMemsetAsync(d_gfim, 0, nout * sizeof(float), st));
+  // ---- outputs and per-item storage (zeroed by fk_enqueue)
+  S.nout = (size_t)nkf * nsp * ctx->nnod;
+  S.gfre = d_gfre; S.gfim = d_gfim; S.gf64 = d_gf64;
   int32_t* status = d_status;
   if (!status) {
     if (grow(ctx, ctx->d_status, ctx->status_cap, (size_t)nkf)) return GEM_ERROR;
     status = ctx->d_status;
   }
-  CK(cudaMemsetAsync(status, 0, (size_t)nkf * sizeof(int32_t), st));
+  S.status = status;
   const int jre = p->jre;
-  size_t nu = (size_t)jre * 6 * nkf, nd = (size_t)(ctx->nnod - jre + 1) * 6 * nkf;
-  if (grow(ctx, ctx->d_um, ctx->um_cap, nu)) return GEM_ERROR;
-  if (grow(ctx, ctx->d_dm, ctx->dm_cap, nd)) return GEM_ERROR;
+  S.nu = (size_t)jre * 6 * nkf;
+  S.nd = (size_t)(ctx->nnod - jre + 1) * 6 * nkf;
+  if (grow(ctx, ctx->d_um, ctx->um_cap, S.nu)) return GEM_ERROR;
+  if (grow(ctx, ctx->d_dm, ctx->dm_cap, S.nd)) return GEM_ERROR;
   if (grow(ctx, ctx->d_rstart, ctx->rstart_cap, 2 * (size_t)nkf)) return GEM_ERROR;
   if (grow(ctx, ctx->d_dets, ctx->dets_cap, (size_t)nkf)) return GEM_ERROR;
-  CK(cudaMemsetAsync(ctx->d_um, 0, nu * sizeof(double2), st));
-  CK(cudaMemsetAsync(ctx->d_dm, 0, nd * sizeof(double2), st));
-  CK(cudaMemsetAsync(ctx->d_dets, 0, (size_t)nkf * sizeof(double2), st));
   // ---- grid: the largest of the three phases sets the per-lane scratch
-  int grid[3];
   long long nthreads = 0;
   for (int ph = 0; ph < 3; ++ph) {
-    grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph) : gem_plain::fk_phase_blocks_per_sm(ph));
-    nthreads = std::max(nthreads, (long long)grid[ph] * FK_BLOCK);
+    S.grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph) : gem_plain::fk_phase_blocks_per_sm(ph));
+    nthreads = std::max(nthreads, (long long)S.grid[ph] * FK_BLOCK);
   }
   size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * gem_plain::fk_lane_slot_per_node();
   if (grow(ctx, ctx->d_scratch, ctx->scratch_cap, scratch_n)) return GEM_ERROR;
-  CK(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned int), st));
-  CK(cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(unsigned long long), st));
-  FKLaunch L;
+  FKLaunch& L = S.L;
   L.spl = ctx->d_spl; L.poly = fast ? ctx->d_poly : nullptr; L.jf = ctx->d_slots; L.koff = ctx->d_slots + nslot; L.items = ctx->d_items;
   L.order = ctx->d_order;
   L.nitems = nitems; L.nkf = nkf; L.gf64 = (double2*)d_gf64; L.gfre = d_gfre; L.gfim = d_gfim;
@@ -440,53 +462,81 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   L.warp_ns = nullptr;
   L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
   L.prop_kopt = nullptr; L.prop_hs = nullptr;
-  if (ctx->d_steplog_n) CK(cudaMemsetAsync(ctx->d_steplog_n, 0, sizeof(unsigned long long), st));
-  if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
-  ctx->last_grid = grid[1];
-  CK(cudaEventRecord(ctx->ev[2], st));
-  auto launch = [&](int ph, const FKLaunch& LX, int g) {
-    return fast ? gem_fast::launch_fk_phase(ph, P, LX, g, st) : gem_plain::launch_fk_phase(ph, P, LX, g, st);
-  };
-  CK(launch(-1, L, ctx->nsm * 8));
-  // learned proposer: features / proposals per (phase, item) from the start radii
-  const bool propose = fast && ctx->prop_use != 0 && ctx->d_propw;
-  if (ctx->dump_feat || propose) {
-    PropArgs A{};
-    A.items = ctx->d_items; A.jf = ctx->d_slots; A.rstart = ctx->d_rstart; A.nkf = nkf; A.nitems = nitems;
-    A.nk = ctx->nk; A.nlay = ctx->nlay; A.use = ctx->prop_use; A.margin = ctx->prop_margin;
-    A.df = P.df; A.rearth = ctx->rearth;
+  ctx->last_grid = S.grid[1];
+  // ---- learned proposer: features / proposals per (phase, item) from the start radii
+  S.propose = fast && ctx->prop_use != 0 && ctx->d_propw;
+  if (ctx->dump_feat || S.propose) {
+    PropArgs& PA = S.PA;
+    PA = PropArgs{};
+    PA.items = ctx->d_items; PA.jf = ctx->d_slots; PA.rstart = ctx->d_rstart; PA.nkf = nkf; PA.nitems = nitems;
+    PA.nk = ctx->nk; PA.nlay = ctx->nlay; PA.use = ctx->prop_use; PA.margin = ctx->prop_margin;
+    PA.df = P.df; PA.rearth = ctx->rearth;
     for (int i = 0; i <= ctx->nk; ++i) {
-      A.rk[i] = ctx->rk[i];
-      A.knot_feat[3 * i + 0] = (float)(ctx->vpv[i] / 1e4);
-      A.knot_feat[3 * i + 1] = (float)(ctx->vsv[i] / 1e4);
-      A.knot_feat[3 * i + 2] = (float)(ctx->ro[i] / 1e4);
+      PA.rk[i] = ctx->rk[i];
+      PA.knot_feat[3 * i + 0] = (float)(ctx->vpv[i] / 1e4);
+      PA.knot_feat[3 * i + 1] = (float)(ctx->vsv[i] / 1e4);
+      PA.knot_feat[3 * i + 2] = (float)(ctx->ro[i] / 1e4);
     }
-    for (int i = 0; i <= ctx->nlay; ++i) A.rb[i] = ctx->rb[i];
-    if (ctx->dump_feat) {
-      if (grow(ctx, ctx->d_feat, ctx->feat_cap, (size_t)3 * nitems * PROP_NF)) return GEM_ERROR;
-      CK(prop_features_launch(A, ctx->d_feat, st));
-      ctx->feat_n = 3LL * nitems * PROP_NF;
-    }
-    if (propose) {
+    for (int i = 0; i <= ctx->nlay; ++i) PA.rb[i] = ctx->rb[i];
+    if (ctx->dump_feat && grow(ctx, ctx->d_feat, ctx->feat_cap, (size_t)3 * nitems * PROP_NF)) return GEM_ERROR;
+    if (S.propose) {
       if (grow(ctx, ctx->d_prop_kopt, ctx->prop_kopt_cap, (size_t)3 * nkf)) return GEM_ERROR;
       if (grow(ctx, ctx->d_prop_hs, ctx->prop_hs_cap, (size_t)3 * nkf)) return GEM_ERROR;
-      CK(prop_infer_launch(A, ctx->d_propw, ctx->d_propnorm, ctx->d_prop_kopt, ctx->d_prop_hs, st));
       L.prop_kopt = ctx->d_prop_kopt;
       L.prop_hs = ctx->d_prop_hs;
     }
   }
+  return GEM_OK;
+}
+
+// The device work of one slab on stream st: zeroing, model preparation, start
+// radii, proposals, the three phases and the per-phase counter snapshots.
+// timed: record the context's events (not inside a graph capture).
+int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
+  const FKStatic& P = S.P;
+  CK(cudaMemsetAsync(ctx->d_spl, 0, S.spl_n * sizeof(double), st));
+  CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  if (timed) CK(cudaEventRecord(ctx->ev[0], st));
+  CK(launch_prep(S.A, ctx->d_err, st));
+  if (S.fast) CK(launch_poly(S.A, ctx->d_poly, st));
+  if (timed) CK(cudaEventRecord(ctx->ev[1], st));
+  if (S.gf64) CK(cudaMemsetAsync(S.gf64, 0, S.nout * 2 * sizeof(double), st));
+  if (S.gfre) CK(cudaMemsetAsync(S.gfre, 0, S.nout * sizeof(float), st));
+  if (S.gfim) CK(cudaMemsetAsync(S.gfim, 0, S.nout * sizeof(float), st));
+  CK(cudaMemsetAsync(S.status, 0, (size_t)S.nkf * sizeof(int32_t), st));
+  CK(cudaMemsetAsync(ctx->d_um, 0, S.nu * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_dm, 0, S.nd * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_dets, 0, (size_t)S.nkf * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(unsigned long long), st));
+  if (ctx->d_steplog_n) CK(cudaMemsetAsync(ctx->d_steplog_n, 0, sizeof(unsigned long long), st));
+  if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
+  if (timed) CK(cudaEventRecord(ctx->ev[2], st));
+  auto launch = [&](int ph, const FKLaunch& LX, int g) {
+    return S.fast ? gem_fast::launch_fk_phase(ph, P, LX, g, st) : gem_plain::launch_fk_phase(ph, P, LX, g, st);
+  };
+  CK(launch(-1, S.L, ctx->nsm * 8));
+  if (ctx->dump_feat) {
+    CK(prop_features_launch(S.PA, ctx->d_feat, st));
+    ctx->feat_n = 3LL * S.nitems * PROP_NF;
+  }
+  if (S.propose) CK(prop_infer_launch(S.PA, ctx->d_propw, ctx->d_propnorm, ctx->d_prop_kopt, ctx->d_prop_hs, st));
   for (int ph = 0; ph < 3; ++ph) {
-    FKLaunch Lp = L;
+    FKLaunch Lp = S.L;
     if (ctx->d_prof) Lp.prof = ctx->d_prof + 8 * ph;
     if (ctx->d_warp_ns && ph == 1) Lp.warp_ns = ctx->d_warp_ns;
-    CK(launch(ph, Lp, grid[ph]));
-    CK(cudaEventRecord(ctx->ev_ph[ph], st));
+    CK(launch(ph, Lp, S.grid[ph]));
+    if (timed) CK(cudaEventRecord(ctx->ev_ph[ph], st));
     // running counters after this phase (stream-ordered snapshot)
     CK(cudaMemcpyAsync(ctx->d_stats + 8 * (ph + 1), ctx->d_stats, 8 * sizeof(unsigned long long),
                        cudaMemcpyDeviceToDevice, st));
   }
-  CK(cudaEventRecord(ctx->ev[3], st));
-  // ---- statistics (synchronises the stream)
+  if (timed) CK(cudaEventRecord(ctx->ev[3], st));
+  return GEM_OK;
+}
+
+// counters and times of the last slab (synchronises the stream)
+int fk_finish(gem_ctx* ctx, const SlabPlan& S, cudaStream_t st, bool timed) {
   unsigned long long hs[32];
   int herr = 0;
   CK(cudaMemcpyAsync(hs, ctx->d_stats, 32 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
@@ -494,11 +544,13 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   CK(cudaStreamSynchronize(st));
   if (herr) return fail(ctx, "Cubic spline interpolation not successful (code %d)", herr);
   float t_prep = 0, t_solve = 0, t0 = 0;
-  cudaEventElapsedTime(&t_prep, ctx->ev[0], ctx->ev[1]);
-  cudaEventElapsedTime(&t_solve, ctx->ev[2], ctx->ev[3]);
+  if (timed) {
+    cudaEventElapsedTime(&t_prep, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&t_solve, ctx->ev[2], ctx->ev[3]);
+  }
   for (int ph = 0; ph < 3; ++ph) {
     float t = 0;
-    cudaEventElapsedTime(&t, ctx->ev[2], ctx->ev_ph[ph]);
+    if (timed) cudaEventElapsedTime(&t, ctx->ev[2], ctx->ev_ph[ph]);
     ctx->phase_ms[ph] = t - t0;
     ctx->stats.phase_ms[ph] = t - t0;
     ctx->stats.phase_flops[ph] = (int64_t)(hs[8 * (ph + 1) + 5] - (ph ? hs[8 * ph + 5] : 0ULL));
@@ -506,8 +558,65 @@ int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf
   }
   ctx->stats.steps_ok = hs[0]; ctx->stats.steps_rej = hs[1]; ctx->stats.attempts = hs[2];
   ctx->stats.sysmats = hs[3]; ctx->stats.matvecs = hs[4]; ctx->stats.flops = hs[5];
-  ctx->stats.items = nitems; ctx->stats.failed = 0;
+  ctx->stats.items = S.nitems; ctx->stats.failed = 0;
   ctx->stats.prep_ms = t_prep; ctx->stats.solve_ms = t_solve;
+  return GEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre, float* d_gfim,
+                      double* d_gf64, int32_t* d_status, void* stream) {
+  if (!ctx) return GEM_ERROR;
+  SlabPlan S;
+  int rc = fk_prepare(ctx, p, jf_first, jf_last, d_gfre, d_gfim, d_gf64, d_status, S);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = fk_enqueue(ctx, S, st, true);
+  if (rc) return rc;
+  return fk_finish(ctx, S, st, true);
+}
+
+// CUDA-graph form of gem_fk_run_device (no counterpart in the reference): the
+// host-side preparation runs once here, the device work of the slab is captured
+// into a graph that gem_fk_graph_launch replays.  The graph reads and writes
+// the same device buffers as a direct run; any later run, graph build, model or
+// node change on this context invalidates it.
+int gem_fk_graph_build(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
+                       float* d_gfim, double* d_gf64, int32_t* d_status) {
+  if (!ctx) return GEM_ERROR;
+  if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+  SlabPlan S;
+  int rc = fk_prepare(ctx, p, jf_first, jf_last, d_gfre, d_gfim, d_gf64, d_status, S);
+  if (rc) return rc;
+  if (!ctx->graph_stream) CK(cudaStreamCreateWithFlags(&ctx->graph_stream, cudaStreamNonBlocking));
+  // run once directly: kernel attributes and lazily loaded modules are set up outside the capture
+  rc = fk_enqueue(ctx, S, ctx->graph_stream, false);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->graph_stream));
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(ctx->graph_stream, cudaStreamCaptureModeThreadLocal));
+  rc = fk_enqueue(ctx, S, ctx->graph_stream, false);
+  cudaError_t e = cudaStreamEndCapture(ctx->graph_stream, &graph);
+  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return fail(ctx, "graph capture: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) { ctx->graph_exec = nullptr; return fail(ctx, "graph instantiate: %s", cudaGetErrorString(e)); }
+  ctx->graph_items = S.nitems;
+  ctx->graph_valid = true;
+  return GEM_OK;
+}
+
+// Replays the graph of gem_fk_graph_build on stream (asynchronous); the outputs
+// and per-item status are complete when the stream reaches this point.
+int gem_fk_graph_launch(gem_ctx* ctx, void* stream) {
+  if (!ctx) return GEM_ERROR;
+  if (!ctx->graph_exec || !ctx->graph_valid) return fail(ctx, "no valid FK graph (build it again)");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaGraphLaunch(ctx->graph_exec, (cudaStream_t)stream));
   return GEM_OK;
 }
 

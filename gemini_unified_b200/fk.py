@@ -59,6 +59,8 @@ def lib() -> ctypes.CDLL:
         L.gem_fk_run.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
         L.gem_fk_run_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
         L.gem_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.gem_fk_graph_build.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
+        L.gem_fk_graph_launch.argtypes = [vp, vp]
         L.gem_synth_run.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp]
         L.gem_synth_run_device.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp]
         L.gem_ifft_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
@@ -220,6 +222,16 @@ class GeminiFK:
         pc = fk_params_c(params, jre)
         self._check(lib().gem_fk_run_device(self._h, ctypes.byref(pc), jf_first, jf_last, gfre, gfim, gf64,
                                             status, stream or None))
+
+    def graph_build(self, params: FKParams, jre: int, jf_first: int, jf_last: int, gfre=None, gfim=None,
+                    gf64=None, status=None):
+        """Capture the device work of a slab into a CUDA graph (device output pointers as in run_device)."""
+        pc = fk_params_c(params, jre)
+        self._check(lib().gem_fk_graph_build(self._h, ctypes.byref(pc), jf_first, jf_last, gfre, gfim, gf64, status))
+
+    def graph_launch(self, stream: int = 0):
+        """Replay the captured slab on a stream (asynchronous)."""
+        self._check(lib().gem_fk_graph_launch(self._h, stream or None))
 
     def synthetics(self, sp: SynthParams, nwn, gfkr, gfki, theta, phi, propdir, mt):
         """Seismograms of all stations x moment tensors: float32 [nsta, nmt, 3 (Z,N,E), nsamp].

@@ -129,6 +129,17 @@ int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
 int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
                       float* d_gfim, double* d_gf64, int32_t* d_status, void* stream);
 
+/* CUDA-graph form of gem_fk_run_device (no counterpart in the reference).
+ * gem_fk_graph_build does the host-side preparation of the slab once (item and
+ * queue tables, buffers) and captures its device work (zeroing, model
+ * preparation, start radii, phase kernels) into a graph on the context;
+ * gem_fk_graph_launch replays it on a stream, asynchronously, writing the
+ * device outputs given at build time.  Any later run, graph build, model or
+ * node change on the context invalidates the graph (launch then fails). */
+int gem_fk_graph_build(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
+                       float* d_gfim, double* d_gf64, int32_t* d_status);
+int gem_fk_graph_launch(gem_ctx* ctx, void* stream);
+
 /* Synthetic seismograms of all stations and moment tensors of one source
  * node: replaces, for every station, computeLegendreFunctions +
  * sphericalHarmonicsDisplacementSpectra (displacementSpectra.f90:49) + event

@@ -191,3 +191,30 @@ def test_force_source_and_stress_outputs(small, istyp, stress, backend):
     pc = M.fk_params_c(params, jre)
     ref = np.concatenate([o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), nsp)[0] for jf in (20, 21, 22)], axis=2)
     assert _cmp_per_spectrum(g64, ref) <= (RTOL if backend == 1 else RTOL_FAST)
+
+
+def test_graph_replay_matches_direct_run(small):
+    """The captured launch sequence of a slab gives the direct run's spectra and
+    status bit for bit, on two replays; a later direct run invalidates it."""
+    import torch
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST
+    from gemini_unified_b200.model import GeminiError
+    w, m, ex, jre, _, o = small
+    g = M.frequency_grid(w.params, m.rearth)
+    for backend in (1, GEM_BACKEND_GPU_FAST):
+        fk = GeminiFK(m, ex, backend=backend)
+        _, _, ref, st = fk.run(w.params, jre, 20, 30, f32=False)
+        nkf = int(g.nwn[19:30].sum())
+        d64 = torch.empty((ex.nnod, 10, nkf, 2), dtype=torch.float64, device="cuda")
+        dst = torch.empty(nkf, dtype=torch.int32, device="cuda")
+        fk.graph_build(w.params, jre, 20, 30, gf64=d64.data_ptr(), status=dst.data_ptr())
+        for _ in range(2):
+            d64.fill_(7.0)
+            fk.graph_launch()
+            torch.cuda.synchronize()
+            got = torch.view_as_complex(d64).cpu().numpy()
+            assert np.array_equal(np.nan_to_num(got, nan=1.0), np.nan_to_num(ref, nan=1.0))
+            assert int(dst.abs().sum()) == 0
+        fk.run(w.params, jre, 3, 3, f32=False)
+        with pytest.raises(GeminiError):
+            fk.graph_launch()
