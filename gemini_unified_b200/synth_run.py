@@ -49,7 +49,7 @@ def main(argv=None):
         theta, phi, propdir = theta[: a.stations], phi[: a.stations], propdir[: a.stations]
     theta, phi, propdir = (np.ascontiguousarray(x) for x in (theta, phi, propdir))
     mt = np.ascontiguousarray(configs.unit_moment_tensors(), np.float64)
-    sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs)
+    sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs, global_=w.params.global_, rearth=m.rearth)
     nwn = np.ascontiguousarray(g.nwn, np.int32)
     d_gr = torch.from_numpy(gr).cuda()
     d_gi = torch.from_numpy(gi).cuda()
