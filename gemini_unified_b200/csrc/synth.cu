@@ -7,7 +7,9 @@
 // frequencyTime.f90:55-113, fourierTransform.f90:118-192.
 //
 // The station loop of the reference evaluates, per station and frequency, 14
-// dot products of length nwn(f).  Here all stations are batched: for each of
+// (moment tensor) or 7 (single force, harmonicDegreeSums.f90:110-171,
+// singleFrequencyDisplacement.f90:35-46) dot products of length nwn(f).  Here
+// all stations are batched: for each of
 // the 8 Legendre table kinds the sums form one matrix product
 //     C[(f, sum, re/im), station] = sum_l A[(f, sum, re/im), l] * T[l, station]
 // with A holding the FK coefficients times (2l+1)/4pi, the degree factor and
@@ -27,12 +29,25 @@
 namespace gem {
 
 // table kinds: 0 plm0 1 plm1 2 plm2 3 dpdt0 4 dpdt1 5 dpdt2 6 pdst1 7 pdst2
-// moment sums k = 1..14 (harmonicDegreeSums.f90:297-351): kind, first l, factor,
-// FK column (0-based offset of (component, jump), greenFKSpectra.f90:204-212)
-__constant__ int c_sum_kind[14] = {0, 0, 1, 2, 3, 3, 4, 5, 6, 7, 4, 5, 6, 7};
-__constant__ int c_sum_l0[14] = {0, 0, 1, 2, 1, 1, 1, 2, 1, 2, 1, 2, 1, 2};
-__constant__ double c_sum_fac[14] = {0, 0, 2, 2, 0, 0, 2, 2, 2, 4, 2, -2, 2, -4};
-__constant__ int c_sum_col[14] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 8, 9, 6, 7};
+// sums k of source type t (first index: 0 single force, k = 1..7,
+// harmonicDegreeSums.f90:110-171; 1 moment tensor, k = 1..14, :297-351):
+// kind, first l, factor, FK column (0-based offset of (component, jump),
+// greenFKSpectra.f90:204-212, with 2 spheroidal jumps for forces and 4 for moments)
+__constant__ int c_sum_kind[2][14] = {{0, 1, 3, 4, 6, 4, 6}, {0, 0, 1, 2, 3, 3, 4, 5, 6, 7, 4, 5, 6, 7}};
+__constant__ int c_sum_l0[2][14] = {{0, 1, 1, 1, 1, 1, 1}, {0, 0, 1, 2, 1, 1, 1, 2, 1, 2, 1, 2, 1, 2}};
+__constant__ double c_sum_fac[2][14] = {{0, -2, 0, -2, -2, 2, 2}, {0, 0, 2, 2, 0, 0, 2, 2, 2, 4, 2, -2, 2, -4}};
+__constant__ int c_sum_col[2][14] = {{0, 1, 2, 3, 4, 4, 3}, {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 8, 9, 6, 7}};
+// sums of each source type and sums per table kind (host copies of the tables above)
+constexpr int SUMS_OF_TYPE[2] = {7, 14};
+constexpr int SUMS_PER_KIND[2][8] = {{1, 1, 0, 1, 2, 0, 2, 0}, {2, 1, 1, 2, 2, 2, 2, 2}};
+
+// rank of sum k among the sums of its table kind: its row pair within the kind
+__device__ __forceinline__ int sum_rank(int t, int k) {
+  const int kind = c_sum_kind[t][k];
+  int s = 0;
+  for (int q = 0; q < k; ++q) s += c_sum_kind[t][q] == kind;
+  return s;
+}
 
 // ---------------------------------------------------------------------------
 //  Legendre tables (legendreFunctions.f90:48-157), one thread per (station, m)
@@ -83,22 +98,20 @@ __global__ void legendre_kernel(int nsta, int lmax, int lcap, const double* __re
 __global__ void coef_kernel(SynthDev S, const float* __restrict__ gr, const float* __restrict__ gi, double* A) {
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = S.nf2 - S.nf1 + 1;
-  if (idx >= (long long)nf * 14 * S.lcap) return;
+  const int t = S.istyp, nsum = S.nsum;
+  if (idx >= (long long)nf * nsum * S.lcap) return;
   int l = (int)(idx % S.lcap);
-  int k = (int)((idx / S.lcap) % 14);
-  int slot = (int)(idx / ((long long)S.lcap * 14));
+  int k = (int)((idx / S.lcap) % nsum);
+  int slot = (int)(idx / ((long long)S.lcap * nsum));
   const int jf = S.nf1 + slot;
   const int nwn = S.nwn[jf - 1];
-  const int kind = c_sum_kind[k];
-  // rank of sum k among the sums of its kind
-  int s = 0;
-  for (int q = 0; q < k; ++q) s += c_sum_kind[q] == kind;
-  long long row = 2LL * ((long long)slot * S.nsk[kind] + s);
+  const int kind = c_sum_kind[t][k];
+  long long row = 2LL * ((long long)slot * S.nsk[kind] + sum_rank(t, k));
   double* Ar = A + (long long)S.aoff[kind] + row * S.lcap;
   double* Ai = Ar + S.lcap;
   double vr = 0.0, vi = 0.0;
   const int lmaxf = nwn - 1;
-  if (l >= c_sum_l0[k] && l <= lmaxf) {
+  if (l >= c_sum_l0[t][k] && l <= lmaxf) {
     // cos^2 taper of this frequency (harmonicDegreeSums.f90:356-369), TAPFRAC = 0.2
     const double tapfrac = 0.2;
     int jt = (int)floor((double)lmaxf * (1.0 - tapfrac) + 0.5);
@@ -111,10 +124,10 @@ __global__ void coef_kernel(SynthDev S, const float* __restrict__ gr, const floa
       double c = cos((double)(float)l / c1 - c2);
       tap = c * c;
     }
-    const long long o = (long long)S.col_off[c_sum_col[k]] * S.nkf + S.koff[slot] + l;
+    const long long o = (long long)S.col_off[c_sum_col[t][k]] * S.nkf + S.koff[slot] + l;
     double g_r = (double)gr[o], g_i = (double)gi[o];
     double w = 1.0;
-    double fac = c_sum_fac[k];
+    double fac = c_sum_fac[t][k];
     if (fac != 0.0) w = fac / (double)(float)(l * (l + 1));
     double sc = w * (2.0 * (double)l + 1.0) / (4.0 * PI_F) * tap;
     vr = sc * g_r;
@@ -139,18 +152,19 @@ __global__ void coef_kernel(SynthDev S, const float* __restrict__ gr, const floa
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double wn_kernel(int kind, double wn, double b0, double b1, double b2, double re,
                                             double x) {
-  switch (kind) {
-    case 0: return wn * b0;                                         // integrals 1, 2
-    case 1: return 2.0 / re * b1;                                   // 3
+  switch (kind) {   // moment integrals; force integrals (wavenumberIntegrals.f90:160-168)
+    case 0: return wn * b0;                                         // 1, 2;    force 1
+    case 1: return 2.0 / re * b1;                                   // 3;       force -2
     case 2: return wn * 2.0 * b2;                                   // 4
-    case 3: return wn * (-wn * re) * b1;                            // 5, 6
-    case 4: return wn * 2.0 * (b0 - b1 / (wn * x));                 // 7, 11
+    case 3: return wn * (-wn * re) * b1;                            // 5, 6;    force 3
+    case 4: return wn * 2.0 * (b0 - b1 / (wn * x));                 // 7, 11;   force -4, 6
     case 5: return wn * 2.0 * wn * re * (b1 - 2.0 * b2 / (wn * x)); // 8, -12
-    case 6: return wn * 2.0 * b1 / (wn * x);                        // 9, 13
+    case 6: return wn * 2.0 * b1 / (wn * x);                        // 9, 13;   force -5, 7
     default: return wn * 4.0 * wn * re * b2 / (wn * x);             // 10, -14
   }
 }
-__constant__ double c_wn_sign[14] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, -1, 1, -1};
+// sign of each integral's kernel against its kind's table (forces, moments)
+__constant__ double c_wn_sign[2][14] = {{1, -1, 1, -1, -1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, -1, 1, -1}};
 
 struct WnGeom {   // the rule's geometry at distance xx (wavenumberIntegrals.f90:337-348)
   double x, xdk, F;
@@ -209,22 +223,21 @@ __device__ __forceinline__ double wn_taper(int nwn, double dwn, int j) {
 __global__ void bessel_coef_kernel(SynthDev S, const float* __restrict__ gr, const float* __restrict__ gi, double* A) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = S.nf2 - S.nf1 + 1;
-  if (idx >= (long long)nf * 14 * S.lcap) return;
+  const int t = S.istyp, nsum = S.nsum;
+  if (idx >= (long long)nf * nsum * S.lcap) return;
   const int jj = (int)(idx % S.lcap);   // j - 1
-  const int k = (int)((idx / S.lcap) % 14);
-  const int slot = (int)(idx / ((long long)S.lcap * 14));
+  const int k = (int)((idx / S.lcap) % nsum);
+  const int slot = (int)(idx / ((long long)S.lcap * nsum));
   const int nwn = S.nwn[S.nf1 + slot - 1];
-  const int kind = c_sum_kind[k];
-  int s = 0;
-  for (int q = 0; q < k; ++q) s += c_sum_kind[q] == kind;
-  const long long row = 2LL * ((long long)slot * S.nsk[kind] + s);
+  const int kind = c_sum_kind[t][k];
+  const long long row = 2LL * ((long long)slot * S.nsk[kind] + sum_rank(t, k));
   double* Ar = A + (long long)S.aoff[kind] + row * S.lcap;
   double vr = 0.0, vi = 0.0;
   if (jj < nwn) {
-    const long long o = (long long)S.col_off[c_sum_col[k]] * S.nkf + S.koff[slot] + jj;
-    const double t = wn_taper(nwn, S.dwn, jj + 1) * c_wn_sign[k];
-    vr = (double)gr[o] * t;
-    vi = (double)gi[o] * t;
+    const long long o = (long long)S.col_off[c_sum_col[t][k]] * S.nkf + S.koff[slot] + jj;
+    const double tp = wn_taper(nwn, S.dwn, jj + 1) * c_wn_sign[t][k];
+    vr = (double)gr[o] * tp;
+    vi = (double)gi[o] * tp;
   }
   Ar[jj] = vr;
   Ar[S.lcap + jj] = vi;
@@ -235,17 +248,18 @@ __global__ void bessel_corr_kernel(SynthDev S, const float* __restrict__ gr, con
                                    const double* __restrict__ theta, double* C) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = S.nf2 - S.nf1 + 1;
-  if (idx >= (long long)nf * 14 * S.nsta) return;
+  const int t = S.istyp, nsum = S.nsum;
+  if (idx >= (long long)nf * nsum * S.nsta) return;
   const int sta = (int)(idx % S.nsta);
-  const int k = (int)((idx / S.nsta) % 14);
-  const int slot = (int)(idx / ((long long)S.nsta * 14));
+  const int k = (int)((idx / S.nsta) % nsum);
+  const int slot = (int)(idx / ((long long)S.nsta * nsum));
   const int nwn = S.nwn[S.nf1 + slot - 1];
   if (nwn < 2) return;
-  const int kind = c_sum_kind[k];
+  const int kind = c_sum_kind[t][k];
   const double re = S.rearth, dwn = S.dwn;
   const WnGeom g = wn_geom(theta[sta] * re, dwn);
-  const long long o = (long long)S.col_off[c_sum_col[k]] * S.nkf + S.koff[slot];
-  const double sg = c_wn_sign[k];
+  const long long o = (long long)S.col_off[c_sum_col[t][k]] * S.nkf + S.koff[slot];
+  const double sg = c_wn_sign[t][k];
   auto G = [&](int j) { return dz{(double)gr[o + j - 1], (double)gi[o + j - 1]}; };
   auto kern = [&](int j) { return sg * wn_kernel_at(kind, (double)(j - 1) * dwn, g.x, re, false); };
   dz corr{0.0, 0.0};
@@ -262,9 +276,7 @@ __global__ void bessel_corr_kernel(SynthDev S, const float* __restrict__ gr, con
     corr = corr - (G(nwn) * kern(nwn)) * (wn_taper(nwn, dwn, nwn) * 0.5 * dwn);   // trapezoid end
   }
   corr = corr * (re * re / (2.0 * PI_F));
-  int s = 0;
-  for (int q = 0; q < k; ++q) s += c_sum_kind[q] == kind;
-  const long long row = 2LL * ((long long)slot * S.nsk[kind] + s);
+  const long long row = 2LL * ((long long)slot * S.nsk[kind] + sum_rank(t, k));
   double* Ck = C + S.coff[kind];
   Ck[row * S.nsta + sta] += corr.re;
   Ck[(row + 1) * S.nsta + sta] += corr.im;
@@ -342,12 +354,11 @@ __global__ void spectra_kernel(SynthDev S, const double* __restrict__ C, const d
   const int sta = (int)(idx % S.nsta);
   const int slot = (int)(idx / S.nsta);
   const int jf = S.nf1 + slot;
+  const int t = S.istyp;
   dz w[15];
-  for (int k = 0; k < 14; ++k) {
-    int kind = c_sum_kind[k];
-    int s = 0;
-    for (int q = 0; q < k; ++q) s += c_sum_kind[q] == kind;
-    long long row = 2LL * ((long long)slot * S.nsk[kind] + s);
+  for (int k = 0; k < S.nsum; ++k) {
+    int kind = c_sum_kind[t][k];
+    long long row = 2LL * ((long long)slot * S.nsk[kind] + sum_rank(t, k));
     const double* Ck = C + S.coff[kind];
     w[k + 1] = dz{Ck[row * S.nsta + sta], Ck[(row + 1) * S.nsta + sta]};
   }
@@ -359,15 +370,23 @@ __global__ void spectra_kernel(SynthDev S, const double* __restrict__ C, const d
   const dz ef = dz{evf[jf].x, evf[jf].y};
   dz tsf = zexp_dev(((ci * TWO_PI_F) * (double)(jf - 1)) * S.df * S.tred) * exp(S.sigma * S.tred);
   for (int im = 0; im < S.nmt; ++im) {
-    const double* m = mt + im * 6;
-    double t1 = m[3] * cphi + m[4] * sphi;
-    double t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
-    double t3 = m[4] * cphi - m[3] * sphi;
-    double t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
     dz z[3];
-    z[0] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
-    z[1] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
-    z[2] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+    if (t == 1) {   // momentSingleFrequencyDisplacement (singleFrequencyDisplacement.f90:108-125)
+      const double* m = mt + im * 6;
+      double t1 = m[3] * cphi + m[4] * sphi;
+      double t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
+      double t3 = m[4] * cphi - m[3] * sphi;
+      double t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
+      z[0] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
+      z[1] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
+      z[2] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+    } else {        // forceSingleFrequencyDisplacement (singleFrequencyDisplacement.f90:35-46), (Fr, Ft, Ff)
+      const double* f = mt + im * 3;
+      const double fh = f[1] * cphi + f[2] * sphi;
+      z[0] = w[1] * f[0] + w[2] * fh;
+      z[1] = w[3] * f[0] + (w[4] + w[5]) * fh;
+      z[2] = (w[6] + w[7]) * (f[1] * sphi - f[2] * cphi);
+    }
     for (int c = 0; c < 3; ++c) z[c] = ((z[c] * ef) * dz{1.0, 0.0}) * tsf;
     if (S.velocity) {
       dz zom{TWO_PI_F * (double)(jf - 1) * S.df, -S.sigma};
@@ -546,11 +565,14 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
                                     const double* propdir, int nmt, const double* mt, float* d_traces,
                                     void* stream) {
   if (!ctx || !p || !nwn || !theta || !phi || !propdir || !mt) return GEM_ERROR;
-  if (p->istyp != 1) return gem_set_error(ctx, "synthetics: only moment-tensor sources are supported");
+  if (p->istyp != 1 && p->istyp != 0) return gem_set_error(ctx, "synthetics: source type must be 0 (force) or 1 (moment)");
   if (p->global_ != 1 && p->global_ != 0) return gem_set_error(ctx, "synthetics: GLOBAL must be 0 or 1");
   if (p->global_ == 0 && (!(p->dwn > 0) || !(p->rearth > 0)))
     return gem_set_error(ctx, "synthetics: the regional mode needs the wavenumber spacing and the earth radius");
-  if (p->nsp < 10) return gem_set_error(ctx, "synthetics: expected the 10 moment spectra U,V (4 jumps) and W (2 jumps)");
+  if (p->istyp == 1 && p->nsp < 10)
+    return gem_set_error(ctx, "synthetics: expected the 10 moment spectra U,V (4 jumps) and W (2 jumps)");
+  if (p->istyp == 0 && p->nsp < 5)
+    return gem_set_error(ctx, "synthetics: expected the 5 force spectra U,V (2 jumps) and W (1 jump)");
   if (nsta < 1 || nmt < 1 || p->nf1 < 2 || p->nf2 < p->nf1 || p->nwnmax < 3) return gem_set_error(ctx, "synthetics: invalid sizes");
   cudaStream_t st = (cudaStream_t)stream;
   // ---- time axis (frequencyTime.f90:55-84)
@@ -563,8 +585,10 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   S.nf1 = p->nf1; S.nf2 = p->nf2; S.nsta = nsta; S.nmt = nmt; S.lmax = p->nwnmax - 1; S.lcap = p->nwnmax;
   S.nkf = p->nkfmax; S.df = p->df; S.sigma = p->sigma; S.tred = p->tred; S.velocity = p->velocity;
   S.dwn = p->dwn; S.rearth = p->rearth;
+  S.istyp = p->istyp; S.nsum = SUMS_OF_TYPE[p->istyp];
+  const int nfo = p->istyp == 1 ? 6 : 3;   // moment tensor elements or force components per source
   S.ns = ns; S.nslog = nslog; S.nsamp = p->nsamp; S.ndec = ndec; S.ldx = p->nf2;
-  const int nsk_h[8] = {2, 1, 1, 2, 2, 2, 2, 2};
+  const int* nsk_h = SUMS_PER_KIND[p->istyp];
   const int nf = p->nf2 - p->nf1 + 1;
   long long ao = 0, co = 0;
   for (int k = 0; k < 8; ++k) {
@@ -606,7 +630,7 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
                             (size_t)co * sizeof(double), (size_t)ntr * S.ldx * sizeof(double2),
                             evf.size() * sizeof(double2), tw.size() * sizeof(double2), fac.size() * sizeof(double),
                             (size_t)p->nf2 * sizeof(int), (size_t)nf * sizeof(int), nsta * sizeof(double),
-                            nsta * sizeof(double), nsta * sizeof(double), (size_t)nmt * 6 * sizeof(double),
+                            nsta * sizeof(double), nsta * sizeof(double), (size_t)nmt * nfo * sizeof(double),
                             fast_fft ? (size_t)ns * sizeof(double2) : 0};
   size_t total = 0;
   for (size_t z : sizes) total += (z + 255) / 256 * 256;
@@ -628,12 +652,12 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   cudaMemcpyAsync(b.theta, theta, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b.phi, phi, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b.propdir, propdir, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(b.mt, mt, (size_t)nmt * 6 * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(b.mt, mt, (size_t)nmt * nfo * sizeof(double), cudaMemcpyHostToDevice, st);
   S.nwn = b.nwn; S.koff = b.koff;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
-  long long ncoef = (long long)nf * 14 * S.lcap;
+  long long ncoef = (long long)nf * S.nsum * S.lcap;
   if (p->global_ == 1) {
     legendre_kernel<<<(nsta * 3 + 127) / 128, 128, 0, st>>>(nsta, S.lmax, S.lcap, b.theta, b.tab);
     coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
@@ -644,7 +668,7 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   }
   if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST) {
     // split-precision products on the tensor cores (FP16 hi/lo operands, FP32 accumulation)
-    const long long mtot = 2LL * nf * 14;
+    const long long mtot = 2LL * nf * S.nsum;
     const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
     void* ws = gem_ctx_aux(ctx, 3, wsb);
     if (!ws) return GEM_ERROR;
@@ -655,7 +679,7 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
     sums_gemm_kernel<<<g, 256, 0, st>>>(S, b.A, b.tab, b.C);
   }
   if (p->global_ == 0) {
-    const long long ncorr = (long long)nf * 14 * nsta;
+    const long long ncorr = (long long)nf * S.nsum * nsta;
     bessel_corr_kernel<<<(unsigned)((ncorr + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.theta, b.C);
   }
   long long nsp_ = (long long)nsta * nf;

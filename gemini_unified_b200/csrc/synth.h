@@ -11,6 +11,7 @@ struct SynthDev {
   long long ldx;            // complex elements between consecutive spectra of the FFT input
   double df, sigma, tred;
   double dwn, rearth;       // regional mode: wavenumber spacing, earth radius
+  int istyp, nsum;          // source type (0 force, 1 moment tensor) and its number of sums
   int nsk[8];               // sums per Legendre table kind
   long long aoff[8], coff[8];   // offsets of each kind's coefficient and result matrices
   int col_off[10];          // FK column of each (component, jump) spectrum

@@ -95,12 +95,14 @@ class SynthParams(ctypes.Structure):
 
 
 def synth_params(grid, nsp, nsamp, dt, filspecs, velocity=False, tred=0.0, global_=1,
-                 rearth=6371000.0) -> SynthParams:
+                 rearth=6371000.0, source_type="MOMENT") -> SynthParams:
     """Parameters as computeSyntheticSeismograms reads them back from the FK file:
     df, sigma, dwn and the earth radius are stored as float32
-    (computeGreenFKSpectraForSynthetics.f90:261-263)."""
+    (computeGreenFKSpectraForSynthetics.f90:261-263).  source_type "MOMENT"
+    (istyp 1, sources are moment tensors) or "FORCE" (istyp 0, single forces)."""
     f32 = lambda v: float(np.float32(v))
-    return SynthParams(grid.nf1, grid.nf2, int(grid.nwnmax), int(grid.nkfmax), nsp, 1, int(global_), f32(grid.df),
+    istyp = {"FORCE": 0, "MOMENT": 1}[source_type]
+    return SynthParams(grid.nf1, grid.nf2, int(grid.nwnmax), int(grid.nkfmax), nsp, istyp, int(global_), f32(grid.df),
                        f32(grid.sigma), int(nsamp), float(dt), 1 if velocity else 0, float(tred),
                        int(round(filspecs[0])), float(filspecs[1]), int(round(filspecs[2])), float(filspecs[3]),
                        f32(grid.dwn), f32(rearth))
@@ -234,14 +236,16 @@ class GeminiFK:
         self._check(lib().gem_fk_graph_launch(self._h, stream or None))
 
     def synthetics(self, sp: SynthParams, nwn, gfkr, gfki, theta, phi, propdir, mt):
-        """Seismograms of all stations x moment tensors: float32 [nsta, nmt, 3 (Z,N,E), nsamp].
+        """Seismograms of all stations x sources: float32 [nsta, nsrc, 3 (Z,N,E), nsamp].
 
-        gfkr/gfki: float32 FK spectra of the source node, shaped (nsp, nkfmax)."""
+        gfkr/gfki: float32 FK spectra of the source node, shaped (nsp, nkfmax).
+        mt: moment tensors (nsrc, 6) for sp.istyp 1, forces (nsrc, 3) as
+        (Fr, Ft, Ff) for sp.istyp 0."""
         gr = np.ascontiguousarray(gfkr, np.float32); gi = np.ascontiguousarray(gfki, np.float32)
         nwn = np.ascontiguousarray(nwn, np.int32)
         th = np.ascontiguousarray(theta, np.float64); ph = np.ascontiguousarray(phi, np.float64)
         pd = np.ascontiguousarray(propdir, np.float64)
-        mt = np.ascontiguousarray(mt, np.float64).reshape(-1, 6)
+        mt = np.ascontiguousarray(mt, np.float64).reshape(-1, 6 if sp.istyp == 1 else 3)
         out = np.zeros((len(th), len(mt), 3, sp.nsamp), np.float32)
         self._check(lib().gem_synth_run(self._h, ctypes.byref(sp), _ptr(nwn), _ptr(gr), _ptr(gi), len(th), _ptr(th),
                                         _ptr(ph), _ptr(pd), len(mt), _ptr(mt), _ptr(out)))

@@ -2,8 +2,9 @@
 
     python -m gemini_unified_b200.synth_run --workload batched_fk --repeat 3
 
-The command-line counterpart of computeSyntheticSeismograms for moment-tensor
-sources (all stations of the workload, six unit moment tensors).  The FK
+The command-line counterpart of computeSyntheticSeismograms (all stations of
+the workload; six unit moment tensors, or with ``--source FORCE`` three unit
+forces Fr, Ft, Ff).  The FK
 spectra are seeded synthetic coefficients with the shape of the workload's
 spectra: amplitudes log-normal with log10|c| ~ N(-3, 1) clipped to [-6, 0]
 and uniform phases (``fk_coefficients``).  Prints one JSON line with the
@@ -13,6 +14,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import dataclasses
 import json
 
 import numpy as np
@@ -38,18 +40,21 @@ def main(argv=None):
     ap.add_argument("--backend", type=int, default=2, choices=[1, 2],
                     help="1 FP64 degree sums, 2 sliced-integer tensor-core degree sums")
     ap.add_argument("--check", action="store_true", help="also run the FP64 form and report the relative error")
+    ap.add_argument("--source", default="MOMENT", choices=["MOMENT", "FORCE"])
     a = ap.parse_args(argv)
     w = configs.WORKLOADS[a.workload]
     m = w.model()
     g = M.frequency_grid(w.params, m.rearth)
-    nsp = M.nsp_for(w.params)
+    params = dataclasses.replace(w.params, source_type=a.source)
+    nsp = M.nsp_for(params)
     gr, gi = fk_coefficients(nsp, int(g.nkfmax))
     theta, phi, propdir = w.stations()
     if a.stations:
         theta, phi, propdir = theta[: a.stations], phi[: a.stations], propdir[: a.stations]
     theta, phi, propdir = (np.ascontiguousarray(x) for x in (theta, phi, propdir))
-    mt = np.ascontiguousarray(configs.unit_moment_tensors(), np.float64)
-    sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs, global_=w.params.global_, rearth=m.rearth)
+    mt = np.ascontiguousarray(configs.unit_moment_tensors() if a.source == "MOMENT" else np.eye(3), np.float64)
+    sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs, global_=w.params.global_, rearth=m.rearth,
+                      source_type=a.source)
     nwn = np.ascontiguousarray(g.nwn, np.int32)
     d_gr = torch.from_numpy(gr).cuda()
     d_gi = torch.from_numpy(gi).cuda()
@@ -73,7 +78,7 @@ def main(argv=None):
 
     out, ms = run(a.backend, a.repeat)
     ntr = len(theta) * len(mt)
-    res = {"workload": a.workload, "backend": a.backend, "stations": len(theta), "moment_tensors": len(mt),
+    res = {"workload": a.workload, "backend": a.backend, "source": a.source, "stations": len(theta), "sources": len(mt),
            "traces": ntr, "nsamp": w.nsamp, "synth_ms": ms, "traces_per_s": ntr / (min(ms) / 1e3),
            "finite": bool(torch.isfinite(out).all().item())}
     if a.check:

@@ -84,7 +84,7 @@ typedef struct gem_synth_params {
   int nf1, nf2, nwnmax;   /* frequency range and largest number of degrees */
   long long nkfmax;       /* wavenumber-frequency extent of the FK spectra */
   int nsp;                /* spectra per node (10: U, V x 4 jumps, W x 2 jumps) */
-  int istyp;              /* 1 MOMENT (only moment tensors are supported) */
+  int istyp;              /* 1 MOMENT (sources: moment tensors [6]), 0 FORCE (forces [3]: Fr, Ft, Ff) */
   int global_;            /* 1: spherical harmonics (Legendre), 0: wavenumber integrals (Bessel) */
   double df, sigma;
   int nsamp;              /* power of two */
@@ -147,8 +147,11 @@ int gem_fk_graph_launch(gem_ctx* ctx, void* stream);
  * (computeSyntheticSeismograms.f90:311-388).  gfkr/gfki: float32 FK spectra
  * of the node in the file layout (nkfmax, nsp); nwn[jf-1] for jf = 1..nf2;
  * theta = epicentral distance (rad), phi = azimuth at the source, propdir =
- * propagation direction at the receiver (rad); mt[nmt][6] = (Mrr, Mtt, Mff,
- * Mrt, Mrf, Mtf).  traces[((sta*nmt + imt)*3 + comp)*nsamp + i], comp Z, N, E.
+ * propagation direction at the receiver (rad); for p->istyp 1 mt[nmt][6] =
+ * (Mrr, Mtt, Mff, Mrt, Mrf, Mtf) and the 10 moment spectra (nsp >= 10), for
+ * p->istyp 0 mt[nmt][3] = (Fr, Ft, Ff) and the 5 force spectra (nsp >= 5;
+ * forceHarmonicDegreeSums, forceSingleFrequencyDisplacement).
+ * traces[((sta*nmt + imt)*3 + comp)*nsamp + i], comp Z, N, E.
  * Host buffers, blocking. */
 int gem_synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* gfkr, const float* gfki,
                   int nsta, const double* theta, const double* phi, const double* propdir, int nmt,

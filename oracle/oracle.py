@@ -67,6 +67,15 @@ def lib():
         L.oracle_freq_time.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                        ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_double,
                                        ctypes.c_void_p]
+        L.oracle_wavenumber_integrals_src.argtypes = [ctypes.c_int] + L.oracle_wavenumber_integrals.argtypes
+        L.oracle_degree_sums_force.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_synthetics_src.argtypes = ([ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 4
+                                            + [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_int] + [ctypes.c_void_p] * 3
+                                            + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_void_p])
         L.oracle_degree_sums.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_void_p]
@@ -241,3 +250,52 @@ def synthetics(nf1, nf2, nwn, nwnmax, df, sigma, gr, gi, theta, phi, propdir, mt
     if rc:
         raise RuntimeError("oracle_synthetics failed")
     return tr.reshape(len(th), len(mt), 3, nsamp)
+
+
+def force_degree_sums(nf1, nf2, nwn, nwnmax, gr, gi, theta):
+    """The 7 force degree sums: gr/gi float32 [nsp >= 5, nkfmax].  complex [nsta, nf2, 7]."""
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkf = gr.shape
+    th = np.ascontiguousarray(theta, np.float64)
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    hd = np.zeros(len(th) * nf2 * 7 * 2)
+    rc = lib().oracle_degree_sums_force(nf1, nf2, _p(nwn), nwnmax, nkf, nsp, _p(gr), _p(gi), len(th), _p(th), _p(hd))
+    if rc:
+        raise RuntimeError("oracle_degree_sums_force failed")
+    return hd.view(np.complex128).reshape(len(th), nf2, 7)
+
+
+def force_wavenumber_integrals(nf1, nf2, nwn, nwnmax, gr, gi, dwn, rearth, x):
+    """The 7 force wavenumber integrals (regional mode): complex [nsta, nf2, 7]; x in m."""
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkf = gr.shape
+    x = np.ascontiguousarray(x, np.float64)
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    hd = np.zeros(len(x) * nf2 * 7 * 2)
+    rc = lib().oracle_wavenumber_integrals_src(0, nf1, nf2, _p(nwn), nwnmax, nkf, nsp, _p(gr), _p(gi), dwn, rearth,
+                                               len(x), _p(x), _p(hd))
+    if rc:
+        raise RuntimeError("oracle_wavenumber_integrals_src failed")
+    return hd.view(np.complex128).reshape(len(x), nf2, 7)
+
+
+def synthetics_src(source_type, global_, nf1, nf2, nwn, nwnmax, df, sigma, dwn, rearth, gr, gi, theta, phi, propdir,
+                   src, filspecs, velocity, tred, nsamp, dt):
+    """Synthetics of either source type ("MOMENT": src (nsrc, 6); "FORCE": src (nsrc, 3)
+    as Fr, Ft, Ff) and either mode (global_ 1 degree sums, 0 wavenumber integrals at
+    distance theta * rearth).  float32 [nsta, nsrc, 3, nsamp]."""
+    istyp = {"FORCE": 0, "MOMENT": 1}[source_type]
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkf = gr.shape
+    th = np.ascontiguousarray(theta, np.float64); ph = np.ascontiguousarray(phi, np.float64)
+    pd = np.ascontiguousarray(propdir, np.float64)
+    src = np.ascontiguousarray(src, np.float64).reshape(-1, 6 if istyp == 1 else 3)
+    fs = np.ascontiguousarray(filspecs, np.float64)
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    out = np.zeros((len(th), len(src), 3, nsamp), np.float32)
+    rc = lib().oracle_synthetics_src(istyp, int(global_), nf1, nf2, _p(nwn), nwnmax, df, sigma, dwn, rearth, nkf, nsp,
+                                     _p(gr), _p(gi), len(th), _p(th), _p(ph), _p(pd), len(src), _p(src), _p(fs),
+                                     int(velocity), tred, nsamp, dt, _p(out))
+    if rc:
+        raise RuntimeError("oracle_synthetics_src failed (%d)" % rc)
+    return out

@@ -111,6 +111,32 @@ const SumDef MSUM[14] = {
     {2, 1, 1, 2.0, 7, 1},  {2, 2, 2, 4.0, 7, 2},  {1, 1, 1, 2.0, 7, 1},  {1, 2, 2, -2.0, 7, 2},
     {2, 1, 1, 2.0, 3, 3},  {2, 2, 2, -4.0, 3, 4}};
 
+// table kind and factor of the 7 force sums (harmonicDegreeSums.f90:110-171):
+// kint 1 P_l0 U1, 2 P_l1 (-2/elp1) U2, 3 dpdt_l0 V1, 4 dpdt_l1 (-2/elp1) V2,
+// 5 pdst_l1 (-2/elp1) W1, 6 dpdt_l1 (+2/elp1) W1, 7 pdst_l1 (+2/elp1) V2
+const SumDef FSUM[7] = {
+    {0, 0, 0, 0.0, 1, 1}, {0, 1, 1, -2.0, 1, 2}, {1, 0, 1, 0.0, 3, 1}, {1, 1, 1, -2.0, 3, 2},
+    {2, 1, 1, -2.0, 7, 1}, {1, 1, 1, 2.0, 7, 1}, {2, 1, 1, 2.0, 3, 2}};
+
+// forceHarmonicDegreeSums for kint 1..7: T (fnum/elp1) G (2l+1)/4pi taper
+zc forceSum(int kint, const float* gr, const float* gi, int nwn, const Legendre& alf, const std::vector<double>& tap) {
+  const SumDef& s = FSUM[kint - 1];
+  const std::vector<double>& T =
+      s.kind == 0 ? alf.plm[s.m] : (s.kind == 1 ? alf.dpdt[s.m] : alf.pdst[s.m]);
+  double fourpi = 4.0 * PI_F;
+  int lmax = nwn - 1;
+  zc z = Z(0.0);
+  for (int l = s.l0; l <= lmax; ++l) {
+    zc g = Z((double)gr[l], (double)gi[l]);
+    zc t;
+    if (s.fnum == 0.0) t = T[l] * g;
+    else t = (T[l] * (s.fnum / (double)(float)(l * (l + 1)))) * g;
+    t = ((t * (2.0 * (double)l + 1.0)) / fourpi) * tap[l];
+    z = z + t;
+  }
+  return z;
+}
+
 // momentHarmonicDegreeSums for kint 1..14 over lmax = nwn-1 terms
 zc momentSum(int kint, const float* gr, const float* gi, int nwn, const Legendre& alf,
              const std::vector<double>& tap) {
@@ -268,6 +294,22 @@ double wnKernel(int kint, double wn, double b0, double b1, double b2, double re,
   }
 }
 
+// integrand factor of force integral kint (1..7) (wavenumberIntegrals.f90:160-168, 172-180)
+double wnKernelForce(int kint, double wn, double b0, double b1, double b2, double re, double x) {
+  (void)b2;
+  switch (kint) {
+    case 1: return wn * b0;
+    case 2: return -2 * b1 / re;
+    case 3: return -wn * wn * b1 * re;
+    case 4: return -2. * wn * (b0 - b1 / (wn * x));
+    case 5: return -2. * wn * b1 / (wn * x);
+    case 6: return +2. * wn * (b0 - b1 / (wn * x));
+    default: return +2. * wn * b1 / (wn * x);   // 7
+  }
+}
+
+typedef double (*WnKernelFn)(int, double, double, double, double, double, double);
+
 // cos^2 taper of the wavenumber integrals (wavenumberIntegrals.f90:480-491), 1-based g[j]
 void taperWn(int nwn, double dwn, double tapfrac, std::vector<double>& g) {
   int jt = std::min((int)std::lround((double)nwn * (1.0 - tapfrac)), nwn);
@@ -280,20 +322,20 @@ void taperWn(int nwn, double dwn, double tapfrac, std::vector<double>& g) {
 
 // momentWavenumberIntegrals (wavenumberIntegrals.f90:320-475) for one frequency:
 // G 1-based [1..nwn] of the integral's FK column, J the Bessel table of distance xx
-zc momentWavenumberIntegral(int kint, const std::vector<zc>& G, int nwn, double dwn, double re, double xx,
-                            const std::vector<double>& J, const std::vector<double>& tap) {
+zc wavenumberIntegral(WnKernelFn kernfn, int kint, const std::vector<zc>& G, int nwn, double dwn, double re,
+                      double xx, const std::vector<double>& J, const std::vector<double>& tap) {
   double x = xx < 3.0 / (dwn * 1.e9) ? 3.0 / (dwn * 1.e9) : xx;
   double wn3 = 3.0 / x;
   int j3 = (int)(wn3 / dwn) + 2;
   wn3 = (double)(j3 - 1) * dwn;
   auto wnb = [&](int j) {
     double wn = (double)(j - 1) * dwn;
-    return wnKernel(kint, wn, J[3 * (j - 1)], J[3 * (j - 1) + 1], J[3 * (j - 1) + 2], re, x);
+    return kernfn(kint, wn, J[3 * (j - 1)], J[3 * (j - 1) + 1], J[3 * (j - 1) + 2], re, x);
   };
   auto ybes = [&](double w) {
     double y0v = ::y0(w * x), y1v = ::y1(w * x);
     double y2v = -y0v + 2.0 / (w * x) * y1v;
-    return wnKernel(kint, w, y0v, y1v, y2v, re, x);
+    return kernfn(kint, w, y0v, y1v, y2v, re, x);
   };
   double wn3besy = ybes(wn3);
   int j33 = std::min(j3, nwn);
@@ -318,13 +360,16 @@ zc momentWavenumberIntegral(int kint, const std::vector<zc>& G, int nwn, double 
 
 extern "C" {
 
-// Wavenumber integrals of the regional mode: hd[(sta*nf2 + jf-1)*14 + k] complex
-// interleaved for the 14 moment integrals; x: distances in m.
-int oracle_wavenumber_integrals(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp,
-                                const float* gr, const float* gi, double dwn, double rearth, int nsta,
-                                const double* x, double* hd) {
-  static const int col[14] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 8, 9, 6, 7};   // FK column of each integral
-  if (nsp < 10) return 2;
+// Wavenumber integrals of the regional mode: hd[(sta*nf2 + jf-1)*nsum + k] complex
+// interleaved for the 14 moment (istyp 1) or 7 force (istyp 0) integrals; x: distances in m.
+int oracle_wavenumber_integrals_src(int istyp, int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp,
+                                    const float* gr, const float* gi, double dwn, double rearth, int nsta,
+                                    const double* x, double* hd) {
+  static const int mcol[14] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 8, 9, 6, 7};   // FK column of each integral
+  static const int fcol[7] = {0, 1, 2, 3, 4, 4, 3};
+  const int nsum = istyp == 1 ? 14 : 7;
+  const int* col = istyp == 1 ? mcol : fcol;
+  if (nsp < (istyp == 1 ? 10 : 5)) return 2;
   std::vector<int> koff(nf2 + 1, 0);
   long long k = 0;
   for (int jf = nf1; jf <= nf2; ++jf) { koff[jf] = (int)k; k += nwn[jf - 1]; }
@@ -336,12 +381,12 @@ int oracle_wavenumber_integrals(int nf1, int nf2, const int* nwn, int nwnmax, in
     for (int jf = nf1; jf <= nf2; ++jf) {
       const int n = nwn[jf - 1];
       taperWn(n, dwn, 0.2, tap);
-      for (int kk = 1; kk <= 14; ++kk) {
+      for (int kk = 1; kk <= nsum; ++kk) {
         G.assign(n + 1, Z(0.0));
         const long long o = (long long)col[kk - 1] * nkfmax + koff[jf];
         for (int j = 1; j <= n; ++j) G[j] = Z((double)gr[o + j - 1], (double)gi[o + j - 1]);
-        zc z = momentWavenumberIntegral(kk, G, n, dwn, rearth, x[is], J, tap);
-        double* h = hd + (((size_t)is * nf2 + (jf - 1)) * 14 + (kk - 1)) * 2;
+        zc z = wavenumberIntegral(istyp == 1 ? wnKernel : wnKernelForce, kk, G, n, dwn, rearth, x[is], J, tap);
+        double* h = hd + (((size_t)is * nf2 + (jf - 1)) * nsum + (kk - 1)) * 2;
         h[0] = z.re; h[1] = z.im;
       }
     }
@@ -349,6 +394,11 @@ int oracle_wavenumber_integrals(int nf1, int nf2, const int* nwn, int nwnmax, in
   return 0;
 }
 
+int oracle_wavenumber_integrals(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp,
+                                const float* gr, const float* gi, double dwn, double rearth, int nsta,
+                                const double* x, double* hd) {
+  return oracle_wavenumber_integrals_src(1, nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, dwn, rearth, nsta, x, hd);
+}
 
 // Legendre tables for the unit tests: out[kind*3*(lmax+1) + m*(lmax+1) + l], kinds
 // plm, dpdt, pdst, d2pdt2, dtpdst.
@@ -419,6 +469,32 @@ int oracle_degree_sums(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax,
   return 0;
 }
 
+// Force degree sums: hd[(sta*nf2 + jf-1)*7 + k] complex interleaved (5 force FK spectra U, V x 2 jumps, W).
+int oracle_degree_sums_force(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp,
+                             const float* gr, const float* gi, int nsta, const double* theta, double* hd) {
+  auto offset = [](int comp, int jump) { return comp == 1 ? jump : (comp == 3 ? 2 + jump : 4 + jump); };
+  for (int is = 0; is < nsta; ++is) {
+    Legendre alf;
+    computeLegendre(nwnmax - 1, theta[is], alf);
+    int nwe = 0;
+    for (int jf = nf1; jf <= nf2; ++jf) {
+      int nwa = nwe + 1;
+      nwe = nwe + nwn[jf - 1];
+      std::vector<double> tap;
+      taper(nwn[jf - 1] - 1, 0.2, tap);
+      for (int k = 1; k <= 7; ++k) {
+        int col = offset(FSUM[k - 1].comp, FSUM[k - 1].jump) - 1;
+        if (col >= nsp) return 2;
+        zc z = forceSum(k, gr + (size_t)col * nkfmax + (nwa - 1), gi + (size_t)col * nkfmax + (nwa - 1),
+                        nwn[jf - 1], alf, tap);
+        size_t o = (((size_t)is * nf2 + (jf - 1)) * 7 + (k - 1)) * 2;
+        hd[o] = z.re; hd[o + 1] = z.im;
+      }
+    }
+  }
+  return 0;
+}
+
 // Full phase 2 for moment tensor sources: traces[((sta*nmt + imt)*3 + comp)*nsamp + i]
 // comp order Z, N, E.  filspecs = {nord_hp, fc_hp, nord_lp, fc_lp}.
 }  // extern "C"
@@ -426,9 +502,10 @@ int oracle_degree_sums(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax,
 namespace {
 // displacement spectra from the 14 sums or integrals hd, filters, rotation and
 // inverse FFT of every station and moment tensor (computeSyntheticSeismograms.f90:336-390)
-int synth_from_sums(const std::vector<double>& hd, int nf1, int nf2, double df, double sigma, int nsta,
+int synth_from_sums(int istyp, const std::vector<double>& hd, int nf1, int nf2, double df, double sigma, int nsta,
                     const double* phi, const double* propdir, int nmt, const double* mt, const double* filspecs,
                     int velocity, double tred, int nsamp, double dt, float* traces) {
+  const int nsum = istyp == 1 ? 14 : 7;
   int rc = 0;
   std::vector<zc> evf;
   eventFilter((int)std::lround(filspecs[0]), filspecs[1], (int)std::lround(filspecs[2]), filspecs[3],
@@ -439,21 +516,28 @@ int synth_from_sums(const std::vector<double>& hd, int nf1, int nf2, double df, 
     double s2phi = std::sin((double)2.0f * phi[is]), c2phi = std::cos((double)2.0f * phi[is]);
     double ca = std::cos(propdir[is]), sa = std::sin(propdir[is]);
     for (int im = 0; im < nmt; ++im) {
-      const double* m = mt + im * 6;
+      const double* m = mt + im * (istyp == 1 ? 6 : 3);
       std::vector<zc> zsp[3];
       for (int c = 0; c < 3; ++c) zsp[c].assign(nf2 + 1, Z(0.0));
       for (int jf = nf1; jf <= nf2; ++jf) {
-        const double* h = &hd[(((size_t)is * nf2 + (jf - 1)) * 14) * 2];
+        const double* h = &hd[(((size_t)is * nf2 + (jf - 1)) * nsum) * 2];
         zc w[15];
-        for (int k = 1; k <= 14; ++k) w[k] = Z(h[(k - 1) * 2], h[(k - 1) * 2 + 1]);
-        // singleFrequencyDisplacement.f90:108-125
-        double t1 = m[3] * cphi + m[4] * sphi;
-        double t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
-        double t3 = m[4] * cphi - m[3] * sphi;
-        double t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
-        zsp[0][jf] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
-        zsp[1][jf] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
-        zsp[2][jf] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+        for (int k = 1; k <= nsum; ++k) w[k] = Z(h[(k - 1) * 2], h[(k - 1) * 2 + 1]);
+        if (istyp == 1) {
+          // momentSingleFrequencyDisplacement (singleFrequencyDisplacement.f90:108-125)
+          double t1 = m[3] * cphi + m[4] * sphi;
+          double t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
+          double t3 = m[4] * cphi - m[3] * sphi;
+          double t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
+          zsp[0][jf] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
+          zsp[1][jf] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
+          zsp[2][jf] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+        } else {
+          // forceSingleFrequencyDisplacement (singleFrequencyDisplacement.f90:35-46)
+          zsp[0][jf] = w[1] * m[0] + w[2] * (m[1] * cphi + m[2] * sphi);
+          zsp[1][jf] = w[3] * m[0] + (w[4] + w[5]) * (m[1] * cphi + m[2] * sphi);
+          zsp[2][jf] = (w[6] + w[7]) * (m[1] * sphi - m[2] * cphi);
+        }
       }
       for (int jf = nf1; jf <= nf2; ++jf) {
         zc tsf = zexp(((ci * TWO_PI_F) * (double)(jf - 1)) * df * tred) * std::exp(sigma * tred);
@@ -491,8 +575,33 @@ int oracle_synthetics(int nf1, int nf2, const int* nwn, int nwnmax, double df, d
   std::vector<double> hd((size_t)nsta * nf2 * 14 * 2, 0.0);
   int rc = oracle_degree_sums(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, nsta, theta, hd.data());
   if (rc) return rc;
-  return synth_from_sums(hd, nf1, nf2, df, sigma, nsta, phi, propdir, nmt, mt, filspecs, velocity, tred, nsamp, dt,
+  return synth_from_sums(1, hd, nf1, nf2, df, sigma, nsta, phi, propdir, nmt, mt, filspecs, velocity, tred, nsamp, dt,
                          traces);
+}
+
+// Synthetics of either source type (istyp 1 moment tensors [nsrc][6], 0 forces
+// [nsrc][3] as Fr, Ft, Ff) in either mode (global 1: degree sums at colatitudes
+// theta; 0: wavenumber integrals at distances theta * rearth).
+int oracle_synthetics_src(int istyp, int global, int nf1, int nf2, const int* nwn, int nwnmax, double df,
+                          double sigma, double dwn, double rearth, int nkfmax, int nsp, const float* gr,
+                          const float* gi, int nsta, const double* theta, const double* phi, const double* propdir,
+                          int nsrc, const double* src, const double* filspecs, int velocity, double tred, int nsamp,
+                          double dt, float* traces) {
+  const int nsum = istyp == 1 ? 14 : 7;
+  std::vector<double> hd((size_t)nsta * nf2 * nsum * 2, 0.0);
+  int rc;
+  if (global == 1) {
+    rc = istyp == 1 ? oracle_degree_sums(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, nsta, theta, hd.data())
+                    : oracle_degree_sums_force(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, nsta, theta, hd.data());
+  } else {
+    std::vector<double> x(nsta);
+    for (int i = 0; i < nsta; ++i) x[i] = theta[i] * rearth;
+    rc = oracle_wavenumber_integrals_src(istyp, nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, dwn, rearth, nsta,
+                                         x.data(), hd.data());
+  }
+  if (rc) return rc;
+  return synth_from_sums(istyp, hd, nf1, nf2, df, sigma, nsta, phi, propdir, nsrc, src, filspecs, velocity, tred,
+                         nsamp, dt, traces);
 }
 
 // Synthetics of the regional mode (wavenumber integrals at distances theta * rearth,
@@ -508,7 +617,7 @@ int oracle_synthetics_bessel(int nf1, int nf2, const int* nwn, int nwnmax, doubl
   int rc = oracle_wavenumber_integrals(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, dwn, rearth, nsta, x.data(),
                                        hd.data());
   if (rc) return rc;
-  return synth_from_sums(hd, nf1, nf2, df, sigma, nsta, phi, propdir, nmt, mt, filspecs, velocity, tred, nsamp, dt,
+  return synth_from_sums(1, hd, nf1, nf2, df, sigma, nsta, phi, propdir, nmt, mt, filspecs, velocity, tred, nsamp, dt,
                          traces);
 }
 

@@ -212,3 +212,59 @@ def test_bessel_functions_of_the_oracle_against_scipy():
         ratio = hd[0, 1, 2].real / hd[0, 1, 0].real
         assert abs(ratio - (2.0 / re * sp.j1(k * x)) / (k * sp.j0(k * x))) < 1e-9 * abs(ratio) + 1e-12
         assert np.isfinite(taper_w)
+
+
+# Each force sum or integral uses a table kind and an FK spectrum that one
+# moment sum also uses, with the factor 2/l(l+1) or its negative
+# (harmonicDegreeSums.f90:110-171 against :297-351, wavenumberIntegrals.f90:160-168
+# against :259-274): with the moment spectra filled from the force spectra
+# (moment column 0, 2, 4, 6, 8 <- force column 0..4) force sum k equals
+# sign x moment sum MATE[k].
+FORCE_MATE = [(0, 1.0), (2, -1.0), (4, 1.0), (6, -1.0), (8, -1.0), (10, 1.0), (12, 1.0)]
+
+
+def _force_and_moment_slabs(nwn, seed):
+    rng = np.random.default_rng(seed)
+    nkf = int(nwn.sum())
+    fr = rng.standard_normal((5, nkf)).astype(np.float32)
+    fi = rng.standard_normal((5, nkf)).astype(np.float32)
+    mr = np.zeros((10, nkf), np.float32); mi = np.zeros_like(mr)
+    mr[0::2] = fr; mi[0::2] = fi
+    return fr, fi, mr, mi
+
+
+def test_force_degree_sums_against_moment_sums():
+    nwn = np.array([0, 40, 48, 56, 64], np.int32)
+    fr, fi, mr, mi = _force_and_moment_slabs(nwn, 5)
+    theta = [0.05, 0.7, 2.9]
+    f = oracle.force_degree_sums(2, 5, nwn, 64, fr, fi, theta)
+    m = oracle.degree_sums(2, 5, nwn, 64, mr, mi, theta)
+    for k, (km, sg) in enumerate(FORCE_MATE):
+        a, b = f[:, 1:, k], sg * m[:, 1:, km]   # the two loops round in their own order
+        assert np.abs(a - b).max() <= 1e-14 * np.abs(b).max()
+
+
+def test_force_wavenumber_integrals_against_moment_integrals():
+    nwn = np.array([0, 400, 480, 560, 640], np.int32)
+    fr, fi, mr, mi = _force_and_moment_slabs(nwn, 6)
+    x = [3000.0, 40000.0, 250000.0]   # trapezoid only, both rules, mostly Filon
+    f = oracle.force_wavenumber_integrals(2, 5, nwn, 640, fr, fi, 2e-6, 6371000.0, x)
+    m = oracle.wavenumber_integrals(2, 5, nwn, 640, mr, mi, 2e-6, 6371000.0, x)
+    for k, (km, sg) in enumerate(FORCE_MATE):
+        a, b = f[:, 1:, k], sg * m[:, 1:, km]
+        assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+
+
+def test_force_synthetics_are_linear_in_the_force():
+    """Traces of (Fr, Ft, Ff) equal the sum of the traces of its components
+    (singleFrequencyDisplacement.f90:35-46 is linear), in both modes."""
+    nwn = np.array([0, 60, 64, 64, 64, 64, 64, 64], np.int32)
+    fr, fi, _, _ = _force_and_moment_slabs(nwn, 7)
+    theta, phi, propdir = [0.02, 0.4], [0.3, 2.0], [0.1, -0.7]
+    F = np.array([[1.0, 0, 0], [0, 1.0, 0], [0, 0, 1.0], [0.5, -2.0, 1.5]])
+    for glob in (1, 0):
+        tr = oracle.synthetics_src("FORCE", glob, 2, 8, nwn, 64, 1.0 / 256, 0.002, 2e-5, 6371000.0, fr, fi, theta, phi,
+                                   propdir, F, [2, 0.005, 4, 0.06], 0, 0.0, 256, 1.0).astype(np.float64)
+        comb = 0.5 * tr[:, 0] - 2.0 * tr[:, 1] + 1.5 * tr[:, 2]
+        assert np.abs(tr).max() > 0
+        assert np.abs(tr[:, 3] - comb).max() <= 1e-5 * np.abs(comb).max()
