@@ -447,7 +447,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   long long nthreads = 0;
   for (int ph = 0; ph < 3; ++ph) {
     S.grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph) : gem_plain::fk_phase_blocks_per_sm(ph));
-    nthreads = std::max(nthreads, (long long)S.grid[ph] * FK_BLOCK);
+    nthreads = std::max(nthreads, (long long)S.grid[ph] * FK_BLOCK_PH[ph]);
   }
   size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * gem_plain::fk_lane_slot_per_node();
   if (grow(ctx, ctx->d_scratch, ctx->scratch_cap, scratch_n)) return GEM_ERROR;
@@ -685,7 +685,7 @@ int gem_instrument_read(gem_ctx* ctx, unsigned long long* prof8, unsigned long l
   if (!ctx || !ctx->d_prof) return fail(ctx, "instrumentation not enabled");
   CK(cudaMemcpy(prof8, ctx->d_prof, 24 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   for (int ph = 0; ph < 3; ++ph) prof8[24 + ph] = (unsigned long long)(ctx->phase_ms[ph] * 1000.0);
-  int nw = ctx->last_grid * (FK_BLOCK / 32);
+  int nw = ctx->last_grid * (FK_BLOCK_PH[1] / 32);   // the spheroidal phase's warps
   if (nwarps) *nwarps = nw;
   if (warp_ns) CK(cudaMemcpy(warp_ns, ctx->d_warp_ns, (size_t)2 * nw * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   return GEM_OK;

@@ -6,7 +6,9 @@
 
 namespace gem {
 
-constexpr int FK_BLOCK = 384;          // threads per block of the solver (12 warps, 1 block per SM)
+// threads per block of the solver phases (toroidal, spheroidal, adjoint); one
+// block per SM, sized by registers and the per-lane Neville diagonal
+constexpr int FK_BLOCK_PH[3] = {512, 384, 512};
 constexpr int MAX_LAYER_KNOTS = 64;    // knots per layer handled by the spline kernel
 
 struct PrepArgs {

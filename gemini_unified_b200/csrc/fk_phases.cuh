@@ -31,7 +31,10 @@ namespace GEM_NS {
 
 enum : int { PH_TOR = 0, PH_SPH = 1, PH_ADJ = 2 };
 template <int PH> struct PhaseNV { static constexpr int NV = PH == PH_TOR ? 2 : (PH == PH_SPH ? 5 : 4); };
-constexpr int DIAG_LEVELS = 6;   // levels 0..5 feed the last attempt
+// levels 0..5 of the per-lane Neville diagonal feed the last attempt; the
+// levels below PhaseDiag::L live in shared memory, the rest (read only by the
+// seventh attempt) in the lane's registers or stack
+template <int PH> struct PhaseDiag { static constexpr int L = (PH == PH_SPH && FK_BLOCK_PH[PH_SPH] > 384) ? 5 : 6; };
 
 // lane states
 enum : int {
@@ -100,7 +103,7 @@ struct ItemStore {
 //  Lockstep Bulirsch-Stoer step of all lanes with `active` set
 //  (complexBulirschStep.f90:111-170,180-238,297-340)
 // ------------------------------------------------------------------------
-template <int SYS, int NVD>
+template <int SYS, int NVD, int DL>
 __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool active, double h, double x,
                                      const dz* y0, dz* yext, int& result, double2* D, int lane, Counters& cnt_out) {
   constexpr int NV = SysNV<SYS>::NV;
@@ -113,6 +116,20 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
   dz ys[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) ys[v] = y0[v];
+#if GEM_FAST
+  // what every attempt shares: A(x) y0 and the matrices at x + h/2 and x + h
+  dz t0[NV];
+  constexpr bool CACHE = SysCache<SYS>::value;
+  SysM<SYS> Mh, Me;
+  if (need) {
+    apply_sys<SYS>(P, e, x, ys, t0);
+    if constexpr (CACHE) {
+      sys_eval<SYS>(P, e, x + (24.0 * h) / 48.0, Mh);
+      sys_eval<SYS>(P, e, x + (48.0 * h) / 48.0, Me);
+    }
+  }
+#endif
+  dz dlast[NV];   // diagonal level DL when DL < 6
   for (int j = 1; j <= 7; ++j) {
     unsigned needm = __ballot_sync(0xffffffffu, need);
     if (!needm) break;
@@ -120,7 +137,11 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
     cnt.warp_attempts += 1;
     if (!need) continue;
     dz Y[NV];
+#if GEM_FAST
+    midpoint<SYS, CACHE>(P, e, j, h, x, ys, t0, Mh, Me, Y);
+#else
     midpoint<SYS>(P, e, j, h, x, ys, Y);
+#endif
     cnt.attempts++;
     cnt.matvecs += SEQDIV[j - 1] + 1;
     cnt.sysmats += NXDIV[j - 1];
@@ -139,24 +160,30 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
 #endif
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
+        const bool shared_level = DL == 6 || m - 1 < DL;
         double2* slot = D + ((m - 1) * NVD + v) * 32 + lane;
-        double2 pv = *slot;
+        dz pv = dlast[v];
+        if (shared_level) { double2 q = *slot; pv = dz{q.x, q.y}; }
 #if GEM_FAST
-        dz u = (c[v] - dz{pv.x, pv.y}) * rhh;
+        dz u = (c[v] - pv) * rhh;
 #else
-        dz u = (c[v] - dz{pv.x, pv.y}) / hh;
+        dz u = (c[v] - pv) / hh;
 #endif
         c[v] = xi * u;
         dz nd = xp * u;
-        *slot = make_double2(pend[v].re, pend[v].im);   // level m-1 of the new diagonal
+        if (shared_level) *slot = make_double2(pend[v].re, pend[v].im);   // level m-1 of the new diagonal
+        else dlast[v] = pend[v];
         pend[v] = nd;
         yy[v] = yy[v] + nd;
         dy[v] = nd;
       }
     }
-    if (p < DIAG_LEVELS) {
+    if (p < DL) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) D[(p * NVD + v) * 32 + lane] = make_double2(pend[v].re, pend[v].im);
+    } else if (p < 6) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) dlast[v] = pend[v];
     }
     if (j >= 3) {
       cnt.flops += (long long)(j * (j - 1) / 2) * 8 * NV + (long long)(j - 1) * 2 * NV + 8 * NV + 3;
@@ -784,7 +811,7 @@ __global__ void __launch_bounds__(128) fk_setup_kernel(const __grid_constant__ F
 //  Lockstep phase kernel
 // ------------------------------------------------------------------------
 template <int PH>
-__global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_constant__ FKStatic P, FKLaunch LL) {
+__global__ void __launch_bounds__(FK_BLOCK_PH[PH], 1) fk_phase_kernel(const __grid_constant__ FKStatic P, FKLaunch LL) {
   constexpr int NVD = PhaseNV<PH>::NV;
   extern __shared__ double2 smem_diag[];
   __shared__ Tab tab;
@@ -795,7 +822,8 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
   __syncthreads();
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  double2* D = smem_diag + (threadIdx.x >> 5) * (DIAG_LEVELS * NVD * 32);
+  constexpr int DL = PhaseDiag<PH>::L;
+  double2* D = smem_diag + (threadIdx.x >> 5) * (DL * NVD * 32);
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   Slot s{LL.scratch + tid, LL.nthreads};
   LaneLayout lay{P.nnod + 1};
@@ -839,21 +867,21 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
     dz yext[5];
     int result = 0;
     if (PH == PH_TOR) {
-      bs_step<SYS_TOROIDAL, NVD>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
+      bs_step<SYS_TOROIDAL, NVD, DL>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
     } else if (PH == PH_ADJ) {
-      bs_step<SYS_SOLIDT, NVD>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
+      bs_step<SYS_SOLIDT, NVD, DL>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
     } else {
       unsigned sysmask = __reduce_or_sync(FULL, integ ? (1u << L.sys) : 0u);
       if (sysmask & (1u << SYS_MINORS))
-        bs_step<SYS_MINORS, NVD>(P, L.e, integ && L.sys == SYS_MINORS, L.h, L.x, L.y, yext, result, D, lane, cnt);
+        bs_step<SYS_MINORS, NVD, DL>(P, L.e, integ && L.sys == SYS_MINORS, L.h, L.x, L.y, yext, result, D, lane, cnt);
       if (sysmask & (1u << SYS_FLUID)) {
         int r = 0;
-        bs_step<SYS_FLUID, NVD>(P, L.e, integ && L.sys == SYS_FLUID, L.h, L.x, L.y, yext, r, D, lane, cnt);
+        bs_step<SYS_FLUID, NVD, DL>(P, L.e, integ && L.sys == SYS_FLUID, L.h, L.x, L.y, yext, r, D, lane, cnt);
         if (integ && L.sys == SYS_FLUID) result = r;
       }
       if (sysmask & (1u << SYS_RADIAL)) {
         int r = 0;
-        bs_step<SYS_RADIAL, NVD>(P, L.e, integ && L.sys == SYS_RADIAL, L.h, L.x, L.y, yext, r, D, lane, cnt);
+        bs_step<SYS_RADIAL, NVD, DL>(P, L.e, integ && L.sys == SYS_RADIAL, L.h, L.x, L.y, yext, r, D, lane, cnt);
         if (integ && L.sys == SYS_RADIAL) result = r;
       }
     }
@@ -910,7 +938,7 @@ __global__ void __launch_bounds__(FK_BLOCK, 1) fk_phase_kernel(const __grid_cons
   if (LL.warp_ns && lane == 0) {
     unsigned long long t_end;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_end));
-    long long w = (long long)blockIdx.x * (FK_BLOCK / 32) + (threadIdx.x >> 5);
+    long long w = (long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     LL.warp_ns[2 * w] = t_start;
     LL.warp_ns[2 * w + 1] = t_end;
   }

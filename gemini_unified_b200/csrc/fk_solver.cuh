@@ -181,6 +181,124 @@ __device__ __forceinline__ double rinv(double x) {
 #endif
 }
 
+#if GEM_FAST
+// Fast build: the system matrix at x in a compact form -- the quantities
+// that depend on x, from which the entries follow with a few products -- so
+// that a Bulirsch-Stoer step evaluates the positions all its attempts share
+// (x0, x0 + h/2, x0 + h) once.  Entries as in the plain build below.
+template <int SYS> struct SysM;
+template <> struct SysM<SYS_MINORS> { dz a, b, c, m23, m24; double rr, ro; };   // a = z2/r, b = 4 z1/r^2, c = N/r^2
+template <> struct SysM<SYS_FLUID> { dz m12; double m11, ro; };
+template <> struct SysM<SYS_RADIAL> { dz m11, m12, m21, m22; };
+template <> struct SysM<SYS_TOROIDAL> { dz m12, m21; double rr; };
+template <> struct SysM<SYS_SOLIDT> { dz z2, zrpc, w, c, a43; double rr, ro; };  // w = z1/r^2, c = N/r^2
+
+template <int SYS>
+__device__ __forceinline__ void sys_eval(const FKStatic& P, const Env& e, double x, SysM<SYS>& M) {
+  double ro;
+  dz el[7];
+  const dz zom{e.omre, e.omim};
+  const double dll1 = e.dll1;
+  if constexpr (SYS == SYS_MINORS) {          // minorsOdeSystem.f90:77-126
+    eval_spline<0x1Fu>(P, e, x, e.nl, ro, el);
+    const double rr = rinv(x), rr2 = rr * rr;
+    const dz zrpc = zinv(el[1]);
+    const dz z1 = el[0] - (el[2] * el[2]) * zrpc - el[4];
+    M.a = ((2.0 * el[2]) * zrpc) * rr;
+    M.b = (4.0 * z1) * rr2;
+    M.c = el[4] * rr2;
+    M.m23 = zinv(el[3]);
+    M.m24 = zrpc;
+    M.rr = rr;
+    M.ro = ro;
+  } else if constexpr (SYS == SYS_FLUID) {   // fluidOdeSystem.f90:78-95
+    eval_spline<0x02u>(P, e, x, e.nl, ro, el);
+    const dz zomro = zom * zom * ro;
+    M.m11 = -2.0 * rinv(x);
+    M.m12 = zinv(el[1]) - dll1 * zinv((zomro * x) * x);
+    M.ro = ro;
+  } else if constexpr (SYS == SYS_RADIAL) {  // radialOdeSystem.f90:78-99
+    eval_spline<0x17u>(P, e, x, e.nl, ro, el);
+    const dz zomro = zom * zom * ro;
+    const double rr = rinv(x), rr2 = rr * rr;
+    const dz rc = zinv(el[1]);
+    M.m11 = ((-2.0 * el[2]) * rr) * rc;
+    M.m12 = rc;
+    M.m21 = (-zomro) + (4.0 * rr2) * ((el[0] - (el[2] * el[2]) * rc) - el[4]);
+    M.m22 = (2.0 * rr) * (el[2] * rc - 1.0);
+  } else if constexpr (SYS == SYS_TOROIDAL) {  // toroidalOdeSystem.f90:81-102
+    eval_spline<0x18u>(P, e, x, e.nl, ro, el);
+    const dz zomro = zom * zom * ro;
+    const double rr = rinv(x), rr2 = rr * rr;
+    M.m12 = zinv(el[3]);
+    M.m21 = (-zomro) - (el[4] * rr2) * (2.0 - dll1);
+    M.rr = rr;
+  } else {                                    // solidtOdeSystem.f90:77-114
+    eval_spline<0x1Fu>(P, e, x, e.nl, ro, el);
+    const double rr = rinv(x), rr2 = rr * rr;
+    const dz zrpc = zinv(el[1]);
+    M.z2 = (el[2] * rr) * zrpc;
+    M.zrpc = zrpc;
+    M.w = (el[0] - (el[2] * el[2]) * zrpc - el[4]) * rr2;
+    M.c = el[4] * rr2;
+    M.a43 = -zinv(el[3]);
+    M.rr = rr;
+    M.ro = ro;
+  }
+}
+
+template <int SYS>
+__device__ __forceinline__ void sys_apply(const SysM<SYS>& M, const Env& e, const dz* z, dz* y) {
+  const dz zom{e.omre, e.omim};
+  const double dll1 = e.dll1;
+  if constexpr (SYS == SYS_MINORS) {
+    const dz zomro = zom * zom * M.ro;
+    const double rr = M.rr, m11 = -2.0 * rr, m13 = dll1 * rr;
+    const dz m12 = (-0.5 * dll1) * M.b;
+    const dz m14 = (-0.5 * dll1) * M.a;
+    const dz m22 = rr - M.a;
+    const dz m32 = (-zomro) + (0.25 * dll1) * M.b + (dll1 - 2.0) * M.c;
+    const dz m33 = (-3.0 * rr) - M.a;
+    const dz m42 = (-zomro) + M.b;
+    const dz m55 = M.a - 5.0 * rr;
+    y[0] = m11 * z[0] + m12 * z[1] + m13 * z[2] + m14 * z[3];
+    y[1] = m22 * z[1] + M.m23 * z[2] + M.m24 * z[3];
+    y[2] = (-M.a) * z[0] + m32 * z[1] + m33 * z[2] + M.m24 * z[4];
+    y[3] = (-m11) * z[0] + m42 * z[1] + (-m22) * z[3] + M.m23 * z[4];
+    y[4] = M.b * z[0] + m42 * z[2] + m32 * z[3] + m55 * z[4];
+  } else if constexpr (SYS == SYS_FLUID) {
+    const dz zomro = zom * zom * M.ro;
+    y[0] = M.m11 * z[0] + M.m12 * z[1];
+    y[1] = (-zomro) * z[0];
+  } else if constexpr (SYS == SYS_RADIAL) {
+    y[0] = M.m11 * z[0] + M.m12 * z[1];
+    y[1] = M.m21 * z[0] + M.m22 * z[1];
+  } else if constexpr (SYS == SYS_TOROIDAL) {
+    y[0] = M.rr * z[0] + M.m12 * z[1];
+    y[1] = M.m21 * z[0] + (-3.0 * M.rr) * z[1];
+  } else {
+    const dz zomro = zom * zom * M.ro;
+    const double rr = M.rr, rr2 = rr * rr;
+    const dz a11 = 2.0 * M.z2;
+    const dz a12 = zomro - 4.0 * M.w;
+    const dz a22 = (-a11) + 2.0 * rr;
+    const dz a32 = (2.0 * dll1) * M.w;
+    const dz a34 = zomro - (dll1 * M.w + (dll1 - 2.0) * M.c);
+    (void)rr2;
+    y[0] = a11 * z[0] + a12 * z[1] + rr * z[2] + (2.0 * M.w) * z[3];
+    y[1] = (-M.zrpc) * z[0] + a22 * z[1] + M.z2 * z[3];
+    y[2] = ((-dll1) * M.z2) * z[0] + a32 * z[1] + (-rr) * z[2] + a34 * z[3];
+    y[3] = ((-dll1) * rr) * z[1] + M.a43 * z[2] + (3.0 * rr) * z[3];
+  }
+}
+
+template <int SYS>
+__device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, double x, const dz* z, dz* y) {
+  SysM<SYS> M;
+  sys_eval<SYS>(P, e, x, M);
+  sys_apply<SYS>(M, e, z, y);
+}
+#else
 template <int SYS>
 __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, double x, const dz* z, dz* y) {
   double ro;
@@ -217,29 +335,17 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
     eval_spline<0x02u>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
     double m11 = -2.0 / x;
-#if GEM_FAST
-    dz m12 = zinv(el[1]) - dll1 * zinv((zomro * x) * x);
-#else
     dz m12 = 1.0 / el[1] - dll1 / ((zomro * x) * x);
-#endif
     y[0] = m11 * z[0] + m12 * z[1];
     y[1] = (-zomro) * z[0];
   } else if (SYS == SYS_RADIAL) {   // radialOdeSystem.f90:78-99
     eval_spline<0x17u>(P, e, x, e.nl, ro, el);
     dz zomro = zom * zom * ro;
     double rr = rinv(x), rr2 = rr * rr;
-#if GEM_FAST
-    dz rc = zinv(el[1]);
-    dz m11 = ((-2.0 * el[2]) * rr) * rc;
-    dz m12 = rc;
-    dz m21 = (-zomro) + (4.0 * rr2) * ((el[0] - (el[2] * el[2]) * rc) - el[4]);
-    dz m22 = (2.0 * rr) * (el[2] * rc - 1.0);
-#else
     dz m11 = ((-2.0 * el[2]) * rr) / el[1];
     dz m12 = 1.0 / el[1];
     dz m21 = (-zomro) + (4.0 * rr2) * ((el[0] - (el[2] * el[2]) / el[1]) - el[4]);
     dz m22 = (2.0 * rr) * (el[2] / el[1] - 1.0);
-#endif
     y[0] = m11 * z[0] + m12 * z[1];
     y[1] = m21 * z[0] + m22 * z[1];
   } else if (SYS == SYS_TOROIDAL) { // toroidalOdeSystem.f90:81-102
@@ -274,10 +380,54 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
     y[3] = a42 * z[1] + a43 * z[2] + (3.0 * rr) * z[3];
   }
 }
+#endif
 
 // ------------------------------------------------------------------------
 //  Bulirsch-Stoer full step (complexBulirschStep.f90:111-240,297-340)
 // ------------------------------------------------------------------------
+#if GEM_FAST
+// The 2-variable systems keep the matrices at x0 + h/2 and x0 + h across the
+// attempts of a step; for the 5- and 4-variable systems holding them costs more
+// in spilled registers than evaluating them again.
+template <int SYS> struct SysCache {
+  static constexpr bool value = SYS == SYS_TOROIDAL || SYS == SYS_FLUID || SYS == SYS_RADIAL;
+};
+
+// Modified midpoint of attempt jtry with t0 = A(xstart) y0 given, and with
+// CACHE the matrices at xstart + h/2 (Mh) and xstart + h (Me): the parts every
+// attempt of a step shares.
+template <int SYS, bool CACHE>
+__device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jtry, double h, double xstart,
+                                         const dz* y0, const dz* t0, const SysM<SYS>& Mh, const SysM<SYS>& Me,
+                                         dz* out) {
+  constexpr int NV = SysNV<SYS>::NV;
+  const int nstep = SEQDIV[jtry - 1];
+  const double hdiv = h / (double)nstep;
+  const int dix = 48 / nstep;
+  dz z0[NV], z1[NV], t[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) { z0[v] = y0[v]; z1[v] = y0[v] + hdiv * t0[v]; }
+  const double h2 = 2.0 * hdiv;
+  for (int m = 1; m <= nstep - 1; ++m) {
+    if (CACHE && m * dix == 24) {
+      sys_apply<SYS>(Mh, e, z1, t);
+    } else {
+      const double x = xstart + ((double)(m * dix) * h) / 48.0;
+      apply_sys<SYS>(P, e, x, z1, t);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      dz z2 = z0[v] + h2 * t[v];
+      z0[v] = z1[v];
+      z1[v] = z2;
+    }
+  }
+  if constexpr (CACHE) sys_apply<SYS>(Me, e, z1, t);
+  else apply_sys<SYS>(P, e, xstart + (48.0 * h) / 48.0, z1, t);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) out[v] = 0.5 * ((z1[v] + z0[v]) + hdiv * t[v]);
+}
+#else
 template <int SYS>
 __device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jtry, double h, double xstart,
                                          const dz* y0, dz* out) {
@@ -306,6 +456,7 @@ __device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jt
 #pragma unroll
   for (int v = 0; v < NV; ++v) out[v] = 0.5 * ((z1[v] + z0[v]) + hdiv * t[v]);
 }
+#endif
 
 // ------------------------------------------------------------------------
 //  Nodes and discontinuities inside an integration range

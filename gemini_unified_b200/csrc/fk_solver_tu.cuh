@@ -8,7 +8,9 @@
 
 namespace GEM_NS {
 template <int PH>
-static size_t phase_smem() { return (size_t)(FK_BLOCK / 32) * DIAG_LEVELS * PhaseNV<PH>::NV * 32 * sizeof(double2); }
+static size_t phase_smem() {
+  return (size_t)(FK_BLOCK_PH[PH] / 32) * PhaseDiag<PH>::L * PhaseNV<PH>::NV * 32 * sizeof(double2);
+}
 
 template <int PH>
 static cudaError_t phase_attr() {
@@ -23,7 +25,7 @@ template <int PH>
 static cudaError_t launch_ph(const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
   cudaError_t e = phase_attr<PH>();
   if (e != cudaSuccess) return e;
-  fk_phase_kernel<PH><<<grid, FK_BLOCK, phase_smem<PH>(), st>>>(P, L);
+  fk_phase_kernel<PH><<<grid, FK_BLOCK_PH[PH], phase_smem<PH>(), st>>>(P, L);
   return cudaGetLastError();
 }
 
@@ -42,7 +44,7 @@ template <int PH>
 static int bps() {
   if (phase_attr<PH>() != cudaSuccess) return 1;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk_phase_kernel<PH>, FK_BLOCK, phase_smem<PH>()) != cudaSuccess) return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk_phase_kernel<PH>, FK_BLOCK_PH[PH], phase_smem<PH>()) != cudaSuccess) return 1;
   return nb < 1 ? 1 : nb;
 }
 
