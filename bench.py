@@ -281,14 +281,19 @@ def main():
     plain_value = total_items / (t_plain / 1e3)
     del plain
 
-    # ---------------- end-to-end through the host C ABI (float32 spectra back to the host)
+    # ---------------- end-to-end through the host C ABI (float32 spectra back to pinned host buffers)
+    host_out = {r: tuple(torch.empty((ex.nnod, nsp, nkf[r]), dtype=torch.float32, pin_memory=True).numpy()
+                         for _ in range(2)) for r in runs}
+    for r in runs:   # warm-up: the context's device buffers of the host entry point
+        fast.run(w.params, jre, r[0], r[1], f32=True, f64=False, out=host_out[r])
     e2e_times = []
     for _ in range(max(1, min(args.steps, 2))):
         if dist: dist.barrier()
         t0 = time.perf_counter()
         for r in runs:
-            fast.run(w.params, jre, r[0], r[1], f32=True, f64=False)
+            fast.run(w.params, jre, r[0], r[1], f32=True, f64=False, out=host_out[r])
         e2e_times.append(time.perf_counter() - t0)
+    del host_out
     e2e_s = max_over_ranks(float(np.mean(e2e_times)))
     d2h = items_rank * nsp * ex.nnod * 4 * 2 + items_rank * 4
     h2d = items_rank * 8 + 9 * (m.nk + 1) * 8
@@ -382,15 +387,25 @@ def time_traces(args, w, m, g, nsp, dev, stream, dist, rank, size, timed):
     fast_ctx, out_fast, t_fast = form(2, max(1, min(args.steps, 3)))
     _, out_plain, t_plain = form(1, 1)
     err = trace_errors(out_fast, out_plain)
-    # end to end through the host C ABI: FK coefficients from the host, traces back to the host
-    tr_h = np.empty((nsta, nmt, 3, w.nsamp), np.float32)
-    if dist: dist.barrier()
-    t0 = time.perf_counter()
-    rc = L.gem_synth_run(fast_ctx._h, ctypes.byref(sp), p(nwn), p(gr_h), p(gi_h), nsta, p(theta), p(phi),
-                         p(propdir), nmt, p(mt), p(tr_h))
-    e2e_s = time.perf_counter() - t0
-    if rc >= 2:
-        raise RuntimeError(L.gem_last_error(fast_ctx._h).decode())
+    # end to end through the host C ABI: FK coefficients from pinned host memory, traces back to it
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
+    gr_p, gi_p = pin(gr_h), pin(gi_h)
+    tr_h = torch.empty((nsta, nmt, 3, w.nsamp), dtype=torch.float32, pin_memory=True).numpy()
+
+    def host_call():
+        rc = L.gem_synth_run(fast_ctx._h, ctypes.byref(sp), p(nwn), p(gr_p), p(gi_p), nsta, p(theta), p(phi),
+                             p(propdir), nmt, p(mt), p(tr_h))
+        if rc >= 2:
+            raise RuntimeError(L.gem_last_error(fast_ctx._h).decode())
+
+    host_call()   # warm-up: the context's device buffers of the host entry point
+    e2e_runs = []
+    for _ in range(max(1, min(args.steps, 3))):
+        if dist: dist.barrier()
+        t0 = time.perf_counter()
+        host_call()
+        e2e_runs.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(e2e_runs))
     if dist:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -65,8 +65,8 @@ struct gem_ctx {
   int last_grid = 0;
   gem_stats stats{};
   // device buffers of the other entry points, grown on demand
-  void* d_aux[8] = {};
-  size_t aux_cap[8] = {};
+  void* d_aux[12] = {};
+  size_t aux_cap[12] = {};
   int kopt = 6;   // order target of the step-size control (gem_order_target; fast backend)
   // captured launch sequence of one slab (gem_fk_graph_build)
   cudaGraphExec_t graph_exec = nullptr;
@@ -177,7 +177,7 @@ void gem_note_synth_ms(gem_ctx* ctx, float ms) { if (ctx) ctx->stats.synth_ms = 
 int gem_ctx_device(const gem_ctx* ctx) { return ctx->device; }
 int gem_ctx_backend(const gem_ctx* ctx) { return ctx->backend; }
 void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes) {
-  if (slot < 0 || slot >= 8) return nullptr;
+  if (slot < 0 || slot >= 12) return nullptr;
   if (ctx->d_aux[slot] && ctx->aux_cap[slot] >= bytes) return ctx->d_aux[slot];
   cudaFree(ctx->d_aux[slot]);
   ctx->d_aux[slot] = nullptr; ctx->aux_cap[slot] = 0;
@@ -633,19 +633,16 @@ int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   long long nkf = 0;
   for (int jf = jf_first; jf <= jf_last; ++jf) nkf += g.nwn[jf];
   size_t nout = (size_t)nkf * nsp_of(p) * ctx->nnod;
-  float *dre = nullptr, *dim = nullptr;
-  double* d64 = nullptr;
-  int32_t* dst = nullptr;
+  // device outputs: context-owned buffers (slots 8..11), grown on demand and
+  // kept for the next call; the host buffers are the caller's (pinned ones copy
+  // at full DMA rate)
+  float* dre = gfre ? (float*)gem_ctx_aux(ctx, 8, nout * sizeof(float)) : nullptr;
+  float* dim = gfim ? (float*)gem_ctx_aux(ctx, 9, nout * sizeof(float)) : nullptr;
+  double* d64 = gf64 ? (double*)gem_ctx_aux(ctx, 10, nout * 2 * sizeof(double)) : nullptr;
+  int32_t* dst = (int32_t*)gem_ctx_aux(ctx, 11, (size_t)nkf * sizeof(int32_t));
+  if ((gfre && !dre) || (gfim && !dim) || (gf64 && !d64) || !dst) return GEM_ERROR;
   int ret = GEM_OK;
   cudaStream_t st = nullptr;
-  auto cleanup = [&]() { cudaFree(dre); cudaFree(dim); cudaFree(d64); cudaFree(dst); };
-  if ((gfre && cudaMalloc(&dre, nout * sizeof(float)) != cudaSuccess) ||
-      (gfim && cudaMalloc(&dim, nout * sizeof(float)) != cudaSuccess) ||
-      (gf64 && cudaMalloc(&d64, nout * 2 * sizeof(double)) != cudaSuccess) ||
-      cudaMalloc(&dst, (size_t)nkf * sizeof(int32_t)) != cudaSuccess) {
-    cleanup();
-    return fail(ctx, "device allocation of %zu outputs failed", nout);
-  }
   ret = gem_fk_run_device(ctx, p, jf_first, jf_last, dre, dim, d64, dst, st);
   if (ret == GEM_OK) {
     std::vector<int32_t> hst((size_t)nkf);
@@ -662,7 +659,6 @@ int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
       if (nfail) ret = fail(ctx, "%lld (omega,l) items failed; see the per-item status", nfail);
     }
   }
-  cleanup();
   return ret;
 }
 

@@ -196,20 +196,28 @@ class GeminiFK:
         return nf1.value, nf2.value, nwnmax.value, nsp.value, nwn[: nf2.value].copy()
 
     def run(self, params: FKParams, jre: int, jf_first: int, jf_last: int, f32: bool = True,
-            f64: bool = True, raise_on_failure: bool = True):
+            f64: bool = True, raise_on_failure: bool = True, out=None):
         """FK spectra of frequencies jf_first..jf_last.
 
         Returns (gfre, gfim, gf64, status) with gf arrays shaped
         (nnod, nsp, nkf) -- the transpose view of the Fortran (nkf, nsp, nnod)
-        layout -- and status per wavenumber-frequency index k.
+        layout -- and status per wavenumber-frequency index k.  out: optional
+        caller-owned float32 (gfre, gfim) arrays of that shape (for example in
+        pinned memory) that receive the float32 spectra.
         """
         grid = frequency_grid(params, self.model.rearth)
         nkf = int(grid.nwn[jf_first - 1: jf_last].sum())
         nsp = nsp_for(params)
         nnod = self.nodes.nnod
         pc = fk_params_c(params, jre)
-        gre = np.zeros((nnod, nsp, nkf), np.float32) if f32 else None
-        gim = np.zeros((nnod, nsp, nkf), np.float32) if f32 else None
+        if out is not None and f32:
+            gre, gim = out
+            for a in (gre, gim):
+                if a.dtype != np.float32 or a.shape != (nnod, nsp, nkf) or not a.flags.c_contiguous:
+                    raise GeminiError("out arrays must be C-contiguous float32 of shape %s" % ((nnod, nsp, nkf),))
+        else:
+            gre = np.zeros((nnod, nsp, nkf), np.float32) if f32 else None
+            gim = np.zeros((nnod, nsp, nkf), np.float32) if f32 else None
         g64 = np.zeros((nnod, nsp, nkf), np.complex128) if f64 else None
         status = np.zeros(nkf, np.int32)
         rc = lib().gem_fk_run(self._h, ctypes.byref(pc), jf_first, jf_last, _ptr(gre), _ptr(gim), _ptr(g64),
