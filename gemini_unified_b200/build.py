@@ -10,6 +10,7 @@ The parity build of the FK solver (and every other file) is compiled with
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -45,13 +46,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
-    logs = []
-    for src in sources():
+
+    def compile_one(src):
         obj = os.path.join(OUT_DIR, os.path.basename(src)[:-3] + ".o")
         fmad = "--fmad=true" if os.path.basename(src) in FMAD_TRUE else "--fmad=false"
         cmd = [NVCC, *ARCH, *FLAGS, fmad, "-c", src, "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    # the translation units are independent: compile them in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as pool:
+        results = list(pool.map(compile_one, sources()))
+    objs, logs = [], []
+    for src, obj, r in results:
         logs.append(r.stdout + r.stderr)
         if r.returncode != 0:
             raise RuntimeError("nvcc failed for %s:\n%s" % (src, r.stdout + r.stderr))

@@ -68,6 +68,10 @@ struct gem_ctx {
   void* d_aux[12] = {};
   size_t aux_cap[12] = {};
   int kopt = 6;   // order target of the step-size control (gem_order_target; fast backend)
+  // schedule of each solver phase (index into FK_SCHED_*), per build: [0] plain, [1] fast
+  int sched[2][3] = {{FK_SCHED_DEFAULT[0], FK_SCHED_DEFAULT[1], FK_SCHED_DEFAULT[2]},
+                     {FK_SCHED_DEFAULT[0], FK_SCHED_DEFAULT[1], FK_SCHED_DEFAULT[2]}};
+  int last_block = 0;   // threads per block of the last spheroidal launch (instrumentation)
   // captured launch sequence of one slab (gem_fk_graph_build)
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t graph_stream = nullptr;
@@ -346,6 +350,7 @@ struct SlabPlan {
   long long nkf;
   size_t spl_n, nout, nu, nd;
   bool fast, propose;
+  int sched[3];
   float* gfre;
   float* gfim;
   double* gf64;
@@ -446,8 +451,10 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   // ---- grid: the largest of the three phases sets the per-lane scratch
   long long nthreads = 0;
   for (int ph = 0; ph < 3; ++ph) {
-    S.grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph) : gem_plain::fk_phase_blocks_per_sm(ph));
-    nthreads = std::max(nthreads, (long long)S.grid[ph] * FK_BLOCK_PH[ph]);
+    const int sc = ctx->sched[fast ? 1 : 0][ph];
+    S.sched[ph] = sc;
+    S.grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph, sc) : gem_plain::fk_phase_blocks_per_sm(ph, sc));
+    nthreads = std::max(nthreads, (long long)S.grid[ph] * FK_SCHED_BLOCK[sc]);
   }
   size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * gem_plain::fk_lane_slot_per_node();
   if (grow(ctx, ctx->d_scratch, ctx->scratch_cap, scratch_n)) return GEM_ERROR;
@@ -463,6 +470,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
   L.prop_kopt = nullptr; L.prop_hs = nullptr;
   ctx->last_grid = S.grid[1];
+  ctx->last_block = FK_SCHED_BLOCK[S.sched[1]];
   // ---- learned proposer: features / proposals per (phase, item) from the start radii
   S.propose = fast && ctx->prop_use != 0 && ctx->d_propw;
   if (ctx->dump_feat || S.propose) {
@@ -513,7 +521,8 @@ int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
   if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
   auto launch = [&](int ph, const FKLaunch& LX, int g) {
-    return S.fast ? gem_fast::launch_fk_phase(ph, P, LX, g, st) : gem_plain::launch_fk_phase(ph, P, LX, g, st);
+    const int sc = ph >= 0 ? S.sched[ph] : 0;
+    return S.fast ? gem_fast::launch_fk_phase(ph, sc, P, LX, g, st) : gem_plain::launch_fk_phase(ph, sc, P, LX, g, st);
   };
   CK(launch(-1, S.L, ctx->nsm * 8));
   if (ctx->dump_feat) {
@@ -681,7 +690,7 @@ int gem_instrument_read(gem_ctx* ctx, unsigned long long* prof8, unsigned long l
   if (!ctx || !ctx->d_prof) return fail(ctx, "instrumentation not enabled");
   CK(cudaMemcpy(prof8, ctx->d_prof, 24 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   for (int ph = 0; ph < 3; ++ph) prof8[24 + ph] = (unsigned long long)(ctx->phase_ms[ph] * 1000.0);
-  int nw = ctx->last_grid * (FK_BLOCK_PH[1] / 32);   // the spheroidal phase's warps
+  int nw = ctx->last_grid * (ctx->last_block / 32);   // the spheroidal phase's warps
   if (nwarps) *nwarps = nw;
   if (warp_ns) CK(cudaMemcpy(warp_ns, ctx->d_warp_ns, (size_t)2 * nw * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   return GEM_OK;
@@ -765,6 +774,82 @@ int gem_proposer_dump_read(gem_ctx* ctx, float* out, long long cap, long long* n
 // Order target of the step-size control (fast backend; no counterpart in the
 // reference, which fixes it at 6, parametersBulirschStep.f90:28-48): k in 3..7;
 // 0 restores 6.
+// Solver schedules (no counterpart in the reference): per phase (toroidal,
+// spheroidal, adjoint) an index into FK_SCHED_BLOCK / FK_SCHED_BIGCACHE, kept
+// per backend.  Every schedule gives bit-identical spectra; only the time differs.
+int gem_fk_schedule_set(gem_ctx* ctx, const int* sched3) {
+  if (!ctx || !sched3) return GEM_ERROR;
+  for (int ph = 0; ph < 3; ++ph)
+    if (sched3[ph] < 0 || sched3[ph] >= FK_NSCHED) return fail(ctx, "schedule index must be 0..%d", FK_NSCHED - 1);
+  const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
+  for (int ph = 0; ph < 3; ++ph) ctx->sched[b][ph] = sched3[ph];
+  ctx->graph_valid = false;
+  return GEM_OK;
+}
+
+int gem_fk_schedule_get(const gem_ctx* ctx, int* sched3) {
+  if (!ctx || !sched3) return GEM_ERROR;
+  const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
+  for (int ph = 0; ph < 3; ++ph) sched3[ph] = ctx->sched[b][ph];
+  return GEM_OK;
+}
+
+// Autotuner: runs frequencies jf_first..jf_last once per candidate schedule
+// (all three phases at once, repeats times, the minimum kept), then keeps per
+// phase the fastest candidate.  ms[c*3 + ph] receives the times (-1 for a
+// candidate not run: the plain build has no matrix-caching variants).
+int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, int repeats, float* ms,
+                    int* sched3) {
+  if (!ctx) return GEM_ERROR;
+  int rc = check_params(ctx, p);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  Grid g;
+  make_grid(p, ctx->rearth, g);
+  if (jf_first < g.nf1 || jf_last > g.nf2 || jf_first > jf_last)
+    return fail(ctx, "frequency range %d..%d outside %d..%d", jf_first, jf_last, g.nf1, g.nf2);
+  long long nkf = 0;
+  for (int jf = jf_first; jf <= jf_last; ++jf) nkf += g.nwn[jf];
+  const size_t nout = (size_t)nkf * nsp_of(p) * ctx->nnod;
+  float* dre = (float*)gem_ctx_aux(ctx, 8, nout * sizeof(float));
+  float* dim = dre ? (float*)gem_ctx_aux(ctx, 9, nout * sizeof(float)) : nullptr;
+  int32_t* dst = dim ? (int32_t*)gem_ctx_aux(ctx, 11, (size_t)nkf * sizeof(int32_t)) : nullptr;
+  if (!dst) return GEM_ERROR;
+  const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
+  const int ncand = b ? FK_NSCHED : 3;
+  const int saved[3] = {ctx->sched[b][0], ctx->sched[b][1], ctx->sched[b][2]};
+  float t[FK_NSCHED][3];
+  for (int c = 0; c < FK_NSCHED; ++c)
+    for (int ph = 0; ph < 3; ++ph) t[c][ph] = -1.0f;
+  for (int c = 0; c < ncand; ++c) {
+    for (int ph = 0; ph < 3; ++ph) ctx->sched[b][ph] = c;
+    for (int r = 0; r < std::max(1, repeats); ++r) {
+      SlabPlan S;
+      rc = fk_prepare(ctx, p, jf_first, jf_last, dre, dim, nullptr, dst, S);
+      if (!rc) rc = fk_enqueue(ctx, S, nullptr, true);
+      if (!rc) rc = fk_finish(ctx, S, nullptr, true);
+      if (rc) {
+        for (int ph = 0; ph < 3; ++ph) ctx->sched[b][ph] = saved[ph];
+        return rc;
+      }
+      for (int ph = 0; ph < 3; ++ph)
+        if (t[c][ph] < 0.0f || ctx->phase_ms[ph] < t[c][ph]) t[c][ph] = ctx->phase_ms[ph];
+    }
+  }
+  for (int ph = 0; ph < 3; ++ph) {
+    int best = 0;
+    for (int c = 1; c < ncand; ++c)
+      if (t[c][ph] < t[best][ph]) best = c;
+    ctx->sched[b][ph] = best;
+    if (sched3) sched3[ph] = best;
+  }
+  if (ms)
+    for (int c = 0; c < FK_NSCHED; ++c)
+      for (int ph = 0; ph < 3; ++ph) ms[c * 3 + ph] = t[c][ph];
+  ctx->graph_valid = false;
+  return GEM_OK;
+}
+
 int gem_order_target(gem_ctx* ctx, int k) {
   if (!ctx) return GEM_ERROR;
   if (k == 0) k = 6;

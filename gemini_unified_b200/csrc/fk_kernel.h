@@ -6,9 +6,15 @@
 
 namespace gem {
 
-// threads per block of the solver phases (toroidal, spheroidal, adjoint); one
-// block per SM, sized by registers and the per-lane Neville diagonal
-constexpr int FK_BLOCK_PH[3] = {512, 384, 512};
+// Schedules of a solver phase kernel (one block per SM): threads per block,
+// and whether the 4- and 5-variable systems keep their half- and end-step
+// matrices across the attempts of a Bulirsch-Stoer step (fast build; the
+// 2-variable systems always do, the plain build never).  The autotuner picks
+// one per phase; defaults measured at the batched configuration.
+constexpr int FK_NSCHED = 6;
+constexpr int FK_SCHED_BLOCK[FK_NSCHED] = {384, 512, 256, 384, 512, 256};
+constexpr int FK_SCHED_BIGCACHE[FK_NSCHED] = {0, 0, 0, 1, 1, 1};
+constexpr int FK_SCHED_DEFAULT[3] = {1, 0, 1};   // toroidal 512, spheroidal 384, adjoint 512 threads
 constexpr int MAX_LAYER_KNOTS = 64;    // knots per layer handled by the spline kernel
 
 struct PrepArgs {
@@ -85,9 +91,11 @@ cudaError_t launch_poly(const PrepArgs& A, double* poly, cudaStream_t st);
 // gem_fast (FMA, division-free spline, reciprocal complex inverses).
 #define GEM_DECLARE_SOLVER(NS)                                                                          \
   namespace NS {                                                                                     \
-  /* phase < 0: start radii; 0 toroidal, 1 spheroidal minors, 2 adjoint + spheroidal spectra */      \
-  cudaError_t launch_fk_phase(int phase, const gem::FKStatic& P, const gem::FKLaunch& L, int grid, cudaStream_t st); \
-  int fk_phase_blocks_per_sm(int phase);                                                             \
+  /* phase < 0: start radii; 0 toroidal, 1 spheroidal minors, 2 adjoint + spheroidal spectra;     */ \
+  /* sched: index into FK_SCHED_BLOCK / FK_SCHED_BIGCACHE                                           */ \
+  cudaError_t launch_fk_phase(int phase, int sched, const gem::FKStatic& P, const gem::FKLaunch& L, int grid,  \
+                              cudaStream_t st);                                                      \
+  int fk_phase_blocks_per_sm(int phase, int sched);                                                  \
   int fk_lane_slot_per_node();                                                                       \
   }
 GEM_DECLARE_SOLVER(gem_plain)

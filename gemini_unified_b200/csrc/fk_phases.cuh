@@ -34,7 +34,7 @@ template <int PH> struct PhaseNV { static constexpr int NV = PH == PH_TOR ? 2 : 
 // levels 0..5 of the per-lane Neville diagonal feed the last attempt; the
 // levels below PhaseDiag::L live in shared memory, the rest (read only by the
 // seventh attempt) in the lane's registers or stack
-template <int PH> struct PhaseDiag { static constexpr int L = (PH == PH_SPH && FK_BLOCK_PH[PH_SPH] > 384) ? 5 : 6; };
+template <int PH, int BLK> struct PhaseDiag { static constexpr int L = (PH == PH_SPH && BLK > 384) ? 5 : 6; };
 
 // lane states
 enum : int {
@@ -103,7 +103,7 @@ struct ItemStore {
 //  Lockstep Bulirsch-Stoer step of all lanes with `active` set
 //  (complexBulirschStep.f90:111-170,180-238,297-340)
 // ------------------------------------------------------------------------
-template <int SYS, int NVD, int DL>
+template <int SYS, int NVD, int DL, bool BIG>
 __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool active, double h, double x,
                                      const dz* y0, dz* yext, int& result, double2* D, int lane, Counters& cnt_out) {
   constexpr int NV = SysNV<SYS>::NV;
@@ -119,7 +119,7 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
 #if GEM_FAST
   // what every attempt shares: A(x) y0 and the matrices at x + h/2 and x + h
   dz t0[NV];
-  constexpr bool CACHE = SysCache<SYS>::value;
+  constexpr bool CACHE = SysCache<SYS, BIG>::value;
   SysM<SYS> Mh, Me;
   if (need) {
     apply_sys<SYS>(P, e, x, ys, t0);
@@ -810,8 +810,8 @@ __global__ void __launch_bounds__(128) fk_setup_kernel(const __grid_constant__ F
 // ------------------------------------------------------------------------
 //  Lockstep phase kernel
 // ------------------------------------------------------------------------
-template <int PH>
-__global__ void __launch_bounds__(FK_BLOCK_PH[PH], 1) fk_phase_kernel(const __grid_constant__ FKStatic P, FKLaunch LL) {
+template <int PH, int BLK, bool BIG>
+__global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant__ FKStatic P, FKLaunch LL) {
   constexpr int NVD = PhaseNV<PH>::NV;
   extern __shared__ double2 smem_diag[];
   __shared__ Tab tab;
@@ -822,7 +822,7 @@ __global__ void __launch_bounds__(FK_BLOCK_PH[PH], 1) fk_phase_kernel(const __gr
   __syncthreads();
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  constexpr int DL = PhaseDiag<PH>::L;
+  constexpr int DL = PhaseDiag<PH, BLK>::L;
   double2* D = smem_diag + (threadIdx.x >> 5) * (DL * NVD * 32);
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   Slot s{LL.scratch + tid, LL.nthreads};
@@ -867,21 +867,21 @@ __global__ void __launch_bounds__(FK_BLOCK_PH[PH], 1) fk_phase_kernel(const __gr
     dz yext[5];
     int result = 0;
     if (PH == PH_TOR) {
-      bs_step<SYS_TOROIDAL, NVD, DL>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
+      bs_step<SYS_TOROIDAL, NVD, DL, BIG>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
     } else if (PH == PH_ADJ) {
-      bs_step<SYS_SOLIDT, NVD, DL>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
+      bs_step<SYS_SOLIDT, NVD, DL, BIG>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
     } else {
       unsigned sysmask = __reduce_or_sync(FULL, integ ? (1u << L.sys) : 0u);
       if (sysmask & (1u << SYS_MINORS))
-        bs_step<SYS_MINORS, NVD, DL>(P, L.e, integ && L.sys == SYS_MINORS, L.h, L.x, L.y, yext, result, D, lane, cnt);
+        bs_step<SYS_MINORS, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_MINORS, L.h, L.x, L.y, yext, result, D, lane, cnt);
       if (sysmask & (1u << SYS_FLUID)) {
         int r = 0;
-        bs_step<SYS_FLUID, NVD, DL>(P, L.e, integ && L.sys == SYS_FLUID, L.h, L.x, L.y, yext, r, D, lane, cnt);
+        bs_step<SYS_FLUID, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_FLUID, L.h, L.x, L.y, yext, r, D, lane, cnt);
         if (integ && L.sys == SYS_FLUID) result = r;
       }
       if (sysmask & (1u << SYS_RADIAL)) {
         int r = 0;
-        bs_step<SYS_RADIAL, NVD, DL>(P, L.e, integ && L.sys == SYS_RADIAL, L.h, L.x, L.y, yext, r, D, lane, cnt);
+        bs_step<SYS_RADIAL, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_RADIAL, L.h, L.x, L.y, yext, r, D, lane, cnt);
         if (integ && L.sys == SYS_RADIAL) result = r;
       }
     }

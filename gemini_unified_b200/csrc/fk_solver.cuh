@@ -387,10 +387,11 @@ __device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, doubl
 // ------------------------------------------------------------------------
 #if GEM_FAST
 // The 2-variable systems keep the matrices at x0 + h/2 and x0 + h across the
-// attempts of a step; for the 5- and 4-variable systems holding them costs more
-// in spilled registers than evaluating them again.
-template <int SYS> struct SysCache {
-  static constexpr bool value = SYS == SYS_TOROIDAL || SYS == SYS_FLUID || SYS == SYS_RADIAL;
+// attempts of a step; the 5- and 4-variable systems do when BIG is set (a
+// schedule choice: at 384-512 threads per block the held matrices cost more in
+// spilled registers than evaluating them again, at 256 they do not).
+template <int SYS, bool BIG> struct SysCache {
+  static constexpr bool value = BIG || SYS == SYS_TOROIDAL || SYS == SYS_FLUID || SYS == SYS_RADIAL;
 };
 
 // Modified midpoint of attempt jtry with t0 = A(xstart) y0 given, and with

@@ -7,52 +7,83 @@
 #include "fk_phases.cuh"
 
 namespace GEM_NS {
-template <int PH>
+template <int PH, int BLK>
 static size_t phase_smem() {
-  return (size_t)(FK_BLOCK_PH[PH] / 32) * PhaseDiag<PH>::L * PhaseNV<PH>::NV * 32 * sizeof(double2);
+  return (size_t)(BLK / 32) * PhaseDiag<PH, BLK>::L * PhaseNV<PH>::NV * 32 * sizeof(double2);
 }
 
-template <int PH>
+template <int PH, int BLK, bool BIG>
 static cudaError_t phase_attr() {
   static bool done = false;
   if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(fk_phase_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)phase_smem<PH>());
+  cudaError_t e = cudaFuncSetAttribute(fk_phase_kernel<PH, BLK, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)phase_smem<PH, BLK>());
   if (e == cudaSuccess) done = true;
   return e;
 }
 
-template <int PH>
+template <int PH, int BLK, bool BIG>
 static cudaError_t launch_ph(const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
-  cudaError_t e = phase_attr<PH>();
+  cudaError_t e = phase_attr<PH, BLK, BIG>();
   if (e != cudaSuccess) return e;
-  fk_phase_kernel<PH><<<grid, FK_BLOCK_PH[PH], phase_smem<PH>(), st>>>(P, L);
+  fk_phase_kernel<PH, BLK, BIG><<<grid, BLK, phase_smem<PH, BLK>(), st>>>(P, L);
   return cudaGetLastError();
 }
 
-cudaError_t launch_fk_phase(int phase, const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
+template <int PH, int BLK, bool BIG>
+static int bps() {
+  if (phase_attr<PH, BLK, BIG>() != cudaSuccess) return 1;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk_phase_kernel<PH, BLK, BIG>, BLK, phase_smem<PH, BLK>()) !=
+      cudaSuccess)
+    return 1;
+  return nb < 1 ? 1 : nb;
+}
+
+// The matrix-caching flag only changes the 4- and 5-variable systems of the
+// fast build: the toroidal phase and the plain build use the schedule's block
+// size alone.
+template <int PH>
+static constexpr bool big_applies() { return GEM_FAST && PH != PH_TOR; }
+
+template <int PH>
+static cudaError_t launch_sched(int sched, const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
+  const bool big = big_applies<PH>() && FK_SCHED_BIGCACHE[sched];
+  switch (FK_SCHED_BLOCK[sched]) {
+    case 256: return big ? launch_ph<PH, 256, big_applies<PH>()>(P, L, grid, st) : launch_ph<PH, 256, false>(P, L, grid, st);
+    case 512: return big ? launch_ph<PH, 512, big_applies<PH>()>(P, L, grid, st) : launch_ph<PH, 512, false>(P, L, grid, st);
+    default: return big ? launch_ph<PH, 384, big_applies<PH>()>(P, L, grid, st) : launch_ph<PH, 384, false>(P, L, grid, st);
+  }
+}
+
+template <int PH>
+static int bps_sched(int sched) {
+  const bool big = big_applies<PH>() && FK_SCHED_BIGCACHE[sched];
+  switch (FK_SCHED_BLOCK[sched]) {
+    case 256: return big ? bps<PH, 256, big_applies<PH>()>() : bps<PH, 256, false>();
+    case 512: return big ? bps<PH, 512, big_applies<PH>()>() : bps<PH, 512, false>();
+    default: return big ? bps<PH, 384, big_applies<PH>()>() : bps<PH, 384, false>();
+  }
+}
+
+cudaError_t launch_fk_phase(int phase, int sched, const FKStatic& P, const FKLaunch& L, int grid, cudaStream_t st) {
+  if (sched < 0 || sched >= FK_NSCHED) sched = 0;
   switch (phase) {
-    case PH_TOR: return launch_ph<PH_TOR>(P, L, grid, st);
-    case PH_SPH: return launch_ph<PH_SPH>(P, L, grid, st);
-    case PH_ADJ: return launch_ph<PH_ADJ>(P, L, grid, st);
+    case PH_TOR: return launch_sched<PH_TOR>(sched, P, L, grid, st);
+    case PH_SPH: return launch_sched<PH_SPH>(sched, P, L, grid, st);
+    case PH_ADJ: return launch_sched<PH_ADJ>(sched, P, L, grid, st);
     default:
       fk_setup_kernel<<<grid, 128, 0, st>>>(P, L);
       return cudaGetLastError();
   }
 }
 
-template <int PH>
-static int bps() {
-  if (phase_attr<PH>() != cudaSuccess) return 1;
-  int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk_phase_kernel<PH>, FK_BLOCK_PH[PH], phase_smem<PH>()) != cudaSuccess) return 1;
-  return nb < 1 ? 1 : nb;
-}
-
-int fk_phase_blocks_per_sm(int phase) {
+int fk_phase_blocks_per_sm(int phase, int sched) {
+  if (sched < 0 || sched >= FK_NSCHED) sched = 0;
   switch (phase) {
-    case PH_TOR: return bps<PH_TOR>();
-    case PH_SPH: return bps<PH_SPH>();
-    case PH_ADJ: return bps<PH_ADJ>();
+    case PH_TOR: return bps_sched<PH_TOR>(sched);
+    case PH_SPH: return bps_sched<PH_SPH>(sched);
+    case PH_ADJ: return bps_sched<PH_ADJ>(sched);
     default: return 8;
   }
 }

@@ -140,6 +140,24 @@ int gem_fk_graph_build(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int j
                        float* d_gfim, double* d_gf64, int32_t* d_status);
 int gem_fk_graph_launch(gem_ctx* ctx, void* stream);
 
+/* Solver schedules and their autotuner (no counterpart in the reference; the
+ * reference runs one solve at a time).  Each phase kernel (toroidal,
+ * spheroidal, adjoint) runs one block per SM under one of GEM_FK_NSCHED
+ * schedules: threads per block (384, 512, 256, 384, 512, 256) and, for
+ * schedules 3..5, the 4- and 5-variable systems of the fast backend keep their
+ * half- and end-step matrices across the attempts of a Bulirsch-Stoer step.
+ * Every schedule gives bit-identical spectra.  sched3[ph] is kept per context
+ * and backend; the default is {1, 0, 1}. */
+#define GEM_FK_NSCHED 6
+int gem_fk_schedule_set(gem_ctx* ctx, const int* sched3);
+int gem_fk_schedule_get(const gem_ctx* ctx, int* sched3);
+/* Runs frequencies jf_first..jf_last once per candidate schedule (repeats
+ * times, minimum kept) and keeps per phase the fastest; ms[c*3 + ph] (may be
+ * NULL) receives the phase times in ms, -1 for candidates not run (the plain
+ * backend tries schedules 0..2 only); sched3 (may be NULL) the choice. */
+int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, int repeats, float* ms,
+                    int* sched3);
+
 /* Synthetic seismograms of all stations and moment tensors of one source
  * node: replaces, for every station, computeLegendreFunctions +
  * sphericalHarmonicsDisplacementSpectra (displacementSpectra.f90:49) + event

@@ -218,3 +218,38 @@ def test_graph_replay_matches_direct_run(small):
         fk.run(w.params, jre, 3, 3, f32=False)
         with pytest.raises(GeminiError):
             fk.graph_launch()
+
+
+def test_every_schedule_gives_identical_spectra(small):
+    """Block size and matrix caching change the time only: every schedule of
+    both backends gives the default schedule's spectra bit for bit."""
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NSCHED
+    from gemini_unified_b200.model import GeminiError
+    w, m, ex, jre, _, o = small
+    for backend in (1, GEM_BACKEND_GPU_FAST):
+        fk = GeminiFK(m, ex, backend=backend)
+        assert fk.schedule() == [1, 0, 1]
+        _, _, ref, st = fk.run(w.params, jre, 40, 52, f32=False)
+        assert np.all(st == 0)
+        for s in range(NSCHED):
+            fk.schedule_set([s, s, s])
+            _, _, got, st = fk.run(w.params, jre, 40, 52, f32=False)
+            assert np.all(st == 0)
+            assert np.array_equal(np.nan_to_num(got, nan=1.0), np.nan_to_num(ref, nan=1.0)), (backend, s)
+        with pytest.raises(GeminiError):
+            fk.schedule_set([0, NSCHED, 0])
+
+
+def test_autotune_keeps_the_fastest_schedule(small):
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NSCHED
+    w, m, ex, jre, _, o = small
+    for backend, ncand in ((1, 3), (GEM_BACKEND_GPU_FAST, NSCHED)):
+        fk = GeminiFK(m, ex, backend=backend)
+        r = fk.autotune(w.params, jre, 44, 52)
+        ms = r["ms"]
+        assert np.all(ms[:ncand] > 0) and np.all(ms[ncand:] == -1)
+        for ph in range(3):
+            assert r["schedule"][ph] == int(np.argmin(ms[:ncand, ph]))
+        assert fk.schedule() == r["schedule"]
+        _, _, g64, st = fk.run(w.params, jre, 44, 52, f32=False)
+        assert np.all(st == 0)
