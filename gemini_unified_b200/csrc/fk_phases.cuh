@@ -846,7 +846,7 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
         base = __shfl_sync(FULL, base, leader);
         if (L.st == S_FETCH) {
           unsigned my = base + __popc(fm & ((1u << lane) - 1u));
-          if (my < (unsigned)LL.nitems) { L.k = (int)my; L.st = S_ITEM_INIT; }
+          if (my < (unsigned)LL.nitems) { L.k = LL.order[my]; L.st = S_ITEM_INIT; }
           else L.st = S_IDLE;
         }
       }
