@@ -71,10 +71,12 @@ def zigzag(nf1, nf2, rank, size):
     return sorted(out)
 
 
-def sched_names(s):
-    """Autotuned schedule per phase as 'threads[+cache]' strings (toroidal, spheroidal, adjoint)."""
-    from gemini_unified_b200.fk import SCHEDULES
-    return ["%d%s" % (SCHEDULES[i][0], "+cache" if SCHEDULES[i][1] else "") for i in s]
+def sched_names(tune):
+    """Autotuned schedule per phase (toroidal, spheroidal, adjoint) as
+    'threads[+cache]/defer<lanes>' strings."""
+    from gemini_unified_b200.fk import DEFERRALS, SCHEDULES
+    return ["%d%s/defer%d" % (SCHEDULES[s][0], "+cache" if SCHEDULES[s][1] else "", DEFERRALS[d][0])
+            for s, d in zip(tune["schedule"], tune["defer"])]
 
 
 def contiguous_runs(js):
@@ -328,7 +330,7 @@ def main():
             "config": {"workload": args.workload, "solves_per_step": total_items, "frequencies": int(g.nf2 - g.nf1 + 1),
                        "lmax": int(g.nwn.max() - 1), "nodes": int(ex.nnod), "parallelism": "frequency zig-zag over %d GPU(s)" % size,
                        "form": "fast FP64 build (FMA, Horner spline table, reciprocals); batched phase kernels",
-                       "schedule": {"fast": sched_names(tune_fast["schedule"]), "plain": sched_names(tune_plain["schedule"]),
+                       "schedule": {"fast": sched_names(tune_fast), "plain": sched_names(tune_plain),
                                     "tuned_on_jf": tune_fast["jf"]},
                        "l2": "flushed between steps (256 MiB write); outputs (1.9 GB) exceed L2"},
             "plain_fp64": {"value": plain_value, "unit": "solves/s", "ms_per_step": t_plain, "steps": plain_steps,

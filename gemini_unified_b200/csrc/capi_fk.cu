@@ -72,6 +72,9 @@ struct gem_ctx {
   int sched[2][3] = {{FK_SCHED_DEFAULT[0], FK_SCHED_DEFAULT[1], FK_SCHED_DEFAULT[2]},
                      {FK_SCHED_DEFAULT[0], FK_SCHED_DEFAULT[1], FK_SCHED_DEFAULT[2]}};
   int last_block = 0;   // threads per block of the last spheroidal launch (instrumentation)
+  // bookkeeping deferral of each phase (index into FK_DEFER_*), per build
+  int defer[2][3] = {{FK_DEFER_DEFAULT, FK_DEFER_DEFAULT, FK_DEFER_DEFAULT},
+                     {FK_DEFER_DEFAULT, FK_DEFER_DEFAULT, FK_DEFER_DEFAULT}};
   // captured launch sequence of one slab (gem_fk_graph_build)
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t graph_stream = nullptr;
@@ -350,7 +353,7 @@ struct SlabPlan {
   long long nkf;
   size_t spl_n, nout, nu, nd;
   bool fast, propose;
-  int sched[3];
+  int sched[3], defer[3];
   float* gfre;
   float* gfim;
   double* gf64;
@@ -453,6 +456,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   for (int ph = 0; ph < 3; ++ph) {
     const int sc = ctx->sched[fast ? 1 : 0][ph];
     S.sched[ph] = sc;
+    S.defer[ph] = ctx->defer[fast ? 1 : 0][ph];
     S.grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph, sc) : gem_plain::fk_phase_blocks_per_sm(ph, sc));
     nthreads = std::max(nthreads, (long long)S.grid[ph] * FK_SCHED_BLOCK[sc]);
   }
@@ -469,6 +473,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   L.warp_ns = nullptr;
   L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
   L.prop_kopt = nullptr; L.prop_hs = nullptr;
+  L.adv_min = 1; L.adv_wait = 0;
   ctx->last_grid = S.grid[1];
   ctx->last_block = FK_SCHED_BLOCK[S.sched[1]];
   // ---- learned proposer: features / proposals per (phase, item) from the start radii
@@ -532,6 +537,8 @@ int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
   if (S.propose) CK(prop_infer_launch(S.PA, ctx->d_propw, ctx->d_propnorm, ctx->d_prop_kopt, ctx->d_prop_hs, st));
   for (int ph = 0; ph < 3; ++ph) {
     FKLaunch Lp = S.L;
+    Lp.adv_min = FK_DEFER_MIN[S.defer[ph]];
+    Lp.adv_wait = FK_DEFER_WAIT[S.defer[ph]];
     if (ctx->d_prof) Lp.prof = ctx->d_prof + 8 * ph;
     if (ctx->d_warp_ns && ph == 1) Lp.warp_ns = ctx->d_warp_ns;
     CK(launch(ph, Lp, S.grid[ph]));
@@ -794,12 +801,33 @@ int gem_fk_schedule_get(const gem_ctx* ctx, int* sched3) {
   return GEM_OK;
 }
 
-// Autotuner: runs frequencies jf_first..jf_last once per candidate schedule
-// (all three phases at once, repeats times, the minimum kept), then keeps per
-// phase the fastest candidate.  ms[c*3 + ph] receives the times (-1 for a
-// candidate not run: the plain build has no matrix-caching variants).
+// Bookkeeping deferral per phase (no counterpart in the reference): an index
+// into FK_DEFER_MIN / FK_DEFER_WAIT, kept per backend; bit-identical spectra.
+int gem_fk_defer_set(gem_ctx* ctx, const int* defer3) {
+  if (!ctx || !defer3) return GEM_ERROR;
+  for (int ph = 0; ph < 3; ++ph)
+    if (defer3[ph] < 0 || defer3[ph] >= FK_NDEFER) return fail(ctx, "deferral index must be 0..%d", FK_NDEFER - 1);
+  const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
+  for (int ph = 0; ph < 3; ++ph) ctx->defer[b][ph] = defer3[ph];
+  ctx->graph_valid = false;
+  return GEM_OK;
+}
+
+int gem_fk_defer_get(const gem_ctx* ctx, int* defer3) {
+  if (!ctx || !defer3) return GEM_ERROR;
+  const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
+  for (int ph = 0; ph < 3; ++ph) defer3[ph] = ctx->defer[b][ph];
+  return GEM_OK;
+}
+
+// Autotuner: runs frequencies jf_first..jf_last once per candidate (all three
+// phases at once, repeats times, the minimum kept) and keeps per phase the
+// fastest.  Stage 1 tries the schedules (block size, matrix caching) under the
+// current deferral, stage 2 the deferrals under the chosen schedules.
+// ms[c*3 + ph]: stage-1 times for c < GEM_FK_NSCHED, stage-2 times after them;
+// -1 for candidates not run (the plain build has no matrix-caching variants).
 int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, int repeats, float* ms,
-                    int* sched3) {
+                    int* sched3, int* defer3) {
   if (!ctx) return GEM_ERROR;
   int rc = check_params(ctx, p);
   if (rc) return rc;
@@ -816,35 +844,51 @@ int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_l
   int32_t* dst = dim ? (int32_t*)gem_ctx_aux(ctx, 11, (size_t)nkf * sizeof(int32_t)) : nullptr;
   if (!dst) return GEM_ERROR;
   const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
-  const int ncand = b ? FK_NSCHED : 3;
-  const int saved[3] = {ctx->sched[b][0], ctx->sched[b][1], ctx->sched[b][2]};
-  float t[FK_NSCHED][3];
-  for (int c = 0; c < FK_NSCHED; ++c)
-    for (int ph = 0; ph < 3; ++ph) t[c][ph] = -1.0f;
-  for (int c = 0; c < ncand; ++c) {
-    for (int ph = 0; ph < 3; ++ph) ctx->sched[b][ph] = c;
+  const int saved_s[3] = {ctx->sched[b][0], ctx->sched[b][1], ctx->sched[b][2]};
+  const int saved_d[3] = {ctx->defer[b][0], ctx->defer[b][1], ctx->defer[b][2]};
+  float t[FK_NSCHED + FK_NDEFER][3];
+  for (auto& row : t)
+    for (float& v : row) v = -1.0f;
+  auto run = [&](float* tc) -> int {
     for (int r = 0; r < std::max(1, repeats); ++r) {
       SlabPlan S;
-      rc = fk_prepare(ctx, p, jf_first, jf_last, dre, dim, nullptr, dst, S);
-      if (!rc) rc = fk_enqueue(ctx, S, nullptr, true);
-      if (!rc) rc = fk_finish(ctx, S, nullptr, true);
-      if (rc) {
-        for (int ph = 0; ph < 3; ++ph) ctx->sched[b][ph] = saved[ph];
-        return rc;
-      }
+      int e = fk_prepare(ctx, p, jf_first, jf_last, dre, dim, nullptr, dst, S);
+      if (!e) e = fk_enqueue(ctx, S, nullptr, true);
+      if (!e) e = fk_finish(ctx, S, nullptr, true);
+      if (e) return e;
       for (int ph = 0; ph < 3; ++ph)
-        if (t[c][ph] < 0.0f || ctx->phase_ms[ph] < t[c][ph]) t[c][ph] = ctx->phase_ms[ph];
+        if (tc[ph] < 0.0f || ctx->phase_ms[ph] < tc[ph]) tc[ph] = ctx->phase_ms[ph];
     }
-  }
-  for (int ph = 0; ph < 3; ++ph) {
-    int best = 0;
-    for (int c = 1; c < ncand; ++c)
+    return GEM_OK;
+  };
+  auto restore = [&]() {
+    for (int ph = 0; ph < 3; ++ph) { ctx->sched[b][ph] = saved_s[ph]; ctx->defer[b][ph] = saved_d[ph]; }
+  };
+  auto argmin = [&](int c0, int n, int ph) {
+    int best = c0;
+    for (int c = c0 + 1; c < c0 + n; ++c)
       if (t[c][ph] < t[best][ph]) best = c;
-    ctx->sched[b][ph] = best;
-    if (sched3) sched3[ph] = best;
+    return best - c0;
+  };
+  // stage 1: schedules
+  const int ncand = b ? FK_NSCHED : 3;
+  for (int c = 0; c < ncand; ++c) {
+    for (int ph = 0; ph < 3; ++ph) ctx->sched[b][ph] = c;
+    if ((rc = run(t[c]))) { restore(); return rc; }
+  }
+  for (int ph = 0; ph < 3; ++ph) ctx->sched[b][ph] = argmin(0, ncand, ph);
+  // stage 2: deferrals under the chosen schedules
+  for (int c = 0; c < FK_NDEFER; ++c) {
+    for (int ph = 0; ph < 3; ++ph) ctx->defer[b][ph] = c;
+    if ((rc = run(t[FK_NSCHED + c]))) { restore(); return rc; }
+  }
+  for (int ph = 0; ph < 3; ++ph) ctx->defer[b][ph] = argmin(FK_NSCHED, FK_NDEFER, ph);
+  for (int ph = 0; ph < 3; ++ph) {
+    if (sched3) sched3[ph] = ctx->sched[b][ph];
+    if (defer3) defer3[ph] = ctx->defer[b][ph];
   }
   if (ms)
-    for (int c = 0; c < FK_NSCHED; ++c)
+    for (int c = 0; c < FK_NSCHED + FK_NDEFER; ++c)
       for (int ph = 0; ph < 3; ++ph) ms[c * 3 + ph] = t[c][ph];
   ctx->graph_valid = false;
   return GEM_OK;

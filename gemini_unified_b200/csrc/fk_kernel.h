@@ -15,6 +15,11 @@ constexpr int FK_NSCHED = 6;
 constexpr int FK_SCHED_BLOCK[FK_NSCHED] = {384, 512, 256, 384, 512, 256};
 constexpr int FK_SCHED_BIGCACHE[FK_NSCHED] = {0, 0, 0, 1, 1, 1};
 constexpr int FK_SCHED_DEFAULT[3] = {1, 0, 1};   // toroidal 512, spheroidal 384, adjoint 512 threads
+// candidate deferrals of the bookkeeping passes (lanes waiting, trips waited)
+constexpr int FK_NDEFER = 6;
+constexpr int FK_DEFER_MIN[FK_NDEFER] = {1, 4, 8, 12, 16, 24};
+constexpr int FK_DEFER_WAIT[FK_NDEFER] = {0, 4, 6, 8, 10, 16};
+constexpr int FK_DEFER_DEFAULT = 2;
 constexpr int MAX_LAYER_KNOTS = 64;    // knots per layer handled by the spline kernel
 
 struct PrepArgs {
@@ -63,6 +68,9 @@ struct FKLaunch {
   struct StepRec* steplog;     // optional record of every step attempt
   unsigned long long steplog_cap;
   unsigned long long* steplog_n;
+  // deferral of the bookkeeping between integrations: a pass runs when
+  // adv_min lanes wait, one has waited adv_wait trips, or none integrates
+  int adv_min, adv_wait;
 };
 
 // One Bulirsch-Stoer step attempt as the step log records it (32 bytes).

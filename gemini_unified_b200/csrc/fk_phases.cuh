@@ -835,9 +835,18 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
   L.e.tab = &tab;
   L.st = S_FETCH;
   unsigned long long cyc_adv = 0, cyc_step = 0;
+  int waited = 0;   // trips this lane has waited for its bookkeeping
   for (;;) {
     unsigned long long c0 = clock64();
-    for (int round = 0; round < 64; ++round) {
+    // The bookkeeping of lanes between integrations runs divergently, so its
+    // cost per pass hardly depends on how many lanes take part: it is deferred
+    // until adv_min lanes wait, one has waited adv_wait trips, or none integrates.
+    const bool pend = L.st != S_INTEG && L.st != S_IDLE;
+    const unsigned pm = __ballot_sync(FULL, pend);
+    waited = pend ? waited + 1 : 0;
+    const bool go = pm && (__popc(pm) >= LL.adv_min || __any_sync(FULL, waited > LL.adv_wait) ||
+                           !__any_sync(FULL, L.st == S_INTEG));
+    for (int round = 0; go && round < 64; ++round) {
       unsigned fm = __ballot_sync(FULL, L.st == S_FETCH);
       if (fm) {
         int leader = __ffs(fm) - 1;

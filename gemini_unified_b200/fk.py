@@ -26,6 +26,9 @@ GEM_BACKEND_GPU_FAST = 2
 # and 5-variable systems keep their half- and end-step matrices (fast backend)
 SCHEDULES = [(384, False), (512, False), (256, False), (384, True), (512, True), (256, True)]
 NSCHED = len(SCHEDULES)
+# bookkeeping deferrals (lanes waiting, steps waited)
+DEFERRALS = [(1, 0), (4, 4), (8, 6), (12, 8), (16, 10), (24, 16)]
+NDEFER = len(DEFERRALS)
 STATUS_TEXT = {0: "ok", 1: "step size smaller than minimum", 2: "maximum number of steps reached",
                3: "continued fraction did not converge", 4: "node/discontinuity bookkeeping",
                5: "non-finite value", 7: "ocean receiver or source not supported"}
@@ -76,7 +79,9 @@ def lib() -> ctypes.CDLL:
         L.gem_order_target.argtypes = [vp, ctypes.c_int]
         L.gem_fk_schedule_set.argtypes = [vp, vp]
         L.gem_fk_schedule_get.argtypes = [vp, vp]
-        L.gem_fk_autotune.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
+        L.gem_fk_autotune.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
+        L.gem_fk_defer_set.argtypes = [vp, vp]
+        L.gem_fk_defer_get.argtypes = [vp, vp]
         L.gem_instrument.argtypes = [vp, ctypes.c_int]
         L.gem_instrument_read.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_int)]
         _lib = L
@@ -276,20 +281,33 @@ class GeminiFK:
         s = (ctypes.c_int * 3)(*[int(x) for x in sched])
         self._check(lib().gem_fk_schedule_set(self._h, s))
 
+    def defer(self):
+        """Bookkeeping deferral index per phase; see DEFERRALS."""
+        s = (ctypes.c_int * 3)()
+        self._check(lib().gem_fk_defer_get(self._h, s))
+        return [int(x) for x in s]
+
+    def defer_set(self, defer):
+        s = (ctypes.c_int * 3)(*[int(x) for x in defer])
+        self._check(lib().gem_fk_defer_set(self._h, s))
+
     def autotune(self, params: FKParams, jre: int, jf_first: int = 0, jf_last: int = 0, repeats: int = 1):
-        """Pick per phase the fastest schedule on frequencies jf_first..jf_last
-        (default: the top quarter of the band, which holds about 44% of the
-        solves).  Returns {"schedule": [tor, sph, adj], "ms": (6, 3) phase times}."""
+        """Pick per phase the fastest schedule, then the fastest bookkeeping
+        deferral, on frequencies jf_first..jf_last (default: the top quarter of
+        the band, which holds about 44% of the solves).  Returns {"schedule":
+        [tor, sph, adj], "defer": [...], "ms": (NSCHED + NDEFER, 3) phase times}."""
         if not jf_first:
             grid = frequency_grid(params, self.model.rearth)
             jf_last = grid.nf2
             jf_first = max(grid.nf1, grid.nf2 - (grid.nf2 - grid.nf1 + 1) // 4)
         pc = fk_params_c(params, jre)
-        ms = np.zeros(3 * NSCHED, np.float32)
+        ms = np.zeros(3 * (NSCHED + NDEFER), np.float32)
         s = (ctypes.c_int * 3)()
+        d = (ctypes.c_int * 3)()
         self._check(lib().gem_fk_autotune(self._h, ctypes.byref(pc), int(jf_first), int(jf_last), int(repeats),
-                                          _ptr(ms), s))
-        return {"schedule": [int(x) for x in s], "ms": ms.reshape(NSCHED, 3), "jf": [int(jf_first), int(jf_last)]}
+                                          _ptr(ms), s, d))
+        return {"schedule": [int(x) for x in s], "defer": [int(x) for x in d],
+                "ms": ms.reshape(NSCHED + NDEFER, 3), "jf": [int(jf_first), int(jf_last)]}
 
     def order_target(self, k: int):
         """Attempt the step-size control aims at (fast backend; 3..7, 0 restores the reference's 6)."""

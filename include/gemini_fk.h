@@ -151,12 +151,22 @@ int gem_fk_graph_launch(gem_ctx* ctx, void* stream);
 #define GEM_FK_NSCHED 6
 int gem_fk_schedule_set(gem_ctx* ctx, const int* sched3);
 int gem_fk_schedule_get(const gem_ctx* ctx, int* sched3);
-/* Runs frequencies jf_first..jf_last once per candidate schedule (repeats
- * times, minimum kept) and keeps per phase the fastest; ms[c*3 + ph] (may be
- * NULL) receives the phase times in ms, -1 for candidates not run (the plain
- * backend tries schedules 0..2 only); sched3 (may be NULL) the choice. */
+/* Deferral of the bookkeeping between integrations, per phase: a lane that
+ * ends an integration sub-interval waits until (1, 4, 8, 12, 16, 24) lanes of
+ * its warp wait or it has waited (0, 4, 6, 8, 10, 16) steps, so that the
+ * divergent bookkeeping runs for many lanes at once.  Index 0..GEM_FK_NDEFER-1,
+ * kept per context and backend, default 2; bit-identical spectra. */
+#define GEM_FK_NDEFER 6
+int gem_fk_defer_set(gem_ctx* ctx, const int* defer3);
+int gem_fk_defer_get(const gem_ctx* ctx, int* defer3);
+/* Autotuner: runs frequencies jf_first..jf_last once per candidate (repeats
+ * times, minimum kept), first the schedules, then the deferrals under the
+ * chosen schedules, and keeps per phase the fastest of each.  ms (may be NULL,
+ * (GEM_FK_NSCHED + GEM_FK_NDEFER) * 3 floats) receives the phase times in ms
+ * of every candidate, -1 for candidates not run (the plain backend tries
+ * schedules 0..2 only); sched3 and defer3 (may be NULL) the choice. */
 int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, int repeats, float* ms,
-                    int* sched3);
+                    int* sched3, int* defer3);
 
 /* Synthetic seismograms of all stations and moment tensors of one source
  * node: replaces, for every station, computeLegendreFunctions +

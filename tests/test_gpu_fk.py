@@ -221,35 +221,43 @@ def test_graph_replay_matches_direct_run(small):
 
 
 def test_every_schedule_gives_identical_spectra(small):
-    """Block size and matrix caching change the time only: every schedule of
-    both backends gives the default schedule's spectra bit for bit."""
-    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NSCHED
+    """Block size, matrix caching and the bookkeeping deferral change the time
+    only: every schedule and deferral of both backends gives the default's
+    spectra bit for bit."""
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NDEFER, NSCHED
     from gemini_unified_b200.model import GeminiError
     w, m, ex, jre, _, o = small
     for backend in (1, GEM_BACKEND_GPU_FAST):
         fk = GeminiFK(m, ex, backend=backend)
-        assert fk.schedule() == [1, 0, 1]
+        assert fk.schedule() == [1, 0, 1] and fk.defer() == [2, 2, 2]
         _, _, ref, st = fk.run(w.params, jre, 40, 52, f32=False)
         assert np.all(st == 0)
+        same = lambda got: np.array_equal(np.nan_to_num(got, nan=1.0), np.nan_to_num(ref, nan=1.0))
         for s in range(NSCHED):
             fk.schedule_set([s, s, s])
             _, _, got, st = fk.run(w.params, jre, 40, 52, f32=False)
-            assert np.all(st == 0)
-            assert np.array_equal(np.nan_to_num(got, nan=1.0), np.nan_to_num(ref, nan=1.0)), (backend, s)
+            assert np.all(st == 0) and same(got), (backend, "schedule", s)
+        for d in range(NDEFER):
+            fk.defer_set([d, d, d])
+            _, _, got, st = fk.run(w.params, jre, 40, 52, f32=False)
+            assert np.all(st == 0) and same(got), (backend, "deferral", d)
         with pytest.raises(GeminiError):
             fk.schedule_set([0, NSCHED, 0])
+        with pytest.raises(GeminiError):
+            fk.defer_set([NDEFER, 0, 0])
 
 
 def test_autotune_keeps_the_fastest_schedule(small):
-    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NSCHED
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NDEFER, NSCHED
     w, m, ex, jre, _, o = small
     for backend, ncand in ((1, 3), (GEM_BACKEND_GPU_FAST, NSCHED)):
         fk = GeminiFK(m, ex, backend=backend)
         r = fk.autotune(w.params, jre, 44, 52)
         ms = r["ms"]
-        assert np.all(ms[:ncand] > 0) and np.all(ms[ncand:] == -1)
+        assert np.all(ms[:ncand] > 0) and np.all(ms[ncand:NSCHED] == -1) and np.all(ms[NSCHED:] > 0)
         for ph in range(3):
             assert r["schedule"][ph] == int(np.argmin(ms[:ncand, ph]))
-        assert fk.schedule() == r["schedule"]
+            assert r["defer"][ph] == int(np.argmin(ms[NSCHED:, ph]))
+        assert fk.schedule() == r["schedule"] and fk.defer() == r["defer"]
         _, _, g64, st = fk.run(w.params, jre, 44, 52, f32=False)
         assert np.all(st == 0)
