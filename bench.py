@@ -73,10 +73,10 @@ def zigzag(nf1, nf2, rank, size):
 
 def sched_names(tune):
     """Autotuned schedule per phase (toroidal, spheroidal, adjoint) as
-    'threads[+cache]/defer<lanes>' strings."""
+    'threads[+cache]/defer<lanes>,<steps>' strings."""
     from gemini_unified_b200.fk import DEFERRALS, SCHEDULES
-    return ["%d%s/defer%d" % (SCHEDULES[s][0], "+cache" if SCHEDULES[s][1] else "", DEFERRALS[d][0])
-            for s, d in zip(tune["schedule"], tune["defer"])]
+    return ["%d%s/defer%d,%d" % (SCHEDULES[s][0], "+cache" if SCHEDULES[s][1] else "", DEFERRALS[d][0],
+                                  DEFERRALS[d][1]) for s, d in zip(tune["schedule"], tune["defer"])]
 
 
 def contiguous_runs(js):

@@ -15,11 +15,13 @@ constexpr int FK_NSCHED = 6;
 constexpr int FK_SCHED_BLOCK[FK_NSCHED] = {384, 512, 256, 384, 512, 256};
 constexpr int FK_SCHED_BIGCACHE[FK_NSCHED] = {0, 0, 0, 1, 1, 1};
 constexpr int FK_SCHED_DEFAULT[3] = {1, 0, 1};   // toroidal 512, spheroidal 384, adjoint 512 threads
-// candidate deferrals of the bookkeeping passes (lanes waiting, trips waited)
+// candidate deferrals of the bookkeeping passes (lanes waiting, trips waited);
+// the last waits for the whole warp: its lanes, on adjacent degrees of one
+// frequency, reach their sub-interval ends within a few steps of each other
 constexpr int FK_NDEFER = 6;
-constexpr int FK_DEFER_MIN[FK_NDEFER] = {1, 4, 8, 12, 16, 24};
-constexpr int FK_DEFER_WAIT[FK_NDEFER] = {0, 4, 6, 8, 10, 16};
-constexpr int FK_DEFER_DEFAULT = 2;
+constexpr int FK_DEFER_MIN[FK_NDEFER] = {1, 8, 16, 32, 32, 32};
+constexpr int FK_DEFER_WAIT[FK_NDEFER] = {0, 6, 10, 24, 48, 1000000};
+constexpr int FK_DEFER_DEFAULT = 4;
 constexpr int MAX_LAYER_KNOTS = 64;    // knots per layer handled by the spline kernel
 
 struct PrepArgs {

@@ -27,7 +27,7 @@ GEM_BACKEND_GPU_FAST = 2
 SCHEDULES = [(384, False), (512, False), (256, False), (384, True), (512, True), (256, True)]
 NSCHED = len(SCHEDULES)
 # bookkeeping deferrals (lanes waiting, steps waited)
-DEFERRALS = [(1, 0), (4, 4), (8, 6), (12, 8), (16, 10), (24, 16)]
+DEFERRALS = [(1, 0), (8, 6), (16, 10), (32, 24), (32, 48), (32, 1000000)]
 NDEFER = len(DEFERRALS)
 STATUS_TEXT = {0: "ok", 1: "step size smaller than minimum", 2: "maximum number of steps reached",
                3: "continued fraction did not converge", 4: "node/discontinuity bookkeeping",

@@ -152,10 +152,11 @@ int gem_fk_graph_launch(gem_ctx* ctx, void* stream);
 int gem_fk_schedule_set(gem_ctx* ctx, const int* sched3);
 int gem_fk_schedule_get(const gem_ctx* ctx, int* sched3);
 /* Deferral of the bookkeeping between integrations, per phase: a lane that
- * ends an integration sub-interval waits until (1, 4, 8, 12, 16, 24) lanes of
- * its warp wait or it has waited (0, 4, 6, 8, 10, 16) steps, so that the
- * divergent bookkeeping runs for many lanes at once.  Index 0..GEM_FK_NDEFER-1,
- * kept per context and backend, default 2; bit-identical spectra. */
+ * ends an integration sub-interval waits until (1, 8, 16, 32, 32, 32) lanes of
+ * its warp wait, it has waited (0, 6, 10, 24, 48, 1000000) steps, or no lane of
+ * the warp integrates, so that the divergent bookkeeping runs for many lanes at
+ * once.  Index 0..GEM_FK_NDEFER-1, kept per context and backend, default 4;
+ * bit-identical spectra. */
 #define GEM_FK_NDEFER 6
 int gem_fk_defer_set(gem_ctx* ctx, const int* defer3);
 int gem_fk_defer_get(const gem_ctx* ctx, int* defer3);

@@ -229,7 +229,7 @@ def test_every_schedule_gives_identical_spectra(small):
     w, m, ex, jre, _, o = small
     for backend in (1, GEM_BACKEND_GPU_FAST):
         fk = GeminiFK(m, ex, backend=backend)
-        assert fk.schedule() == [1, 0, 1] and fk.defer() == [2, 2, 2]
+        assert fk.schedule() == [1, 0, 1] and fk.defer() == [4, 4, 4]
         _, _, ref, st = fk.run(w.params, jre, 40, 52, f32=False)
         assert np.all(st == 0)
         same = lambda got: np.array_equal(np.nan_to_num(got, nan=1.0), np.nan_to_num(ref, nan=1.0))
