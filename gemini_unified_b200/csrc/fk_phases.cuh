@@ -846,6 +846,13 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
     waited = pend ? waited + 1 : 0;
     const bool go = pm && (__popc(pm) >= LL.adv_min || __any_sync(FULL, waited > LL.adv_wait) ||
                            !__any_sync(FULL, L.st == S_INTEG));
+    // A lane at a sub-interval end inside its integration has a short pass
+    // (renormalisation, node store, next sub-interval) and takes it at once;
+    // waiting for it cost more than it saved at every threshold measured.
+    if (!go && pm) {
+      const bool pshort = L.st == S_SUB_END && fabs(L.x2 - L.xe) > MINSIZE_IS;
+      if (__any_sync(FULL, pshort) && pshort) advance<PH>(P, LL, s, lay, L);
+    }
     for (int round = 0; go && round < 64; ++round) {
       unsigned fm = __ballot_sync(FULL, L.st == S_FETCH);
       if (fm) {
