@@ -834,7 +834,7 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
   Lane L;
   L.e.tab = &tab;
   L.st = S_FETCH;
-  unsigned long long cyc_adv = 0, cyc_step = 0;
+  unsigned long long cyc_adv = 0, cyc_step = 0, mixed_trips = 0, cyc_minor_sys = 0;
   int waited = 0;   // trips this lane has waited for its bookkeeping
   for (;;) {
     unsigned long long c0 = clock64();
@@ -888,8 +888,10 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
       bs_step<SYS_SOLIDT, NVD, DL, BIG>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
     } else {
       unsigned sysmask = __reduce_or_sync(FULL, integ ? (1u << L.sys) : 0u);
+      mixed_trips += __popc(sysmask) > 1;
       if (sysmask & (1u << SYS_MINORS))
         bs_step<SYS_MINORS, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_MINORS, L.h, L.x, L.y, yext, result, D, lane, cnt);
+      const unsigned long long c2 = clock64();
       if (sysmask & (1u << SYS_FLUID)) {
         int r = 0;
         bs_step<SYS_FLUID, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_FLUID, L.h, L.x, L.y, yext, r, D, lane, cnt);
@@ -900,6 +902,7 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
         bs_step<SYS_RADIAL, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_RADIAL, L.h, L.x, L.y, yext, r, D, lane, cnt);
         if (integ && L.sys == SYS_RADIAL) result = r;
       }
+      cyc_minor_sys += clock64() - c2;
     }
     cyc_step += clock64() - c1;
     if (LL.steplog) {
@@ -950,6 +953,8 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
     atomicAdd(LL.prof + 3, (unsigned long long)cnt.lane_attempts);
     atomicAdd(LL.prof + 4, cyc_adv);
     atomicAdd(LL.prof + 5, cyc_step);
+    atomicAdd(LL.prof + 6, mixed_trips);     // spheroidal: trips with lanes in two systems
+    atomicAdd(LL.prof + 7, cyc_minor_sys);   // spheroidal: cycles in the fluid and l = 0 steps
   }
   if (LL.warp_ns && lane == 0) {
     unsigned long long t_end;
