@@ -368,7 +368,8 @@ __global__ void spectra_kernel(SynthDev S, const double* __restrict__ C, const d
   const double ca = cos(propdir[sta]), sa = sin(propdir[sta]);
   const dz ci{0.0, 1.0};
   const dz ef = dz{evf[jf].x, evf[jf].y};
-  dz tsf = zexp_dev(((ci * TWO_PI_F) * (double)(jf - 1)) * S.df * S.tred) * exp(S.sigma * S.tred);
+  const double tred = S.tred_sta ? S.tred_sta[sta] : S.tred;
+  dz tsf = zexp_dev(((ci * TWO_PI_F) * (double)(jf - 1)) * S.df * tred) * exp(S.sigma * tred);
   for (int im = 0; im < S.nmt; ++im) {
     dz z[3];
     if (t == 1) {   // momentSingleFrequencyDisplacement (singleFrequencyDisplacement.f90:108-125)
@@ -387,7 +388,14 @@ __global__ void spectra_kernel(SynthDev S, const double* __restrict__ C, const d
       z[1] = w[3] * f[0] + (w[4] + w[5]) * fh;
       z[2] = (w[6] + w[7]) * (f[1] * sphi - f[2] * cphi);
     }
-    for (int c = 0; c < 3; ++c) z[c] = ((z[c] * ef) * dz{1.0, 0.0}) * tsf;
+    for (int c = 0; c < 3; ++c) {
+      dz sf{1.0, 0.0};   // station filter (computeSyntheticSeismograms.f90:361-363), unit by default
+      if (S.stafil) {
+        const double2 q = S.stafil[((long long)sta * 3 + c) * S.nf2 + (jf - 1)];
+        sf = dz{q.x, q.y};
+      }
+      z[c] = ((z[c] * ef) * sf) * tsf;
+    }
     if (S.velocity) {
       dz zom{TWO_PI_F * (double)(jf - 1) * S.df, -S.sigma};
       for (int c = 0; c < 3; ++c) z[c] = (z[c] * ci) * zom;
@@ -484,6 +492,37 @@ using namespace gem;
 
 namespace {
 
+// convolveWithSourceWavelet (computeSyntheticSeismograms.f90:463-484), one block per trace,
+// in place: the trace and the wavelet are staged in shared memory first.  The sum over the
+// wavelet runs in double and is stored to single precision after every term, as the
+// reference's real f(k).  Samples at and beyond nd (nsamp_true of the station) become 0.
+__global__ void __launch_bounds__(256) wavelet_kernel(int nsamp, int nmt, const int* __restrict__ nstrue, int nstf,
+                                                      int nhm, double dt, const float* __restrict__ stf,
+                                                      float* traces) {
+  extern __shared__ float wsm[];
+  float* u = wsm;
+  float* w = wsm + nsamp;
+  const long long tr = blockIdx.x;
+  const int sta = (int)(tr / (3LL * nmt));
+  const int nd = nstrue ? nstrue[sta] : nsamp;
+  float* t = traces + tr * nsamp;
+  for (int i = threadIdx.x; i < nsamp; i += blockDim.x) u[i] = t[i];
+  for (int i = threadIdx.x; i < nstf; i += blockDim.x) w[i] = stf[i];
+  __syncthreads();
+  for (int k = threadIdx.x + 1; k <= nsamp; k += blockDim.x) {
+    float out = 0.0f;
+    if (k <= nd) {
+      if (nstf > 0) {
+        const int n0 = max(1, k - nd + nhm + 1), n1 = min(k + nhm, nstf);
+        for (int n = n0; n <= n1; ++n) out = (float)((double)out + (dt * (double)u[k - (n - nhm)]) * (double)w[n - 1]);
+      } else {
+        out = u[k - 1];
+      }
+    }
+    t[k - 1] = out;
+  }
+}
+
 struct SynthBuffers {
   double* tab = nullptr;
   double* A = nullptr;
@@ -559,12 +598,23 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
                                     const double* propdir, int nmt, const double* mt, float* d_traces,
                                     void* stream);
 
-// Phase-2 run on device FK spectra (d_gr/d_gi: float32 (nkfmax, nsp)), host station/moment arrays.
-extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gr,
-                                    const float* d_gi, int nsta, const double* theta, const double* phi,
-                                    const double* propdir, int nmt, const double* mt, float* d_traces,
-                                    void* stream) {
+namespace {
+// Phase-2 run on device FK spectra (d_gr/d_gi: float32 (nkfmax, nsp)), host station/moment
+// arrays; o (may be null) holds the per-station options of the station loop.
+int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gr, const float* d_gi, int nsta,
+              const double* theta, const double* phi, const double* propdir, int nmt, const double* mt,
+              const gem_synth_station_opts* o, float* d_traces, void* stream) {
   if (!ctx || !p || !nwn || !theta || !phi || !propdir || !mt) return GEM_ERROR;
+  const int nstf = o ? o->nstf : 0;
+  if (o) {
+    if (nstf < 0 || nstf > 8192 || (nstf > 0 && !o->stf))
+      return gem_set_error(ctx, "synthetics: the source wavelet needs 1..8192 samples");
+    if (p->nsamp > 8192) return gem_set_error(ctx, "synthetics: station options need nsamp <= 8192");
+    if (o->nsamp_true)
+      for (int i = 0; i < nsta; ++i)
+        if (o->nsamp_true[i] < 1 || o->nsamp_true[i] > p->nsamp)
+          return gem_set_error(ctx, "synthetics: nsamp_true must be 1..nsamp");
+  }
   if (p->istyp != 1 && p->istyp != 0) return gem_set_error(ctx, "synthetics: source type must be 0 (force) or 1 (moment)");
   if (p->global_ != 1 && p->global_ != 0) return gem_set_error(ctx, "synthetics: GLOBAL must be 0 or 1");
   if (p->global_ == 0 && (!(p->dwn > 0) || !(p->rearth > 0)))
@@ -626,18 +676,21 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   const long long ntr = (long long)nsta * nmt * 3;
   // all buffers of one run in one context-owned allocation, grown on demand
   const bool fast_fft = gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST && ifft_fast_supported(ns);
-  const size_t sizes[14] = {(size_t)8 * S.lcap * nsta * sizeof(double), (size_t)ao * sizeof(double),
+  const bool o_tred = o && o->tred, o_ns = o && o->nsamp_true, o_sf = o && o->stafilter;
+  const size_t sizes[18] = {(size_t)8 * S.lcap * nsta * sizeof(double), (size_t)ao * sizeof(double),
                             (size_t)co * sizeof(double), (size_t)ntr * S.ldx * sizeof(double2),
                             evf.size() * sizeof(double2), tw.size() * sizeof(double2), fac.size() * sizeof(double),
                             (size_t)p->nf2 * sizeof(int), (size_t)nf * sizeof(int), nsta * sizeof(double),
                             nsta * sizeof(double), nsta * sizeof(double), (size_t)nmt * nfo * sizeof(double),
-                            fast_fft ? (size_t)ns * sizeof(double2) : 0};
+                            fast_fft ? (size_t)ns * sizeof(double2) : 0,
+                            o_tred ? nsta * sizeof(double) : 0, o_ns ? nsta * sizeof(int) : 0,
+                            o_sf ? (size_t)nsta * 3 * p->nf2 * sizeof(double2) : 0, (size_t)nstf * sizeof(float)};
   size_t total = 0;
   for (size_t z : sizes) total += (z + 255) / 256 * 256;
   char* pool = (char*)gem_ctx_aux(ctx, 4, total);
   if (!pool) return GEM_ERROR;
-  void* parts[14];
-  for (int i = 0; i < 14; ++i) { parts[i] = sizes[i] ? pool : nullptr; pool += (sizes[i] + 255) / 256 * 256; }
+  void* parts[18];
+  for (int i = 0; i < 18; ++i) { parts[i] = sizes[i] ? pool : nullptr; pool += (sizes[i] + 255) / 256 * 256; }
   b.tab = (double*)parts[0]; b.A = (double*)parts[1]; b.C = (double*)parts[2]; b.X = (double2*)parts[3];
   b.evf = (double2*)parts[4]; b.tw = (double2*)parts[5]; b.fac = (double*)parts[6]; b.nwn = (int*)parts[7];
   b.koff = (int*)parts[8]; b.theta = (double*)parts[9]; b.phi = (double*)parts[10]; b.propdir = (double*)parts[11];
@@ -654,6 +707,14 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   cudaMemcpyAsync(b.propdir, propdir, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b.mt, mt, (size_t)nmt * nfo * sizeof(double), cudaMemcpyHostToDevice, st);
   S.nwn = b.nwn; S.koff = b.koff;
+  S.tred_sta = o_tred ? (const double*)parts[14] : nullptr;
+  S.stafil = o_sf ? (const double2*)parts[16] : nullptr;
+  const int* d_nstrue = o_ns ? (const int*)parts[15] : nullptr;
+  if (o_tred) cudaMemcpyAsync(parts[14], o->tred, nsta * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (o_ns) cudaMemcpyAsync(parts[15], o->nsamp_true, nsta * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (o_sf)
+    cudaMemcpyAsync(parts[16], o->stafilter, (size_t)nsta * 3 * p->nf2 * sizeof(double2), cudaMemcpyHostToDevice, st);
+  if (nstf > 0) cudaMemcpyAsync(parts[17], o->stf, (size_t)nstf * sizeof(float), cudaMemcpyHostToDevice, st);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
@@ -692,6 +753,13 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
     cudaFuncSetAttribute(ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     ifft_kernel<<<(unsigned)ntr, 512, smem, st>>>(S, b.X, b.tw, b.fac, d_traces);
   }
+  if (o_ns || nstf > 0) {   // source wavelet and samples kept per station
+    const size_t smem = (size_t)(p->nsamp + nstf) * sizeof(float);
+    const int nhm = o ? (int)std::floor(std::fabs(o->tanf_stf) / p->dt + 0.5) : 0;
+    cudaFuncSetAttribute(wavelet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    wavelet_kernel<<<(unsigned)ntr, 256, smem, st>>>(p->nsamp, nmt, d_nstrue, nstf, nhm, p->dt,
+                                                     (const float*)parts[17], d_traces);
+  }
   cudaEventRecord(e1, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -703,9 +771,42 @@ extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, con
   return GEM_OK;
 }
 
+int synth_run_host(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* gr, const float* gi,
+                   int nsta, const double* theta, const double* phi, const double* propdir, int nmt, const double* mt,
+                   const gem_synth_station_opts* o, float* traces);
+}  // namespace
+
+extern "C" int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gr,
+                                    const float* d_gi, int nsta, const double* theta, const double* phi,
+                                    const double* propdir, int nmt, const double* mt, float* d_traces,
+                                    void* stream) {
+  return synth_run(ctx, p, nwn, d_gr, d_gi, nsta, theta, phi, propdir, nmt, mt, nullptr, d_traces, stream);
+}
+
+extern "C" int gem_synth_run_device_opts(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gr,
+                                         const float* d_gi, int nsta, const double* theta, const double* phi,
+                                         const double* propdir, int nmt, const double* mt,
+                                         const gem_synth_station_opts* opts, float* d_traces, void* stream) {
+  return synth_run(ctx, p, nwn, d_gr, d_gi, nsta, theta, phi, propdir, nmt, mt, opts, d_traces, stream);
+}
+
 extern "C" int gem_synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* gr, const float* gi,
                              int nsta, const double* theta, const double* phi, const double* propdir, int nmt,
                              const double* mt, float* traces) {
+  return synth_run_host(ctx, p, nwn, gr, gi, nsta, theta, phi, propdir, nmt, mt, nullptr, traces);
+}
+
+extern "C" int gem_synth_run_opts(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* gr,
+                                  const float* gi, int nsta, const double* theta, const double* phi,
+                                  const double* propdir, int nmt, const double* mt,
+                                  const gem_synth_station_opts* opts, float* traces) {
+  return synth_run_host(ctx, p, nwn, gr, gi, nsta, theta, phi, propdir, nmt, mt, opts, traces);
+}
+
+namespace {
+int synth_run_host(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* gr, const float* gi,
+                   int nsta, const double* theta, const double* phi, const double* propdir, int nmt, const double* mt,
+                   const gem_synth_station_opts* o, float* traces) {
   if (!ctx || !p || !gr || !gi || !traces) return GEM_ERROR;
   size_t nin = (size_t)p->nkfmax * p->nsp;
   size_t nout = (size_t)nsta * nmt * 3 * p->nsamp;
@@ -719,11 +820,12 @@ extern "C" int gem_synth_run(gem_ctx* ctx, const gem_synth_params* p, const int*
       cudaMemcpy(dgi, gi, nin * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
     rc = gem_set_error(ctx, "synthetics: copy of the FK spectra failed");
   }
-  if (rc == GEM_OK) rc = gem_synth_run_device(ctx, p, nwn, dgr, dgi, nsta, theta, phi, propdir, nmt, mt, dtr, nullptr);
+  if (rc == GEM_OK) rc = synth_run(ctx, p, nwn, dgr, dgi, nsta, theta, phi, propdir, nmt, mt, o, dtr, nullptr);
   if (rc == GEM_OK && cudaMemcpy(traces, dtr, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
     rc = gem_set_error(ctx, "synthetics: copy of the traces failed");
   return rc;
 }
+}  // namespace
 
 // ---------------------------------------------------------------------------
 //  Batched transformFrequencyTime on device buffers (frequencyTime.f90:55-113)

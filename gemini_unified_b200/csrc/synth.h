@@ -12,6 +12,8 @@ struct SynthDev {
   double df, sigma, tred;
   double dwn, rearth;       // regional mode: wavenumber spacing, earth radius
   int istyp, nsum;          // source type (0 force, 1 moment tensor) and its number of sums
+  const double* tred_sta;   // [nsta] reduction time per station, or null: tred
+  const double2* stafil;    // [nsta][3][nf2] station filter per component, or null: unit filter
   int nsk[8];               // sums per Legendre table kind
   long long aoff[8], coff[8];   // offsets of each kind's coefficient and result matrices
   int col_off[10];          // FK column of each (component, jump) spectrum

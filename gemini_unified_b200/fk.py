@@ -70,6 +70,9 @@ def lib() -> ctypes.CDLL:
         L.gem_fk_graph_launch.argtypes = [vp, vp]
         L.gem_synth_run.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp]
         L.gem_synth_run_device.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp]
+        L.gem_synth_run_opts.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp]
+        L.gem_synth_run_device_opts.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp,
+                                                vp, vp]
         L.gem_ifft_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, vp]
         L.gem_ifft_run_device.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
@@ -104,6 +107,13 @@ class SynthParams(ctypes.Structure):
                 ("tred", ctypes.c_double), ("order_highpass", ctypes.c_int), ("fc_highpass", ctypes.c_double),
                 ("order_lowpass", ctypes.c_int), ("fc_lowpass", ctypes.c_double), ("dwn", ctypes.c_double),
                 ("rearth", ctypes.c_double)]
+
+
+class StationOpts(ctypes.Structure):
+    """C layout of ``gem_synth_station_opts`` (include/gemini_fk.h)."""
+
+    _fields_ = [("tred", ctypes.c_void_p), ("nsamp_true", ctypes.c_void_p), ("stafilter", ctypes.c_void_p),
+                ("nstf", ctypes.c_int), ("tanf_stf", ctypes.c_double), ("stf", ctypes.c_void_p)]
 
 
 def synth_params(grid, nsp, nsamp, dt, filspecs, velocity=False, tred=0.0, global_=1,
@@ -255,20 +265,38 @@ class GeminiFK:
         """Replay the captured slab on a stream (asynchronous)."""
         self._check(lib().gem_fk_graph_launch(self._h, stream or None))
 
-    def synthetics(self, sp: SynthParams, nwn, gfkr, gfki, theta, phi, propdir, mt):
+    def synthetics(self, sp: SynthParams, nwn, gfkr, gfki, theta, phi, propdir, mt, tred=None, nsamp_true=None,
+                   stafilter=None, stf=None, tanf_stf=0.0):
         """Seismograms of all stations x sources: float32 [nsta, nsrc, 3 (Z,N,E), nsamp].
 
         gfkr/gfki: float32 FK spectra of the source node, shaped (nsp, nkfmax).
         mt: moment tensors (nsrc, 6) for sp.istyp 1, forces (nsrc, 3) as
-        (Fr, Ft, Ff) for sp.istyp 0."""
+        (Fr, Ft, Ff) for sp.istyp 0.  Per-station options of the station loop
+        (gem_synth_station_opts): tred [nsta] reduction times, nsamp_true [nsta]
+        samples kept, stafilter complex [nsta, 3, nf2], stf float32 source wavelet
+        whose first sample is at tanf_stf."""
+        keep = []
+        opts = None
+        if tred is not None or nsamp_true is not None or stafilter is not None or stf is not None:
+            conv = lambda a, t: None if a is None else np.ascontiguousarray(a, t)
+            arrs = [conv(tred, np.float64), conv(nsamp_true, np.int32), conv(stafilter, np.complex128),
+                    conv(stf, np.float32)]
+            keep += arrs
+            opts = StationOpts(_ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), 0 if arrs[3] is None else len(arrs[3]),
+                               float(tanf_stf), _ptr(arrs[3]))
         gr = np.ascontiguousarray(gfkr, np.float32); gi = np.ascontiguousarray(gfki, np.float32)
         nwn = np.ascontiguousarray(nwn, np.int32)
         th = np.ascontiguousarray(theta, np.float64); ph = np.ascontiguousarray(phi, np.float64)
         pd = np.ascontiguousarray(propdir, np.float64)
         mt = np.ascontiguousarray(mt, np.float64).reshape(-1, 6 if sp.istyp == 1 else 3)
         out = np.zeros((len(th), len(mt), 3, sp.nsamp), np.float32)
-        self._check(lib().gem_synth_run(self._h, ctypes.byref(sp), _ptr(nwn), _ptr(gr), _ptr(gi), len(th), _ptr(th),
-                                        _ptr(ph), _ptr(pd), len(mt), _ptr(mt), _ptr(out)))
+        if opts is None:
+            self._check(lib().gem_synth_run(self._h, ctypes.byref(sp), _ptr(nwn), _ptr(gr), _ptr(gi), len(th),
+                                            _ptr(th), _ptr(ph), _ptr(pd), len(mt), _ptr(mt), _ptr(out)))
+        else:
+            self._check(lib().gem_synth_run_opts(self._h, ctypes.byref(sp), _ptr(nwn), _ptr(gr), _ptr(gi), len(th),
+                                                 _ptr(th), _ptr(ph), _ptr(pd), len(mt), _ptr(mt),
+                                                 ctypes.byref(opts), _ptr(out)))
         return out
 
     def schedule(self):

@@ -191,6 +191,34 @@ int gem_synth_run_device(gem_ctx* ctx, const gem_synth_params* p, const int* nwn
                          const float* d_gfki, int nsta, const double* theta, const double* phi,
                          const double* propdir, int nmt, const double* mt, float* d_traces, void* stream);
 
+/* Per-station options of the reference's station loop
+ * (computeSyntheticSeismograms.f90:344-397); host arrays, any member may be NULL / 0:
+ *   tred        [nsta] reduction time of each station (s), as getTravelTimes - TIME_SHIFT_BUFFER
+ *               gives it with AUTOMATIC_TIMESHIFT; NULL: p->tred for all stations;
+ *   nsamp_true  [nsta] samples kept per station (1..nsamp, the reference's nstrue); the
+ *               samples after them are written as 0; NULL: all nsamp;
+ *   stafilter   [nsta][3][nf2] complex interleaved station filter (the reference's
+ *               stafilter(nf2, 3, nstat)), applied per component before the ZNE rotation;
+ *               NULL: the unit filter;
+ *   nstf, tanf_stf, stf  source wavelet of nstf <= 8192 float32 samples, the first at time
+ *               tanf_stf (s); convolveWithSourceWavelet (:463-484) after the inverse FFT.
+ * The options need nsamp <= 8192. */
+typedef struct gem_synth_station_opts {
+  const double* tred;
+  const int* nsamp_true;
+  const double* stafilter;
+  int nstf;
+  double tanf_stf;
+  const float* stf;
+} gem_synth_station_opts;
+int gem_synth_run_opts(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* gfkr, const float* gfki,
+                       int nsta, const double* theta, const double* phi, const double* propdir, int nmt,
+                       const double* mt, const gem_synth_station_opts* opts, float* traces);
+int gem_synth_run_device_opts(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const float* d_gfkr,
+                              const float* d_gfki, int nsta, const double* theta, const double* phi,
+                              const double* propdir, int nmt, const double* mt,
+                              const gem_synth_station_opts* opts, float* d_traces, void* stream);
+
 /* Batched transformFrequencyTime (frequencyTime.f90:55-113): ntr complex
  * spectra to ntr float32 time series.  Spectrum t is interleaved complex128
  * at sp + 2*t*ldsp; element j (0-based) is frequency j*df; elements

@@ -76,6 +76,13 @@ def lib():
                                                ctypes.c_int] + [ctypes.c_void_p] * 3
                                             + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                                ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_void_p])
+        L.oracle_synthetics_opts.argtypes = ([ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 4
+                                             + [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_int] + [ctypes.c_void_p] * 3
+                                             + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_double] + [ctypes.c_void_p] * 3
+                                             + [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_double, ctypes.c_void_p])
         L.oracle_degree_sums.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_void_p]
@@ -89,7 +96,7 @@ def lib():
 
 
 def _p(a):
-    return a.ctypes.data_as(ctypes.c_void_p)
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
 
 class Oracle:
@@ -298,4 +305,32 @@ def synthetics_src(source_type, global_, nf1, nf2, nwn, nwnmax, df, sigma, dwn, 
                                      int(velocity), tred, nsamp, dt, _p(out))
     if rc:
         raise RuntimeError("oracle_synthetics_src failed (%d)" % rc)
+    return out
+
+
+def synthetics_opts(source_type, global_, nf1, nf2, nwn, nwnmax, df, sigma, dwn, rearth, gr, gi, theta, phi, propdir,
+                    src, filspecs, velocity, tred, nsamp, dt, tred_sta=None, nstrue=None, stafilter=None, stf=None,
+                    tanf_stf=0.0):
+    """synthetics_src with the station loop's per-station options: tred_sta [nsta] reduction
+    times, nstrue [nsta] samples kept (later samples 0), stafilter complex [nsta, 3, nf2],
+    stf float32 [nstf] source wavelet starting at tanf_stf (computeSyntheticSeismograms.f90:344-397)."""
+    istyp = {"FORCE": 0, "MOMENT": 1}[source_type]
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkf = gr.shape
+    th = np.ascontiguousarray(theta, np.float64); ph = np.ascontiguousarray(phi, np.float64)
+    pd = np.ascontiguousarray(propdir, np.float64)
+    src = np.ascontiguousarray(src, np.float64).reshape(-1, 6 if istyp == 1 else 3)
+    fs = np.ascontiguousarray(filspecs, np.float64)
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    ts = None if tred_sta is None else np.ascontiguousarray(tred_sta, np.float64)
+    nt = None if nstrue is None else np.ascontiguousarray(nstrue, np.int32)
+    sf = None if stafilter is None else np.ascontiguousarray(stafilter, np.complex128)
+    w = None if stf is None else np.ascontiguousarray(stf, np.float32)
+    out = np.zeros((len(th), len(src), 3, nsamp), np.float32)
+    rc = lib().oracle_synthetics_opts(istyp, int(global_), nf1, nf2, _p(nwn), nwnmax, df, sigma, dwn, rearth, nkf, nsp,
+                                      _p(gr), _p(gi), len(th), _p(th), _p(ph), _p(pd), len(src), _p(src), _p(fs),
+                                      int(velocity), tred, _p(ts), _p(nt), _p(sf), 0 if w is None else len(w),
+                                      float(tanf_stf), _p(w), nsamp, dt, _p(out))
+    if rc:
+        raise RuntimeError("oracle_synthetics_opts failed (%d)" % rc)
     return out

@@ -500,11 +500,41 @@ int oracle_degree_sums_force(int nf1, int nf2, const int* nwn, int nwnmax, int n
 }  // extern "C"
 
 namespace {
+// Per-station options of the station loop (computeSyntheticSeismograms.f90:344-397); a null
+// member keeps the default: the common reduction time, all nsamp samples, the unit station
+// filter, no source wavelet.
+struct StationOpts {
+  const double* tred = nullptr;      // [nsta] reduction time of each station
+  const int* nstrue = nullptr;       // [nsta] samples kept (the rest are written as 0)
+  const double* stafil = nullptr;    // [nsta][3][nf2] complex interleaved station filter
+  int nstf = 0;                      // source wavelet samples
+  double tanfstf = 0.0;              // time of the wavelet's first sample
+  const float* stf = nullptr;
+};
+
+// convolveWithSourceWavelet (computeSyntheticSeismograms.f90:463-484): the sum runs in
+// double and is stored to single precision after every term, as the reference's real f(k)
+void convolveWavelet(int nd, int nstf, double tanf, double dt, const float* stf, float* urs) {
+  const int nhm = (int)std::floor(std::fabs(tanf) / dt + 0.5);
+  std::vector<float> f(nd);
+  for (int k = 1; k <= nd; ++k) {
+    float acc = 0.0f;
+    const int n0 = std::max(1, k - nd + nhm + 1), n1 = std::min(k + nhm, nstf);
+    for (int n = n0; n <= n1; ++n) {
+      const int j = n - nhm;
+      acc = (float)((double)acc + (dt * (double)urs[k - j]) * (double)stf[n - 1]);
+    }
+    f[k - 1] = acc;
+  }
+  for (int k = 0; k < nd; ++k) urs[k] = f[k];
+}
+
 // displacement spectra from the 14 sums or integrals hd, filters, rotation and
-// inverse FFT of every station and moment tensor (computeSyntheticSeismograms.f90:336-390)
+// inverse FFT of every station and moment tensor (computeSyntheticSeismograms.f90:336-397)
 int synth_from_sums(int istyp, const std::vector<double>& hd, int nf1, int nf2, double df, double sigma, int nsta,
                     const double* phi, const double* propdir, int nmt, const double* mt, const double* filspecs,
-                    int velocity, double tred, int nsamp, double dt, float* traces) {
+                    int velocity, double tred_all, int nsamp, double dt, float* traces,
+                    const StationOpts& o = StationOpts()) {
   const int nsum = istyp == 1 ? 14 : 7;
   int rc = 0;
   std::vector<zc> evf;
@@ -512,6 +542,9 @@ int synth_from_sums(int istyp, const std::vector<double>& hd, int nf1, int nf2, 
               nf1, nf2, df, sigma, evf);
   const zc ci = Z(0.0, 1.0);
   for (int is = 0; is < nsta; ++is) {
+    const double tred = o.tred ? o.tred[is] : tred_all;
+    const int nd = o.nstrue ? o.nstrue[is] : nsamp;
+    if (nd < 1 || nd > nsamp) return 2;
     double sphi = std::sin(phi[is]), cphi = std::cos(phi[is]);
     double s2phi = std::sin((double)2.0f * phi[is]), c2phi = std::cos((double)2.0f * phi[is]);
     double ca = std::cos(propdir[is]), sa = std::sin(propdir[is]);
@@ -541,7 +574,12 @@ int synth_from_sums(int istyp, const std::vector<double>& hd, int nf1, int nf2, 
       }
       for (int jf = nf1; jf <= nf2; ++jf) {
         zc tsf = zexp(((ci * TWO_PI_F) * (double)(jf - 1)) * df * tred) * std::exp(sigma * tred);
-        for (int c = 0; c < 3; ++c) zsp[c][jf] = ((zsp[c][jf] * evf[jf]) * Z(1.0, 0.0)) * tsf;
+        for (int c = 0; c < 3; ++c) {
+          const zc sf = o.stafil ? Z(o.stafil[(((size_t)is * 3 + c) * nf2 + (jf - 1)) * 2],
+                                     o.stafil[(((size_t)is * 3 + c) * nf2 + (jf - 1)) * 2 + 1])
+                                 : Z(1.0, 0.0);
+          zsp[c][jf] = ((zsp[c][jf] * evf[jf]) * sf) * tsf;
+        }
       }
       for (int jf = nf1; jf <= nf2; ++jf) {
         if (velocity) {
@@ -554,9 +592,11 @@ int synth_from_sums(int istyp, const std::vector<double>& hd, int nf1, int nf2, 
         zsp[0][jf] = ur; zsp[1][jf] = un; zsp[2][jf] = ue;
       }
       for (int c = 0; c < 3; ++c) {
-        rc = freqTime(nf1, nf2, df, sigma, zsp[c], nsamp, dt,
-                      traces + (((size_t)is * nmt + im) * 3 + c) * nsamp);
+        float* tr = traces + (((size_t)is * nmt + im) * 3 + c) * nsamp;
+        rc = freqTime(nf1, nf2, df, sigma, zsp[c], nsamp, dt, tr);
         if (rc) return rc;
+        if (o.nstf > 0) convolveWavelet(nd, o.nstf, o.tanfstf, dt, o.stf, tr);
+        for (int k = nd; k < nsamp; ++k) tr[k] = 0.0f;
       }
     }
   }
@@ -602,6 +642,34 @@ int oracle_synthetics_src(int istyp, int global, int nf1, int nf2, const int* nw
   if (rc) return rc;
   return synth_from_sums(istyp, hd, nf1, nf2, df, sigma, nsta, phi, propdir, nsrc, src, filspecs, velocity, tred,
                          nsamp, dt, traces);
+}
+
+// oracle_synthetics_src with the per-station options of the station loop: reduction time
+// per station, samples kept per station, station filter, source wavelet (any may be null / 0).
+int oracle_synthetics_opts(int istyp, int global, int nf1, int nf2, const int* nwn, int nwnmax, double df,
+                           double sigma, double dwn, double rearth, int nkfmax, int nsp, const float* gr,
+                           const float* gi, int nsta, const double* theta, const double* phi, const double* propdir,
+                           int nsrc, const double* src, const double* filspecs, int velocity, double tred,
+                           const double* tred_sta, const int* nstrue, const double* stafil, int nstf,
+                           double tanfstf, const float* stf, int nsamp, double dt, float* traces) {
+  const int nsum = istyp == 1 ? 14 : 7;
+  std::vector<double> hd((size_t)nsta * nf2 * nsum * 2, 0.0);
+  int rc;
+  if (global == 1) {
+    rc = istyp == 1 ? oracle_degree_sums(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, nsta, theta, hd.data())
+                    : oracle_degree_sums_force(nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, nsta, theta, hd.data());
+  } else {
+    std::vector<double> x(nsta);
+    for (int i = 0; i < nsta; ++i) x[i] = theta[i] * rearth;
+    rc = oracle_wavenumber_integrals_src(istyp, nf1, nf2, nwn, nwnmax, nkfmax, nsp, gr, gi, dwn, rearth, nsta,
+                                         x.data(), hd.data());
+  }
+  if (rc) return rc;
+  StationOpts o;
+  o.tred = tred_sta; o.nstrue = nstrue; o.stafil = stafil; o.nstf = nstf; o.tanfstf = tanfstf; o.stf = stf;
+  if (nstf > 0 && !stf) return 2;
+  return synth_from_sums(istyp, hd, nf1, nf2, df, sigma, nsta, phi, propdir, nsrc, src, filspecs, velocity, tred,
+                         nsamp, dt, traces, o);
 }
 
 // Synthetics of the regional mode (wavenumber integrals at distances theta * rearth,

@@ -109,3 +109,35 @@ def test_mixed_precision_synthetics_many_stations(gpu):
     assert np.all(np.isfinite(got))
     num, den = _rel(got, ref, w.nsamp)
     assert np.max(num / den) <= RTOL_MIXED
+
+
+@pytest.mark.parametrize("backend", [1, 2])
+def test_station_options_match_oracle(fkdata, backend):
+    """Per-station reduction times (as AUTOMATIC_TIMESHIFT sets them), samples kept per
+    station, station filters and a source wavelet (computeSyntheticSeismograms.f90:344-397,
+    463-484) against the oracle's station loop."""
+    import oracle
+    from gemini_unified_b200.fk import GeminiFK, synth_params
+    w, m, ex, g, fk, gr, gi = fkdata
+    theta, phi, propdir = w.stations()
+    theta, phi, propdir = theta[::5], phi[::5] + 0.4, propdir[::5] - 0.2
+    nsta = len(theta)
+    rng = np.random.default_rng(7)
+    mt = configs.unit_moment_tensors()[[0, 3, 5]]
+    tred = 30.0 + 4.0 * np.arange(nsta)
+    nstrue = np.full(nsta, w.nsamp, np.int32); nstrue[::3] = w.nsamp - 500
+    sf = (1.0 + 0.2 * rng.standard_normal((nsta, 3, g.nf2))) * np.exp(1j * 0.3 * rng.standard_normal((nsta, 3, g.nf2)))
+    tt = np.arange(40) * w.dt
+    stf = (np.exp(-((tt - 8.0) / 3.0) ** 2)).astype(np.float32)
+    sp = synth_params(g, 10, w.nsamp, w.dt, w.filspecs)
+    got = GeminiFK(m, ex, backend=backend).synthetics(sp, g.nwn, gr, gi, theta, phi, propdir, mt, tred=tred,
+                                                       nsamp_true=nstrue, stafilter=sf, stf=stf, tanf_stf=-4.0)
+    ref = oracle.synthetics_opts("MOMENT", 1, g.nf1, g.nf2, g.nwn, g.nwnmax, sp.df, sp.sigma, 0.0, m.rearth, gr, gi,
+                                 theta, phi, propdir, mt, w.filspecs, False, 0.0, w.nsamp, w.dt, tred_sta=tred,
+                                 nstrue=nstrue, stafilter=sf, stf=stf, tanf_stf=-4.0)
+    assert np.all(np.isfinite(got))
+    for s in range(0, nsta, 3):
+        assert np.all(got[s, :, :, nstrue[s]:] == 0)
+    num, den = _rel(got, ref, w.nsamp)
+    assert np.all(den > 0)
+    assert np.max(num / den) <= (1e-7 if backend == 1 else RTOL_MIXED)

@@ -268,3 +268,58 @@ def test_force_synthetics_are_linear_in_the_force():
         comb = 0.5 * tr[:, 0] - 2.0 * tr[:, 1] + 1.5 * tr[:, 2]
         assert np.abs(tr).max() > 0
         assert np.abs(tr[:, 3] - comb).max() <= 1e-5 * np.abs(comb).max()
+
+
+def _station_case():
+    nwn = np.array([0, 60, 64, 64, 64, 64, 64, 64], np.int32)
+    rng = np.random.default_rng(11)
+    gr = rng.standard_normal((10, int(nwn.sum()))).astype(np.float32)
+    gi = rng.standard_normal((10, int(nwn.sum()))).astype(np.float32)
+    mt = np.array([[1.0, -0.5, -0.5, 0.3, -0.2, 0.7]])
+    args = dict(nf1=2, nf2=8, nwn=nwn, nwnmax=64, df=1.0 / 256, sigma=0.002, dwn=2e-5, rearth=6371000.0, gr=gr, gi=gi,
+                theta=[0.02, 0.4, 1.3], phi=[0.3, 2.0, 4.0], propdir=[0.1, -0.7, 2.5], src=mt,
+                filspecs=[2, 0.005, 4, 0.06], velocity=0, nsamp=256, dt=1.0)
+    return args
+
+
+def test_station_options_default_to_the_plain_station_loop():
+    a = _station_case()
+    ref = oracle.synthetics_src("MOMENT", 1, tred=5.0, **a)
+    got = oracle.synthetics_opts("MOMENT", 1, tred=0.0, tred_sta=[5.0, 5.0, 5.0], nstrue=[256] * 3,
+                                 stafilter=np.ones((3, 3, 8), np.complex128), **a)
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_station_filter_scales_and_samples_are_cut():
+    a = _station_case()
+    ref = oracle.synthetics_src("MOMENT", 1, tred=0.0, **a).astype(np.float64)
+    sf = np.ones((3, 3, 8), np.complex128)
+    sf[1, 2, :] = 2.0   # station 1, third component (before rotation) doubled
+    got = oracle.synthetics_opts("MOMENT", 1, tred=0.0, stafilter=sf, nstrue=[256, 200, 100], **a).astype(np.float64)
+    np.testing.assert_array_equal(got[0], ref[0])
+    assert np.all(got[1, :, :, 200:] == 0) and np.all(got[2, :, :, 100:] == 0)
+    np.testing.assert_array_equal(got[2, :, :, :100], ref[2, :, :, :100])
+    # the transverse component before rotation is doubled: Z is unchanged, N and E change
+    np.testing.assert_array_equal(got[1, :, 0, :200], ref[1, :, 0, :200])
+    assert np.abs(got[1, :, 1:, :200] - ref[1, :, 1:, :200]).max() > 0
+
+
+def test_source_wavelet_convolution_against_a_direct_loop():
+    """convolveWithSourceWavelet as written in the reference: f(k) = sum over the wavelet
+    of dt * u(k - n + nhm + 1) * stf(n), nhm samples of it before t = 0, rounded to
+    single precision after every term."""
+    a = _station_case()
+    stf = np.array([0.1, 0.5, 1.0, 0.4, -0.2, 0.05], np.float32)
+    tanf = -2.0
+    plain = oracle.synthetics_opts("MOMENT", 1, tred=0.0, nstrue=[256, 180, 256], **a)
+    got = oracle.synthetics_opts("MOMENT", 1, tred=0.0, nstrue=[256, 180, 256], stf=stf, tanf_stf=tanf, **a)
+    nhm = int(np.floor(abs(tanf) / a["dt"] + 0.5))
+    for s, nd in ((0, 256), (1, 180)):
+        for c in range(3):
+            u = plain[s, 0, c]
+            for k in (1, 2, 3, 50, nd - 2, nd):
+                acc = np.float32(0.0)
+                for n in range(max(1, k - nd + nhm + 1), min(k + nhm, len(stf)) + 1):
+                    j = n - nhm
+                    acc = np.float32(float(acc) + (a["dt"] * float(u[k - j])) * float(stf[n - 1]))
+                assert got[s, 0, c, k - 1] == acc
