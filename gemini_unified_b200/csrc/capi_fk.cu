@@ -894,6 +894,72 @@ int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_l
   return GEM_OK;
 }
 
+// Travel-time table by ray tracing (computeTravelTimeTable.f90:160-226) on the
+// context's model and nodes: model at the reference frequency, one GPU thread per
+// turning radius.  Host outputs sized by ntp_cap; *ntp receives the count.
+int gem_ray_table(gem_ctx* ctx, int stype, int attmode, double eps, double drtp, double rtmax, int ntp_cap,
+                  int* ntp, double* rtp, double* slowness, float* table, int32_t* status) {
+  if (!ctx) return GEM_ERROR;
+  if (!ctx->have_model || !ctx->have_nodes) return fail(ctx, "travel times: load the model and the nodes first");
+  if (stype != 0 && stype != 1) return fail(ctx, "travel times: ray type must be 0 (P) or 1 (S)");
+  if (attmode < 0 || attmode > 3 || !(eps > 0) || !(drtp > 0)) return fail(ctx, "travel times: invalid parameters");
+  if (!ntp || !rtp || !slowness || !table || !status) return fail(ctx, "travel times: null output");
+  const int n = (int)((double)(int)(rtmax - ctx->roc) / drtp + 1.0);   // computeTravelTimeTable.f90:163
+  *ntp = n;
+  if (n < 1) return fail(ctx, "travel times: TURNING_NODES_RMAX below the core-mantle boundary");
+  if (n > ntp_cap) return fail(ctx, "travel times: %d turning radii do not fit %d", n, ntp_cap);
+  CK(cudaSetDevice(ctx->device));
+  FKStatic P;
+  memset(&P, 0, sizeof P);
+  P.nlay = ctx->nlay; P.nk = ctx->nk; P.noc = ctx->noc; P.nic = ctx->nic; P.equidis = ctx->equidis;
+  P.fsflag = ctx->fsflag; P.nnod = ctx->nnod;
+  P.rearth = ctx->rearth; P.ric = ctx->ric; P.roc = ctx->roc; P.rhs = ctx->rb[1];
+  for (int i = 1; i <= ctx->nlay; ++i) {
+    P.rb[i] = ctx->rb[i]; P.drk[i] = ctx->drk[i]; P.iflso[i] = ctx->iflso[i]; P.iktop[i] = ctx->iktop[i];
+  }
+  for (int i = 1; i <= ctx->nk; ++i) P.rk[i] = ctx->rk[i];
+  for (int i = 1; i <= ctx->nnod; ++i) { P.rnod[i] = ctx->rnod[i]; P.state[i] = ctx->state[i]; P.layer[i] = ctx->layer[i]; }
+  // the model at the reference frequency: one slot with f = (2 - 1) * fref
+  const int K1 = ctx->nk + 1;
+  if (grow(ctx, ctx->d_spl, ctx->spl_cap, (size_t)K1 * SPL_STRIDE)) return GEM_ERROR;
+  if (grow(ctx, ctx->d_slots, ctx->slots_cap, (size_t)2)) return GEM_ERROR;
+  const int slots[2] = {2, 0};
+  CK(cudaMemcpy(ctx->d_slots, slots, sizeof slots, cudaMemcpyHostToDevice));
+  PrepArgs A;
+  A.nslot = 1; A.nk = ctx->nk; A.nlay = ctx->nlay; A.attmode = attmode; A.df = ctx->fref; A.fref = ctx->fref;
+  A.jf = ctx->d_slots;
+  A.ro = ctx->d_knots; A.vpv = ctx->d_knots + K1; A.vph = ctx->d_knots + 2 * K1; A.vsv = ctx->d_knots + 3 * K1;
+  A.vsh = ctx->d_knots + 4 * K1; A.eta = ctx->d_knots + 5 * K1; A.qkinv = ctx->d_knots + 6 * K1;
+  A.qminv = ctx->d_knots + 7 * K1; A.rk = ctx->d_knots + 8 * K1;
+  A.iktop = ctx->d_lay; A.ikbot = ctx->d_lay + (ctx->nlay + 1);
+  A.spl = ctx->d_spl;
+  CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
+  CK(launch_prep(A, ctx->d_err, nullptr));
+  // outputs
+  const size_t tb = (size_t)n * ctx->nnod * 2 * sizeof(float);
+  char* d = nullptr;
+  CK(cudaMalloc(&d, tb + (size_t)n * (2 * sizeof(double) + sizeof(int)) + 64));
+  double* d_rtp = (double*)d;
+  double* d_slow = d_rtp + n;
+  int* d_st = (int*)(d_slow + n);
+  float* d_tab = (float*)(((uintptr_t)(d_st + n) + 15) / 16 * 16);
+  const double a0 = std::atan(std::sqrt(2.0 * eps));   // the start values of the ray (:204)
+  cudaError_t e = gem_ray::launch_ray_table(P, ctx->d_spl, n, stype, eps, drtp, a0, d_rtp, d_slow, d_tab, d_st, nullptr);
+  int herr = 0;
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(rtp, d_rtp, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(slowness, d_slow, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(status, d_st, n * sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(table, d_tab, tb, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(ctx, "travel times: %s", cudaGetErrorString(e));
+  if (herr) return fail(ctx, "Cubic spline interpolation not successful (code %d)", herr);
+  for (int i = 0; i < n; ++i)
+    if (status[i]) return fail(ctx, "travel times: the ray of turning radius %g failed (status %d)", rtp[i], status[i]);
+  return GEM_OK;
+}
+
 int gem_order_target(gem_ctx* ctx, int k) {
   if (!ctx) return GEM_ERROR;
   if (k == 0) k = 6;

@@ -110,5 +110,10 @@ cudaError_t launch_poly(const PrepArgs& A, double* poly, cudaStream_t st);
   }
 GEM_DECLARE_SOLVER(gem_plain)
 GEM_DECLARE_SOLVER(gem_fast)
+namespace gem_ray {
+// travel-time table by ray tracing (raytable.cu): one thread per turning radius
+cudaError_t launch_ray_table(const gem::FKStatic& P, const double* spl, int ntp, int stype, double eps, double drtp,
+                             double a0, double* rtp, double* slowness, float* table, int* status, cudaStream_t st);
+}
 namespace gem {
 }  // namespace gem

@@ -80,6 +80,10 @@ def lib() -> ctypes.CDLL:
         L.gem_steplog.argtypes = [vp, ctypes.c_longlong]
         L.gem_steplog_read.argtypes = [vp, vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
         L.gem_order_target.argtypes = [vp, ctypes.c_int]
+        L.gem_ray_table.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp, vp, vp, vp]
+        L.gem_travel_times.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_int, vp, vp, vp]
         L.gem_fk_schedule_set.argtypes = [vp, vp]
         L.gem_fk_schedule_get.argtypes = [vp, vp]
         L.gem_fk_autotune.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
@@ -336,6 +340,37 @@ class GeminiFK:
                                           _ptr(ms), s, d))
         return {"schedule": [int(x) for x in s], "defer": [int(x) for x in d],
                 "ms": ms.reshape(NSCHED + NDEFER, 3), "jf": [int(jf_first), int(jf_last)]}
+
+    def ray_table(self, stype: str = "P", attmode: int = 3, eps: float = 1e-6, drtp: float = 10000.0,
+                  rtmax: float = 0.0):
+        """Travel-time table by ray tracing (computeTravelTimeTable): returns
+        (rtp [ntp], slowness [ntp], table float32 [ntp, nnod, 2] of (Delta, T)).
+        rtmax defaults to the radius of the top node."""
+        if not rtmax:
+            rtmax = float(self.nodes.r[-1])
+        cap = int((rtmax - self.model.roc) / drtp) + 2
+        n = ctypes.c_int()
+        rtp = np.zeros(cap); slow = np.zeros(cap)
+        table = np.zeros((cap, self.nodes.nnod, 2), np.float32)
+        status = np.zeros(cap, np.int32)
+        self._check(lib().gem_ray_table(self._h, {"P": 0, "S": 1}[stype], int(attmode), float(eps), float(drtp),
+                                        float(rtmax), cap, ctypes.byref(n), _ptr(rtp), _ptr(slow), _ptr(table),
+                                        _ptr(status)))
+        k = n.value
+        return rtp[:k], slow[:k], table[:k]
+
+    def travel_times(self, rtp, slowness, table, rs, re, delta, tele=True):
+        """Travel times (s) of the table (float32 as stored) for source radius rs and
+        receivers at radii re and distances delta (rad) (getTravelTimes)."""
+        rnod = np.ascontiguousarray(self.nodes.r, np.float32)
+        rtp = np.ascontiguousarray(rtp, np.float32); sl = np.ascontiguousarray(slowness, np.float32)
+        tb = np.ascontiguousarray(table, np.float32)
+        re = np.ascontiguousarray(np.broadcast_to(re, np.shape(delta)), np.float64)
+        de = np.ascontiguousarray(delta, np.float64)
+        tt = np.zeros(len(de))
+        self._check(lib().gem_travel_times(self._h, len(rnod), len(rtp), _ptr(rnod), _ptr(rtp), _ptr(sl), _ptr(tb),
+                                           1 if tele else 0, float(rs), len(de), _ptr(re), _ptr(de), _ptr(tt)))
+        return tt
 
     def order_target(self, k: int):
         """Attempt the step-size control aims at (fast backend; 3..7, 0 restores the reference's 6)."""

@@ -219,6 +219,28 @@ int gem_synth_run_device_opts(gem_ctx* ctx, const gem_synth_params* p, const int
                               const double* propdir, int nmt, const double* mt,
                               const gem_synth_station_opts* opts, float* d_traces, void* stream);
 
+/* Travel-time table by ray tracing: replaces computeTravelTimeTable
+ * (computeTravelTimeTable.f90:160-226) on the context's model and nodes.  stype 0
+ * P, 1 S; the model at its reference frequency under attmode; eps the accuracy
+ * (ACCURACY), drtp and rtmax the spacing and the largest turning radius
+ * (TURNING_NODES_DR, TURNING_NODES_RMAX, m).  ntp = int(rtmax - roc)/drtp + 1 turning
+ * radii rtp[i] = roc + i*drtp with slowness[i] = rtp/v(rtp) (s/rad), and
+ * table[(i*nnod + j)*2 + {0,1}] = (Delta (rad), T (s)) of ray i at node j (0 where
+ * the ray does not reach): the reference's rayTable(2, nnod, ntp).  One GPU thread
+ * per ray; *ntp is set before the size check against ntp_cap. */
+int gem_ray_table(gem_ctx* ctx, int stype, int attmode, double eps, double drtp, double rtmax, int ntp_cap,
+                  int* ntp, double* rtp, double* slowness, float* table, int32_t* status);
+
+/* Travel times from such a table as the reference reads it back (float32 radii,
+ * slownesses and table; getTravelTimes, travelTimes.f90:105-260): source radius rs,
+ * receivers at radii re[s] and epicentral distances delta[s] (rad) -> tt[s] (s).
+ * istele 1 for a TELE table (turning points in the lower mantle), 0 LOCAL.  The
+ * reduction time of AUTOMATIC_TIMESHIFT is tt - TIME_SHIFT_BUFFER
+ * (computeSyntheticSeismograms.f90:344-350); pass it in gem_synth_station_opts. */
+int gem_travel_times(gem_ctx* ctx, int nnod, int ntp, const float* rnod, const float* rtp, const float* slowness,
+                     const float* table, int istele, double rs, int n, const double* re, const double* delta,
+                     double* tt);
+
 /* Batched transformFrequencyTime (frequencyTime.f90:55-113): ntr complex
  * spectra to ntr float32 time series.  Spectrum t is interleaved complex128
  * at sp + 2*t*ldsp; element j (0-based) is frequency j*df; elements

@@ -83,6 +83,9 @@ def lib():
                                                 ctypes.c_double] + [ctypes.c_void_p] * 3
                                              + [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
                                                 ctypes.c_double, ctypes.c_void_p])
+        L.oracle_ray_table.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_degree_sums.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_void_p]
@@ -129,6 +132,16 @@ class Oracle:
         if getattr(self, "h", None):
             lib().oracle_destroy(self.h)
             self.h = None
+
+    def ray_table(self, stype, attmode, eps, drtp, rtmax, cap, nnod):
+        """computeTravelTimeTable: (ntp, rtp, slowness, table float32 [ntp, nnod, 2], status)."""
+        n = ctypes.c_int()
+        rtp = np.zeros(cap); slow = np.zeros(cap)
+        table = np.zeros((cap, nnod, 2), np.float32); st = np.zeros(cap, np.int32)
+        rc = lib().oracle_ray_table(self.h, {"P": 0, "S": 1}[stype], attmode, eps, drtp, rtmax, cap, ctypes.byref(n),
+                                    _p(rtp), _p(slow), _p(table), _p(st))
+        k = n.value
+        return rc, rtp[:k], slow[:k], table[:k], st[:k]
 
     def nodes(self):
         n = lib().oracle_nnod(self.h)

@@ -1519,6 +1519,202 @@ struct Ctx {
   Nodes ex;
 };
 
+// ===========================================================================
+//  Travel-time table by ray tracing (computeTravelTimeTable.f90:178-226): for
+//  each turning radius, Delta(r) and T(r) of the ray integrated upward to the
+//  top node with the real Bulirsch-Stoer step (episode/realBulirschStep.f90)
+//  and the ray system (rayOdeSystem.f90:151-170).
+// ===========================================================================
+struct RayEnv {
+  const Model* m;
+  const Nodes* ex;
+  const Spline* s;
+  int nl;
+  int stype;   // 0 P, 1 S
+  double p;    // angular slowness r/v at the turning point
+};
+
+// getPVelocitySplineEarthmodel / getSVelocitySplineEarthmodel (splineEarthmodelCoefficients.f90:192-210)
+static double rayVelocity(const RayEnv& e, int nl, double r) {
+  double ro;
+  zc z[7];
+  evalSpline(*e.s, r, nl, ro, z);
+  if (e.stype == 0) return std::sqrt((z[5].re + (4.0 / 3.0) * z[6].re) / ro);
+  return std::sqrt(z[6].re / ro);
+}
+
+// derivativeRealRayOdeSystem (rayOdeSystem.f90:151-170)
+static void rayDerivative(const RayEnv& e, double x, double* dy) {
+  const double v = rayVelocity(e, e.nl, x);
+  const double t = x / v;
+  const double ur2 = t * t;
+  const double q = std::sqrt(ur2 - e.p * e.p);
+  dy[0] = e.p / (q * x);
+  dy[1] = ur2 / (q * x);
+}
+
+struct RayEngine {
+  const RayEnv* env;
+  double eps;
+  int donetry;
+  bool success;
+  double ysol[7][2];
+  double yext[2];
+
+  // doNonLinearModifiedMidpointRealBulirsch (realBulirschStep.f90:222-252)
+  void midpoint(int jtry, double h, double xstart, const double* y0) {
+    const int nstep = SEQDIV_BS[jtry - 1];
+    const double hdiv = h / (double)nstep;
+    double z0[2], z1[2], z2[2], d[2];
+    for (int i = 0; i < 2; ++i) z0[i] = y0[i];
+    rayDerivative(*env, xstart, d);
+    for (int i = 0; i < 2; ++i) z1[i] = z0[i] + hdiv * d[i];
+    for (int m = 1; m <= nstep - 1; ++m) {
+      const double x = xstart + (double)m * hdiv;
+      rayDerivative(*env, x, d);
+      for (int i = 0; i < 2; ++i) z2[i] = z0[i] + (2.0 * hdiv) * d[i];
+      for (int i = 0; i < 2; ++i) { z0[i] = z1[i]; z1[i] = z2[i]; }
+    }
+    rayDerivative(*env, xstart + h, d);
+    for (int i = 0; i < 2; ++i) ysol[jtry - 1][i] = 0.5 * ((z1[i] + z0[i]) + hdiv * d[i]);
+    donetry = jtry;
+  }
+  // extrapolateRealBulirsch (:258-290): the whole tableau from the stored solutions
+  void extrapolate(double hs, double* yy, double* dy) {
+    const int n = donetry;
+    double x[7], c[7][2], dd[7][2], u[2];
+    for (int j = 0; j < n; ++j) x[j] = hs / (double)SEQDIV_BS[j];
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < 2; ++i) { c[j][i] = ysol[j][i]; dd[j][i] = ysol[j][i]; }
+    int js = n;
+    for (int i = 0; i < 2; ++i) yy[i] = ysol[js - 1][i];
+    for (int m = 1; m <= n - 1; ++m) {
+      for (int i = 1; i <= n - m; ++i) {
+        const double h = x[i - 1] - x[i + m - 1];
+        for (int v = 0; v < 2; ++v) {
+          u[v] = (c[i][v] - dd[i - 1][v]) / h;
+          c[i - 1][v] = x[i - 1] * u[v];
+          dd[i - 1][v] = x[i + m - 1] * u[v];
+        }
+      }
+      for (int v = 0; v < 2; ++v) { yy[v] = yy[v] + dd[js - 2][v]; dy[v] = dd[js - 2][v]; }
+      js = js - 1;
+    }
+  }
+  // doFullStepRealBulirsch (:130-176)
+  void fullStep(double h, double xstart, const double* y) {
+    success = false;
+    donetry = 0;
+    int ntry = MINTRY_BS, nfirst = 1;
+    double yy[2], dy[2];
+    for (;;) {
+      for (int j = nfirst; j <= ntry; ++j) midpoint(j, h, xstart, y);
+      extrapolate(h, yy, dy);
+      const double errmax = std::sqrt((dy[0] * dy[0] + dy[1] * dy[1]) / (yy[0] * yy[0] + yy[1] * yy[1]));
+      if (errmax / eps < 1.0) {
+        yext[0] = yy[0]; yext[1] = yy[1];
+        success = true;
+        return;
+      }
+      if (ntry < MAXTRY_BS) { ntry = ntry + 1; nfirst = ntry; }
+      else return;
+    }
+  }
+  // adjustStepSizeRealBulirsch (:295-307)
+  void adjust(double& h, bool ok) {
+    if (ok) {
+      if (donetry > OPTTRY_BS) h = h * SHRINK_BS;
+      else if (donetry < OPTTRY_BS) h = h * GROW_BS;
+    } else {
+      h = 0.5 * h / 1.0;
+    }
+  }
+};
+
+// integrationStep.f90:98-190 for the ray system
+static int rayIntegrationStep(RayEngine& eng, double& hdid, double x1, double x2, double* y) {
+  if (std::fabs(x2 - x1) < MINSIZE_IS) return 0;
+  double x = x1;
+  double h = std::copysign(hdid, x2 - x1);
+  double ys[2] = {y[0], y[1]};
+  int nstep = 0;
+  while (nstep < MAXNUM_IS) {
+    if ((x + h - x2) * (x + h - x1) > 0.0) h = x2 - x;
+    eng.fullStep(h, x, ys);
+    nstep++;
+    if (eng.success) {
+      x = x + h;
+      ys[0] = eng.yext[0]; ys[1] = eng.yext[1];
+      if (std::fabs(x - x2) < MINSIZE_IS) { y[0] = ys[0]; y[1] = ys[1]; return 0; }
+      eng.adjust(h, true);
+      hdid = h;
+    } else {
+      eng.adjust(h, false);
+      if (std::fabs(h) < MINSIZE_IS) return 1;
+    }
+  }
+  return 2;
+}
+
+// propagateOde.f90:132-331 for the ray system (no renormalisation); yn[k*2 + v]
+// holds the solution at the k-th node of the interval, jl..jr its indices.
+static int rayPropagate(RayEnv& env, double eps, double x1, double x2, double htry, const double* ystart,
+                        std::vector<double>& yn, int& jlo, int& jro) {
+  double y[2] = {ystart[0], ystart[1]};
+  std::vector<double> xn, xd;
+  int jl, jr;
+  Env ge;   // node and discontinuity lists of the gemini environment (same rules, rayIntegrationEnvironment.f90:43-121)
+  ge.m = env.m; ge.ex = env.ex; ge.s = env.s; ge.nl = env.nl; ge.omre = ge.omim = ge.dll1 = 0.0;
+  getNodes(ge, x1, x2, jl, jr, xn);
+  jlo = jl; jro = jr;
+  const int nnod = (int)xn.size();
+  getDiscos(ge, x1, x2, jl, jr, xd);
+  const int nd = (int)xd.size();
+  yn.assign((size_t)nnod * 2, 0.0);
+  const int idir = (int)std::copysign(1.0, x2 - x1);
+  if (nd > 0 && ((x1 - xd[0]) * idir > 0 || (xd[nd - 1] - x2) * idir > 0)) return 4;
+  if (nnod > 0 && ((x1 - xn[0]) * idir > 0 || (xn[nnod - 1] - x2) * idir > 0)) return 4;
+  int jnod = 1, jd = 1;
+  if (std::fabs(x2 - x1) < MINSIZE_IS && nnod == 0) return 0;
+  if (std::fabs(x2 - x1) < MINSIZE_IS && nnod > 1) return 4;
+  if (std::fabs(x2 - x1) < MINSIZE_IS && nnod == 1) {
+    yn[0] = y[0]; yn[1] = y[1];
+    jnod = 2;
+  } else {
+    RayEngine eng;
+    eng.env = &env; eng.eps = eps;
+    double hdid = htry, xa = x1;
+    while (std::fabs(x2 - xa) > MINSIZE_IS) {
+      double steps[3];
+      steps[2] = std::fabs(x2 - xa);
+      steps[0] = 2.0 * std::fabs(x2 - x1);
+      steps[1] = 3.0 * std::fabs(x2 - x1);
+      if (jnod <= nnod) steps[0] = std::fabs(xn[jnod - 1] - xa);
+      if (jd <= nd) steps[1] = std::fabs(xd[jd - 1] - xa);
+      int kmin = 0;
+      for (int k = 1; k < 3; ++k) if (steps[k] < steps[kmin]) kmin = k;
+      const double xe = xa + idir * steps[kmin];
+      int rc = rayIntegrationStep(eng, hdid, xa, xe, y);
+      if (rc) return rc;
+      if (kmin == 0) {
+        yn[(jnod - 1) * 2] = y[0]; yn[(jnod - 1) * 2 + 1] = y[1];
+        jnod++;
+        if (std::fabs(steps[0] - steps[1]) < MINSIZE_IS) { env.nl += idir; jd++; }
+      } else if (kmin == 1) {
+        jd++;
+        env.nl += idir;
+        if (std::fabs(steps[0] - steps[1]) < MINSIZE_IS) {
+          yn[(jnod - 1) * 2] = y[0]; yn[(jnod - 1) * 2 + 1] = y[1];
+          jnod++;
+        }
+      }
+      xa = xe;
+    }
+  }
+  if (jnod - 1 != nnod || jd - 1 != nd) return 4;
+  return 0;
+}
+
 extern "C" {
 
 typedef struct {
@@ -1564,6 +1760,49 @@ int oracle_node_index(void* h, double rs) {
 }
 
 // spline coefficients at frequency f: ro, ro2 [nk], el, el2 [nk*7] interleaved complex
+// Travel-time table (computeTravelTimeTable.f90:160-226): turning radii rtp[i] =
+// roc + i*drtp for i < ntp = int(rtmax - roc)/drtp + 1, slowness[i] = rtp/v(rtp), and
+// table[(i*nnod + j)*2 + {0,1}] = (Delta, T) of that ray at node j (0 where the ray
+// does not reach).  stype 0 P, 1 S.  Returns 0, or 2 if ntp > ntp_cap, or the first
+// integrator status.
+int oracle_ray_table(void* h, int stype, int attmode, double eps, double drtp, double rtmax, int ntp_cap,
+                     int* ntp_out, double* rtp_out, double* slowness, float* table, int* status) {
+  Ctx* c = (Ctx*)h;
+  const Model& m = c->m;
+  const int ntp = (int)((double)(int)(rtmax - m.roc) / drtp + 1.0);
+  *ntp_out = ntp;
+  if (ntp > ntp_cap || ntp < 1) return 2;
+  Spline s;
+  if (computeSpline(m, m.fref, attmode, s)) return 2;
+  const int nnod = c->ex.nnod;
+  const double a0 = std::atan(std::sqrt(2.0 * eps));
+  int first = 0;
+  for (int n = 0; n < ntp; ++n) {
+    const double rtp = m.roc + (double)n * drtp;
+    rtp_out[n] = rtp;
+    int nl, top;
+    layerIndex(m, rtp, nl, top);
+    if (top == 1) nl = nl + 1;
+    RayEnv e;
+    e.m = &m; e.ex = &c->ex; e.s = &s; e.nl = nl; e.stype = stype;
+    e.p = rtp / rayVelocity(e, nl, rtp);
+    slowness[n] = e.p;
+    const double ys[2] = {a0, e.p * a0};
+    std::vector<double> yn;
+    int jl = 0, jr = -1;
+    for (int j = 0; j < nnod; ++j) table[((size_t)n * nnod + j) * 2] = table[((size_t)n * nnod + j) * 2 + 1] = 0.0f;
+    int rc = rayPropagate(e, eps, rtp * (1.0 + eps), c->ex.r[nnod], drtp, ys, yn, jl, jr);
+    if (!rc && jr - jl < 0) rc = 4;
+    status[n] = rc;
+    if (rc) { if (!first) first = rc; continue; }
+    for (int j = jl; j <= jr; ++j) {
+      table[((size_t)n * nnod + (j - 1)) * 2] = (float)yn[(j - jl) * 2];
+      table[((size_t)n * nnod + (j - 1)) * 2 + 1] = (float)yn[(j - jl) * 2 + 1];
+    }
+  }
+  return first;
+}
+
 int oracle_spline(void* h, double f, int attmode, double* ro, double* ro2, double* el, double* el2) {
   Ctx* c = (Ctx*)h;
   Spline s;

@@ -323,3 +323,23 @@ def test_source_wavelet_convolution_against_a_direct_loop():
                     j = n - nhm
                     acc = np.float32(float(acc) + (a["dt"] * float(u[k - j])) * float(stf[n - 1]))
                 assert got[s, 0, c, k - 1] == acc
+
+
+def test_ray_table_slowness_is_the_travel_time_slope():
+    """Along the surface node, T(p) and Delta(p) of the rays obey dT/dDelta = p
+    (computeTravelTimeTable's table; the ray parameter is the slope of the
+    travel-time curve)."""
+    m = configs.WORKLOADS["batched_fk"].model()
+    ex = configs.WORKLOADS["batched_fk"].nodes(m)
+    o = oracle.Oracle(m, ex)
+    rc, rtp, slow, tab, st = o.ray_table("P", 3, 1e-6, 20000.0, float(ex.r[-1]), 400, ex.nnod)
+    assert rc == 0 and np.all(st == 0) and len(rtp) == int(int(ex.r[-1] - m.roc) / 20000.0 + 1)
+    # lower-mantle turning points (the upper mantle's discontinuities fold the curve)
+    low = rtp <= 5600000.0
+    d = tab[low, -1, 0].astype(np.float64); t = tab[low, -1, 1].astype(np.float64)
+    assert np.all(np.diff(d) < 0) and np.all(np.diff(t) < 0)   # deeper turning points go farther
+    slope = np.diff(t) / np.diff(d)
+    pm = 0.5 * (slow[low][1:] + slow[low][:-1])
+    assert np.abs(slope / pm - 1.0).max() < 2e-3
+    # the deepest ray grazes the core-mantle boundary near 98 degrees (two legs)
+    assert 95.0 < 2 * np.degrees(d[0]) < 101.0
