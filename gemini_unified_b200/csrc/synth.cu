@@ -820,9 +820,47 @@ int synth_run_host(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, cons
       cudaMemcpy(dgi, gi, nin * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
     rc = gem_set_error(ctx, "synthetics: copy of the FK spectra failed");
   }
-  if (rc == GEM_OK) rc = synth_run(ctx, p, nwn, dgr, dgi, nsta, theta, phi, propdir, nmt, mt, o, dtr, nullptr);
-  if (rc == GEM_OK && cudaMemcpy(traces, dtr, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
-    rc = gem_set_error(ctx, "synthetics: copy of the traces failed");
+  if (rc != GEM_OK) return rc;
+  // Into pinned host memory the traces of a group of stations travel while the
+  // next group is computed; otherwise all stations at once, then one copy.
+  cudaPointerAttributes pa{};
+  const bool pinned = cudaPointerGetAttributes(&pa, traces) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  cudaGetLastError();   // clear the error state of a failed query (pageable memory on some drivers)
+  const int ngroups = (pinned && nsta >= 1024) ? 4 : 1;
+  if (ngroups == 1) {
+    rc = synth_run(ctx, p, nwn, dgr, dgi, nsta, theta, phi, propdir, nmt, mt, o, dtr, nullptr);
+    if (rc == GEM_OK && cudaMemcpy(traces, dtr, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = gem_set_error(ctx, "synthetics: copy of the traces failed");
+    return rc;
+  }
+  cudaStream_t cs = nullptr;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+    return gem_set_error(ctx, "synthetics: copy stream creation failed");
+  const size_t per_sta = (size_t)nmt * 3 * p->nsamp;
+  double ms_sum = 0.0;
+  for (int g = 0; g < ngroups && rc == GEM_OK; ++g) {
+    const int s0 = (int)((long long)nsta * g / ngroups), s1 = (int)((long long)nsta * (g + 1) / ngroups);
+    gem_synth_station_opts og{};
+    const gem_synth_station_opts* op = nullptr;
+    if (o) {
+      og = *o;
+      if (o->tred) og.tred = o->tred + s0;
+      if (o->nsamp_true) og.nsamp_true = o->nsamp_true + s0;
+      if (o->stafilter) og.stafilter = o->stafilter + (size_t)s0 * 3 * p->nf2 * 2;
+      op = &og;
+    }
+    rc = synth_run(ctx, p, nwn, dgr, dgi, s1 - s0, theta + s0, phi + s0, propdir + s0, nmt, mt, op,
+                   dtr + (size_t)s0 * per_sta, nullptr);
+    gem_stats stt;
+    if (rc == GEM_OK && gem_stats_get(ctx, &stt) == GEM_OK) ms_sum += stt.synth_ms;
+    if (rc == GEM_OK &&
+        cudaMemcpyAsync(traces + (size_t)s0 * per_sta, dtr + (size_t)s0 * per_sta, (size_t)(s1 - s0) * per_sta *
+                        sizeof(float), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+      rc = gem_set_error(ctx, "synthetics: copy of the traces failed");
+  }
+  if (cudaStreamSynchronize(cs) != cudaSuccess && rc == GEM_OK) rc = gem_set_error(ctx, "synthetics: copy of the traces failed");
+  cudaStreamDestroy(cs);
+  gem_note_synth_ms(ctx, (float)ms_sum);   // device time of all groups
   return rc;
 }
 }  // namespace

@@ -141,3 +141,39 @@ def test_station_options_match_oracle(fkdata, backend):
     num, den = _rel(got, ref, w.nsamp)
     assert np.all(den > 0)
     assert np.max(num / den) <= (1e-7 if backend == 1 else RTOL_MIXED)
+
+
+@pytest.mark.parametrize("backend", [1, 2])
+def test_pinned_output_overlaps_station_groups(gpu, backend):
+    """Into pinned host memory the host entry point computes the stations in groups
+    and copies each group's traces while the next one runs.  The FP64 form gives the
+    single-pass traces bit for bit (every station's sums and transforms are its own);
+    the mixed form's degree scales span the stations of a call, so it agrees to its
+    seismogram bar."""
+    import ctypes
+    import torch
+    from gemini_unified_b200.fk import GeminiFK, lib, synth_params, _ptr
+    from gemini_unified_b200.synth_run import fk_coefficients
+    w = configs.WORKLOADS["batched_fk"]
+    m = w.model()
+    ex = w.nodes(m)
+    g = M.frequency_grid(w.params, m.rearth)
+    gr, gi = fk_coefficients(10, int(g.nkfmax))
+    theta, phi, propdir = w.stations()
+    sel = slice(0, 4000, 3)   # 1334 stations: four groups
+    theta, phi, propdir = (np.ascontiguousarray(a[sel]) for a in (theta, phi, propdir))
+    mt = np.ascontiguousarray(configs.unit_moment_tensors()[[0, 4]], np.float64)
+    sp = synth_params(g, 10, w.nsamp, w.dt, w.filspecs)
+    fk = GeminiFK(m, ex, backend=backend)
+    ref = fk.synthetics(sp, g.nwn, gr, gi, theta, phi, propdir, mt)
+    out = torch.zeros(ref.shape, dtype=torch.float32, pin_memory=True).numpy()
+    nwn = np.ascontiguousarray(g.nwn, np.int32)
+    for _ in range(2):
+        out[:] = 0
+        fk._check(lib().gem_synth_run(fk._h, ctypes.byref(sp), _ptr(nwn), _ptr(gr), _ptr(gi), len(theta), _ptr(theta),
+                                      _ptr(phi), _ptr(propdir), len(mt), _ptr(mt), _ptr(out)))
+        if backend == 1:
+            np.testing.assert_array_equal(out, ref)
+        else:
+            num, den = _rel(out, ref, w.nsamp)
+            assert np.max(num / den) <= RTOL_MIXED
