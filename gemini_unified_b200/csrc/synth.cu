@@ -651,7 +651,7 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
   // frequency offsets in the FK slab
   std::vector<int> koff(nf);
   long long kk = 0;
-  for (int jf = 1; jf < p->nf1; ++jf) kk += 0;   // the FK file starts at nf1 (nwn(jf < nf1) = 0)
+  // the FK file starts at nf1: frequencies below it hold no wavenumbers
   for (int s = 0; s < nf; ++s) { koff[s] = (int)kk; kk += nwn[p->nf1 + s - 1]; }
   if (kk > p->nkfmax) return gem_set_error(ctx, "synthetics: nwn does not fit nkfmax");
   for (int s = 0; s < nf; ++s) if (nwn[p->nf1 + s - 1] > p->nwnmax) return gem_set_error(ctx, "synthetics: nwn > nwnmax");
@@ -695,8 +695,6 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
   b.evf = (double2*)parts[4]; b.tw = (double2*)parts[5]; b.fac = (double*)parts[6]; b.nwn = (int*)parts[7];
   b.koff = (int*)parts[8]; b.theta = (double*)parts[9]; b.phi = (double*)parts[10]; b.propdir = (double*)parts[11];
   b.mt = (double*)parts[12]; b.twx = (double2*)parts[13];
-  const bool ok = true;
-  (void)ok;
   cudaMemcpyAsync(b.evf, evf.data(), evf.size() * sizeof(double2), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b.tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b.fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice, st);
@@ -728,7 +726,7 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
     bessel_coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
   }
   if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST) {
-    // split-precision products on the tensor cores (FP16 hi/lo operands, FP32 accumulation)
+    // sliced-integer products on the tensor cores (7 INT8 slices per operand, exact INT32 accumulation)
     const long long mtot = 2LL * nf * S.nsum;
     const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
     void* ws = gem_ctx_aux(ctx, 3, wsb);

@@ -67,8 +67,9 @@ def test_synthetics_velocity_and_shift(fkdata):
 
 
 # The mixed-precision form (fast backend) computes the degree sums on the
-# tensor cores from FP16 hi/lo operands with FP32 accumulation; its seismograms
-# must agree with the FP64 form to 1e-5 relative L2 per trace.
+# tensor cores from 7-bit integer slices of both operands with exact INT32
+# accumulation, and its inverse FFT uses exact twiddles; its seismograms must
+# agree with the FP64 form to 1e-5 relative L2 per trace.
 RTOL_MIXED = 1e-5
 
 
