@@ -14,6 +14,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/gemini_fk.h"
 #include "fk_kernel.h"
 #include "fk_types.cuh"
@@ -535,13 +537,18 @@ int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
     ctx->feat_n = 3LL * S.nitems * PROP_NF;
   }
   if (S.propose) CK(prop_infer_launch(S.PA, ctx->d_propw, ctx->d_propnorm, ctx->d_prop_kopt, ctx->d_prop_hs, st));
+  static const char* const phase_name[3] = {"gem_fk: toroidal phase", "gem_fk: spheroidal phase",
+                                            "gem_fk: adjoint phase"};
   for (int ph = 0; ph < 3; ++ph) {
+    nvtxRangePushA(phase_name[ph]);   // profiler range per phase launch (no cost without a tool)
     FKLaunch Lp = S.L;
     Lp.adv_min = FK_DEFER_MIN[S.defer[ph]];
     Lp.adv_wait = FK_DEFER_WAIT[S.defer[ph]];
     if (ctx->d_prof) Lp.prof = ctx->d_prof + 8 * ph;
     if (ctx->d_warp_ns && ph == 1) Lp.warp_ns = ctx->d_warp_ns;
-    CK(launch(ph, Lp, S.grid[ph]));
+    const cudaError_t le = launch(ph, Lp, S.grid[ph]);
+    nvtxRangePop();
+    CK(le);
     if (timed) CK(cudaEventRecord(ctx->ev_ph[ph], st));
     // running counters after this phase (stream-ordered snapshot)
     CK(cudaMemcpyAsync(ctx->d_stats + 8 * (ph + 1), ctx->d_stats, 8 * sizeof(unsigned long long),

@@ -17,6 +17,7 @@
 // products run as tiled FP64 kernels; ZRT assembly, filters, rotation and the
 // inverse FFT follow per trace.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
 #include <cstring>
@@ -716,6 +717,7 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
+  nvtxRangePushA("gem_synth: sums, spectra, inverse FFT");   // profiler range (no cost without a tool)
   long long ncoef = (long long)nf * S.nsum * S.lcap;
   if (p->global_ == 1) {
     legendre_kernel<<<(nsta * 3 + 127) / 128, 128, 0, st>>>(nsta, S.lmax, S.lcap, b.theta, b.tab);
@@ -730,8 +732,12 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
     const long long mtot = 2LL * nf * S.nsum;
     const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
     void* ws = gem_ctx_aux(ctx, 3, wsb);
-    if (!ws) return GEM_ERROR;
-    if (const char* why = sums_tc_run(S, mtot, b.tab, b.A, b.C, ws, wsb, st)) return gem_set_error(ctx, why);
+    const char* why = ws ? sums_tc_run(S, mtot, b.tab, b.A, b.C, ws, wsb, st) : "";
+    if (why) {
+      nvtxRangePop();
+      cudaEventDestroy(e0); cudaEventDestroy(e1);
+      return ws ? gem_set_error(ctx, why) : GEM_ERROR;
+    }
   } else {
     int mmax = 2 * nf * 2;
     dim3 g((nsta + GT_N - 1) / GT_N, (mmax + GT_M - 1) / GT_M, 8);
@@ -758,6 +764,7 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
     wavelet_kernel<<<(unsigned)ntr, 256, smem, st>>>(p->nsamp, nmt, d_nstrue, nstf, nhm, p->dt,
                                                      (const float*)parts[17], d_traces);
   }
+  nvtxRangePop();
   cudaEventRecord(e1, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = cudaGetLastError();

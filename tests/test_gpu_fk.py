@@ -261,3 +261,26 @@ def test_autotune_keeps_the_fastest_schedule(small):
         assert fk.schedule() == r["schedule"] and fk.defer() == r["defer"]
         _, _, g64, st = fk.run(w.params, jre, 44, 52, f32=False)
         assert np.all(st == 0)
+
+
+@pytest.mark.parametrize("corrupt", ["knots_not_monotone", "nan_velocity", "inf_density"])
+def test_corrupted_model_is_rejected(small, corrupt):
+    """A corrupted earth model is refused on the host when it is loaded, with an
+    error and no kernel launched: knot depths that do not increase monotonically,
+    or non-finite values."""
+    from gemini_unified_b200.fk import GeminiFK
+    from gemini_unified_b200.model import GeminiError
+    w, m, ex, jre, fk, o = small
+    bad = dataclasses.replace(m, depth=m.depth.copy(), vpv=m.vpv.copy(), ro=m.ro.copy())
+    if corrupt == "knots_not_monotone":
+        k = len(bad.depth) // 2
+        bad.depth[k], bad.depth[k + 1] = bad.depth[k + 1] + 1000.0, bad.depth[k]
+    elif corrupt == "nan_velocity":
+        bad.vpv[3] = np.nan
+    else:
+        bad.ro[5] = np.inf
+    with pytest.raises(GeminiError):
+        GeminiFK(bad, ex)
+    # the context that loaded the good model still runs
+    _, _, g64, st = fk.run(w.params, jre, 3, 3, f32=False)
+    assert np.all(st == 0)
