@@ -284,3 +284,19 @@ def test_corrupted_model_is_rejected(small, corrupt):
     # the context that loaded the good model still runs
     _, _, g64, st = fk.run(w.params, jre, 3, 3, f32=False)
     assert np.all(st == 0)
+
+
+def test_batched_run_with_resume_matches_one_call(small, tmp_path):
+    """fk_batches over the whole band in batches of 16 frequencies, on the GPU, gives
+    the float32 spectra of one call for the whole band; a second run computes nothing."""
+    from gemini_unified_b200 import fk_batches
+    w, m, ex, jre, fk, o = small
+    g = M.frequency_grid(w.params, m.rearth)
+    res = fk_batches.run(fk, w.params, jre, str(tmp_path), 16)
+    assert all(c for _, c in res)
+    gre, gim, st = fk_batches.load(str(tmp_path))
+    ref_re, ref_im, _, ref_st = fk.run(w.params, jre, g.nf1, g.nf2, f64=False)
+    np.testing.assert_array_equal(st, ref_st)
+    np.testing.assert_array_equal(np.nan_to_num(gre, nan=1.0), np.nan_to_num(ref_re, nan=1.0))
+    np.testing.assert_array_equal(np.nan_to_num(gim, nan=1.0), np.nan_to_num(ref_im, nan=1.0))
+    assert not any(c for _, c in fk_batches.run(fk, w.params, jre, str(tmp_path), 16))
