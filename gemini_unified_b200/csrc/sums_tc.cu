@@ -11,7 +11,7 @@
 //   a = sum_i a_i 128^-(i+1), t = sum_j t_j 128^-(j+1), a_i, t_j in [-127, 127]
 //   C[m, n] = r_m c_n sum_{w=0}^{S-1} 128^-(w+2) sum_{i+j=w} (sum_l a_i t_j)
 //
-// with S = 7 slices of 7 bits (49 bits of each operand relative to its row or
+// with S = 6 slices of 7 bits (42 bits of each operand relative to its row or
 // column scale; terms with i + j >= S are dropped).  The slice products are
 // accumulated exactly in INT32 by tcgen05.mma kind::i8 and combined in FP64,
 // so the result keeps FP64-level accuracy even where the degree sum cancels by
@@ -19,9 +19,9 @@
 // FP32 accumulation cannot.
 //
 // GEMM kernel: one CTA per 128 x 64 output tile.  Per k-block of 64 degrees,
-// warp 0 issues TMA loads (64-byte swizzle) of the 7 slices of A and of T into
-// a 2-stage shared-memory ring; warp 1 issues the 28 slice products (2 MMAs of
-// K 32 each) into 7 TMEM accumulators of 64 columns, one per weight w = i + j;
+// warp 0 issues TMA loads (64-byte swizzle) of the S slices of A and of T into
+// a 2-stage shared-memory ring; warp 1 issues the S(S+1)/2 slice products (2 MMAs
+// of K 32 each) into S TMEM accumulators of 64 columns, one per weight w = i + j;
 // warps 2-5 combine the accumulators in FP64 and write C.  All mbarrier waits
 // are bounded by a 1 s timer: a wait that runs out records an error flag, the
 // CTA stops issuing work, waits (bounded) for its own copies and products,
@@ -36,14 +36,18 @@
 
 namespace gem {
 
-constexpr int TC_S = 7;                                  // slices per operand
+// Slices per operand.  Measured on the tensor-core-sums configuration (synthetics step,
+// worst trace error against the FP64 form): 7: 12.6 ms; 6: 11.3 ms, both at the FFT's
+// own 1.75e-7; 5: 10.1 ms, but near-zero traces of the global configuration then miss
+// the 1e-5 per-trace bar (1.4e-4); 4: 9.1 ms, 2.5e-6.
+constexpr int TC_S = 6;
 constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 64;      // tile; BK int8 = 64 bytes = one swizzle row
 constexpr int TC_STAGES = 2;
 constexpr int TC_A_BYTES = TC_BM * TC_BK;               // 8 KiB per slice
 constexpr int TC_B_BYTES = TC_BN * TC_BK;               // 4 KiB per slice
-constexpr int TC_STAGE_BYTES = TC_S * (TC_A_BYTES + TC_B_BYTES);   // 84 KiB
+constexpr int TC_STAGE_BYTES = TC_S * (TC_A_BYTES + TC_B_BYTES);   // 72 KiB
 constexpr int TC_THREADS = 192;
-constexpr int TC_TMEM_COLS = 512;                       // 7 accumulators of 64 columns
+constexpr int TC_TMEM_COLS = 512;                       // S accumulators of 64 columns (power-of-two allocation)
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
 constexpr unsigned long long TC_WAIT_NS = 1000000000ull;
 
@@ -282,7 +286,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0 && lane == 0) {
-    // ---- producer: the 7 slices of A and of T per k-block
+    // ---- producer: the S slices of A and of T per k-block
     int issued = 0;
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % TC_STAGES;

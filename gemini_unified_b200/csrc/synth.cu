@@ -728,7 +728,7 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
     bessel_coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
   }
   if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST) {
-    // sliced-integer products on the tensor cores (7 INT8 slices per operand, exact INT32 accumulation)
+    // sliced-integer products on the tensor cores (6 INT8 slices per operand, exact INT32 accumulation)
     const long long mtot = 2LL * nf * S.nsum;
     const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
     void* ws = gem_ctx_aux(ctx, 3, wsb);
