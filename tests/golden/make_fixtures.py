@@ -8,6 +8,11 @@ Run in the build container, where the reference tree is mounted:
   configurations and by the reference's own model-reader known-answer test
   (f90/testReadNodeEarthmodel.f90).  They are input data, copied verbatim so
   the GPU tests and the bench can run where the reference is absent.
+* oracle_fk_global_small.npz: the CPU oracle's FK spectra (complex128, as
+  (frequency index, degree index, node, spectrum)) of frequencies 8 and 30 of
+  the global configuration.  Regression vectors: they pin the oracle and the
+  GPU parity form against later changes (made with --oracle; no reference tree
+  needed).
 """
 import os
 import shutil
@@ -15,6 +20,29 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 MODELS = ["prem-no-ocean_si.json", "ak135q.json"]
+
+
+def oracle_vectors():
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+    sys.path.insert(0, os.path.join(HERE, "..", ".."))
+    import numpy as np
+    import oracle
+    from gemini_unified_b200 import configs, model as M
+    w = configs.WORKLOADS["global_small"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    o = oracle.Oracle(m, ex)
+    pc = M.fk_params_c(w.params, jre)
+    out = {}
+    for jf in (8, 30):
+        n = int(g.nwn[jf - 1])
+        spec, status, _ = o.fk_frequency(pc, jf, n, M.nsp_for(w.params))
+        out["jf%d" % jf] = spec
+        out["status%d" % jf] = status
+    np.savez_compressed(os.path.join(HERE, "oracle_fk_global_small.npz"), **out)
+    print("wrote oracle_fk_global_small.npz")
 
 
 def main(ref):
@@ -25,4 +53,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if "--oracle" in sys.argv:
+        oracle_vectors()
+    else:
+        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -300,3 +300,18 @@ def test_batched_run_with_resume_matches_one_call(small, tmp_path):
     np.testing.assert_array_equal(np.nan_to_num(gre, nan=1.0), np.nan_to_num(ref_re, nan=1.0))
     np.testing.assert_array_equal(np.nan_to_num(gim, nan=1.0), np.nan_to_num(ref_im, nan=1.0))
     assert not any(c for _, c in fk_batches.run(fk, w.params, jre, str(tmp_path), 16))
+
+
+def test_plain_form_against_regression_vectors(small):
+    """The parity form against the committed oracle vectors (frequencies 8 and 30):
+    the same bar as against the live oracle, 1e-10 of each spectrum's largest value."""
+    import os
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle_fk_global_small.npz"))
+    w, m, ex, jre, fk, o = small
+    g = M.frequency_grid(w.params, m.rearth)
+    for jf in (8, 30):
+        _, _, g64, st = fk.run(w.params, jre, jf, jf, f32=False)
+        ref = gold["jf%d" % jf]
+        assert np.all(st == gold["status%d" % jf])
+        assert g64.shape == ref.shape
+        assert _cmp(g64, ref) <= 1e-10

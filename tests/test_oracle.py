@@ -343,3 +343,21 @@ def test_ray_table_slowness_is_the_travel_time_slope():
     assert np.abs(slope / pm - 1.0).max() < 2e-3
     # the deepest ray grazes the core-mantle boundary near 98 degrees (two legs)
     assert 95.0 < 2 * np.degrees(d[0]) < 101.0
+
+
+def test_oracle_reproduces_its_regression_vectors():
+    """The committed oracle FK spectra of frequencies 8 and 30 of the global
+    configuration (tests/golden/make_fixtures.py --oracle): bit for bit."""
+    import os
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle_fk_global_small.npz"))
+    w = configs.WORKLOADS["global_small"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    o = oracle.Oracle(m, ex)
+    pc = M.fk_params_c(w.params, jre)
+    for jf in (8, 30):
+        spec, status, _ = o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), M.nsp_for(w.params))
+        np.testing.assert_array_equal(status, gold["status%d" % jf])
+        np.testing.assert_array_equal(np.nan_to_num(spec, nan=1.0), np.nan_to_num(gold["jf%d" % jf], nan=1.0))
