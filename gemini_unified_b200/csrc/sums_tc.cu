@@ -18,10 +18,10 @@
 // five orders of magnitude (near-antipodal stations), which FP16 operands with
 // FP32 accumulation cannot.
 //
-// GEMM kernel: one CTA per 128 x 64 output tile.  Per k-block of 64 degrees,
+// GEMM kernel: one CTA per 128 x 80 output tile (TC_BM x TC_BN).  Per k-block of 64 degrees,
 // warp 0 issues TMA loads (64-byte swizzle) of the S slices of A and of T into
 // a 2-stage shared-memory ring; warp 1 issues the S(S+1)/2 slice products (2 MMAs
-// of K 32 each) into S TMEM accumulators of 64 columns, one per weight w = i + j;
+// of K 32 each) into S TMEM accumulators of TC_BN columns, one per weight w = i + j;
 // warps 2-5 combine the accumulators in FP64 and write C.  All mbarrier waits
 // are bounded by a 1 s timer: a wait that runs out records an error flag, the
 // CTA stops issuing work, waits (bounded) for its own copies and products,
@@ -39,15 +39,19 @@ namespace gem {
 // Slices per operand.  Measured on the tensor-core-sums configuration (synthetics step,
 // worst trace error against the FP64 form): 7: 12.6 ms; 6: 11.3 ms, both at the FFT's
 // own 1.75e-7; 5: 10.1 ms, but near-zero traces of the global configuration then miss
-// the 1e-5 per-trace bar (1.4e-4); 4: 9.1 ms, 2.5e-6.
+// the 1e-5 per-trace bar (1.4e-4); 4: 9.1 ms, 2.5e-6 (all with 128 x 64 tiles).  With six
+// slices, 128 x 80 tiles (480 of the 512 TMEM columns) take the step from 11.3 to 10.4 ms
+// at the same error: each A tile is loaded for 80 stations instead of 64.
 constexpr int TC_S = 6;
-constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 64;      // tile; BK int8 = 64 bytes = one swizzle row
+constexpr int TC_BM = 128, TC_BN = 80, TC_BK = 64;      // tile; BK int8 = 64 bytes = one swizzle row
 constexpr int TC_STAGES = 2;
 constexpr int TC_A_BYTES = TC_BM * TC_BK;               // 8 KiB per slice
-constexpr int TC_B_BYTES = TC_BN * TC_BK;               // 4 KiB per slice
-constexpr int TC_STAGE_BYTES = TC_S * (TC_A_BYTES + TC_B_BYTES);   // 72 KiB
+constexpr int TC_B_BYTES = TC_BN * TC_BK;               // 5 KiB per slice (10 swizzle atoms of 512 B)
+constexpr int TC_STAGE_BYTES = TC_S * (TC_A_BYTES + TC_B_BYTES);   // 78 KiB
 constexpr int TC_THREADS = 192;
-constexpr int TC_TMEM_COLS = 512;                       // S accumulators of 64 columns (power-of-two allocation)
+constexpr int TC_TMEM_COLS = 512;                       // S accumulators of TC_BN columns (power-of-two allocation)
+static_assert(TC_S * TC_BN <= TC_TMEM_COLS, "the accumulators must fit the tensor memory");
+static_assert(TC_BN % 16 == 0 && TC_BN >= 16 && TC_BN <= 256, "MMA N of kind::i8 with M = 128");
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
 constexpr unsigned long long TC_WAIT_NS = 1000000000ull;
 
@@ -243,7 +247,7 @@ __device__ __forceinline__ uint64_t smem_desc_sw64(const void* p) {
   return d;
 }
 
-// kind::i8 instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = 64, M = 128
+// kind::i8 instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = TC_BN, M = 128
 constexpr uint32_t TC_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
                               ((uint32_t)(TC_BM >> 4) << 24);
 
@@ -305,7 +309,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     for (int kb = (issued > TC_STAGES ? issued - TC_STAGES : 0); kb < issued; ++kb)
       mbar_drain(&full[kb % TC_STAGES], (kb / TC_STAGES) & 1);
   } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer: accumulator w = i + j at TMEM columns 64 w
+    // ---- MMA issuer: accumulator w = i + j at TMEM columns TC_BN w
     bool ok = true;
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % TC_STAGES;
@@ -350,33 +354,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const double rs = row_ok ? rscale[kind_rowoff[kind] + r] : 0.0;
     double* crow = C + coff[kind] + (long long)r * nsta;
     const double* cs = cscale + (long long)kind * nsta;
+    // columns in chunks of 16 (TC_BN is a multiple of 16)
 #pragma unroll 1
-    for (int c = 0; c < TC_BN / 32; ++c) {
-      double sum[32];
+    for (int c = 0; c < TC_BN / 16; ++c) {
+      double sum[16];
 #pragma unroll
-      for (int jj = 0; jj < 32; ++jj) sum[jj] = 0.0;
+      for (int jj = 0; jj < 16; ++jj) sum[jj] = 0.0;
 #pragma unroll 1
       for (int w = TC_S - 1; w >= 0; --w) {
-        uint32_t v[32];
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * TC_BN + c * 32);
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * TC_BN + c * 16);
         asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-              "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
-              "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
-              "=r"(v[30]), "=r"(v[31])
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const double wgt = ldexp(1.0, -7 * (w + 2));
 #pragma unroll
-        for (int jj = 0; jj < 32; ++jj) sum[jj] += (double)(int)v[jj] * wgt;   // smallest weights first
+        for (int jj = 0; jj < 16; ++jj) sum[jj] += (double)(int)v[jj] * wgt;   // smallest weights first
       }
       if (row_ok) {
-        const int nb = n0 + c * 32;
+        const int nb = n0 + c * 16;
 #pragma unroll
-        for (int jj = 0; jj < 32; ++jj)
+        for (int jj = 0; jj < 16; ++jj)
           if (nb + jj < nsta) crow[nb + jj] = sum[jj] * rs * cs[nb + jj];
       }
     }
