@@ -271,9 +271,11 @@ def main():
 
     # ---------------- batched + mixed-precision form (fast FP64 build): the headline
     fast = GeminiFK(m, ex, device=local, backend=2)
-    # the autotuner picks each phase's schedule (block size, matrix caching) on
-    # the top quarter of the band, untimed
-    tune_fast = fast.autotune(w.params, jre)
+    # the autotuner picks each phase's schedule (block size, matrix caching) and
+    # bookkeeping deferral on the whole band, untimed.  On the top quarter alone the two
+    # best spheroidal schedules differ by less than the run-to-run noise (262 against
+    # 265 ms) while over the whole band they differ by 5% (380 against 399 ms).
+    tune_fast = fast.autotune(w.params, jre, g.nf1, g.nf2)
     for _ in range(args.warmup):
         fk_step(fast)
     torch.cuda.synchronize()
@@ -286,7 +288,7 @@ def main():
 
     # ---------------- plain FP64 form (reference rounding, one operation at a time)
     plain = GeminiFK(m, ex, device=local, backend=1)
-    tune_plain = plain.autotune(w.params, jre)
+    tune_plain = plain.autotune(w.params, jre, g.nf1, g.nf2)
     fk_step(plain)
     plain_steps = max(1, min(args.steps, 2))
     t_plain, _ = timed(lambda: fk_step(plain), plain_steps)

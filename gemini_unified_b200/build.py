@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
          "-I" + os.path.join(ROOT, "include")]
 # files compiled with FMA contraction; all others repeat the reference's rounding (--fmad=false)
-FMAD_TRUE = {"fk_solver_fast.cu", "ifft_fast.cu", "proposer.cu"}
+FMAD_TRUE = {"fk_solver_fast.cu", "ifft_fast.cu", "legendre_fast.cu", "proposer.cu"}
 
 
 def sources():

@@ -165,10 +165,17 @@ __global__ void __launch_bounds__(H / 16) ifft_fast_kernel(SynthDev S, const dou
   const int lo = S.nf1 - 1, hi = S.nf2 - 1;   // 0-based bins of the spectrum
   double2 v[16];
   int idx[16];
-  // ---- pass 0 (radix 16, NS = 1): Z_k formed on the fly, k = tid + r T
+  // ---- pass 0 (radix 16, NS = 1): Z_k formed on the fly, k = tid + r T.  Z_k is
+  // zero unless k or H - k is a bin of the band, so a block of T consecutive k
+  // outside both ranges skips its loads (a branch uniform over the CTA)
 #pragma unroll
   for (int r = 0; r < 16; ++r) {
     const int k = tid + r * T;
+    const int ka = r * T, kb = r * T + T - 1;
+    if (!((ka <= hi && kb >= lo) || (H - kb <= hi && H - ka >= lo))) {
+      v[r] = make_double2(0.0, 0.0);
+      continue;
+    }
     const double2 a = (k >= lo && k <= hi) ? x[k] : make_double2(0.0, 0.0);
     const int kk = H - k;
     double2 b = make_double2(0.0, 0.0);

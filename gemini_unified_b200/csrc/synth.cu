@@ -720,7 +720,10 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
   nvtxRangePushA("gem_synth: sums, spectra, inverse FFT");   // profiler range (no cost without a tool)
   long long ncoef = (long long)nf * S.nsum * S.lcap;
   if (p->global_ == 1) {
-    legendre_kernel<<<(nsta * 3 + 127) / 128, 128, 0, st>>>(nsta, S.lmax, S.lcap, b.theta, b.tab);
+    if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST && legendre_fast_supported(S.lmax))
+      legendre_fast_launch(nsta, S.lmax, S.lcap, b.theta, b.tab, st);
+    else
+      legendre_kernel<<<(nsta * 3 + 127) / 128, 128, 0, st>>>(nsta, S.lmax, S.lcap, b.theta, b.tab);
     coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.A);
   } else {
     const long long ntab = (long long)S.lcap * nsta;

@@ -55,6 +55,11 @@ cudaError_t ifft_fast_launch(const SynthDev& S, long long ntr, const double2* X,
 cudaError_t ifft_fast_twiddles_launch(int N, double2* tw, cudaStream_t st);
 inline bool ifft_fast_supported(int ns) { return ns >= 512 && ns <= IFFT_MAX_NS; }
 
+// fast-form Legendre tables (legendre_fast.cu): the tables of legendre_kernel with
+// the recurrence's division replaced by a reciprocal table; lmax up to 25,599
+bool legendre_fast_supported(int lmax);
+cudaError_t legendre_fast_launch(int nsta, int lmax, int lcap, const double* theta, double* tab, cudaStream_t st);
+
 // sliced-integer tensor-core degree sums (sums_tc.cu): workspace size and run
 size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out);
 const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, const double* A, double* C, void* ws,
