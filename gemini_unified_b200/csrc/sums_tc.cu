@@ -67,16 +67,25 @@ __device__ __forceinline__ double pow2_above(double x) {
   return ldexp(1.0, e);
 }
 
-// the 7-bit slices of x, |x| < 1: x = sum_i q_i 128^-(i+1) + O(128^-S)
+// the 7-bit slices of x, |x| < 1: x = sum_i q_i 128^-(i+1) + O(128^-S).  The
+// slices are the base-128 digits of u = trunc(|x| 128^S) with the sign of x
+// (x 128^S is exact and the conversion truncates), the same digits as S
+// rounds of x *= 128, q = trunc(x), x -= q, all of which are exact.
+static_assert(TC_S <= 8, "the digits must fit a 64-bit integer");
 __device__ __forceinline__ void slices_of(double x, signed char q[TC_S]) {
+  const long long y = (long long)(x * (double)(1ull << (7 * TC_S)));
+  const unsigned long long u = y < 0 ? (unsigned long long)(-y) : (unsigned long long)y;
 #pragma unroll
   for (int i = 0; i < TC_S; ++i) {
-    x *= 128.0;
-    const double a = trunc(x);
-    x -= a;
-    q[i] = (signed char)(int)a;
+    const int d = (int)((u >> (7 * (TC_S - 1 - i))) & 127u);
+    q[i] = (signed char)(y < 0 ? -d : d);
   }
 }
+
+// 1/s for a power of two s whose reciprocal is a normal double (then x * (1/s)
+// equals x / s exactly), else 0: the callers then divide
+__device__ __forceinline__ double inv_pow2(double s) { return s >= 0x1p-1021 && s <= 0x1p1021 ? 1.0 / s : 0.0; }
+__device__ __forceinline__ double div_pow2(double x, double s, double inv) { return inv != 0.0 ? x * inv : x / s; }
 
 __device__ __forceinline__ double block_max(double m) {
   __shared__ double red[256];
@@ -108,12 +117,18 @@ __global__ void tab_scale_kernel(int nsta, int lcap, int K, const double* __rest
 // 128 stations x 64 degrees
 __global__ void tab_colmax_kernel(int nsta, int lcap, int K, int Kp, const double* __restrict__ tab,
                                   const double* __restrict__ lscale, unsigned long long* colmax) {
+  __shared__ double sl[64], il[64];
   const int sta = blockIdx.x * blockDim.x + threadIdx.x, kind = blockIdx.z;
-  if (sta >= nsta) return;
   const int l0 = blockIdx.y * 64, l1 = min(l0 + 64, K);
+  if (threadIdx.x < 64 && l0 + (int)threadIdx.x < l1) {
+    sl[threadIdx.x] = lscale[(long long)kind * Kp + l0 + threadIdx.x];
+    il[threadIdx.x] = inv_pow2(sl[threadIdx.x]);
+  }
+  __syncthreads();
+  if (sta >= nsta) return;
   double m = 0.0;
   for (int l = l0; l < l1; ++l)
-    m = fmax(m, fabs(tab[((long long)kind * lcap + l) * nsta + sta] / lscale[(long long)kind * Kp + l]));
+    m = fmax(m, fabs(div_pow2(tab[((long long)kind * lcap + l) * nsta + sta], sl[l - l0], il[l - l0])));
   atomicMax(colmax + (long long)kind * nsta + sta, (unsigned long long)__double_as_longlong(m));
 }
 
@@ -123,32 +138,44 @@ __global__ void tab_colscale_kernel(int n, const unsigned long long* __restrict_
   if (i < n) cscale[i] = pow2_above(__longlong_as_double((long long)colmax[i]));
 }
 
-// T8[j][kind*nsta + sta][l] = slice j of T / (s_l c_sta), through a 64 x 64 shared-memory transpose
+// T8[j][kind*nsta + sta][l] = slice j of T / (s_l c_sta) for a tile of 64 degrees x 64
+// stations: slices formed on the coalesced read (consecutive stations) into a
+// shared byte tile [slice][station][degree], written back as 4-degree words
 __global__ void tab_slice_kernel(int nsta, int lcap, int K, int Kp, const double* __restrict__ tab,
                                  const double* __restrict__ lscale, const double* __restrict__ cscale,
                                  signed char* T8) {
-  __shared__ double tile[64][65];
+  constexpr int ROW = 68;   // bytes per station row: 17 words, so the byte writes of a warp hit distinct banks
+  __shared__ __align__(16) signed char dig[TC_S][64][ROW];
+  __shared__ double sl[64], il[64];
   const int kind = blockIdx.z;
   const int l0 = blockIdx.x * 64, s0 = blockIdx.y * 64;
   const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;   // 256 threads: 64 x 4
+  if (threadIdx.x < 64) {
+    const int l = l0 + threadIdx.x;
+    sl[threadIdx.x] = l < K ? lscale[(long long)kind * Kp + l] : 1.0;
+    il[threadIdx.x] = inv_pow2(sl[threadIdx.x]);
+  }
+  __syncthreads();
+  const int sta = s0 + tx;
+  const double cs = sta < nsta ? cscale[(long long)kind * nsta + sta] : 1.0, ic = inv_pow2(cs);
   for (int r = ty; r < 64; r += 4) {
-    const int l = l0 + r, sta = s0 + tx;
+    const int l = l0 + r;
     double v = 0.0;
-    if (l < K && sta < nsta)
-      v = tab[((long long)kind * lcap + l) * nsta + sta] / lscale[(long long)kind * Kp + l] /
-          cscale[(long long)kind * nsta + sta];
-    tile[r][tx] = v;
+    if (l < K && sta < nsta) v = div_pow2(div_pow2(tab[((long long)kind * lcap + l) * nsta + sta], sl[r], il[r]), cs, ic);
+    signed char q[TC_S];
+    slices_of(v, q);
+#pragma unroll
+    for (int j = 0; j < TC_S; ++j) dig[j][tx][r] = q[j];
   }
   __syncthreads();
   const long long plane = 8LL * nsta * Kp;
-  for (int r = ty; r < 64; r += 4) {
-    const int sta = s0 + r, l = l0 + tx;
-    if (sta >= nsta) continue;
-    signed char q[TC_S];
-    slices_of(tile[tx][r], q);
-    const long long o = ((long long)kind * nsta + sta) * Kp + l;
+  for (int e = threadIdx.x; e < 64 * 16; e += 256) {
+    const int r = e >> 4, w = e & 15;   // station row of the tile, word of 4 degrees
+    if (s0 + r >= nsta) continue;
+    const long long o = ((long long)kind * nsta + s0 + r) * Kp + l0 + 4 * w;   // Kp, l0: multiples of 64
 #pragma unroll
-    for (int j = 0; j < TC_S; ++j) T8[j * plane + o] = q[j];
+    for (int j = 0; j < TC_S; ++j)
+      *reinterpret_cast<uint32_t*>(T8 + j * plane + o) = *reinterpret_cast<const uint32_t*>(&dig[j][r][4 * w]);
   }
 }
 
@@ -162,12 +189,12 @@ __global__ void coef_slice_kernel(SynthDev S, long long mtot, int K, int Kp, con
   const double* sl = lscale + (long long)kind * Kp;
   double m = 0.0;
   for (int l = threadIdx.x; l < K; l += blockDim.x) m = fmax(m, fabs(a[l] * sl[l]));
-  const double r = pow2_above(block_max(m));
+  const double r = pow2_above(block_max(m)), ir = inv_pow2(r);
   if (threadIdx.x == 0) rscale[row] = r;
   const long long plane = mtot * Kp;
   for (int l = threadIdx.x; l < Kp; l += blockDim.x) {
     signed char q[TC_S];
-    slices_of(l < K ? a[l] * sl[l] / r : 0.0, q);
+    slices_of(l < K ? div_pow2(a[l] * sl[l], r, ir) : 0.0, q);
 #pragma unroll
     for (int i = 0; i < TC_S; ++i) A8[i * plane + row * Kp + l] = q[i];
   }
@@ -519,7 +546,7 @@ const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, co
   tab_slice_kernel<<<dim3(Kp / 64, (S.nsta + 63) / 64, 8), 256, 0, st>>>(S.nsta, S.lcap, K, Kp, tab, lscale, cscale,
                                                                          T8);
   coef_slice_kernel<<<(unsigned)mtot, 256, 0, st>>>(S, mtot, K, Kp, A, lscale, row_kind, A8, rscale);
-  // tensor maps over A8 [7 mtot][Kp] and T8 [7 * 8 nsta][Kp]
+  // tensor maps over A8 [TC_S mtot][Kp] and T8 [TC_S * 8 nsta][Kp]
   CUtensorMap mA, mB;
   if (!make_map(&mA, A8, TC_S * mtot, Kp, TC_BM) || !make_map(&mB, T8, TC_S * 8LL * S.nsta, Kp, TC_BN))
     return "sums_tc: cuTensorMapEncodeTiled failed";
