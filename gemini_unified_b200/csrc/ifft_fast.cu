@@ -109,9 +109,10 @@ __device__ __forceinline__ void dftR(double2* v) {
 // One Stockham pass of radix R over the H points in shared memory (NS: length of
 // the sub-transforms already done).  Each of the H/16 threads runs 16/R
 // butterflies.  The last pass hands its 16 results (point indices idx) back.
+// twp: the pass's twiddles twp[(r - 1) NS + k] = e^{2 pi i r k / (NS R)}, laid out
+// so that the threads of a warp (consecutive k) read consecutive entries.
 template <int H, int R, int NS, bool LAST>
-__device__ __forceinline__ void stockham_pass(double2* buf, double2* v, int* idx, const double2* __restrict__ tw,
-                                              int N) {
+__device__ __forceinline__ void stockham_pass(double2* buf, double2* v, int* idx, const double2* __restrict__ twp) {
   constexpr int T = H / 16, NB = 16 / R;
   const int tid = threadIdx.x;
 #pragma unroll
@@ -121,14 +122,13 @@ __device__ __forceinline__ void stockham_pass(double2* buf, double2* v, int* idx
     for (int r = 0; r < R; ++r) v[b * R + r] = buf[pad(j + r * (H / R))];
   }
   __syncthreads();
-  const int stride = N / (NS * R);   // tw[m] = e^{2 pi i m / N}
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const int j = tid + b * T;
     const int k = j % NS;
     if (NS > 1) {
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[b * R + r] = cmul(v[b * R + r], tw[r * k * stride]);
+      for (int r = 1; r < R; ++r) v[b * R + r] = cmul(v[b * R + r], twp[(r - 1) * NS + k]);
     }
     dftR<R>(v + b * R);
     const int d = (j / NS) * NS * R + k;
@@ -143,17 +143,31 @@ __device__ __forceinline__ void stockham_pass(double2* buf, double2* v, int* idx
 
 }  // namespace
 
-// tw[m] = e^{2 pi i m / N}, m < N
+// tw[m] = e^{2 pi i m / N}, m < N, then the pass tables: tw + N + IFFT_TWA for the
+// pass (NS 16, R 16) and tw + N + IFFT_TWB for the last pass (NS 256, R H/256),
+// entry (r - 1) NS + k = e^{2 pi i r k / (NS R)}.  Both angles are the same double
+// as the m = r k N / (NS R) of the full table, so the entries equal tw[m].
 __global__ void ifft_fast_twiddles(int N, double2* tw) {
-  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < N; m += blockDim.x * gridDim.x) {
+  const int H = N / 2, RB = H / 256;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < N + IFFT_TW_EXTRA; m += blockDim.x * gridDim.x) {
+    long long num = 0, den = 1;
+    if (m < N) {
+      num = m; den = N;
+    } else if (m < N + IFFT_TWB) {
+      const int a = m - N - IFFT_TWA;
+      if (a < 15 * 16) { num = (long long)(a / 16 + 1) * (a % 16); den = 256; }
+    } else {
+      const int b = m - N - IFFT_TWB;
+      if (b < (RB - 1) * 256) { num = (long long)(b / 256 + 1) * (b % 256); den = 256LL * RB; }
+    }
     double s, c;
-    sincospi(2.0 * (double)m / (double)N, &s, &c);
+    sincospi(2.0 * (double)num / (double)den, &s, &c);
     tw[m] = make_double2(c, s);
   }
 }
 
 template <int H>
-__global__ void __launch_bounds__(H / 16) ifft_fast_kernel(SynthDev S, const double2* __restrict__ X,
+__global__ void __launch_bounds__(H / 16, H == 4096 ? 3 : 1) ifft_fast_kernel(SynthDev S, const double2* __restrict__ X,
                                                           const double2* __restrict__ tw,
                                                           const double* __restrict__ fac, float* traces) {
   extern __shared__ double2 buf[];
@@ -190,20 +204,20 @@ __global__ void __launch_bounds__(H / 16) ifft_fast_kernel(SynthDev S, const dou
   __syncthreads();
   // ---- remaining passes
   if constexpr (H == 256) {
-    stockham_pass<H, 16, 16, true>(buf, v, idx, tw, N);
+    stockham_pass<H, 16, 16, true>(buf, v, idx, tw + N + IFFT_TWA);
   } else if constexpr (H == 512) {
-    stockham_pass<H, 16, 16, false>(buf, v, idx, tw, N);
-    stockham_pass<H, 2, 256, true>(buf, v, idx, tw, N);
+    stockham_pass<H, 16, 16, false>(buf, v, idx, tw + N + IFFT_TWA);
+    stockham_pass<H, 2, 256, true>(buf, v, idx, tw + N + IFFT_TWB);
   } else if constexpr (H == 1024) {
-    stockham_pass<H, 16, 16, false>(buf, v, idx, tw, N);
-    stockham_pass<H, 4, 256, true>(buf, v, idx, tw, N);
+    stockham_pass<H, 16, 16, false>(buf, v, idx, tw + N + IFFT_TWA);
+    stockham_pass<H, 4, 256, true>(buf, v, idx, tw + N + IFFT_TWB);
   } else if constexpr (H == 2048) {
-    stockham_pass<H, 16, 16, false>(buf, v, idx, tw, N);
-    stockham_pass<H, 8, 256, true>(buf, v, idx, tw, N);
+    stockham_pass<H, 16, 16, false>(buf, v, idx, tw + N + IFFT_TWA);
+    stockham_pass<H, 8, 256, true>(buf, v, idx, tw + N + IFFT_TWB);
   } else {
     static_assert(H == 4096, "supported half lengths: 256..4096");
-    stockham_pass<H, 16, 16, false>(buf, v, idx, tw, N);
-    stockham_pass<H, 16, 256, true>(buf, v, idx, tw, N);
+    stockham_pass<H, 16, 16, false>(buf, v, idx, tw + N + IFFT_TWA);
+    stockham_pass<H, 16, 256, true>(buf, v, idx, tw + N + IFFT_TWB);
   }
   // ---- x_{2n} = Re z_n, x_{2n+1} = Im z_n; ts(i) = x(ndec i) df fac(i)
   float* out = traces + tr * S.nsamp;
@@ -214,8 +228,8 @@ __global__ void __launch_bounds__(H / 16) ifft_fast_kernel(SynthDev S, const dou
     const int t0 = 2 * n, t1 = 2 * n + 1;
     if (ndec == 1) {
       if (t1 < S.nsamp) {
-        *reinterpret_cast<float2*>(out + t0) =
-            make_float2((float)(v[q].x * S.df * fac[t0]), (float)(v[q].y * S.df * fac[t1]));
+        const double2 f = *reinterpret_cast<const double2*>(fac + t0);   // t0 even: 16-byte aligned
+        *reinterpret_cast<float2*>(out + t0) = make_float2((float)(v[q].x * S.df * f.x), (float)(v[q].y * S.df * f.y));
       } else if (t0 < S.nsamp) {
         out[t0] = (float)(v[q].x * S.df * fac[t0]);
       }
@@ -226,13 +240,15 @@ __global__ void __launch_bounds__(H / 16) ifft_fast_kernel(SynthDev S, const dou
   }
 }
 
-// Launch: ns in 512..8192.  tw: N = ns twiddles e^{2 pi i m/N}; fac: nsamp factors.
+// Launch: ns in 512..8192.  tw: the ns + IFFT_TW_EXTRA twiddles of ifft_fast_twiddles; fac: nsamp factors.
 cudaError_t ifft_fast_launch(const SynthDev& S, long long ntr, const double2* X, const double2* tw, const double* fac,
                              float* traces, cudaStream_t st) {
   const int H = S.ns / 2;
   const size_t smem = (size_t)(H + H / 16) * sizeof(double2);
   auto go = [&](auto kern, int threads) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)   // all of the unified L1 as shared memory: more CTAs of the longest transforms per SM
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     kern<<<(unsigned)ntr, threads, smem, st>>>(S, X, tw, fac, traces);
     return cudaGetLastError();
@@ -248,7 +264,7 @@ cudaError_t ifft_fast_launch(const SynthDev& S, long long ntr, const double2* X,
 }
 
 cudaError_t ifft_fast_twiddles_launch(int N, double2* tw, cudaStream_t st) {
-  ifft_fast_twiddles<<<(N + 255) / 256, 256, 0, st>>>(N, tw);
+  ifft_fast_twiddles<<<(N + IFFT_TW_EXTRA + 255) / 256, 256, 0, st>>>(N, tw);
   return cudaGetLastError();
 }
 

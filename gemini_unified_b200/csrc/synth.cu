@@ -683,7 +683,7 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
                             evf.size() * sizeof(double2), tw.size() * sizeof(double2), fac.size() * sizeof(double),
                             (size_t)p->nf2 * sizeof(int), (size_t)nf * sizeof(int), nsta * sizeof(double),
                             nsta * sizeof(double), nsta * sizeof(double), (size_t)nmt * nfo * sizeof(double),
-                            fast_fft ? (size_t)ns * sizeof(double2) : 0,
+                            fast_fft ? ifft_fast_twiddle_bytes(ns) : 0,
                             o_tred ? nsta * sizeof(double) : 0, o_ns ? nsta * sizeof(int) : 0,
                             o_sf ? (size_t)nsta * 3 * p->nf2 * sizeof(double2) : 0, (size_t)nstf * sizeof(float)};
   size_t total = 0;
@@ -887,7 +887,7 @@ extern "C" int gem_ifft_run_device(gem_ctx* ctx, int nf1, int nf2, double df, do
   if (cudaSetDevice(gem_ctx_device(ctx)) != cudaSuccess) return gem_set_error(ctx, "ifft: cudaSetDevice failed");
   const bool fast = gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST && ifft_fast_supported(g.ns);
   const size_t tbytes = ifft_table_bytes(g.ns, nsamp);
-  char* tab = (char*)gem_ctx_aux(ctx, 0, tbytes + (fast ? (size_t)g.ns * sizeof(double2) + 16 : 0));
+  char* tab = (char*)gem_ctx_aux(ctx, 0, tbytes + (fast ? ifft_fast_twiddle_bytes(g.ns) + 16 : 0));
   if (!tab) return GEM_ERROR;
   double2* tw = (double2*)tab;
   double* fac = (double*)(tab + (size_t)g.ns * sizeof(double2));

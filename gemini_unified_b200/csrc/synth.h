@@ -49,7 +49,10 @@ __global__ void __launch_bounds__(512) ifft_kernel(SynthDev S, const double2* __
 inline size_t ifft_table_bytes(int ns, int nsamp) { return (size_t)ns * sizeof(double2) + (size_t)nsamp * sizeof(double); }
 
 // fast-form inverse FFT (ifft_fast.cu): real output from a half-length radix-16
-// transform; ns in 512..8192; tw = e^{2 pi i m/ns}, m < ns
+// transform; ns in 512..8192; tw: ns + IFFT_TW_EXTRA entries, e^{2 pi i m/ns} for
+// m < ns followed by the tables of the radix-16 passes (IFFT_TWA, IFFT_TWB)
+constexpr int IFFT_TWA = 0, IFFT_TWB = 256, IFFT_TW_EXTRA = 4096;
+inline size_t ifft_fast_twiddle_bytes(int ns) { return ((size_t)ns + IFFT_TW_EXTRA) * sizeof(double2); }
 cudaError_t ifft_fast_launch(const SynthDev& S, long long ntr, const double2* X, const double2* tw, const double* fac,
                              float* traces, cudaStream_t st);
 cudaError_t ifft_fast_twiddles_launch(int N, double2* tw, cudaStream_t st);
