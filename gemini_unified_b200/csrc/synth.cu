@@ -343,18 +343,25 @@ __global__ void __launch_bounds__(256) sums_gemm_kernel(SynthDev S, const double
 
 // ---------------------------------------------------------------------------
 //  ZRT spectra from the sums, filters, velocity, rotation; writes the FFT
-//  input of every trace (sta, mt, comp) at bins nf1..nf2 (1-based), the rest 0.
-//  X[trace][ns] complex (double2).
+//  input of every trace (sta, mt, comp) at bins nf1..nf2 (1-based).
+//  X[trace][ldx] complex (double2).  One thread per (station, frequency) of a
+//  tile of SP_STA stations x SP_SLOT frequencies: the sums are read along
+//  stations (coalesced), and per moment tensor the tile's spectra pass through
+//  shared memory so that each trace's SP_SLOT consecutive bins are written as
+//  one contiguous run.
 // ---------------------------------------------------------------------------
-__global__ void spectra_kernel(SynthDev S, const double* __restrict__ C, const double2* __restrict__ evf,
-                               const double* __restrict__ phi, const double* __restrict__ propdir,
-                               const double* __restrict__ mt, double2* X) {
-  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int SP_STA = 32, SP_SLOT = 16, SP_THREADS = SP_STA * SP_SLOT;
+__global__ void __launch_bounds__(SP_THREADS) spectra_kernel(SynthDev S, const double* __restrict__ C,
+                                                             const double2* __restrict__ evf,
+                                                             const double* __restrict__ phi,
+                                                             const double* __restrict__ propdir,
+                                                             const double* __restrict__ mt, double2* X) {
+  __shared__ double2 tile[3][SP_STA][SP_SLOT + 1];
   const int nf = S.nf2 - S.nf1 + 1;
-  if (idx >= (long long)S.nsta * nf) return;
-  const int sta = (int)(idx % S.nsta);
-  const int slot = (int)(idx / S.nsta);
-  const int jf = S.nf1 + slot;
+  const int tx = threadIdx.x % SP_STA, ty = threadIdx.x / SP_STA;
+  const int sta0 = blockIdx.x * SP_STA, slot0 = blockIdx.y * SP_SLOT;
+  const int sta = min(sta0 + tx, S.nsta - 1), slot = min(slot0 + ty, nf - 1);   // clamped: edge threads compute
+  const int jf = S.nf1 + slot;                                                   // a copy that is not written
   const int t = S.istyp;
   dz w[15];
   for (int k = 0; k < S.nsum; ++k) {
@@ -404,10 +411,17 @@ __global__ void spectra_kernel(SynthDev S, const double* __restrict__ C, const d
     dz ue = sa * z[1] + ca * z[2];
     dz un = (-ca) * z[1] + sa * z[2];
     dz out[3] = {z[0], un, ue};
-    for (int c = 0; c < 3; ++c) {
-      long long tr = ((long long)sta * S.nmt + im) * 3 + c;
-      X[tr * S.ldx + (jf - 1)] = make_double2(out[c].re, out[c].im);
+    for (int c = 0; c < 3; ++c) tile[c][tx][ty] = make_double2(out[c].re, out[c].im);
+    __syncthreads();
+    // the tile's 3 SP_STA traces of this moment tensor, SP_SLOT consecutive bins each
+    for (int e = threadIdx.x; e < 3 * SP_STA * SP_SLOT; e += SP_THREADS) {
+      const int s = e % SP_SLOT, c = (e / SP_SLOT) % 3, r = e / (3 * SP_SLOT);
+      if (sta0 + r < S.nsta && slot0 + s < nf) {
+        const long long tr = ((long long)(sta0 + r) * S.nmt + im) * 3 + c;
+        X[tr * S.ldx + (S.nf1 - 1 + slot0 + s)] = tile[c][r][s];
+      }
     }
+    __syncthreads();
   }
 }
 
@@ -750,8 +764,8 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
     const long long ncorr = (long long)nf * S.nsum * nsta;
     bessel_corr_kernel<<<(unsigned)((ncorr + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, b.theta, b.C);
   }
-  long long nsp_ = (long long)nsta * nf;
-  spectra_kernel<<<(unsigned)((nsp_ + 127) / 128), 128, 0, st>>>(S, b.C, b.evf, b.phi, b.propdir, b.mt, b.X);
+  spectra_kernel<<<dim3((unsigned)((nsta + SP_STA - 1) / SP_STA), (unsigned)((nf + SP_SLOT - 1) / SP_SLOT)), SP_THREADS, 0,
+                   st>>>(S, b.C, b.evf, b.phi, b.propdir, b.mt, b.X);
   if (fast_fft) {
     ifft_fast_twiddles_launch(ns, b.twx, st);
     ifft_fast_launch(S, ntr, b.X, b.twx, b.fac, d_traces, st);
