@@ -43,7 +43,11 @@ namespace gem {
 // slices, 128 x 80 tiles (480 of the 512 TMEM columns) take the step from 11.3 to 10.4 ms
 // at the same error: each A tile is loaded for 80 stations instead of 64.
 constexpr int TC_S = 6;
-constexpr int TC_BM = 128, TC_BN = 80, TC_BK = 64;      // tile; BK int8 = 64 bytes = one swizzle row
+constexpr int TC_BM = 128, TC_BN = 80, TC_BK = 64;      // tile; BK int8 = one swizzle row (64 or 32 bytes)
+static_assert(TC_BK == 64 || TC_BK == 32, "swizzle spans of 64 or 32 bytes");
+// Two stages: measured on the same step, 3 stages at N = 64 (8.51 ms) and 5 stages of BK = 32
+// at N = 80 (8.74 ms) both lose to 2 stages of BK = 64 at N = 80 (7.63 ms): the operand bytes
+// per product from L2 bound the main loop, not the depth of the pipeline.
 constexpr int TC_STAGES = 2;
 constexpr int TC_A_BYTES = TC_BM * TC_BK;               // 8 KiB per slice
 constexpr int TC_B_BYTES = TC_BN * TC_BK;               // 5 KiB per slice (10 swizzle atoms of 512 B)
@@ -262,15 +266,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-// K-major operand, 64-byte swizzle: rows of 64 bytes, 8-row groups 512 bytes apart
-__device__ __forceinline__ uint64_t smem_desc_sw64(const void* p) {
+// K-major operand swizzled over rows of TC_BK bytes (64 or 32): 8-row groups 8 TC_BK bytes apart
+__device__ __forceinline__ uint64_t smem_desc_kmajor(const void* p) {
   const uint64_t addr = smem_u32(p);
   uint64_t d = 0;
-  d |= (addr >> 4) & 0x3FFFull;          // start address
-  d |= (uint64_t)1 << 16;                // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(512 >> 4) << 32;       // stride byte offset: 8 rows x 64 B
-  d |= (uint64_t)1 << 46;                // descriptor version (tcgen05)
-  d |= (uint64_t)4 << 61;                // SWIZZLE_64B
+  d |= (addr >> 4) & 0x3FFFull;                   // start address
+  d |= (uint64_t)1 << 16;                         // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)((8 * TC_BK) >> 4) << 32;        // stride byte offset: 8 rows x TC_BK bytes
+  d |= (uint64_t)1 << 46;                         // descriptor version (tcgen05)
+  d |= (uint64_t)(TC_BK == 64 ? 4 : 6) << 61;     // SWIZZLE_64B / SWIZZLE_32B
   return d;
 }
 
@@ -345,10 +349,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       const unsigned char* st = smem + s * TC_STAGE_BYTES;
 #pragma unroll 1
       for (int i = 0; i < TC_S; ++i) {
-        const uint64_t da = smem_desc_sw64(st + i * TC_A_BYTES);
+        const uint64_t da = smem_desc_kmajor(st + i * TC_A_BYTES);
 #pragma unroll 1
         for (int j = 0; j + i < TC_S; ++j) {
-          const uint64_t db = smem_desc_sw64(st + TC_S * TC_A_BYTES + j * TC_B_BYTES);
+          const uint64_t db = smem_desc_kmajor(st + TC_S * TC_A_BYTES + j * TC_B_BYTES);
           const uint32_t dtm = tmem + (uint32_t)((i + j) * TC_BN);
 #pragma unroll
           for (int kk = 0; kk < TC_BK / 32; ++kk) {
@@ -443,7 +447,7 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 2D map over int8 rows of Kp bytes, box 64 bytes x box_rows, 64-byte swizzle
+// 2D map over int8 rows of Kp bytes, box TC_BK bytes x box_rows, swizzled over TC_BK bytes
 bool make_map(CUtensorMap* map, const signed char* base, long long rows, long long kp, int box_rows) {
   EncodeTiledFn f = encode_fn();
   if (!f) return false;
@@ -452,7 +456,7 @@ bool make_map(CUtensorMap* map, const signed char* base, long long rows, long lo
   cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   return f(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
-           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, TC_BK == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -464,7 +468,7 @@ struct TcLayout {
 TcLayout tc_layout(const SynthDev& S, long long mtot) {
   TcLayout L{};
   const int K = S.lmax + 1;
-  L.Kp = (K + TC_BK - 1) / TC_BK * TC_BK;
+  L.Kp = (K + 63) / 64 * 64;   // the slicing kernels work on 64-degree tiles
   const size_t sz[10] = {(size_t)TC_S * 8 * S.nsta * L.Kp,            // T8
                         (size_t)TC_S * mtot * L.Kp,                   // A8
                         (size_t)8 * L.Kp * sizeof(double),            // lscale
