@@ -29,6 +29,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 
@@ -284,9 +285,9 @@ constexpr uint32_t TC_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T
 
 __global__ void __launch_bounds__(TC_THREADS, 1)
     sums_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                   const int2* __restrict__ tiles, const int* __restrict__ kind_rows,
+                   const int4* __restrict__ tiles, const int* __restrict__ kind_rows,
                    const long long* __restrict__ kind_rowoff, const long long* __restrict__ coff, int nsta,
-                   long long mtot, int nkb, const double* __restrict__ rscale, const double* __restrict__ cscale,
+                   long long mtot, const double* __restrict__ rscale, const double* __restrict__ cscale,
                    double* C, int* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -297,8 +298,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int2 t = tiles[blockIdx.y];      // (kind, first row of the tile within the kind)
-  const int kind = t.x, m0 = t.y;
+  // (kind, first row of the tile within the kind, k-blocks): the tile's rows are zero
+  // beyond its largest wavenumber count, so its k-loop stops there
+  const int4 t = tiles[blockIdx.y];
+  const int kind = t.x, m0 = t.y, nkb = t.z;
   const int n0 = blockIdx.x * TC_BN;
   const int Mk = kind_rows[kind];
   const long long rowA = kind_rowoff[kind] + m0;
@@ -475,7 +478,7 @@ TcLayout tc_layout(const SynthDev& S, long long mtot) {
                         (size_t)8 * S.nsta * sizeof(double),          // cscale
                         (size_t)mtot * sizeof(double),                // rscale
                         (size_t)mtot * sizeof(int),                   // row kind
-                        (size_t)(mtot / TC_BM + 16) * sizeof(int2),   // tiles
+                        (size_t)(mtot / TC_BM + 16) * sizeof(int4),   // tiles
                         (size_t)24 * sizeof(long long),               // per-kind tables
                         (size_t)16 * sizeof(int),                     // kind rows + error flag
                         (size_t)8 * S.nsta * sizeof(unsigned long long)};   // column maxima
@@ -501,8 +504,8 @@ size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out) {
 // Sliced-integer sums: from the FP64 tables tab[kind][l][sta] and coefficients
 // A[kind rows][lcap], write C[kind][row][sta] in FP64.  ws: device workspace of
 // sums_tc_workspace bytes.  Blocking (synchronises the stream).
-const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, const double* A, double* C, void* ws,
-                        size_t ws_bytes, cudaStream_t st) {
+const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const double* tab, const double* A,
+                        double* C, void* ws, size_t ws_bytes, cudaStream_t st) {
   TcLayout L = tc_layout(S, mtot);
   if (ws_bytes < L.total) return "sums_tc: workspace too small";
   if (7LL * mtot >= (1LL << 31) || 7LL * 8 * S.nsta >= (1LL << 31)) return "sums_tc: operand rows exceed 2^31";
@@ -516,13 +519,13 @@ const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, co
   double* cscale = (double*)(base + L.off[3]);
   double* rscale = (double*)(base + L.off[4]);
   int* row_kind = (int*)(base + L.off[5]);
-  int2* tiles = (int2*)(base + L.off[6]);
+  int4* tiles = (int4*)(base + L.off[6]);
   long long* tabs = (long long*)(base + L.off[7]);
   int* ints = (int*)(base + L.off[8]);   // [0..7] rows per kind, [8] error flag
   unsigned long long* colmax = (unsigned long long*)(base + L.off[9]);
   int krows[16] = {0};
   long long htabs[24];
-  std::vector<int2> htiles;
+  std::vector<int4> htiles;
   std::vector<int> hrk((size_t)mtot);
   long long ro = 0;
   for (int k = 0; k < 8; ++k) {
@@ -530,12 +533,22 @@ const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, co
     htabs[k] = 0;
     htabs[8 + k] = ro;
     htabs[16 + k] = S.coff[k];
-    for (int m = 0; m < krows[k]; m += TC_BM) htiles.push_back(make_int2(k, m));
+    for (int m = 0; m < krows[k]; m += TC_BM) {
+      // rows 2 (slot nsk + rank) + re/im; the coefficients of frequency slot are zero
+      // from degree nwn[nf1 - 1 + slot] on (coef_kernel, bessel_coef_kernel)
+      const int s0 = m / (2 * S.nsk[k]), s1 = std::min(nf - 1, (m + TC_BM - 1) / (2 * S.nsk[k]));
+      int ext = 0;
+      for (int s = s0; s <= s1; ++s) ext = std::max(ext, nwn[S.nf1 - 1 + s]);
+      ext = std::min(ext, K);
+      htiles.push_back(make_int4(k, m, std::max(1, (ext + TC_BK - 1) / TC_BK), 0));
+    }
     for (int m = 0; m < krows[k]; ++m) hrk[(size_t)(ro + m)] = k;
     ro += krows[k];
   }
   if (ro != mtot) return "sums_tc: row count mismatch";
-  if (cudaMemcpyAsync(tiles, htiles.data(), htiles.size() * sizeof(int2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+  // longest k-loops first: the short tiles fill the last wave
+  std::stable_sort(htiles.begin(), htiles.end(), [](const int4& a, const int4& b) { return a.z > b.z; });
+  if (cudaMemcpyAsync(tiles, htiles.data(), htiles.size() * sizeof(int4), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(row_kind, hrk.data(), hrk.size() * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(tabs, htabs, sizeof htabs, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(ints, krows, sizeof krows, cudaMemcpyHostToDevice, st) != cudaSuccess)
@@ -559,7 +572,7 @@ const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, co
   if (cudaMemsetAsync(ints + 8, 0, sizeof(int), st) != cudaSuccess) return "sums_tc: upload failed";
   dim3 grid((S.nsta + TC_BN - 1) / TC_BN, (unsigned)htiles.size());
   sums_tc_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(mA, mB, tiles, ints, tabs + 8, tabs + 16, S.nsta, mtot,
-                                                    Kp / TC_BK, rscale, cscale, C, ints + 8);
+                                                    rscale, cscale, C, ints + 8);
   if (cudaGetLastError() != cudaSuccess) return "sums_tc: launch failed";
   int herr = 0;
   if (cudaMemcpyAsync(&herr, ints + 8, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||

@@ -285,7 +285,10 @@ __global__ void bessel_corr_kernel(SynthDev S, const float* __restrict__ gr, con
 
 // ---------------------------------------------------------------------------
 //  FP64 tiled product C[kind][row][sta] = sum_l A[kind][row][l] * T[kind][l][sta]
-//  64x64 output tile per block of 256 threads, 4x4 per thread, K step 16.
+//  64x64 output tile per block of 256 threads, 4x4 per thread, K step 16.  Rows
+//  2 (slot nsk + rank) + re/im hold zero coefficients from degree
+//  nwn[nf1 - 1 + slot] on, so a tile's K loop ends at its largest count (the
+//  skipped terms would add exact zeros).
 // ---------------------------------------------------------------------------
 constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
 
@@ -293,9 +296,16 @@ __global__ void __launch_bounds__(256) sums_gemm_kernel(SynthDev S, const double
                                                         const double* __restrict__ T, double* C) {
   const int kind = blockIdx.z;
   const int M = 2 * (S.nf2 - S.nf1 + 1) * S.nsk[kind];
-  const int N = S.nsta, K = S.lmax + 1;
+  const int N = S.nsta;
   const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
   if (m0 >= M) return;
+  int K = 0;
+  {
+    const int nf = S.nf2 - S.nf1 + 1, s0 = m0 / (2 * S.nsk[kind]);
+    const int s1 = min(nf - 1, (m0 + GT_M - 1) / (2 * S.nsk[kind]));
+    for (int s = s0; s <= s1; ++s) K = max(K, S.nwn[S.nf1 - 1 + s]);
+    K = min(K, S.lmax + 1);
+  }
   const double* Ak = A + S.aoff[kind];
   const double* Tk = T + (long long)kind * S.lcap * N;
   double* Ck = C + S.coff[kind];
@@ -749,7 +759,7 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
     const long long mtot = 2LL * nf * S.nsum;
     const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
     void* ws = gem_ctx_aux(ctx, 3, wsb);
-    const char* why = ws ? sums_tc_run(S, mtot, b.tab, b.A, b.C, ws, wsb, st) : "";
+    const char* why = ws ? sums_tc_run(S, nwn, mtot, b.tab, b.A, b.C, ws, wsb, st) : "";
     if (why) {
       nvtxRangePop();
       cudaEventDestroy(e0); cudaEventDestroy(e1);

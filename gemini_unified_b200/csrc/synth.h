@@ -63,10 +63,11 @@ inline bool ifft_fast_supported(int ns) { return ns >= 512 && ns <= IFFT_MAX_NS;
 bool legendre_fast_supported(int lmax);
 cudaError_t legendre_fast_launch(int nsta, int lmax, int lcap, const double* theta, double* tab, cudaStream_t st);
 
-// sliced-integer tensor-core degree sums (sums_tc.cu): workspace size and run
+// sliced-integer tensor-core degree sums (sums_tc.cu): workspace size and run;
+// nwn: host copy of the wavenumber counts per frequency (1-based frequency index)
 size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out);
-const char* sums_tc_run(const SynthDev& S, long long mtot, const double* tab, const double* A, double* C, void* ws,
-                        size_t ws_bytes, cudaStream_t st);
+const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const double* tab, const double* A,
+                        double* C, void* ws, size_t ws_bytes, cudaStream_t st);
 
 }  // namespace gem
 
