@@ -70,6 +70,7 @@ struct gem_ctx {
   void* d_aux[12] = {};
   size_t aux_cap[12] = {};
   int kopt = 6;   // order target of the step-size control (gem_order_target; fast backend)
+  int dsv = 0;    // set by gem_fk_run_dsv* for the length of one run: DSV spectra with derivatives
   // schedule of each solver phase (index into FK_SCHED_*), per build: [0] plain, [1] fast
   int sched[2][3] = {{FK_SCHED_DEFAULT[0], FK_SCHED_DEFAULT[1], FK_SCHED_DEFAULT[2]},
                      {FK_SCHED_DEFAULT[0], FK_SCHED_DEFAULT[1], FK_SCHED_DEFAULT[2]}};
@@ -164,6 +165,13 @@ int nsp_of(const gem_fk_params* p) {
   return p->stressflag ? 4 * njsph + 2 * njtor : 2 * njsph + njtor;
 }
 
+// spectra per node of a run: U, V, dU/dr, dV/dr and W, dW/dr in DSV mode
+// (computeGreenFKSpectraForASKI.f90:231-233,328)
+int nsp_run(const gem_ctx* ctx, const gem_fk_params* p) {
+  int njsph = p->istyp == 0 ? 2 : 4, njtor = p->istyp == 0 ? 1 : 2;
+  return ctx->dsv ? 4 * njsph + 2 * njtor : nsp_of(p);
+}
+
 int check_params(gem_ctx* ctx, const gem_fk_params* p) {
   if (!ctx->have_model) return fail(ctx, "no earth model loaded");
   if (!ctx->have_nodes) return fail(ctx, "no external nodes set");
@@ -174,6 +182,9 @@ int check_params(gem_ctx* ctx, const gem_fk_params* p) {
   if (p->jre < 1 || p->jre > ctx->nnod) return fail(ctx, "Invalid index for receiver node");
   if (p->global_ == 0 && !(p->xlen > 0)) return fail(ctx, "invalid XLEN");
   if (ctx->state[p->jre] == 1) return fail(ctx, "receiver in an ocean layer is not supported");
+  if (ctx->dsv)
+    for (int n = 1; n <= ctx->nnod; ++n)
+      if (ctx->state[n] != 0) return fail(ctx, "DSV spectra: node %d lies in a fluid layer (not supported)", n);
   if (ctx->rnod[1] < ctx->rb[1])
     return fail(ctx, "External nodes within inner homogeneous sphere (halfspace) are not allowed.");
   return GEM_OK;
@@ -373,7 +384,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   if (jf_first < g.nf1 || jf_last > g.nf2 || jf_first > jf_last)
     return fail(ctx, "frequency range %d..%d outside %d..%d", jf_first, jf_last, g.nf1, g.nf2);
   const int nslot = jf_last - jf_first + 1;
-  const int nsp = nsp_of(p);
+  const int nsp = nsp_run(ctx, p);
   S.nslot = nslot; S.nsp = nsp;
   // ---- parameter block
   FKStatic& P = S.P;
@@ -386,6 +397,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   P.ncsph = 4; P.nctor = 2;
   P.njsph = p->istyp == 0 ? 2 : 4; P.njtor = p->istyp == 0 ? 1 : 2;
   P.dsvstep = p->stressflag ? 1 : 2;
+  P.dsv = ctx->dsv;
   P.rearth = ctx->rearth; P.ric = ctx->ric; P.roc = ctx->roc; P.rhs = ctx->rb[1];
   P.ruc = P.hasocean ? ctx->rb[ctx->nlay - 1] : ctx->rearth;
   P.eps = p->eps; P.sigma = g.sigma; P.df = g.df; P.dwn = g.dwn;
@@ -655,7 +667,7 @@ int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
     return fail(ctx, "frequency range %d..%d outside %d..%d", jf_first, jf_last, g.nf1, g.nf2);
   long long nkf = 0;
   for (int jf = jf_first; jf <= jf_last; ++jf) nkf += g.nwn[jf];
-  size_t nout = (size_t)nkf * nsp_of(p) * ctx->nnod;
+  size_t nout = (size_t)nkf * nsp_run(ctx, p) * ctx->nnod;
   // device outputs: context-owned buffers (slots 8..11), grown on demand and
   // kept for the next call; the host buffers are the caller's (pinned ones copy
   // at full DMA rate)
@@ -683,6 +695,32 @@ int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
     }
   }
   return ret;
+}
+
+// DSV spectra with radial derivatives of one source node (the body of the
+// source-node loop of computeGreenFKSpectraForASKI.f90:451-541): the same
+// phase kernels as gem_fk_run with the source at node p->jre and output mode
+// dsv, for the length of this call.
+namespace {
+struct DsvScope {
+  gem_ctx* c;
+  explicit DsvScope(gem_ctx* ctx) : c(ctx) { c->dsv = 1; }
+  ~DsvScope() { c->dsv = 0; }
+};
+}  // namespace
+
+int gem_fk_run_dsv(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* gfre, float* gfim,
+                   double* gf64, int32_t* status) {
+  if (!ctx) return GEM_ERROR;
+  DsvScope scope(ctx);
+  return gem_fk_run(ctx, p, jf_first, jf_last, gfre, gfim, gf64, status);
+}
+
+int gem_fk_run_dsv_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
+                          float* d_gfim, double* d_gf64, int32_t* d_status, void* stream) {
+  if (!ctx) return GEM_ERROR;
+  DsvScope scope(ctx);
+  return gem_fk_run_device(ctx, p, jf_first, jf_last, d_gfre, d_gfim, d_gf64, d_status, stream);
 }
 
 // Instrumentation of the solver (not part of the reference interface):

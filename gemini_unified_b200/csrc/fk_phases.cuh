@@ -331,10 +331,107 @@ __device__ __forceinline__ void put_out(const FKStatic& P, const FKLaunch& LL, i
   if (LL.gfim) LL.gfim[o] = (float)v.im;
 }
 
+// ------------------------------------------------------------------------
+//  DSV spectra with radial derivatives (computeGreenFKSpectraForASKI.f90:
+//  471-541): the source sits at node P.jre, the unit-jump Green functions of
+//  node n times the source terms give the field at n (no reciprocity), and
+//  its radial derivative is A(r) times the field (dsvDerivatives.f90:39-72),
+//  A the solid (solidOdeSystem.f90:77-114) or toroidal
+//  (toroidalOdeSystem.f90:81-102) system matrix of the layer in which
+//  getLayerIndexNodeEarthmodel places r.  Every node is solid (the host
+//  rejects fluid nodes in this mode).
+// ------------------------------------------------------------------------
+__device__ void dsv_sph_derivative(const FKStatic& P, const Env& e, double r, int nj, const dz g[4][4],
+                                   dz d[4][4]) {
+  int nl, top;
+  layer_index(P, r, nl, top);
+  Env el_env = e;
+  el_env.nl = nl;
+  double ro; dz el[7];
+  eval_spline<0x1Fu>(P, el_env, r, nl, ro, el);
+  const dz zom{e.omre, e.omim};
+  const double dll1 = e.dll1, rr = 1.0 / r, rr2 = rr * rr;
+  const dz zrpc = 1.0 / el[1];
+  const dz z1 = el[0] - (el[2] * el[2]) * zrpc - el[4];
+  const dz z2 = (el[2] * rr) * zrpc;
+  const dz zdlz1 = dll1 * z1;
+  const dz zomro = zom * zom * ro;
+  dz a[4][4];
+  a[0][0] = -(2.0 * z2); a[0][1] = zrpc; a[0][2] = dll1 * z2; a[0][3] = dz{-0.0, 0.0};
+  a[1][0] = (-zomro) + (4.0 * z1) * rr2; a[1][1] = 2.0 * z2 - 2.0 * rr; a[1][2] = -((2.0 * rr2) * zdlz1);
+  a[1][3] = dz{dll1 * rr, 0.0};
+  a[2][0] = dz{-rr, 0.0}; a[2][1] = dz{-0.0, 0.0}; a[2][2] = dz{rr, 0.0}; a[2][3] = 1.0 / el[3];
+  a[3][0] = -((2.0 * z1) * rr2); a[3][1] = -z2; a[3][2] = (-zomro) + (zdlz1 + (dll1 - 2.0) * el[4]) * rr2;
+  a[3][3] = dz{-3.0 * rr, 0.0};
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i < 4; ++i) {
+      dz v{0.0, 0.0};
+      for (int kk = 0; kk < 4; ++kk) v = v + a[i][kk] * g[kk][j];
+      d[i][j] = v;
+    }
+}
+
+__device__ void dsv_tor_derivative(const FKStatic& P, const Env& e, double r, int nj, const dz g[2][2],
+                                   dz d[2][2]) {
+  int nl, top;
+  layer_index(P, r, nl, top);
+  Env el_env = e;
+  el_env.nl = nl;
+  double ro; dz el[7];
+  eval_spline<0x18u>(P, el_env, r, nl, ro, el);
+  const dz zom{e.omre, e.omim};
+  const double rr = 1.0 / r, rr2 = rr * rr;
+  const dz zomro = zom * zom * ro;
+  dz a[2][2];
+  a[0][0] = dz{rr, 0.0}; a[0][1] = 1.0 / el[3];
+  a[1][0] = (-zomro) - (el[4] * rr2) * (2.0 - e.dll1); a[1][1] = dz{-3.0 * rr, 0.0};
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i < 2; ++i) {
+      dz v{0.0, 0.0};
+      for (int kk = 0; kk < 2; ++kk) v = v + a[i][kk] * g[kk][j];
+      d[i][j] = v;
+    }
+}
+
+// spheroidal part of node n: U, V for every jump, then dU/dr, dV/dr
+__device__ void output_dsv_sph_node(const FKStatic& P, const Env& e, const Slot& s, const LaneLayout& lay, int n,
+                                    const FKLaunch& LL, int k) {
+  dz zsph[4][4], ztor[2][2];
+  source_terms(P, e, P.jre, zsph, ztor);
+  dz g[4][4], d[4][4];
+  for (int j = 0; j < P.njsph; ++j)
+    for (int i = 0; i < 4; ++i) {
+      dz v{0.0, 0.0};
+      for (int kk = 0; kk < 4; ++kk) v = v + s.get(lay.sph(n, kk, i)) * zsph[kk][j];
+      g[i][j] = v;
+    }
+  dsv_sph_derivative(P, e, P.rnod[n], P.njsph, g, d);
+  int isp = 0;
+  for (int i = 0; i < 4; i += 2)
+    for (int j = 0; j < P.njsph; ++j) put_out(P, LL, k, isp++, n, g[i][j]);
+  for (int i = 0; i < 4; i += 2)
+    for (int j = 0; j < P.njsph; ++j) put_out(P, LL, k, isp++, n, d[i][j]);
+}
+
+// toroidal part of node n: W for every jump, then dW/dr
+__device__ void output_dsv_tor_node(const FKStatic& P, const Env& e, const dz ti[2][2], int n, const FKLaunch& LL,
+                                    int k) {
+  dz zsph[4][4], ztor[2][2];
+  source_terms(P, e, P.jre, zsph, ztor);
+  dz g[2][2], d[2][2];
+  for (int j = 0; j < P.njtor; ++j)
+    for (int i = 0; i < 2; ++i) g[i][j] = (dz{0.0, 0.0} + ti[i][0] * ztor[0][j]) + ti[i][1] * ztor[1][j];
+  dsv_tor_derivative(P, e, P.rnod[n], P.njtor, g, d);
+  int isp = 4 * P.njsph;
+  for (int j = 0; j < P.njtor; ++j) put_out(P, LL, k, isp++, n, g[0][j]);
+  for (int j = 0; j < P.njtor; ++j) put_out(P, LL, k, isp++, n, d[0][j]);
+}
+
 // spheroidal spectra of node n: reciprocity (reciprocity.f90:82-153) and
 // gfsph = bgsph * zsph (computeGreenFKSpectraForSynthetics.f90:445-494)
 __device__ void output_sph_node(const FKStatic& P, const Env& e, const Slot& s, const LaneLayout& lay, int n,
                                 const FKLaunch& LL, int k) {
+  if (P.dsv) { output_dsv_sph_node(P, e, s, lay, n, LL, k); return; }
   const double re = P.rnod[P.jre], r = P.rnod[n];
   const double elp1 = e.dll1, rlp1 = 1.0 / elp1, f = (r / re) * (r / re);
   const bool fluid = P.state[n] == 1;
@@ -373,6 +470,7 @@ __device__ void output_sph_node(const FKStatic& P, const Env& e, const Slot& s, 
 // toroidal spectra of node n (reciprocity.f90:169-180, :485-490)
 __device__ void output_tor_node(const FKStatic& P, const Env& e, const dz ti[2][2], int n, const FKLaunch& LL,
                                 int k) {
+  if (P.dsv) { output_dsv_tor_node(P, e, ti, n, LL, k); return; }
   const double re = P.rnod[P.jre], r = P.rnod[n], f = (r / re) * (r / re);
   const bool fluid = P.state[n] == 1;
   dz zsph[4][4], ztor[2][2];
@@ -559,7 +657,9 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
         if (L.jr - L.jl < 0) { FAIL(ST_BOOKKEEPING); break; }
         L.det = s.get(lay.ut(jre, 0)) * s.get(lay.dt(jre, 1)) - s.get(lay.dt(jre, 0)) * s.get(lay.ut(jre, 1));
         if (!(zabs(L.det) > TINY_D)) { L.st = S_ITEM_END; break; }
-        const int tor_mask = P.stressflag ? 3 : 2;   // jumps whose Green functions are stored
+        // jumps whose Green functions are stored: the DSV spectra of a moment
+        // source use both, those of a force only the second
+        const int tor_mask = (P.dsv ? P.istyp == 1 : P.stressflag) ? 3 : 2;
         dz dcoef[2], ecoef[2];
         for (int j = 0; j < 2; ++j) {
           double u1 = j == 0 ? 1.0 : 0.0, u2 = j == 1 ? 1.0 : 0.0;
@@ -667,7 +767,8 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
         break;
       }
       case S_ADJ_NEXT: {   // stage = 2*jump + (0 up, 1 down)  (:303-372)
-        const int sph_mask = P.stressflag ? 15 : 10;   // jumps 2 and 4 without stresses
+        // jumps 2 and 4 only without stresses, and for the DSV spectra of a force
+        const int sph_mask = (P.dsv ? P.istyp == 1 : P.stressflag) ? 15 : 10;
         int stg = L.stage + 1;
         for (; stg < 8; ++stg) {
           int j = stg >> 1;

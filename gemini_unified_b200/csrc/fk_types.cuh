@@ -13,6 +13,7 @@ struct FKStatic {
   int ncsph, nctor, njsph, njtor, dsvstep;
   double rearth, ric, roc, rhs, ruc, eps, sigma, df, dwn;
   int kopt;   // attempt the step-size control aims at (opttry, parametersBulirschStep.f90:28-48: 6)
+  int dsv;    // 1: DSV spectra with radial derivatives of a source at node jre (no reciprocity)
   double rb[MAXLAY + 1];
   double drk[MAXLAY + 1];
   int iflso[MAXLAY + 1];

@@ -9,13 +9,14 @@ or a GPU every call raises.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import os
 from typing import Optional
 
 import numpy as np
 
-from .model import (ExternalRadialNodes, FKParams, GeminiError, NodeEarthModel, fk_params_c,
-                    frequency_grid, nsp_for)
+from .model import (ExternalRadialNodes, FKParams, GeminiError, NodeEarthModel, aski_nf1, fk_params_c,
+                    frequency_grid, nsp_dsv, nsp_for)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libgemini_fk.so")
@@ -65,6 +66,8 @@ def lib() -> ctypes.CDLL:
         L.gem_fk_grid.argtypes = [vp, vp, ip, ip, ip, ip, vp, ctypes.c_int]
         L.gem_fk_run.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
         L.gem_fk_run_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
+        L.gem_fk_run_dsv.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
+        L.gem_fk_run_dsv_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
         L.gem_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
         L.gem_fk_graph_build.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
         L.gem_fk_graph_launch.argtypes = [vp, vp]
@@ -251,6 +254,46 @@ class GeminiFK:
         if rc >= 2 and (raise_on_failure or not np.any(status)):
             raise GeminiError(lib().gem_last_error(self._h).decode())
         return gre, gim, g64, status
+
+    def run_dsv(self, params: FKParams, jsrc: int, jf_first: int, jf_last: int, f32: bool = True,
+                f64: bool = True, raise_on_failure: bool = True):
+        """DSV spectra with radial derivatives of a source at node jsrc (type
+        params.source_type), the body of the source-node loop of
+        computeGreenFKSpectraForASKI.f90:451-541.  Returns (gfre, gfim, gf64,
+        status) shaped (nnod, nsp, nkf) with nsp = nsp_dsv(source type): U, V
+        for each spheroidal jump, then dU/dr, dV/dr, then W and dW/dr."""
+        grid = frequency_grid(params, self.model.rearth)
+        nkf = int(grid.nwn[jf_first - 1: jf_last].sum())
+        nsp = nsp_dsv(params.source_type)
+        nnod = self.nodes.nnod
+        pc = fk_params_c(params, jsrc)
+        gre = np.zeros((nnod, nsp, nkf), np.float32) if f32 else None
+        gim = np.zeros((nnod, nsp, nkf), np.float32) if f32 else None
+        g64 = np.zeros((nnod, nsp, nkf), np.complex128) if f64 else None
+        status = np.zeros(nkf, np.int32)
+        rc = lib().gem_fk_run_dsv(self._h, ctypes.byref(pc), jf_first, jf_last, _ptr(gre), _ptr(gim), _ptr(g64),
+                                  _ptr(status))
+        if rc >= 2 and (raise_on_failure or not np.any(status)):
+            raise GeminiError(lib().gem_last_error(self._h).decode())
+        return gre, gim, g64, status
+
+    def aski_spectra(self, params: FKParams, jsnod, jre: int, jf_first: int, jf_last: int, f32: bool = True,
+                     f64: bool = True, raise_on_failure: bool = True):
+        """The FK spectra of computeGreenFKSpectraForASKI for frequencies
+        jf_first..jf_last: one DSV run per source node in jsnod (type
+        params.source_type), then one for a force at the receiver node jre,
+        which must be among the source nodes (:196-209).  Returns a list of
+        (gfre, gfim, gf64, status), the force last, as the program's files
+        <DSVBASENAME>.<type>.<js> hold them."""
+        jsnod = [int(j) for j in jsnod]
+        if jre not in jsnod:
+            raise GeminiError("receiver node must also be a source node")
+        if jf_first < aski_nf1(params):
+            raise GeminiError("frequency index %d below the first ASKI frequency %d" % (jf_first, aski_nf1(params)))
+        force = dataclasses.replace(params, source_type="FORCE")
+        out = [self.run_dsv(params, js, jf_first, jf_last, f32, f64, raise_on_failure) for js in jsnod]
+        out.append(self.run_dsv(force, jre, jf_first, jf_last, f32, f64, raise_on_failure))
+        return out
 
     def run_device(self, params: FKParams, jre: int, jf_first: int, jf_last: int, gfre=None, gfim=None,
                    gf64=None, status=None, stream: int = 0):

@@ -467,6 +467,21 @@ def frequency_grid(p: FKParams, rearth: float) -> FrequencyGrid:
     return FrequencyGrid(df, sigma, nf1, nf2, nwn, nwnmax, dwn)
 
 
+def nsp_dsv(source_type: str) -> int:
+    """Spectra per node of the DSV spectra with radial derivatives (U, V, dU/dr,
+    dV/dr per spheroidal jump, W, dW/dr per toroidal jump) of a source in the
+    solid (computeGreenFKSpectraForASKI.f90:231-233,306-328)."""
+    njsph, njtor = (2, 1) if source_type == "FORCE" else (4, 2)
+    return 4 * njsph + 2 * njtor
+
+
+def aski_nf1(p: FKParams) -> int:
+    """First frequency index of the ASKI FK program, max(nint(fmin/df), 1) + 1
+    (computeGreenFKSpectraForASKI.f90:218-220); the rest of its grid is that of
+    the synthetics program."""
+    return max(_nint(p.fmin / (1.0 / p.tlen)), 1) + 1
+
+
 def nsp_for(p: FKParams) -> int:
     """Number of FK spectra per node for a receiver in the solid (:274-313)."""
     njsph, njtor = (2, 1) if p.source_type == "FORCE" else (4, 2)

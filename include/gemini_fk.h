@@ -129,6 +129,23 @@ int gem_fk_run(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
 int gem_fk_run_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
                       float* d_gfim, double* d_gf64, int32_t* d_status, void* stream);
 
+/* DSV spectra with radial derivatives for a source at node p->jre (type
+ * p->istyp): replaces the body of the source-node loop of
+ * computeGreenFKSpectraForASKI.f90:451-541 -- unit-jump Green functions of the
+ * source node (unitJumpGreenFunctions.f90:62-380), gfsph = ujgf * zsph and
+ * gftor = ujgf * ztor at every node (no reciprocity), and their radial
+ * derivatives A(r) * gf (dsvDerivatives.f90:39-72, solidOdeSystem.f90:77-114,
+ * toroidalOdeSystem.f90:81-102).  Spectra per node: U, V for each spheroidal
+ * jump, then dU/dr, dV/dr, then W, dW/dr for each toroidal jump, i.e.
+ * nsp = 4*njsph + 2*njtor (20 for a moment, 10 for a force); p->stressflag is
+ * ignored.  Every node must be solid.  The ASKI program's set of source nodes
+ * (SOURCE_NODE_RADII) plus the force at the receiver is one call per source
+ * node.  Layout, buffers and return codes as gem_fk_run / gem_fk_run_device. */
+int gem_fk_run_dsv(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* gfre, float* gfim,
+                   double* gf64, int32_t* status);
+int gem_fk_run_dsv_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
+                          float* d_gfim, double* d_gf64, int32_t* d_status, void* stream);
+
 /* CUDA-graph form of gem_fk_run_device (no counterpart in the reference).
  * gem_fk_graph_build does the host-side preparation of the slab once (item and
  * queue tables, buffers) and captures its device work (zeroing, model

@@ -52,6 +52,9 @@ def lib():
         L.oracle_nwn.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.oracle_fk_frequency.argtypes = [vp, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.oracle_dsv_frequency.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.oracle_legendre.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
         L.oracle_fft.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_wavenumber_integrals.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
@@ -183,6 +186,26 @@ class Oracle:
             raise RuntimeError(f"nsp mismatch {rc} != {nsp}")
         g = gf.view(np.complex128).reshape(nnod, nsp, nwn)
         return g, status, st.asdict()
+
+    def dsv_frequency(self, pc, jsnod, jf, nwn, iwn_lo=1, iwn_hi=1 << 30):
+        """DSV spectra with radial derivatives of one frequency for the source
+        nodes jsnod (type pc.istyp) and a force at pc.jre, as the ASKI FK driver
+        computes them: a list of complex128 [nnod, nsp_js, nwn], one per source
+        (the force last), plus per-iwn status and stats."""
+        nnod = lib().oracle_nnod(self.h)
+        js = np.ascontiguousarray(jsnod, np.int32)
+        ns = len(js)
+        gf = np.zeros((ns + 1) * nwn * 20 * nnod * 2)
+        nsp = np.zeros(ns + 1, np.int32)
+        status = np.zeros(nwn, np.int32)
+        st = Stats()
+        rc = lib().oracle_dsv_frequency(self.h, ctypes.byref(pc), _p(js), ns, jf, nwn, _p(gf), _p(nsp), _p(status),
+                                        ctypes.byref(st), iwn_lo, iwn_hi)
+        if rc < 0:
+            raise RuntimeError("oracle_dsv_frequency: unsupported configuration")
+        blocks = gf.view(np.complex128).reshape(ns + 1, -1)
+        out = [blocks[j, :nwn * int(nsp[j]) * nnod].reshape(nnod, int(nsp[j]), nwn) for j in range(ns + 1)]
+        return out, status, st.asdict()
 
 
 def legendre(lmax, theta):

@@ -17,6 +17,8 @@
 //    spheroidalAdjoint.f90:53-159, unitJumpGreenFunctions.f90:62-380,
 //    reciprocity.f90:82-180, sourceTerms.f90:59-118,
 //    computeGreenFKSpectraForSynthetics.f90:186-236,380-501 (FK driver)
+//    computeGreenFKSpectraForASKI.f90:196-233,451-541, dsvDerivatives.f90:39-72,
+//    solidOdeSystem.f90:77-114               (DSV spectra with derivatives)
 // =============================================================================
 #include <algorithm>
 #include <cstdio>
@@ -1938,6 +1940,158 @@ int oracle_fk_frequency(void* h, const or_fk_params* p, int jf, int nwn, double*
     stats_out->matvecs = tot.matvecs; stats_out->flops = tot.flops;
   }
   return nsp;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+//  DSV spectra with radial derivatives for several source nodes
+//  (computeGreenFKSpectraForASKI.f90:451-560, dsvDerivatives.f90:39-72)
+// ===========================================================================
+// solid system matrix (solidOdeSystem.f90:77-114), column-major a[i + 4*j]
+static void solidSysmat(const Env& e, double x, zc* a) {
+  double ro; zc el[7];
+  evalSpline(*e.s, x, e.nl, ro, el);
+  zc zom = Z(e.omre, e.omim);
+  double dll1 = e.dll1, rr = 1.0 / x, rr2 = rr * rr;
+  zc zrpc = 1.0 / el[1];
+  zc z1 = el[0] - (el[2] * el[2]) * zrpc - el[4];
+  zc z2 = (el[2] * rr) * zrpc;
+  zc zdlz1 = dll1 * z1;
+  zc zomro = zom * zom * ro;
+#define A(i, j) a[((i)-1) + 4 * ((j)-1)]
+  A(1, 1) = -(2.0 * z2);
+  A(1, 2) = zrpc;
+  A(1, 3) = dll1 * z2;
+  A(1, 4) = Z(-0.0);
+  A(2, 1) = (-zomro) + (4.0 * z1) * rr2;
+  A(2, 2) = 2.0 * z2 - 2.0 * rr;
+  A(2, 3) = -((2.0 * rr2) * zdlz1);
+  A(2, 4) = Z(dll1 * rr);
+  A(3, 1) = Z(-rr);
+  A(3, 2) = Z(-0.0);
+  A(3, 3) = Z(rr);
+  A(3, 4) = 1.0 / el[3];
+  A(4, 1) = -((2.0 * z1) * rr2);
+  A(4, 2) = -z2;
+  A(4, 3) = (-zomro) + (zdlz1 + (dll1 - 2.0) * el[4]) * rr2;
+  A(4, 4) = Z(-3.0 * rr);
+#undef A
+}
+
+// gfd = A(r) gf for nj jump vectors of nv components (computeDsvDerivatives:
+// layer of r by getLayerIndexNodeEarthmodel, gfortran matmul order)
+static void dsvDerivatives(const Env& gem, double r, bool tor, int nj, const zc gf[4][4], zc gfd[4][4]) {
+  Env e = gem;
+  int nl, top;
+  layerIndex(*gem.m, r, nl, top);
+  e.nl = nl;
+  const int nv = tor ? 2 : 4;
+  zc a[16];
+  if (tor) sysmat(SYS_TOROIDAL, e, r, a); else solidSysmat(e, r, a);
+  for (int j = 0; j < nj; ++j) {
+    for (int i = 0; i < nv; ++i) gfd[i][j] = Z(0.0);
+    for (int k = 0; k < nv; ++k)
+      for (int i = 0; i < nv; ++i) gfd[i][j] = gfd[i][j] + a[i + nv * k] * gf[k][j];
+  }
+}
+
+extern "C" {
+// One frequency jf of the ASKI variant: minors once over the source-node range
+// min(jsnod)..max(jsnod), then for each source node jsnod[js] (js < nsnod,
+// source type p->istyp) and for a force at p->jre (js = nsnod): U, V, dU/dr,
+// dV/dr for every spheroidal jump, then W, dW/dr for every toroidal jump, at
+// every node.  gf holds (nsnod+1) blocks of nwn*20*nnod complex values; block
+// js is indexed [(iwn-1) + nwn*(isp + nsp_js*(n-1))] and nsp_js goes to
+// nsp_out[js].  Sources and nodes in fluid layers are not restated (-1).
+int oracle_dsv_frequency(void* h, const or_fk_params* p, const int* jsnod, int nsnod, int jf, int nwn,
+                         double* gf, int* nsp_out, int* status, or_stats* stats_out, int iwn_lo, int iwn_hi) {
+  Ctx* c = (Ctx*)h;
+  const Model& m = c->m;
+  const Nodes& ex = c->ex;
+  const int nnod = ex.nnod;
+  if (nsnod < 1) return -1;
+  for (int n = 1; n <= nnod; ++n) if (ex.state[n] != 0) return -1;
+  int jsl = jsnod[0], jsr = jsnod[0];
+  bool jre_in = false;
+  for (int js = 0; js < nsnod; ++js) {
+    if (jsnod[js] < 1 || jsnod[js] > nnod) return -1;
+    jsl = std::min(jsl, jsnod[js]); jsr = std::max(jsr, jsnod[js]);
+    jre_in = jre_in || jsnod[js] == p->jre;
+  }
+  if (!jre_in) return -1;   // receiver node must also be a source node (:206-209)
+  const double df = 1.0 / p->tlen, sigma = 5.0 * df, dwn = TWO_PI_F / p->xlen;
+  const double f = (double)(jf - 1) * df, omre = 2.0 * PI_F * f;
+  Spline s;
+  if (computeSpline(m, f, p->attmode, s)) return 2;
+  const size_t block = (size_t)nwn * 20 * nnod * 2;
+  for (int js = 0; js <= nsnod; ++js) {
+    int ty = js == nsnod ? 0 : p->istyp;
+    nsp_out[js] = 4 * (ty == 0 ? 2 : 4) + 2 * (ty == 0 ? 1 : 2);
+  }
+  const int iwa = (p->global == 1) ? 1 : 2;
+  Stats tot;
+  for (int iwn = 1; iwn <= nwn; ++iwn) status[iwn - 1] = 0;
+  const int lo = std::max(iwa, iwn_lo), hi = std::min(nwn, iwn_hi);
+  for (int iwn = lo; iwn <= hi; ++iwn) {
+    double wn = (double)(iwn - 1) * dwn;
+    if (p->global == 1) wn = std::sqrt((double)((int64_t)(iwn - 1) * iwn)) / m.rearth;
+    Env gem; gem.m = &m; gem.ex = &ex; gem.s = &s; gem.nl = 1;
+    gem.dll1 = (wn * m.rearth) * (wn * m.rearth);
+    gem.omre = omre; gem.omim = -sigma;
+    Stats st;
+    TorMin T; SphMin S;
+    int rc = computeToroidalMinors(T, jsl, jsr, gem, p->eps, st);
+    if (!rc) rc = computeSpheroidalMinors(S, jsl, jsr, gem, p->eps, st);
+    for (int js = 0; js <= nsnod && !rc; ++js) {
+      const int ty = js == nsnod ? 0 : p->istyp;
+      const int jsh = js == nsnod ? p->jre : jsnod[js];
+      const int njsph = ty == 0 ? 2 : 4, njtor = ty == 0 ? 1 : 2, nsp = nsp_out[js];
+      UJGF U;
+      rc = computeUJGF(U, T, S, jsh, gem, p->eps, st);
+      if (rc) break;
+      zc zsph[4][4], ztor[2][2];
+      sourceTerms(ty, gem.dll1, gem.omre, ex.r[jsh], ex.state[jsh], ex.layer[jsh], s, zsph, ztor);
+      double* g = gf + js * block;
+      for (int n = 1; n <= nnod; ++n) {
+        zc gfsph[4][4], gftor[4][4], gfds[4][4], gfdt[4][4];
+        for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) gfsph[i][j] = gftor[i][j] = Z(0.0);
+        for (int j = 0; j < njsph; ++j) for (int k = 0; k < 4; ++k) for (int i = 0; i < 4; ++i)
+          gfsph[i][j] = gfsph[i][j] + U.sph[((size_t)n * 4 + k) * 4 + i] * zsph[k][j];
+        for (int j = 0; j < njtor; ++j) for (int k = 0; k < 2; ++k) for (int i = 0; i < 2; ++i)
+          gftor[i][j] = gftor[i][j] + U.tor[((size_t)n * 2 + k) * 2 + i] * ztor[k][j];
+        dsvDerivatives(gem, ex.r[n], false, njsph, gfsph, gfds);
+        dsvDerivatives(gem, ex.r[n], true, njtor, gftor, gfdt);
+        int isp = 0;
+        auto put = [&](zc v) {
+          size_t o = ((size_t)(iwn - 1) + (size_t)nwn * ((size_t)isp + (size_t)nsp * (n - 1))) * 2;
+          g[o] = v.re; g[o + 1] = v.im; isp++;
+        };
+        for (int i = 0; i < 4; i += 2) for (int j = 0; j < njsph; ++j) put(gfsph[i][j]);
+        for (int i = 0; i < 4; i += 2) for (int j = 0; j < njsph; ++j) put(gfds[i][j]);
+        for (int j = 0; j < njtor; ++j) put(gftor[0][j]);
+        for (int j = 0; j < njtor; ++j) put(gfdt[0][j]);
+      }
+    }
+    tot.add(st);
+    if (rc) {
+      status[iwn - 1] = rc;
+      for (int js = 0; js <= nsnod; ++js) {   // a failed item leaves zeros, as the GPU path does
+        double* g = gf + js * block;
+        for (int n = 1; n <= nnod; ++n)
+          for (int isp = 0; isp < nsp_out[js]; ++isp) {
+            size_t o = ((size_t)(iwn - 1) + (size_t)nwn * ((size_t)isp + (size_t)nsp_out[js] * (n - 1))) * 2;
+            g[o] = 0.0; g[o + 1] = 0.0;
+          }
+      }
+    }
+  }
+  if (stats_out) {
+    stats_out->steps_ok = tot.steps_ok; stats_out->steps_rej = tot.steps_rej;
+    stats_out->attempts = tot.attempts; stats_out->sysmats = tot.sysmats;
+    stats_out->matvecs = tot.matvecs; stats_out->flops = tot.flops;
+  }
+  return nsnod + 1;
 }
 
 }  // extern "C"
