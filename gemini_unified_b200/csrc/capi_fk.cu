@@ -71,6 +71,7 @@ struct gem_ctx {
   size_t aux_cap[12] = {};
   int kopt = 6;   // order target of the step-size control (gem_order_target; fast backend)
   int dsv = 0;    // set by gem_fk_run_dsv* for the length of one run: DSV spectra with derivatives
+  int jsl = 0, jsr = 0;   // set by gem_fk_run_aski* for one run: node range of the minors (0: the receiver)
   // schedule of each solver phase (index into FK_SCHED_*), per build: [0] plain, [1] fast
   int sched[2][3] = {{FK_SCHED_DEFAULT[0], FK_SCHED_DEFAULT[1], FK_SCHED_DEFAULT[2]},
                      {FK_SCHED_DEFAULT[0], FK_SCHED_DEFAULT[1], FK_SCHED_DEFAULT[2]}};
@@ -364,7 +365,7 @@ struct SlabPlan {
   int grid[3];
   int nslot, nitems, nsp;
   long long nkf;
-  size_t spl_n, nout, nu, nd;
+  size_t spl_n, nout, nu, nd, ndet;
   bool fast, propose;
   int sched[3], defer[3];
   float* gfre;
@@ -398,6 +399,8 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   P.njsph = p->istyp == 0 ? 2 : 4; P.njtor = p->istyp == 0 ? 1 : 2;
   P.dsvstep = p->stressflag ? 1 : 2;
   P.dsv = ctx->dsv;
+  P.jsl = ctx->jsl ? ctx->jsl : p->jre;
+  P.jsr = ctx->jsr ? ctx->jsr : p->jre;
   P.rearth = ctx->rearth; P.ric = ctx->ric; P.roc = ctx->roc; P.rhs = ctx->rb[1];
   P.ruc = P.hasocean ? ctx->rb[ctx->nlay - 1] : ctx->rearth;
   P.eps = p->eps; P.sigma = g.sigma; P.df = g.df; P.dwn = g.dwn;
@@ -458,13 +461,14 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
     status = ctx->d_status;
   }
   S.status = status;
-  const int jre = p->jre;
-  S.nu = (size_t)jre * 6 * nkf;
-  S.nd = (size_t)(ctx->nnod - jre + 1) * 6 * nkf;
+  // minors at nodes 1..jsr (up) and jsl..nnod (down), determinants at jsl..jsr
+  S.nu = (size_t)P.jsr * 6 * nkf;
+  S.nd = (size_t)(ctx->nnod - P.jsl + 1) * 6 * nkf;
+  S.ndet = (size_t)(P.jsr - P.jsl + 1) * nkf;
   if (grow(ctx, ctx->d_um, ctx->um_cap, S.nu)) return GEM_ERROR;
   if (grow(ctx, ctx->d_dm, ctx->dm_cap, S.nd)) return GEM_ERROR;
   if (grow(ctx, ctx->d_rstart, ctx->rstart_cap, 2 * (size_t)nkf)) return GEM_ERROR;
-  if (grow(ctx, ctx->d_dets, ctx->dets_cap, (size_t)nkf)) return GEM_ERROR;
+  if (grow(ctx, ctx->d_dets, ctx->dets_cap, S.ndet)) return GEM_ERROR;
   // ---- grid: the largest of the three phases sets the per-lane scratch
   long long nthreads = 0;
   for (int ph = 0; ph < 3; ++ph) {
@@ -533,7 +537,7 @@ int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
   CK(cudaMemsetAsync(S.status, 0, (size_t)S.nkf * sizeof(int32_t), st));
   CK(cudaMemsetAsync(ctx->d_um, 0, S.nu * sizeof(double2), st));
   CK(cudaMemsetAsync(ctx->d_dm, 0, S.nd * sizeof(double2), st));
-  CK(cudaMemsetAsync(ctx->d_dets, 0, (size_t)S.nkf * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_dets, 0, S.ndet * sizeof(double2), st));
   CK(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned int), st));
   CK(cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(unsigned long long), st));
   if (ctx->d_steplog_n) CK(cudaMemsetAsync(ctx->d_steplog_n, 0, sizeof(unsigned long long), st));
@@ -567,6 +571,67 @@ int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
                        cudaMemcpyDeviceToDevice, st));
   }
   if (timed) CK(cudaEventRecord(ctx->ev[3], st));
+  return GEM_OK;
+}
+
+// The device work of the ASKI program's FK spectra for a set of source nodes
+// (computeGreenFKSpectraForASKI.f90:451-541): start radii and spheroidal
+// minors once over the node range jsl..jsr of the plan, then per source node
+// (the moment or force sources jsnod[b], then the force at jre) the toroidal
+// phase and the adjoint phase with that node as the source, each writing its
+// own output block (block b at b * blk_m; the force block is blk_f long).
+int fk_enqueue_aski(gem_ctx* ctx, SlabPlan& S, int nsnod, const int* jsnod, int jre, int istyp, float* gre,
+                    float* gim, double* g64, size_t blk_m, size_t blk_f, cudaStream_t st) {
+  CK(cudaMemsetAsync(ctx->d_spl, 0, S.spl_n * sizeof(double), st));
+  CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  CK(launch_prep(S.A, ctx->d_err, st));
+  if (S.fast) CK(launch_poly(S.A, ctx->d_poly, st));
+  const size_t ntot = blk_m * nsnod + blk_f;
+  if (g64) CK(cudaMemsetAsync(g64, 0, ntot * 2 * sizeof(double), st));
+  if (gre) CK(cudaMemsetAsync(gre, 0, ntot * sizeof(float), st));
+  if (gim) CK(cudaMemsetAsync(gim, 0, ntot * sizeof(float), st));
+  CK(cudaMemsetAsync(S.status, 0, (size_t)S.nkf * sizeof(int32_t), st));
+  CK(cudaMemsetAsync(ctx->d_um, 0, S.nu * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_dm, 0, S.nd * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_dets, 0, S.ndet * sizeof(double2), st));
+  CK(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(ctx->d_stats, 0, 32 * sizeof(unsigned long long), st));
+  if (ctx->d_steplog_n) CK(cudaMemsetAsync(ctx->d_steplog_n, 0, sizeof(unsigned long long), st));
+  if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
+  auto launch = [&](int ph, const FKStatic& PX, FKLaunch LX) {
+    const int sc = ph >= 0 ? S.sched[ph] : 0;
+    if (ph >= 0) { LX.adv_min = FK_DEFER_MIN[S.defer[ph]]; LX.adv_wait = FK_DEFER_WAIT[S.defer[ph]]; }
+    const int g = ph >= 0 ? S.grid[ph] : ctx->nsm * 8;
+    return S.fast ? gem_fast::launch_fk_phase(ph, sc, PX, LX, g, st) : gem_plain::launch_fk_phase(ph, sc, PX, LX, g, st);
+  };
+  FKLaunch L0 = S.L;
+  L0.prop_kopt = nullptr; L0.prop_hs = nullptr;
+  CK(launch(-1, S.P, L0));
+  nvtxRangePushA("gem_fk: spheroidal phase over the source-node range");
+  const cudaError_t le = launch(1, S.P, L0);
+  nvtxRangePop();
+  CK(le);
+  for (int b = 0; b <= nsnod; ++b) {
+    const bool force = b == nsnod;
+    const int js = force ? jre : jsnod[b], ty = force ? 0 : istyp;
+    FKStatic Pb = S.P;
+    Pb.jre = js; Pb.istyp = ty;
+    Pb.njsph = ty == 0 ? 2 : 4; Pb.njtor = ty == 0 ? 1 : 2;
+    Pb.nsp = 4 * Pb.njsph + 2 * Pb.njtor;
+    FKLaunch Lb = L0;
+    const size_t off = (size_t)b * blk_m;
+    Lb.gf64 = g64 ? reinterpret_cast<double2*>(g64) + off : nullptr;
+    Lb.gfre = gre ? gre + off : nullptr;
+    Lb.gfim = gim ? gim + off : nullptr;
+    Lb.dets = reinterpret_cast<double2*>(ctx->d_dets) + (size_t)(js - S.P.jsl) * S.nkf;
+    CK(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned int), st));
+    CK(launch(0, Pb, Lb));
+    CK(launch(2, Pb, Lb));
+  }
+  // totals only: the per-phase split is not recorded for a set of sources
+  for (int ph = 0; ph < 3; ++ph)
+    CK(cudaMemcpyAsync(ctx->d_stats + 8 * (ph + 1), ctx->d_stats, 8 * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToDevice, st));
   return GEM_OK;
 }
 
@@ -721,6 +786,85 @@ int gem_fk_run_dsv_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, in
   if (!ctx) return GEM_ERROR;
   DsvScope scope(ctx);
   return gem_fk_run_device(ctx, p, jf_first, jf_last, d_gfre, d_gfim, d_gf64, d_status, stream);
+}
+
+// FK spectra of computeGreenFKSpectraForASKI for a set of source nodes: the
+// minors once over the node range, then per source node the unit-jump Green
+// functions and the DSV spectra with derivatives (see fk_enqueue_aski).
+namespace {
+struct AskiScope {
+  gem_ctx* c;
+  AskiScope(gem_ctx* ctx, int lo, int hi) : c(ctx) { c->dsv = 1; c->jsl = lo; c->jsr = hi; }
+  ~AskiScope() { c->dsv = 0; c->jsl = 0; c->jsr = 0; }
+};
+}  // namespace
+
+int gem_fk_aski_nsp(int istyp) { return istyp == 0 ? 10 : 20; }
+
+int gem_fk_run_aski_device(gem_ctx* ctx, const gem_fk_params* p, int nsnod, const int* jsnod, int jf_first,
+                           int jf_last, float* d_gfre, float* d_gfim, double* d_gf64, int32_t* d_status,
+                           void* stream) {
+  if (!ctx) return GEM_ERROR;
+  if (!p) return fail(ctx, "null parameters");
+  if (nsnod < 1 || !jsnod) return fail(ctx, "ASKI spectra: no source nodes");
+  if (!ctx->have_nodes) return fail(ctx, "no external nodes set");
+  int lo = ctx->nnod + 1, hi = 0;
+  bool has_re = false;
+  for (int i = 0; i < nsnod; ++i) {
+    if (jsnod[i] < 1 || jsnod[i] > ctx->nnod) return fail(ctx, "ASKI spectra: source node %d out of range", jsnod[i]);
+    lo = std::min(lo, jsnod[i]); hi = std::max(hi, jsnod[i]);
+    has_re = has_re || jsnod[i] == p->jre;
+  }
+  if (!has_re) return fail(ctx, "receiver node must also be a source node");
+  AskiScope scope(ctx, lo, hi);
+  SlabPlan S;
+  int rc = fk_prepare(ctx, p, jf_first, jf_last, nullptr, nullptr, nullptr, d_status, S);
+  if (rc) return rc;
+  const size_t blk_m = (size_t)S.nkf * gem_fk_aski_nsp(p->istyp) * ctx->nnod;
+  const size_t blk_f = (size_t)S.nkf * gem_fk_aski_nsp(0) * ctx->nnod;
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = fk_enqueue_aski(ctx, S, nsnod, jsnod, p->jre, p->istyp, d_gfre, d_gfim, d_gf64, blk_m, blk_f, st);
+  if (rc) return rc;
+  return fk_finish(ctx, S, st, false);
+}
+
+int gem_fk_run_aski(gem_ctx* ctx, const gem_fk_params* p, int nsnod, const int* jsnod, int jf_first, int jf_last,
+                    float* gfre, float* gfim, double* gf64, int32_t* status) {
+  if (!ctx) return GEM_ERROR;
+  if (!p) return fail(ctx, "null parameters");
+  if (!ctx->have_model) return fail(ctx, "no earth model loaded");
+  if (!ctx->have_nodes) return fail(ctx, "no external nodes set");
+  CK(cudaSetDevice(ctx->device));
+  Grid g;
+  make_grid(p, ctx->rearth, g);
+  if (jf_first < g.nf1 || jf_last > g.nf2 || jf_first > jf_last)
+    return fail(ctx, "frequency range %d..%d outside %d..%d", jf_first, jf_last, g.nf1, g.nf2);
+  long long nkf = 0;
+  for (int jf = jf_first; jf <= jf_last; ++jf) nkf += g.nwn[jf];
+  if (nsnod < 1) return fail(ctx, "ASKI spectra: no source nodes");
+  const size_t nout = (size_t)nkf * ctx->nnod * ((size_t)nsnod * gem_fk_aski_nsp(p->istyp) + gem_fk_aski_nsp(0));
+  float* dre = gfre ? (float*)gem_ctx_aux(ctx, 8, nout * sizeof(float)) : nullptr;
+  float* dim = gfim ? (float*)gem_ctx_aux(ctx, 9, nout * sizeof(float)) : nullptr;
+  double* d64 = gf64 ? (double*)gem_ctx_aux(ctx, 10, nout * 2 * sizeof(double)) : nullptr;
+  int32_t* dst = (int32_t*)gem_ctx_aux(ctx, 11, (size_t)nkf * sizeof(int32_t));
+  if ((gfre && !dre) || (gfim && !dim) || (gf64 && !d64) || !dst) return GEM_ERROR;
+  int ret = gem_fk_run_aski_device(ctx, p, nsnod, jsnod, jf_first, jf_last, dre, dim, d64, dst, nullptr);
+  if (ret == GEM_OK) {
+    std::vector<int32_t> hst((size_t)nkf);
+    if ((gfre && cudaMemcpy(gfre, dre, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (gfim && cudaMemcpy(gfim, dim, nout * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (gf64 && cudaMemcpy(gf64, d64, nout * 2 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        cudaMemcpy(hst.data(), dst, (size_t)nkf * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      ret = fail(ctx, "copy of FK spectra to the host failed");
+    } else {
+      long long nfail = 0;
+      for (auto v : hst) nfail += v != 0;
+      ctx->stats.failed = nfail;
+      if (status) memcpy(status, hst.data(), hst.size() * sizeof(int32_t));
+      if (nfail) ret = fail(ctx, "%lld (omega,l) items failed; see the per-item status", nfail);
+    }
+  }
+  return ret;
 }
 
 // Instrumentation of the solver (not part of the reference interface):

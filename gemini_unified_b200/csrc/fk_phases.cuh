@@ -90,7 +90,7 @@ struct ItemStore {
   __device__ __forceinline__ void put_um(int k, int n, int c, dz v) const {
     LL->um[((long long)(n - 1) * 6 + c) * LL->nkf + k] = make_double2(v.re, v.im);
   }
-  __device__ __forceinline__ dz dm(int k, int n, int c, int jre) const {   // n = jre..nnod
+  __device__ __forceinline__ dz dm(int k, int n, int c, int jre) const {   // n = jre..nnod (jre: P.jsl)
     double2 v = LL->dm[((long long)(n - jre) * 6 + c) * LL->nkf + k];
     return dz{v.x, v.y};
   }
@@ -502,8 +502,8 @@ __device__ void sink_node(const FKStatic& P, const FKLaunch& LL, const Slot& s, 
       s.put(lay.lg(n), dz{L.lgnorm, 0.0});
       break;
     case K_DM:
-      for (int c = 0; c < L.nv; ++c) IS.put_dm(L.k, n, c, P.jre, L.y[c]);
-      IS.put_dm(L.k, n, 5, P.jre, (-L.y[0]) / L.e.dll1);
+      for (int c = 0; c < L.nv; ++c) IS.put_dm(L.k, n, c, P.jsl, L.y[c]);
+      IS.put_dm(L.k, n, 5, P.jsl, (-L.y[0]) / L.e.dll1);
       s.put(lay.lg(n), dz{L.lgnorm, 0.0});
       break;
     case K_ADJIC:
@@ -516,7 +516,7 @@ __device__ void sink_node(const FKStatic& P, const FKLaunch& LL, const Slot& s, 
       else use = n < P.jre && P.state[n] == 0 && P.rnod[n] >= L.rstart_s && P.rnod[n] > P.roc;
       if (!use) return;
       dz m[6], out[4];
-      for (int c = 0; c < 6; ++c) m[c] = up ? IS.dm(L.k, n, c, P.jre) : IS.um(L.k, n, c);
+      for (int c = 0; c < 6; ++c) m[c] = up ? IS.dm(L.k, n, c, P.jsl) : IS.um(L.k, n, c);
       mtil_times(m, L.y, out);
       for (int c = 0; c < 4; ++c) s.put(lay.sph(n, L.stage >> 1, c), out[c]);
     }
@@ -600,9 +600,9 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
           prop_begin<PH>(P, LL, s, lay, L, SYS_TOROIDAL, rsurf, rmin, htry * L.hs, ys, false, 0.0, K_DT, S_TOR_UP);
         } else if (PH == PH_SPH) {   // spheroidalMinors.f90:155-182
           for (int el = 0; el < lay.NN; ++el) s.put(lay.lg(el), dz{0.0, 0.0});
-          if (L.rstart_s >= P.rnod[jre]) { L.st = S_ITEM_END; break; }
+          if (L.rstart_s >= P.rnod[P.jsr]) { L.st = S_ITEM_END; break; }
           L.up = 1;
-          L.rbeg = L.rstart_s; L.rend = L.rstart_s; L.rlim = P.rnod[jre];
+          L.rbeg = L.rstart_s; L.rend = L.rstart_s; L.rlim = P.rnod[P.jsr];
           L.lgnorm_g = 0.0; L.lgnormend = 0.0; L.htry_g = 0.0; L.liq_old = 0;
           L.st = S_SPH_GROUP;
         } else {   // unitJumpGreenFunctions.f90:194-372
@@ -613,10 +613,10 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
           if (L.e.dll1 < EPS_D) {   // l = 0 (:201-220)
             for (int j = 0; j < 2; ++j) {
               double u1 = j == 0 ? 1.0 : 0.0, u2 = j == 1 ? 1.0 : 0.0;
-              dz dd = (u2 * IS.dm(L.k, jre, 0, jre) - u1 * IS.dm(L.k, jre, 1, jre)) / L.det;
+              dz dd = (u2 * IS.dm(L.k, jre, 0, P.jsl) - u1 * IS.dm(L.k, jre, 1, P.jsl)) / L.det;
               dz ee = (u2 * IS.um(L.k, jre, 0) - u1 * IS.um(L.k, jre, 1)) / L.det;
               for (int n = jre; n <= nnod; ++n)
-                for (int c = 0; c < 2; ++c) s.put(lay.sph(n, j, c), ee * IS.dm(L.k, n, c, jre));
+                for (int c = 0; c < 2; ++c) s.put(lay.sph(n, j, c), ee * IS.dm(L.k, n, c, P.jsl));
               for (int n = jre - 1; n >= 1; --n)
                 for (int c = 0; c < 2; ++c) s.put(lay.sph(n, j, c), dd * IS.um(L.k, n, c));
             }
@@ -688,26 +688,29 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
         const bool up = L.up == 1;
         if (!(up ? L.rend < L.rlim : L.rend > L.rlim)) {
           // normalise to the final normalisation factor (spheroidalMinors.f90:360-365,552-557)
-          int n0 = up ? 1 : jre, n1 = up ? jre : nnod;
+          int n0 = up ? 1 : P.jsl, n1 = up ? P.jsr : nnod;
           for (int n = n0; n <= n1; ++n) {
             double fct = pow(10.0, s.get(lay.lg(n)).re - L.lgnormend);
             for (int c = 0; c < 6; ++c) {
               if (up) IS.put_um(L.k, n, c, IS.um(L.k, n, c) * fct);
-              else IS.put_dm(L.k, n, c, jre, IS.dm(L.k, n, c, jre) * fct);
+              else IS.put_dm(L.k, n, c, P.jsl, IS.dm(L.k, n, c, P.jsl) * fct);
             }
           }
           if (up) {
             for (int el = 0; el < lay.NN; ++el) s.put(lay.lg(el), dz{0.0, 0.0});
             L.up = 0;
-            L.rbeg = P.rearth; L.rend = P.rearth; L.rlim = fmax(L.rstart_s, P.rnod[jre]);
+            L.rbeg = P.rearth; L.rend = P.rearth; L.rlim = fmax(L.rstart_s, P.rnod[P.jsl]);
             L.lgnorm_g = 0.0; L.lgnormend = 0.0; L.liq_old = 0;
             break;
           }
-          dz u[6], d[6];
-          for (int c = 0; c < 6; ++c) { u[c] = IS.um(L.k, jre, c); d[c] = IS.dm(L.k, jre, c, jre); }
-          if (P.state[jre] == 1 || L.e.dll1 < EPS_D) L.det = u[0] * d[1] - d[0] * u[1];
-          else L.det = ((((u[0] * d[5] + u[5] * d[0]) - u[1] * d[4]) + u[2] * d[3]) + u[3] * d[2]) - u[4] * d[1];
-          LL.dets[L.k] = make_double2(L.det.re, L.det.im);
+          // determinants at the source nodes jsl..jsr (spheroidalMinors.f90:566-575)
+          for (int js = P.jsl; js <= P.jsr; ++js) {
+            dz u[6], d[6];
+            for (int c = 0; c < 6; ++c) { u[c] = IS.um(L.k, js, c); d[c] = IS.dm(L.k, js, c, P.jsl); }
+            if (P.state[js] == 1 || L.e.dll1 < EPS_D) L.det = u[0] * d[1] - d[0] * u[1];
+            else L.det = ((((u[0] * d[5] + u[5] * d[0]) - u[1] * d[4]) + u[2] * d[3]) + u[3] * d[2]) - u[4] * d[1];
+            LL.dets[(long long)(js - P.jsl) * LL.nkf + L.k] = make_double2(L.det.re, L.det.im);
+          }
           L.st = S_ITEM_END;
           break;
         }
@@ -781,7 +784,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
         const int j = stg >> 1;
         const bool upd = (stg & 1) == 0;
         dz m[6], col[4], ys[5];
-        for (int c = 0; c < 6; ++c) m[c] = upd ? IS.um(L.k, jre, c) : IS.dm(L.k, jre, c, jre);
+        for (int c = 0; c < 6; ++c) m[c] = upd ? IS.um(L.k, jre, c) : IS.dm(L.k, jre, c, P.jsl);
         meps_col(m, j, col);
         for (int c = 0; c < 4; ++c) ys[c] = upd ? dz{0.0, 0.0} - col[c] / L.det : dz{0.0, 0.0} + col[c] / L.det;
         ys[4] = dz{0, 0};
@@ -798,7 +801,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
           if (L.ocean_above)
             for (int n = jre; n <= nnod; ++n)
               if (P.state[n] == 1 && P.rnod[n] > P.ruc)
-                for (int c = 0; c < 2; ++c) s.put(lay.sph(n, j, c), L.y[2] * IS.dm(L.k, n, c, jre));
+                for (int c = 0; c < 2; ++c) s.put(lay.sph(n, j, c), L.y[2] * IS.dm(L.k, n, c, P.jsl));
         } else if (L.core_below) {
           dz a3 = L.y[2];
           for (int n = jre - 1; n >= 1; --n) {

@@ -14,6 +14,7 @@ struct FKStatic {
   double rearth, ric, roc, rhs, ruc, eps, sigma, df, dwn;
   int kopt;   // attempt the step-size control aims at (opttry, parametersBulirschStep.f90:28-48: 6)
   int dsv;    // 1: DSV spectra with radial derivatives of a source at node jre (no reciprocity)
+  int jsl, jsr;   // node range of the minors (spheroidalMinors.f90:72-585): jre..jre, or a set of source nodes
   double rb[MAXLAY + 1];
   double drk[MAXLAY + 1];
   int iflso[MAXLAY + 1];

@@ -9,7 +9,6 @@ or a GPU every call raises.
 from __future__ import annotations
 
 import ctypes
-import dataclasses
 import os
 from typing import Optional
 
@@ -68,6 +67,9 @@ def lib() -> ctypes.CDLL:
         L.gem_fk_run_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
         L.gem_fk_run_dsv.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
         L.gem_fk_run_dsv_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
+        L.gem_fk_run_aski.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
+        L.gem_fk_run_aski_device.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp,
+                                             vp]
         L.gem_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
         L.gem_fk_graph_build.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
         L.gem_fk_graph_launch.argtypes = [vp, vp]
@@ -280,19 +282,38 @@ class GeminiFK:
     def aski_spectra(self, params: FKParams, jsnod, jre: int, jf_first: int, jf_last: int, f32: bool = True,
                      f64: bool = True, raise_on_failure: bool = True):
         """The FK spectra of computeGreenFKSpectraForASKI for frequencies
-        jf_first..jf_last: one DSV run per source node in jsnod (type
-        params.source_type), then one for a force at the receiver node jre,
-        which must be among the source nodes (:196-209).  Returns a list of
-        (gfre, gfim, gf64, status), the force last, as the program's files
-        <DSVBASENAME>.<type>.<js> hold them."""
-        jsnod = [int(j) for j in jsnod]
-        if jre not in jsnod:
+        jf_first..jf_last in one call (gem_fk_run_aski): the minors once over the
+        source-node range, then the DSV spectra of each source node in jsnod
+        (type params.source_type) and of a force at the receiver node jre, which
+        must be among the source nodes (:196-209).  Returns a list of (gfre,
+        gfim, gf64, status) shaped (nnod, nsp, nkf), the force last, as the
+        program's files <DSVBASENAME>.<type>.<js> hold them."""
+        jsnod = np.ascontiguousarray([int(j) for j in jsnod], np.int32)
+        if jre not in list(jsnod):
             raise GeminiError("receiver node must also be a source node")
         if jf_first < aski_nf1(params):
             raise GeminiError("frequency index %d below the first ASKI frequency %d" % (jf_first, aski_nf1(params)))
-        force = dataclasses.replace(params, source_type="FORCE")
-        out = [self.run_dsv(params, js, jf_first, jf_last, f32, f64, raise_on_failure) for js in jsnod]
-        out.append(self.run_dsv(force, jre, jf_first, jf_last, f32, f64, raise_on_failure))
+        grid = frequency_grid(params, self.model.rearth)
+        nkf = int(grid.nwn[jf_first - 1: jf_last].sum())
+        nnod = self.nodes.nnod
+        nsp_m, nsp_f = nsp_dsv(params.source_type), nsp_dsv("FORCE")
+        ntot = nnod * nkf * (len(jsnod) * nsp_m + nsp_f)
+        gre = np.zeros(ntot, np.float32) if f32 else None
+        gim = np.zeros(ntot, np.float32) if f32 else None
+        g64 = np.zeros(ntot, np.complex128) if f64 else None
+        status = np.zeros(nkf, np.int32)
+        pc = fk_params_c(params, jre)
+        rc = lib().gem_fk_run_aski(self._h, ctypes.byref(pc), len(jsnod), _ptr(jsnod), jf_first, jf_last, _ptr(gre),
+                                   _ptr(gim), _ptr(g64), _ptr(status))
+        if rc >= 2 and (raise_on_failure or not np.any(status)):
+            raise GeminiError(lib().gem_last_error(self._h).decode())
+        out, off = [], 0
+        for b in range(len(jsnod) + 1):
+            nsp = nsp_f if b == len(jsnod) else nsp_m
+            n = nnod * nsp * nkf
+            blk = [None if a is None else a[off:off + n].reshape(nnod, nsp, nkf) for a in (gre, gim, g64)]
+            out.append((blk[0], blk[1], blk[2], status))
+            off += n
         return out
 
     def run_device(self, params: FKParams, jre: int, jf_first: int, jf_last: int, gfre=None, gfim=None,

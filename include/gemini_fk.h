@@ -146,6 +146,24 @@ int gem_fk_run_dsv(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_la
 int gem_fk_run_dsv_device(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, float* d_gfre,
                           float* d_gfim, double* d_gf64, int32_t* d_status, void* stream);
 
+/* All FK spectra of computeGreenFKSpectraForASKI for frequencies
+ * jf_first..jf_last in one call (the wavenumber loop :439-560 for the whole
+ * slab): minors once over the node range min(jsnod)..max(jsnod)
+ * (toroidalMinors.f90:71-268, spheroidalMinors.f90:72-585, as the program
+ * calls them at :444-447), then for each source node jsnod[0..nsnod-1] (type
+ * p->istyp) and for a force at the receiver node p->jre, which must be among
+ * jsnod (:206-209), the DSV spectra of gem_fk_run_dsv.  The outputs hold
+ * nsnod + 1 blocks, block b at offset b * nkf * gem_fk_aski_nsp(p->istyp) *
+ * nnod (the force block last, gem_fk_aski_nsp(0) spectra per node), each in
+ * the (nkf, nsp, nnod) layout of the program's file <DSVBASENAME>.<type>.<b+1>.
+ * Every node must be solid. */
+int gem_fk_aski_nsp(int istyp);
+int gem_fk_run_aski(gem_ctx* ctx, const gem_fk_params* p, int nsnod, const int* jsnod, int jf_first, int jf_last,
+                    float* gfre, float* gfim, double* gf64, int32_t* status);
+int gem_fk_run_aski_device(gem_ctx* ctx, const gem_fk_params* p, int nsnod, const int* jsnod, int jf_first,
+                           int jf_last, float* d_gfre, float* d_gfim, double* d_gf64, int32_t* d_status,
+                           void* stream);
+
 /* CUDA-graph form of gem_fk_run_device (no counterpart in the reference).
  * gem_fk_graph_build does the host-side preparation of the slab once (item and
  * queue tables, buffers) and captures its device work (zeroing, model

@@ -1,12 +1,12 @@
 """GPU parity of the DSV spectra with radial derivatives (the FK spectra of
 computeGreenFKSpectraForASKI.f90) against the CPU oracle, through the C ABI
-(gem_fk_run_dsv).
+(gem_fk_run_dsv per source node, gem_fk_run_aski for a set of them).
 
 Tolerances as for the synthetics FK spectra: the FP64 build agrees with the
 oracle to 1e-10 relative to the largest value of the compared spectra, the
-fast build to 1e-8.  The GPU runs the minors once per source node, the
-reference once over the node range; the two agree to round-off (the oracle's
-range run is compared too)."""
+fast build to 1e-8.  gem_fk_run_dsv integrates the minors for one source
+node, gem_fk_run_aski once over the node range as the reference does; the two
+agree to round-off."""
 import dataclasses
 
 import numpy as np
@@ -65,8 +65,9 @@ def test_dsv_moment_and_force_match_oracle(aski, src):
 
 
 def test_aski_spectra_match_the_reference_node_range_run(aski):
-    """aski_spectra (one run per source node plus the force at the receiver)
-    against the oracle's single minors integration over the node range."""
+    """aski_spectra (one set run: minors over the node range, then every source
+    node and the force at the receiver) against the oracle's restatement of
+    the program's loop."""
     w, m, ex, jre, g, fk, o = aski
     srcs = [1, 5, 8, jre]
     jf = 40
@@ -78,6 +79,23 @@ def test_aski_spectra_match_the_reference_node_range_run(aski):
         assert _rel(a, b) <= RTOL
 
 
+@pytest.mark.parametrize("source_type", ["MOMENT", "FORCE"])
+def test_aski_set_run_equals_per_node_runs(aski, source_type):
+    """One set run (minors once over the node range 1..11) against one
+    gem_fk_run_dsv per source node: equal to round-off (the minors' final
+    normalisation differs between the two ranges)."""
+    w, m, ex, jre, g, fk, o = aski
+    p = dataclasses.replace(w.params, source_type=source_type)
+    srcs = [1, 3, 6, 9, jre]
+    res = fk.aski_spectra(p, srcs, jre, JF1, JF2, f32=False)
+    force = dataclasses.replace(w.params, source_type="FORCE")
+    for (_, _, a, sa), (s, q) in zip(res, [(s, p) for s in srcs] + [(jre, force)]):
+        assert np.all(sa == 0)
+        _, _, b, sb = fk.run_dsv(q, s, JF1, JF2, f32=False)
+        assert a.shape == b.shape
+        assert _rel(a, b) <= 1e-12, s
+
+
 def test_dsv_fast_backend(aski):
     from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST
     w, m, ex, jre, g, fk, o = aski
@@ -85,6 +103,10 @@ def test_dsv_fast_backend(aski):
     for src in (1, jre):
         _, _, a, sa = fast.run_dsv(w.params, src, JF1, JF2, f32=False)
         _, _, b, sb = fk.run_dsv(w.params, src, JF1, JF2, f32=False)
+        assert np.all(sa == 0) and np.all(sb == 0)
+        assert _rel(a, b) <= RTOL_FAST
+    for (_, _, a, sa), (_, _, b, sb) in zip(fast.aski_spectra(w.params, [1, 6, jre], jre, JF1, JF2, f32=False),
+                                            fk.aski_spectra(w.params, [1, 6, jre], jre, JF1, JF2, f32=False)):
         assert np.all(sa == 0) and np.all(sb == 0)
         assert _rel(a, b) <= RTOL_FAST
 
@@ -96,6 +118,7 @@ def test_synthetics_spectra_unchanged_after_a_dsv_run(aski):
     jf = 20
     n = int(g.nwn[jf - 1])
     fk.run_dsv(w.params, 5, jf, jf)
+    fk.aski_spectra(w.params, [2, 7, jre], jre, jf, jf)
     _, _, got, st = fk.run(w.params, jre, jf, jf, f32=False)
     ref, sto, _ = o.fk_frequency(M.fk_params_c(w.params, jre), jf, n, M.nsp_for(w.params))
     assert np.all(st == 0) and got.shape == ref.shape
