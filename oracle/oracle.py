@@ -56,6 +56,10 @@ def lib():
                                            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.oracle_legendre.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
+        L.oracle_coupling.argtypes = ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_double] * 3 +
+                                      [ctypes.c_void_p] * 3 + [ctypes.c_double, ctypes.c_int] + [ctypes.c_double] * 5 +
+                                      [ctypes.c_int] + [ctypes.c_void_p] * 3 + [ctypes.c_int] + [ctypes.c_void_p] * 3)
         L.oracle_fft.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_wavenumber_integrals.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
@@ -370,3 +374,33 @@ def synthetics_opts(source_type, global_, nf1, nf2, nwn, nwnmax, df, sigma, dwn,
     if rc:
         raise RuntimeError("oracle_synthetics_opts failed (%d)" % rc)
     return out
+
+
+def coupling(nf1, nf2, nwn, nwnmax, gr, gi, df, sigma, re, zelcon, mt, filspecs, tred, nsamp, dt, thetas, phis,
+             thetac, phic, delta, xi, nrm, spectra=False, debug=False):
+    """SPECFEM-coupling synthetics of a moment source at boundary points
+    (computeSyntheticsForSpecfemCoupling.f90:677-793).  gr/gi: float32 DSV
+    spectra with derivatives of the points' node, shape (nsp >= 20, nkfmax);
+    zelcon: complex [nf2, 7] elastic constants of the node per frequency.
+    Returns (spectra complex [npts, 6, nf2] or None, traces float32 [npts, 6,
+    nsamp] or None, debug complex [npts, nf2, 4, 3] or None)."""
+    gr = np.ascontiguousarray(gr, np.float32); gi = np.ascontiguousarray(gi, np.float32)
+    nsp, nkfmax = gr.shape
+    nwn = np.ascontiguousarray(nwn, np.int32)
+    zel = np.ascontiguousarray(zelcon, np.complex128).reshape(-1)
+    mt = np.ascontiguousarray(mt, np.float64); fs = np.ascontiguousarray(filspecs, np.float64)
+    delta = np.ascontiguousarray(delta, np.float64); xi = np.ascontiguousarray(xi, np.float64)
+    nrm = np.ascontiguousarray(nrm, np.float64).reshape(-1)
+    npts = len(delta)
+    spec = np.zeros(npts * 6 * nf2, np.complex128) if spectra else None
+    tr = None if spectra else np.zeros(npts * 6 * nsamp, np.float32)
+    dbg = np.zeros(npts * nf2 * 12, np.complex128) if debug else None
+    rc = lib().oracle_coupling(nf1, nf2, _p(nwn), nwnmax, nkfmax, nsp, _p(gr), _p(gi), df, sigma, re, _p(zel),
+                               _p(mt), _p(fs), tred, nsamp, dt, thetas, phis, thetac, phic, npts, _p(delta), _p(xi),
+                               _p(nrm), 1 if spectra else 0, _p(spec), _p(tr), _p(dbg))
+    if rc:
+        raise RuntimeError("oracle_coupling: level %d" % rc)
+    return (None if spec is None else spec.reshape(npts, 6, nf2),
+            None if tr is None else tr.reshape(npts, 6, nsamp),
+            None if dbg is None else dbg.reshape(npts, nf2, 4, 3))
+

@@ -689,4 +689,237 @@ int oracle_synthetics_bessel(int nf1, int nf2, const int* nwn, int nwnmax, doubl
                          traces);
 }
 
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+//  SPECFEM coupling: displacement and traction at boundary points
+//  (computeSyntheticsForSpecfemCoupling.f90:677-793), moment sources, from the
+//  DSV spectra with radial derivatives (nsp = 20: U, V, dU/dr, dV/dr x 4 jumps,
+//  W, dW/dr x 2 jumps, computeGreenFKSpectraForASKI.f90:516-541).
+// ---------------------------------------------------------------------------
+namespace {
+
+// the 42 moment sums with derivatives (harmonicDegreeSums.f90:186-351, index map
+// :34-45); kind: 0 plm, 1 dpdt, 2 pdst, 3 d2pdt2, 4 dtpdst
+const SumDef DSUM[42] = {
+    {0, 0, 0, 0.0, 1, 1},  {0, 0, 0, 0.0, 1, 2},  {0, 1, 1, 2.0, 1, 3},  {0, 2, 2, 2.0, 1, 4},
+    {1, 0, 1, 0.0, 3, 1},  {1, 0, 1, 0.0, 3, 2},  {1, 1, 1, 2.0, 3, 3},  {1, 2, 2, 2.0, 3, 4},
+    {2, 1, 1, 2.0, 7, 1},  {2, 2, 2, 4.0, 7, 2},  {1, 1, 1, 2.0, 7, 1},  {1, 2, 2, -2.0, 7, 2},
+    {2, 1, 1, 2.0, 3, 3},  {2, 2, 2, -4.0, 3, 4},
+    {0, 0, 0, 0.0, 5, 1},  {0, 0, 0, 0.0, 5, 2},  {0, 1, 1, 2.0, 5, 3},  {0, 2, 2, 2.0, 5, 4},
+    {1, 0, 1, 0.0, 6, 1},  {1, 0, 1, 0.0, 6, 2},  {1, 1, 1, 2.0, 6, 3},  {1, 2, 2, 2.0, 6, 4},
+    {2, 1, 1, 2.0, 9, 1},  {2, 2, 2, 4.0, 9, 2},  {1, 1, 1, 2.0, 9, 1},  {1, 2, 2, -2.0, 9, 2},
+    {2, 1, 1, 2.0, 6, 3},  {2, 2, 2, -4.0, 6, 4},
+    {1, 0, 1, 0.0, 1, 1},  {1, 0, 1, 0.0, 1, 2},  {1, 1, 1, 2.0, 1, 3},  {1, 2, 2, 2.0, 1, 4},
+    {3, 0, 1, 0.0, 3, 1},  {3, 0, 1, 0.0, 3, 2},  {3, 1, 1, 2.0, 3, 3},  {3, 2, 2, 2.0, 3, 4},
+    {4, 1, 1, 2.0, 7, 1},  {4, 2, 2, 4.0, 7, 2},  {3, 1, 1, 2.0, 7, 1},  {3, 2, 2, -2.0, 7, 2},
+    {4, 1, 1, 2.0, 3, 3},  {4, 2, 2, -4.0, 3, 4}};
+
+// column of (component, jump) in the DSV spectra with derivatives
+int dsvColumn(int comp, int jump) {
+  switch (comp) {
+    case 1: return jump - 1;        // U
+    case 3: return 4 + jump - 1;    // V
+    case 5: return 8 + jump - 1;    // dU/dr
+    case 6: return 12 + jump - 1;   // dV/dr
+    case 7: return 16 + jump - 1;   // W
+    default: return 18 + jump - 1;  // dW/dr
+  }
+}
+
+zc derivSum(int kint, const float* gr, const float* gi, int nwn, const Legendre& alf,
+            const std::vector<double>& tap) {
+  const SumDef& s = DSUM[kint - 1];
+  const std::vector<double>& T = s.kind == 0 ? alf.plm[s.m] : s.kind == 1 ? alf.dpdt[s.m] : s.kind == 2 ?
+                                 alf.pdst[s.m] : s.kind == 3 ? alf.d2pdt2[s.m] : alf.dtpdst[s.m];
+  const double fourpi = 4.0 * PI_F;
+  zc z = Z(0.0);
+  for (int l = s.l0; l <= nwn - 1; ++l) {
+    zc g = Z((double)gr[l], (double)gi[l]);
+    zc t;
+    if (s.fnum == 0.0) t = T[l] * g;
+    else t = ((T[l] * s.fnum) / (double)(float)(l * (l + 1))) * g;
+    t = ((t * (2.0 * (double)l + 1.0)) / fourpi) * tap[l];
+    z = z + t;
+  }
+  return z;
+}
+
+// rotations of complex vectors and tensors (axesRotation.f90:143-152,199-212,321-426,473-477)
+void vecLCfromLS(double d, double x, const zc* u, zc* o) {
+  double cd = std::cos(d), sd = std::sin(d), cx = std::cos(x), sx = std::sin(x);
+  o[0] = ((sd * cx) * u[0] + (cd * cx) * u[1]) - sx * u[2];
+  o[1] = ((sd * sx) * u[0] + (cd * sx) * u[1]) + cx * u[2];
+  o[2] = cd * u[0] - sd * u[1];
+}
+void vecGCfromLC(double t, double p, const zc* u, zc* o) {
+  double ct = std::cos(t), st = std::sin(t), cp = std::cos(p), sp = std::sin(p);
+  o[0] = ((ct * cp) * u[0] - sp * u[1]) + (st * cp) * u[2];
+  o[1] = ((ct * sp) * u[0] + cp * u[1]) + (st * sp) * u[2];
+  o[2] = (-st) * u[0] + ct * u[2];
+}
+void vecLCfromGC(double t, double p, const zc* u, zc* o) {
+  double ct = std::cos(t), st = std::sin(t), cp = std::cos(p), sp = std::sin(p);
+  o[0] = ((ct * cp) * u[0] + (ct * sp) * u[1]) - st * u[2];
+  o[1] = (-sp) * u[0] + cp * u[1];
+  o[2] = ((st * cp) * u[0] + (st * sp) * u[1]) + ct * u[2];
+}
+// tensor rotation T' = R T R^T with the row rule v -> R v of a vector rotation
+typedef void (*VecRot)(double, double, const zc*, zc*);
+void tenRot(VecRot f, double a, double b, const zc t[3][3], zc o[3][3]) {
+  zc tp[3][3];
+  for (int j = 0; j < 3; ++j) {   // tp(:, j) = R t(:, j): rows combined column by column
+    zc col[3] = {t[0][j], t[1][j], t[2][j]}, r[3];
+    f(a, b, col, r);
+    for (int i = 0; i < 3; ++i) tp[i][j] = r[i];
+  }
+  for (int i = 0; i < 3; ++i) {   // o(i, :) = R tp(i, :)
+    zc row[3] = {tp[i][0], tp[i][1], tp[i][2]}, r[3];
+    f(a, b, row, r);
+    for (int j = 0; j < 3; ++j) o[i][j] = r[j];
+  }
+}
+void vecLSrot(double d, double x, const zc* u, zc* o) { vecLCfromLS(d, x, u, o); }
+
+}  // namespace
+
+extern "C" {
+// Per boundary point p (epicentral distance delta[p], azimuth xi[p] from south over
+// east, outward normal nrm[3p..3p+2] in box coordinates) at radius re of the DSV node:
+// the 42 degree sums, displacement and its derivatives, strain and stress
+// (singleFrequencyDisplacement.f90:108-278 with zelcon of the node per frequency,
+// zelcon[(jf-1)*14 + 2c + {0,1}]), rotation to the box (computeTension :677-705),
+// traction = stress * n.  spectra != 0 (COMPUTE_SPECTRA): spec[((p*6 + c)*nf2 + jf-1)*2]
+// holds displacement x,y,z then traction x,y,z, unfiltered.  Otherwise velocity and
+// traction through the event filter and the time shift of tred, then the inverse FFT:
+// traces[(p*6 + c)*nsamp + i].  dbg (nullable): the LS displacement, d/dr, (1/r)d/dtheta
+// and (1/(r sin)) d/dphi at dbg[((p*nf2 + jf-1)*12 + 3q + c)*2].
+int oracle_coupling(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp, const float* gr,
+                    const float* gi, double df, double sigma, double re, const double* zelcon, const double* mt,
+                    const double* filspecs, double tred, int nsamp, double dt, double thetas, double phis,
+                    double thetac, double phic, int npts, const double* delta, const double* xi,
+                    const double* nrm, int spectra, double* spec, float* traces, double* dbg) {
+  if (nsp < 20) return 2;
+  std::vector<zc> evf;
+  eventFilter((int)std::lround(filspecs[0]), filspecs[1], (int)std::lround(filspecs[2]), filspecs[3], nf1, nf2, df,
+              sigma, evf);
+  const zc ci = Z(0.0, 1.0);
+  const double gam = 0.5 * PI_F;
+  for (int ip = 0; ip < npts; ++ip) {
+    Legendre alf;
+    computeLegendre(nwnmax - 1, delta[ip], alf);
+    const double phi = xi[ip], dl = delta[ip];
+    const double sphi = std::sin(phi), cphi = std::cos(phi);
+    const double s2phi = std::sin(2.0 * phi), c2phi = std::cos(2.0 * phi);
+    std::vector<zc> out[6];
+    for (int c = 0; c < 6; ++c) out[c].assign(nf2 + 1, Z(0.0));
+    int nwe = 0;
+    for (int jf = nf1; jf <= nf2; ++jf) {
+      const int nwa = nwe + 1;
+      nwe += nwn[jf - 1];
+      std::vector<double> tap;
+      taper(nwn[jf - 1] - 1, 0.2, tap);
+      zc w[43];
+      for (int k = 1; k <= 42; ++k) {
+        const int col = dsvColumn(DSUM[k - 1].comp, DSUM[k - 1].jump);
+        w[k] = derivSum(k, gr + (size_t)col * nkfmax + (nwa - 1), gi + (size_t)col * nkfmax + (nwa - 1),
+                        nwn[jf - 1], alf, tap);
+      }
+      const double* m = mt;
+      const double t1 = m[3] * cphi + m[4] * sphi, t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
+      const double t3 = m[4] * cphi - m[3] * sphi, t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
+      zc u[3], ur[3], ut[3], uf[3];
+      // momentSingleFrequencyDisplacement (:108-125)
+      u[0] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
+      u[1] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
+      u[2] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+      // momentRadDerivSingleFrequencyDisplacement (:130-148)
+      ur[0] = w[15] * m[0] + w[16] * (m[1] + m[2]) + w[17] * t1 + w[18] * t2;
+      ur[1] = w[19] * m[0] + w[20] * (m[1] + m[2]) + (w[21] + w[23]) * t1 + (w[22] + w[24]) * t2;
+      ur[2] = (w[25] + w[27]) * t3 + (w[26] + w[28]) * t4;
+      // momentThetaDerivSingleFrequencyDisplacement (:155-173)
+      ut[0] = w[29] * m[0] + w[30] * (m[1] + m[2]) + w[31] * t1 + w[32] * t2;
+      ut[1] = w[33] * m[0] + w[34] * (m[1] + m[2]) + (w[35] + w[37]) * t1 + (w[36] + w[38]) * t2;
+      ut[2] = (w[39] + w[41]) * t3 + (w[40] + w[42]) * t4;
+      for (int c = 0; c < 3; ++c) ut[c] = ut[c] / re;
+      // momentPhiDerivSingleFrequencyDisplacement (:181-199)
+      const double p1 = (-m[3]) * sphi + m[4] * cphi;
+      const double p2 = (-2.0) * (m[2] - m[1]) * s2phi - 4.0 * m[5] * c2phi;
+      const double p3 = (-m[4]) * sphi - m[3] * cphi;
+      const double p4 = 2.0 * (m[2] - m[1]) * c2phi - 4.0 * m[5] * s2phi;
+      const double rst = re * std::sin(dl);
+      uf[0] = w[3] * p1 + w[4] * p2;
+      uf[1] = (w[7] + w[9]) * p1 + (w[8] + w[10]) * p2;
+      uf[2] = (w[11] + w[13]) * p3 + (w[12] + w[14]) * p4;
+      for (int c = 0; c < 3; ++c) uf[c] = uf[c] / rst;
+      if (dbg) {
+        const zc* q[4] = {u, ur, ut, uf};
+        for (int a = 0; a < 4; ++a)
+          for (int c = 0; c < 3; ++c) {
+            size_t o = ((((size_t)ip * nf2 + (jf - 1)) * 12) + 3 * a + c) * 2;
+            dbg[o] = q[a][c].re; dbg[o + 1] = q[a][c].im;
+          }
+      }
+      // sphericalStrainSingleFrequencyDisplacement (:229-244)
+      const double rtd = re * std::tan(dl);
+      zc e[3][3];
+      e[0][0] = ur[0];
+      e[1][1] = ut[1] + u[0] / re;
+      e[2][2] = (uf[2] + u[0] / re) + u[1] / rtd;
+      e[0][1] = 0.5 * ((ut[0] + ur[1]) - u[1] / re);
+      e[0][2] = 0.5 * ((uf[0] + ur[2]) - u[2] / re);
+      e[1][2] = 0.5 * ((uf[1] + ut[2]) - u[2] / rtd);
+      e[2][1] = e[1][2]; e[2][0] = e[0][2]; e[1][0] = e[0][1];
+      // sphericalStressSingleFrequencyDisplacement (:250-262)
+      zc el[5];
+      for (int c = 0; c < 5; ++c) el[c] = Z(zelcon[((size_t)(jf - 1) * 7 + c) * 2], zelcon[((size_t)(jf - 1) * 7 + c) * 2 + 1]);
+      zc sg[3][3];
+      sg[0][0] = el[1] * e[0][0] + el[2] * (e[1][1] + e[2][2]);
+      sg[1][1] = (el[2] * e[0][0] + el[0] * (e[1][1] + e[2][2])) - (2.0 * el[4]) * e[2][2];
+      sg[2][2] = (el[2] * e[0][0] + el[0] * (e[1][1] + e[2][2])) - (2.0 * el[4]) * e[1][1];
+      sg[0][1] = (2.0 * el[3]) * e[0][1];
+      sg[0][2] = (2.0 * el[3]) * e[0][2];
+      sg[1][2] = (2.0 * el[4]) * e[1][2];
+      sg[1][0] = sg[0][1]; sg[2][0] = sg[0][2]; sg[2][1] = sg[1][2];
+      // computeTension (:677-705): epicentral LS -> LC -> global -> box LC -> box RC
+      zc a[3], b[3];
+      vecLCfromLS(dl, phi, u, a);
+      vecGCfromLC(thetas, phis, a, b);
+      vecLCfromGC(thetac, phic, b, a);
+      vecLCfromGC(0.0, gam, a, b);
+      zc ta[3][3], tb[3][3];
+      tenRot(vecLSrot, dl, phi, sg, ta);
+      tenRot(vecGCfromLC, thetas, phis, ta, tb);
+      tenRot(vecLCfromGC, thetac, phic, tb, ta);
+      tenRot(vecLCfromGC, 0.0, gam, ta, tb);
+      const double* n = nrm + 3 * ip;
+      zc tr[3];
+      for (int i = 0; i < 3; ++i) tr[i] = ((Z(0.0) + tb[i][0] * n[0]) + tb[i][1] * n[1]) + tb[i][2] * n[2];
+      if (!spectra) {
+        const zc zom = Z(TWO_PI_F * (double)(jf - 1) * df, -sigma);
+        const zc tsf = zexp(((ci * TWO_PI_F) * (double)(jf - 1)) * df * tred) * std::exp(sigma * tred);
+        for (int c = 0; c < 3; ++c) {
+          b[c] = (((b[c] * evf[jf]) * ci) * zom) * tsf;
+          tr[c] = (tr[c] * evf[jf]) * tsf;
+        }
+      }
+      for (int c = 0; c < 3; ++c) { out[c][jf] = b[c]; out[3 + c][jf] = tr[c]; }
+    }
+    for (int c = 0; c < 6; ++c) {
+      if (spectra) {
+        if (spec)
+          for (int jf = 1; jf <= nf2; ++jf) {
+            size_t o = (((size_t)ip * 6 + c) * nf2 + (jf - 1)) * 2;
+            spec[o] = out[c][jf].re; spec[o + 1] = out[c][jf].im;
+          }
+      } else if (traces) {
+        int rc = freqTime(nf1, nf2, df, sigma, out[c], nsamp, dt, traces + ((size_t)ip * 6 + c) * nsamp);
+        if (rc) return rc;
+      }
+    }
+  }
+  return 0;
+}
+
 }  // extern "C"
