@@ -67,8 +67,8 @@ struct gem_ctx {
   int last_grid = 0;
   gem_stats stats{};
   // device buffers of the other entry points, grown on demand
-  void* d_aux[12] = {};
-  size_t aux_cap[12] = {};
+  void* d_aux[16] = {};
+  size_t aux_cap[16] = {};
   int kopt = 6;   // order target of the step-size control (gem_order_target; fast backend)
   int dsv = 0;    // set by gem_fk_run_dsv* for the length of one run: DSV spectra with derivatives
   int jsl = 0, jsr = 0;   // set by gem_fk_run_aski* for one run: node range of the minors (0: the receiver)
@@ -198,7 +198,7 @@ void gem_note_synth_ms(gem_ctx* ctx, float ms) { if (ctx) ctx->stats.synth_ms = 
 int gem_ctx_device(const gem_ctx* ctx) { return ctx->device; }
 int gem_ctx_backend(const gem_ctx* ctx) { return ctx->backend; }
 void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes) {
-  if (slot < 0 || slot >= 12) return nullptr;
+  if (slot < 0 || slot >= 16) return nullptr;
   if (ctx->d_aux[slot] && ctx->aux_cap[slot] >= bytes) return ctx->d_aux[slot];
   cudaFree(ctx->d_aux[slot]);
   ctx->d_aux[slot] = nullptr; ctx->aux_cap[slot] = 0;

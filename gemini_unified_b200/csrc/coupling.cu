@@ -1,0 +1,422 @@
+// Synthetics for SPECFEM coupling on the GPU: displacement (as velocity) and
+// traction at the boundary points of a SPECFEM box, from the DSV spectra with
+// radial derivatives of the points' node (computeSyntheticsForSpecfemCoupling.f90:
+// computeSynthetics :714-793, computeTension :677-705; moment sources).
+//
+//   cpl_legendre_kernel  P_l^m, dP/dtheta, P/sin, d2P/dtheta2, d/dtheta(P/sin)
+//                        for m <= 2 at every point (legendreFunctions.f90:48-157)
+//   cpl_sums_kernel      the 42 degree sums of each (point, frequency)
+//                        (harmonicDegreeSums.f90:186-369, index map :34-45)
+//   cpl_point_kernel     displacement and its derivatives, strain, stress, the
+//                        rotation to the box frame, traction = stress * n,
+//                        event filter, i omega and time shift
+//                        (singleFrequencyDisplacement.f90:108-262)
+//   gem_ifft_run_device  the six time series of every point
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "synth.h"
+
+namespace gem {
+namespace {
+
+constexpr int CPL_NSUM = 42;
+constexpr int CPL_NKIND = 13;   // plm m0-2, dpdt m0-2, pdst m1-2, d2pdt2 m0-2, dtpdst m1-2
+
+// per sum: table kind, first degree, factor numerator over l(l+1) (0: none),
+// column of its (component, jump) in the DSV spectra U, V, dU/dr, dV/dr (x 4
+// jumps), W, dW/dr (x 2 jumps)
+struct CplSum { int kind, l0; double fac; int col; };
+__constant__ CplSum c_cpl[CPL_NSUM] = {
+    {0, 0, 0.0, 0}, {0, 0, 0.0, 1}, {1, 1, 2.0, 2}, {2, 2, 2.0, 3},
+    {3, 1, 0.0, 4}, {3, 1, 0.0, 5}, {4, 1, 2.0, 6}, {5, 2, 2.0, 7},
+    {6, 1, 2.0, 16}, {7, 2, 4.0, 17}, {4, 1, 2.0, 16}, {5, 2, -2.0, 17},
+    {6, 1, 2.0, 6}, {7, 2, -4.0, 7}, {0, 0, 0.0, 8}, {0, 0, 0.0, 9},
+    {1, 1, 2.0, 10}, {2, 2, 2.0, 11}, {3, 1, 0.0, 12}, {3, 1, 0.0, 13},
+    {4, 1, 2.0, 14}, {5, 2, 2.0, 15}, {6, 1, 2.0, 18}, {7, 2, 4.0, 19},
+    {4, 1, 2.0, 18}, {5, 2, -2.0, 19}, {6, 1, 2.0, 14}, {7, 2, -4.0, 15},
+    {3, 1, 0.0, 0}, {3, 1, 0.0, 1}, {4, 1, 2.0, 2}, {5, 2, 2.0, 3},
+    {8, 1, 0.0, 4}, {8, 1, 0.0, 5}, {9, 1, 2.0, 6}, {10, 2, 2.0, 7},
+    {11, 1, 2.0, 16}, {12, 2, 4.0, 17}, {9, 1, 2.0, 16}, {10, 2, -2.0, 17},
+    {11, 1, 2.0, 6}, {12, 2, -4.0, 7}};
+
+struct CplDev {
+  int nf1, nf2, npts, lcap, spectra;
+  long long nkf;
+  double df, sigma, re, tred;
+  double thetas, phis, thetac, phic;
+  double mt[6];
+  const int* nwn;       // [nf2]
+  const int* koff;      // [nf] first wavenumber index of each frequency in the spectra
+  const double* delta;  // [npts]
+  const double* xi;     // [npts]
+  const double* nrm;    // [npts * 3]
+  const double2* evf;   // [nf2 + 1]
+  const double2* zel;   // [nf2 * 7]
+};
+
+// tab[(pt * 13 + kind) * lcap + l]; one thread per (point, m)
+__global__ void cpl_legendre_kernel(int npts, int lmax, int lcap, const double* __restrict__ delta, double* tab) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= npts * 3) return;
+  const int pt = idx % npts, m = idx / npts;
+  const double ct = cos(delta[pt]), st = sin(delta[pt]);
+  const bool atpoles = !(st > 0.0);
+  double* base = tab + (long long)pt * CPL_NKIND * lcap;
+  double* Tp = base + (long long)m * lcap;
+  double* Td = base + (long long)(3 + m) * lcap;
+  double* Ts = m >= 1 ? base + (long long)(5 + m) * lcap : nullptr;
+  double* T2 = base + (long long)(8 + m) * lcap;
+  double* Tt = m >= 1 ? base + (long long)(10 + m) * lcap : nullptr;
+  double pmm = 1.0, fact = 1.0;
+  for (int j = 1; j <= m; ++j) { pmm = pmm * fact * st; fact = fact + 2.0; }
+  const double rst = 1.0 / st;
+  const double isct = ct >= 0.0 ? 1.0 : -1.0;
+  double pl2 = 0.0, pl1 = 0.0;
+  for (int l = 0; l <= lmax; ++l) {
+    double p;
+    if (l < m) p = 0.0;
+    else if (l == m) p = pmm;
+    else if (l == m + 1) p = ct * (double)(2 * m + 1) * pmm;
+    else p = (ct * (double)(2 * l - 1) * pl1 - (double)(l + m - 1) * pl2) / (double)(l - m);
+    double dp = 0.0, ps = 0.0, d2 = 0.0, dts = 0.0;
+    const double ll1 = (double)l * (double)(l + 1);
+    if (!atpoles) {
+      if (l == m) dp = (double)m * ct * p * rst;
+      else if (l > m) dp = ((double)l * ct * p - (double)(l + m) * pl1) * rst;
+      if (l >= m) {
+        if (m >= 1) ps = p * rst;
+        d2 = ((-ct) * rst) * dp + ((double)(m * m) * (rst * rst) - ll1) * p;
+        if (m >= 1) dts = rst * (dp - (ct * rst) * p);
+      }
+    } else {
+      const double sl = (l % 2 == 0) ? 1.0 : isct;          // isct^l
+      const double sl1 = (l % 2 == 0) ? isct : 1.0;         // isct^(l+1)
+      const double q = (double)(l + 2) * (double)(l + 1) * (double)l * (double)(l - 1);
+      if (m == 1) dp = 0.5 * ll1 * sl;
+      if (m == 1 && l >= 1) ps = 0.5 * ll1 * sl1;
+      if (m == 0) d2 = 0.5 * ll1 * sl;
+      if (m == 2) d2 = 0.25 * q * sl;
+      if (m == 2 && l >= 1) dts = 0.125 * q * sl1;
+    }
+    if (l < lcap) {
+      Tp[l] = p; Td[l] = dp; T2[l] = d2;
+      if (Ts) Ts[l] = ps;
+      if (Tt) Tt[l] = dts;
+    }
+    pl2 = pl1;
+    pl1 = p;
+  }
+}
+
+// hd[((pt * nf) + slot) * 42 + k]; one block of 8 warps per (frequency, point):
+// the block forms w_l = (2l+1)/(4 pi) taper_l in shared memory, each warp then
+// takes every eighth sum and its lanes every 32nd degree
+constexpr int CPL_SUM_THREADS = 256;
+__global__ void __launch_bounds__(CPL_SUM_THREADS) cpl_sums_kernel(CplDev S, const float* __restrict__ gr,
+                                                                   const float* __restrict__ gi,
+                                                                   const double* __restrict__ tab, double2* hd) {
+  extern __shared__ double wl[];
+  const int pt = blockIdx.x, slot = blockIdx.y;
+  const int jf = S.nf1 + slot, nf = S.nf2 - S.nf1 + 1;
+  const int nwn = S.nwn[jf - 1], lmax = nwn - 1;
+  // cos^2 taper of this frequency (harmonicDegreeSums.f90:356-369), TAPFRAC = 0.2
+  const double tapfrac = 0.2;
+  int jt = (int)floor((double)lmax * (1.0 - tapfrac) + 0.5);
+  jt = jt < lmax ? jt : lmax;
+  jt = jt > 1 ? jt : 1;
+  const double c1 = (double)lmax * tapfrac * 2.0 / PI_F;
+  const double c2 = (1.0 - tapfrac) / tapfrac * 0.5 * PI_F;
+  for (int l = threadIdx.x; l < nwn; l += blockDim.x) {
+    double tap = 1.0;
+    if (l >= jt) { const double c = cos((double)(float)l / c1 - c2); tap = c * c; }
+    wl[l] = (2.0 * (double)l + 1.0) / (4.0 * PI_F) * tap;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double* tp = tab + (long long)pt * CPL_NKIND * S.lcap;
+  const long long g0 = S.koff[slot];
+  for (int k = warp; k < CPL_NSUM; k += CPL_SUM_THREADS / 32) {
+    const CplSum cs = c_cpl[k];
+    const double* T = tp + (long long)cs.kind * S.lcap;
+    const float* gre = gr + (long long)cs.col * S.nkf + g0;
+    const float* gim = gi + (long long)cs.col * S.nkf + g0;
+    double sr = 0.0, si = 0.0;
+    for (int l = cs.l0 + lane; l < nwn; l += 32) {
+      double c = T[l] * wl[l];
+      if (cs.fac != 0.0) c = c * (cs.fac / (double)(float)(l * (l + 1)));
+      sr += c * (double)gre[l];
+      si += c * (double)gim[l];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) hd[((long long)pt * nf + slot) * CPL_NSUM + k] = make_double2(sr, si);
+  }
+}
+
+__device__ __forceinline__ void vec_lc_from_ls(double d, double x, const dz* u, dz* o) {
+  const double cd = cos(d), sd = sin(d), cx = cos(x), sx = sin(x);
+  o[0] = ((sd * cx) * u[0] + (cd * cx) * u[1]) - sx * u[2];
+  o[1] = ((sd * sx) * u[0] + (cd * sx) * u[1]) + cx * u[2];
+  o[2] = cd * u[0] - sd * u[1];
+}
+__device__ __forceinline__ void vec_gc_from_lc(double t, double p, const dz* u, dz* o) {
+  const double ct = cos(t), st = sin(t), cp = cos(p), sp = sin(p);
+  o[0] = ((ct * cp) * u[0] - sp * u[1]) + (st * cp) * u[2];
+  o[1] = ((ct * sp) * u[0] + cp * u[1]) + (st * sp) * u[2];
+  o[2] = (-st) * u[0] + ct * u[2];
+}
+__device__ __forceinline__ void vec_lc_from_gc(double t, double p, const dz* u, dz* o) {
+  const double ct = cos(t), st = sin(t), cp = cos(p), sp = sin(p);
+  o[0] = ((ct * cp) * u[0] + (ct * sp) * u[1]) - st * u[2];
+  o[1] = (-sp) * u[0] + cp * u[1];
+  o[2] = ((st * cp) * u[0] + (st * sp) * u[1]) + ct * u[2];
+}
+// T' = R T R^T: every column, then every row through the vector rule
+// (axesRotation.f90:199-212,377-426,486-560)
+template <int W>
+__device__ __forceinline__ void ten_rot(double a, double b, const dz t[3][3], dz o[3][3]) {
+  auto f = [&](const dz* u, dz* v) {
+    if (W == 0) vec_lc_from_ls(a, b, u, v);
+    else if (W == 1) vec_gc_from_lc(a, b, u, v);
+    else vec_lc_from_gc(a, b, u, v);
+  };
+  dz tp[3][3];
+  for (int j = 0; j < 3; ++j) {
+    dz col[3] = {t[0][j], t[1][j], t[2][j]}, r[3];
+    f(col, r);
+    for (int i = 0; i < 3; ++i) tp[i][j] = r[i];
+  }
+  for (int i = 0; i < 3; ++i) {
+    dz row[3] = {tp[i][0], tp[i][1], tp[i][2]}, r[3];
+    f(row, r);
+    for (int j = 0; j < 3; ++j) o[i][j] = r[j];
+  }
+}
+
+// one thread per (point, frequency): X[(pt * 6 + c) * nf2 + jf - 1], c = displacement
+// (or velocity) x, y, z, traction x, y, z in the box frame (x east, y north)
+__global__ void cpl_point_kernel(CplDev S, const double2* __restrict__ hd, double2* X) {
+  const int nf = S.nf2 - S.nf1 + 1;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)S.npts * nf) return;
+  const int slot = (int)(idx % nf), pt = (int)(idx / nf);
+  const int jf = S.nf1 + slot;
+  dz w[CPL_NSUM + 1];
+  for (int k = 0; k < CPL_NSUM; ++k) {
+    const double2 v = hd[((long long)pt * nf + slot) * CPL_NSUM + k];
+    w[k + 1] = dz{v.x, v.y};
+  }
+  const double* m = S.mt;
+  const double phi = S.xi[pt], dl = S.delta[pt], re = S.re;
+  const double sphi = sin(phi), cphi = cos(phi), s2phi = sin(2.0 * phi), c2phi = cos(2.0 * phi);
+  const double t1 = m[3] * cphi + m[4] * sphi, t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
+  const double t3 = m[4] * cphi - m[3] * sphi, t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
+  dz u[3], ur[3], ut[3], uf[3];
+  u[0] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
+  u[1] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
+  u[2] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+  ur[0] = w[15] * m[0] + w[16] * (m[1] + m[2]) + w[17] * t1 + w[18] * t2;
+  ur[1] = w[19] * m[0] + w[20] * (m[1] + m[2]) + (w[21] + w[23]) * t1 + (w[22] + w[24]) * t2;
+  ur[2] = (w[25] + w[27]) * t3 + (w[26] + w[28]) * t4;
+  ut[0] = w[29] * m[0] + w[30] * (m[1] + m[2]) + w[31] * t1 + w[32] * t2;
+  ut[1] = w[33] * m[0] + w[34] * (m[1] + m[2]) + (w[35] + w[37]) * t1 + (w[36] + w[38]) * t2;
+  ut[2] = (w[39] + w[41]) * t3 + (w[40] + w[42]) * t4;
+  for (int c = 0; c < 3; ++c) ut[c] = ut[c] / re;
+  const double p1 = (-m[3]) * sphi + m[4] * cphi;
+  const double p2 = (-2.0) * (m[2] - m[1]) * s2phi - 4.0 * m[5] * c2phi;
+  const double p3 = (-m[4]) * sphi - m[3] * cphi;
+  const double p4 = 2.0 * (m[2] - m[1]) * c2phi - 4.0 * m[5] * s2phi;
+  const double rst = re * sin(dl);
+  uf[0] = w[3] * p1 + w[4] * p2;
+  uf[1] = (w[7] + w[9]) * p1 + (w[8] + w[10]) * p2;
+  uf[2] = (w[11] + w[13]) * p3 + (w[12] + w[14]) * p4;
+  for (int c = 0; c < 3; ++c) uf[c] = uf[c] / rst;
+  // strain and stress (singleFrequencyDisplacement.f90:229-262)
+  const double rtd = re * tan(dl);
+  dz e[3][3];
+  e[0][0] = ur[0];
+  e[1][1] = ut[1] + u[0] / re;
+  e[2][2] = (uf[2] + u[0] / re) + u[1] / rtd;
+  e[0][1] = 0.5 * ((ut[0] + ur[1]) - u[1] / re);
+  e[0][2] = 0.5 * ((uf[0] + ur[2]) - u[2] / re);
+  e[1][2] = 0.5 * ((uf[1] + ut[2]) - u[2] / rtd);
+  e[2][1] = e[1][2]; e[2][0] = e[0][2]; e[1][0] = e[0][1];
+  dz el[5];
+  for (int c = 0; c < 5; ++c) { const double2 v = S.zel[(long long)(jf - 1) * 7 + c]; el[c] = dz{v.x, v.y}; }
+  dz sg[3][3];
+  sg[0][0] = el[1] * e[0][0] + el[2] * (e[1][1] + e[2][2]);
+  sg[1][1] = (el[2] * e[0][0] + el[0] * (e[1][1] + e[2][2])) - (2.0 * el[4]) * e[2][2];
+  sg[2][2] = (el[2] * e[0][0] + el[0] * (e[1][1] + e[2][2])) - (2.0 * el[4]) * e[1][1];
+  sg[0][1] = (2.0 * el[3]) * e[0][1];
+  sg[0][2] = (2.0 * el[3]) * e[0][2];
+  sg[1][2] = (2.0 * el[4]) * e[1][2];
+  sg[1][0] = sg[0][1]; sg[2][0] = sg[0][2]; sg[2][1] = sg[1][2];
+  // to the box frame (computeTension, :677-705)
+  const double gam = 0.5 * PI_F;
+  dz a[3], b[3];
+  vec_lc_from_ls(dl, phi, u, a);
+  vec_gc_from_lc(S.thetas, S.phis, a, b);
+  vec_lc_from_gc(S.thetac, S.phic, b, a);
+  vec_lc_from_gc(0.0, gam, a, b);
+  dz ta[3][3], tb[3][3];
+  ten_rot<0>(dl, phi, sg, ta);
+  ten_rot<1>(S.thetas, S.phis, ta, tb);
+  ten_rot<2>(S.thetac, S.phic, tb, ta);
+  ten_rot<2>(0.0, gam, ta, tb);
+  const double* n = S.nrm + 3 * pt;
+  dz tr[3];
+  for (int i = 0; i < 3; ++i) tr[i] = ((dz{0.0, 0.0} + tb[i][0] * n[0]) + tb[i][1] * n[1]) + tb[i][2] * n[2];
+  if (!S.spectra) {
+    const dz ci{0.0, 1.0};
+    const dz ef{S.evf[jf].x, S.evf[jf].y};
+    const dz zom{TWO_PI_F * (double)(jf - 1) * S.df, -S.sigma};
+    const dz tsf = zexp_dev(((ci * TWO_PI_F) * (double)(jf - 1)) * S.df * S.tred) * exp(S.sigma * S.tred);
+    for (int c = 0; c < 3; ++c) {
+      b[c] = (((b[c] * ef) * ci) * zom) * tsf;
+      tr[c] = (tr[c] * ef) * tsf;
+    }
+  }
+  for (int c = 0; c < 3; ++c) {
+    X[((long long)pt * 6 + c) * S.nf2 + (jf - 1)] = make_double2(b[c].re, b[c].im);
+    X[((long long)pt * 6 + 3 + c) * S.nf2 + (jf - 1)] = make_double2(tr[c].re, tr[c].im);
+  }
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+}  // namespace gem
+
+using namespace gem;
+
+// SPECFEM-coupling synthetics of a moment source at npts boundary points of one
+// node (the loops of computeSyntheticsForSpecfemCoupling.f90:509-549, 571-590 over
+// computeSynthetics :714-793).  d_gr/d_gi: float32 DSV spectra with radial
+// derivatives of the node, (nkfmax, nsp >= 20).  Host arrays: nwn[nf2], zelcon
+// [nf2 * 7] interleaved complex elastic constants of the node per frequency
+// (getComplexConstantsSelectedExternalRadialNodes), mt[6], delta/xi[npts] (rad),
+// nrm[npts * 3] box-frame normals.  Outputs (device): spectra != 0:
+// d_spec[(p * 6 + c) * nf2 + jf - 1] complex, unfiltered; otherwise
+// d_traces[(p * 6 + c) * nsamp + i], c = velocity x, y, z, traction x, y, z.
+extern "C" int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* p, const int* nwn, const float* d_gr,
+                                       const float* d_gi, const double* zelcon, const double* mt, int npts,
+                                       const double* delta, const double* xi, const double* nrm, double* d_spec,
+                                       float* d_traces, void* stream) {
+  if (!ctx) return GEM_ERROR;
+  if (!p || !nwn || !d_gr || !d_gi || !zelcon || !mt || !delta || !xi || !nrm)
+    return gem_set_error(ctx, "coupling: null argument");
+  if (npts < 1) return gem_set_error(ctx, "coupling: no boundary points");
+  if (p->nf2 - p->nf1 + 1 > 65535) return gem_set_error(ctx, "coupling: more than 65535 frequencies");
+  if (p->nsp < 20) return gem_set_error(ctx, "coupling: the DSV spectra need radial derivatives (nsp >= 20)");
+  if (p->nf1 < 1 || p->nf2 < p->nf1 || p->nwnmax < 1 || !(p->re > 0))
+    return gem_set_error(ctx, "coupling: invalid frequency range, degrees or radius");
+  if (p->spectra ? !d_spec : !d_traces) return gem_set_error(ctx, "coupling: null output");
+  const int nf = p->nf2 - p->nf1 + 1;
+  std::vector<int> koff(nf);
+  long long k = 0;
+  for (int jf = 1; jf < p->nf1; ++jf) k += nwn[jf - 1];
+  for (int s = 0; s < nf; ++s) {
+    const int n = nwn[p->nf1 + s - 1];
+    if (n < 1 || n > p->nwnmax) return gem_set_error(ctx, "coupling: number of degrees outside 1..nwnmax");
+    koff[s] = (int)k;
+    k += n;
+  }
+  if (k > p->nkfmax) return gem_set_error(ctx, "coupling: the wavenumber counts exceed nkfmax");
+  if (cudaSetDevice(gem_ctx_device(ctx)) != cudaSuccess) return gem_set_error(ctx, "coupling: cudaSetDevice failed");
+  cudaStream_t st = (cudaStream_t)stream;
+  // event filter at the synthetics' frequencies (Butterworth band-pass, eventFilter.f90:40-83)
+  gem_synth_params sp{};
+  sp.nf1 = p->nf1; sp.nf2 = p->nf2; sp.df = p->df; sp.sigma = p->sigma;
+  sp.order_highpass = p->order_highpass; sp.fc_highpass = p->fc_highpass;
+  sp.order_lowpass = p->order_lowpass; sp.fc_lowpass = p->fc_lowpass;
+  std::vector<double2> evf;
+  if (p->spectra) evf.assign(p->nf2 + 1, make_double2(0, 0));
+  else event_filter_host(&sp, evf);
+  // workspace: tables, sums, spectra, small inputs
+  const int lcap = p->nwnmax;
+  const size_t b_tab = align256((size_t)npts * CPL_NKIND * lcap * sizeof(double));
+  const size_t b_hd = align256((size_t)npts * nf * CPL_NSUM * sizeof(double2));
+  const size_t b_x = align256((size_t)npts * 6 * p->nf2 * sizeof(double2));
+  const size_t b_in = align256((size_t)nf * sizeof(int)) + align256((size_t)p->nf2 * sizeof(int)) +
+                      3 * align256((size_t)npts * 3 * sizeof(double)) + align256(evf.size() * sizeof(double2)) +
+                      align256((size_t)p->nf2 * 7 * sizeof(double2));
+  char* ws = (char*)gem_ctx_aux(ctx, 12, b_tab + b_hd + b_x + b_in);
+  if (!ws) return GEM_ERROR;
+  double* tab = (double*)ws;
+  double2* hd = (double2*)(ws + b_tab);
+  double2* X = p->spectra ? (double2*)d_spec : (double2*)(ws + b_tab + b_hd);
+  char* q = ws + b_tab + b_hd + b_x;
+  auto take = [&](size_t bytes) { char* r = q; q += align256(bytes); return r; };
+  int* d_koff = (int*)take((size_t)nf * sizeof(int));
+  int* d_nwn = (int*)take((size_t)p->nf2 * sizeof(int));
+  double* d_delta = (double*)take((size_t)npts * 3 * sizeof(double));
+  double* d_xi = (double*)take((size_t)npts * 3 * sizeof(double));
+  double* d_nrm = (double*)take((size_t)npts * 3 * sizeof(double));
+  double2* d_evf = (double2*)take(evf.size() * sizeof(double2));
+  double2* d_zel = (double2*)take((size_t)p->nf2 * 7 * sizeof(double2));
+  if (cudaMemcpyAsync(d_koff, koff.data(), (size_t)nf * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_nwn, nwn, (size_t)p->nf2 * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_delta, delta, (size_t)npts * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_xi, xi, (size_t)npts * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_nrm, nrm, (size_t)npts * 3 * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_evf, evf.data(), evf.size() * sizeof(double2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_zel, zelcon, (size_t)p->nf2 * 7 * sizeof(double2), cudaMemcpyHostToDevice, st) !=
+          cudaSuccess ||
+      cudaMemsetAsync(X, 0, (size_t)npts * 6 * p->nf2 * sizeof(double2), st) != cudaSuccess)
+    return gem_set_error(ctx, "coupling: input copy failed");
+  CplDev S{};
+  S.nf1 = p->nf1; S.nf2 = p->nf2; S.npts = npts; S.lcap = lcap; S.spectra = p->spectra; S.nkf = p->nkfmax;
+  S.df = p->df; S.sigma = p->sigma; S.re = p->re; S.tred = p->tred;
+  S.thetas = p->thetas; S.phis = p->phis; S.thetac = p->thetac; S.phic = p->phic;
+  for (int i = 0; i < 6; ++i) S.mt[i] = mt[i];
+  S.nwn = d_nwn; S.koff = d_koff; S.delta = d_delta; S.xi = d_xi; S.nrm = d_nrm; S.evf = d_evf; S.zel = d_zel;
+  cpl_legendre_kernel<<<(npts * 3 + 127) / 128, 128, 0, st>>>(npts, p->nwnmax - 1, lcap, d_delta, tab);
+  const size_t smem = (size_t)p->nwnmax * sizeof(double);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(cpl_sums_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return gem_set_error(ctx, "coupling: too many degrees for the shared-memory weights");
+  cpl_sums_kernel<<<dim3((unsigned)npts, (unsigned)nf), CPL_SUM_THREADS, smem, st>>>(S, d_gr, d_gi, tab, hd);
+  const long long nthr = (long long)npts * nf;
+  cpl_point_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, st>>>(S, hd, X);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return gem_set_error(ctx, cudaGetErrorString(e));
+  if (p->spectra) return GEM_OK;
+  return gem_ifft_run_device(ctx, p->nf1, p->nf2, p->df, p->sigma, npts * 6, (const double*)X, p->nf2, p->nsamp,
+                             p->dt, d_traces, stream);
+}
+
+// Same with host buffers (blocking): spectra gr/gi (nkfmax, nsp) float32, outputs
+// spec [npts * 6 * nf2] complex or traces [npts * 6 * nsamp] float32.
+extern "C" int gem_coupling_run(gem_ctx* ctx, const gem_coupling_params* p, const int* nwn, const float* gr,
+                                const float* gi, const double* zelcon, const double* mt, int npts,
+                                const double* delta, const double* xi, const double* nrm, double* spec,
+                                float* traces) {
+  if (!ctx) return GEM_ERROR;
+  if (!p || !gr || !gi || npts < 1) return gem_set_error(ctx, "coupling: null argument or no boundary points");
+  if (p->nsp < 1 || p->nkfmax < 1) return gem_set_error(ctx, "coupling: invalid spectra extent");
+  if (p->spectra ? !spec : !traces) return gem_set_error(ctx, "coupling: null output");
+  if (cudaSetDevice(gem_ctx_device(ctx)) != cudaSuccess) return gem_set_error(ctx, "coupling: cudaSetDevice failed");
+  const size_t nin = (size_t)p->nkfmax * p->nsp;
+  const size_t nout = p->spectra ? (size_t)npts * 6 * p->nf2 * 2 * sizeof(double)
+                                 : (size_t)npts * 6 * p->nsamp * sizeof(float);
+  char* buf = (char*)gem_ctx_aux(ctx, 13, 2 * align256(nin * sizeof(float)) + align256(nout));
+  if (!buf) return GEM_ERROR;
+  float* dgr = (float*)buf;
+  float* dgi = (float*)(buf + align256(nin * sizeof(float)));
+  char* dout = buf + 2 * align256(nin * sizeof(float));
+  if (cudaMemcpy(dgr, gr, nin * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(dgi, gi, nin * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    return gem_set_error(ctx, "coupling: copy of the spectra failed");
+  int rc = gem_coupling_run_device(ctx, p, nwn, dgr, dgi, zelcon, mt, npts, delta, xi, nrm,
+                                   p->spectra ? (double*)dout : nullptr, p->spectra ? nullptr : (float*)dout,
+                                   nullptr);
+  if (rc) return rc;
+  if (cudaMemcpy(p->spectra ? (void*)spec : (void*)traces, dout, nout, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return gem_set_error(ctx, "coupling: copy of the results failed");
+  return GEM_OK;
+}

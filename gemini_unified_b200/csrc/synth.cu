@@ -591,6 +591,8 @@ void event_filter(const gem_synth_params* p, std::vector<double2>& h) {
 }  // namespace
 
 namespace gem {
+void event_filter_host(const gem_synth_params* p, std::vector<double2>& h) { event_filter(p, h); }
+
 const char* fft_geometry(int nf1, int nf2, double df, int nsamp, double dt, FftGeometry& g) {
   if (nf1 < 1 || nf2 < nf1 || nsamp < 1 || !(df > 0) || !(dt > 0)) return "ifft: invalid frequency range or sampling";
   if (nf2 > IFFT_MAX_NS / 2 || nsamp > IFFT_MAX_NS) return "ifft: FFT length above 8192 (2*nf2 and nsamp must be <= 8192)";

@@ -1,5 +1,6 @@
 // Launch-level structure of the synthetics kernels (device pointers only).
 #pragma once
+#include <vector>
 #include "../../include/gemini_fk.h"
 #include "gem_device.cuh"
 
@@ -62,6 +63,9 @@ inline bool ifft_fast_supported(int ns) { return ns >= 512 && ns <= IFFT_MAX_NS;
 // the recurrence's division replaced by a reciprocal table; lmax up to 25,599
 bool legendre_fast_supported(int lmax);
 cudaError_t legendre_fast_launch(int nsta, int lmax, int lcap, const double* theta, double* tab, cudaStream_t st);
+
+// event filter of the synthetics (Butterworth band-pass at f - i sigma/2pi), h[jf] for jf = nf1..nf2
+void event_filter_host(const gem_synth_params* p, std::vector<double2>& h);
 
 // sliced-integer tensor-core degree sums (sums_tc.cu): workspace size and run;
 // nwn: host copy of the wavenumber counts per frequency (1-based frequency index)

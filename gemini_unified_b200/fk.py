@@ -68,6 +68,8 @@ def lib() -> ctypes.CDLL:
         L.gem_fk_run_dsv.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
         L.gem_fk_run_dsv_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
         L.gem_fk_run_aski.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
+        L.gem_coupling_run.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, vp, vp]
+        L.gem_coupling_run_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, vp, vp, vp]
         L.gem_fk_run_aski_device.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp,
                                              vp]
         L.gem_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -104,6 +106,17 @@ def lib() -> ctypes.CDLL:
 STEP_DTYPE = np.dtype([("x", "<f8"), ("h", "<f8"), ("k", "<i4"), ("lgy", "<f4"), ("nl", "<i2"), ("sys", "i1"),
                        ("result", "i1"), ("phase", "<i2"), ("nstep", "<i2")])
 assert STEP_DTYPE.itemsize == 32
+
+
+class CouplingParams(ctypes.Structure):
+    """C layout of ``gem_coupling_params`` (include/gemini_fk.h)."""
+    _fields_ = [("nf1", ctypes.c_int), ("nf2", ctypes.c_int), ("nwnmax", ctypes.c_int),
+                ("nkfmax", ctypes.c_longlong), ("nsp", ctypes.c_int), ("df", ctypes.c_double),
+                ("sigma", ctypes.c_double), ("re", ctypes.c_double), ("nsamp", ctypes.c_int),
+                ("dt", ctypes.c_double), ("tred", ctypes.c_double), ("order_highpass", ctypes.c_int),
+                ("fc_highpass", ctypes.c_double), ("order_lowpass", ctypes.c_int), ("fc_lowpass", ctypes.c_double),
+                ("thetas", ctypes.c_double), ("phis", ctypes.c_double), ("thetac", ctypes.c_double),
+                ("phic", ctypes.c_double), ("spectra", ctypes.c_int)]
 
 
 class SynthParams(ctypes.Structure):
@@ -366,6 +379,30 @@ class GeminiFK:
                                                  _ptr(th), _ptr(ph), _ptr(pd), len(mt), _ptr(mt),
                                                  ctypes.byref(opts), _ptr(out)))
         return out
+
+    def coupling(self, cp: CouplingParams, nwn, gr, gi, zelcon, mt, delta, xi, nrm):
+        """Synthetics for SPECFEM coupling (gem_coupling_run) at boundary points
+        of one node: gr/gi float32 (nsp, nkfmax) DSV spectra with derivatives,
+        zelcon complex [nf2, 7].  Returns complex spectra [npts, 6, nf2] when
+        cp.spectra, else float32 traces [npts, 6, nsamp] (velocity x, y, z,
+        traction x, y, z in the box frame)."""
+        gr = np.ascontiguousarray(gr, np.float32)
+        gi = np.ascontiguousarray(gi, np.float32)
+        nwn = np.ascontiguousarray(nwn, np.int32)
+        zel = np.ascontiguousarray(zelcon, np.complex128)
+        mt = np.ascontiguousarray(mt, np.float64)
+        delta = np.ascontiguousarray(delta, np.float64)
+        xi = np.ascontiguousarray(xi, np.float64)
+        nrm = np.ascontiguousarray(nrm, np.float64)
+        npts = len(delta)
+        if gr.shape != (cp.nsp, cp.nkfmax) or gi.shape != gr.shape or zel.shape != (cp.nf2, 7) or \
+                nrm.shape != (npts, 3) or len(xi) != npts or len(nwn) < cp.nf2 or len(mt) != 6:
+            raise GeminiError("coupling: inconsistent input shapes")
+        spec = np.zeros((npts, 6, cp.nf2), np.complex128) if cp.spectra else None
+        tr = None if cp.spectra else np.zeros((npts, 6, cp.nsamp), np.float32)
+        self._check(lib().gem_coupling_run(self._h, ctypes.byref(cp), _ptr(nwn), _ptr(gr), _ptr(gi), _ptr(zel),
+                                           _ptr(mt), npts, _ptr(delta), _ptr(xi), _ptr(nrm), _ptr(spec), _ptr(tr)))
+        return spec if cp.spectra else tr
 
     def schedule(self):
         """Schedule index per phase (toroidal, spheroidal, adjoint); see SCHEDULES."""

@@ -99,6 +99,28 @@ typedef struct gem_synth_params {
   double rearth;          /* earth radius of the FK file (regional mode; float32 there) */
 } gem_synth_params;
 
+/* Parameters of the synthetics for SPECFEM coupling
+ * (computeSyntheticsForSpecfemCoupling.f90:136-250,376-453): the FK slab's
+ * frequency range and extent as stored with the DSV spectra, the radius of the
+ * boundary points' node, the event filter (BUTTERWORTH_BANDPASS specs), the
+ * reduction time, the source's and the box centre's colatitude and longitude
+ * (rad), and COMPUTE_SPECTRA. */
+typedef struct gem_coupling_params {
+  int nf1, nf2, nwnmax;
+  long long nkfmax;
+  int nsp;               /* >= 20: U, V, dU/dr, dV/dr x 4 jumps, W, dW/dr x 2 jumps */
+  double df, sigma;
+  double re;             /* radius of the node of the boundary points (m) */
+  int nsamp;
+  double dt, tred;
+  int order_highpass;
+  double fc_highpass;
+  int order_lowpass;
+  double fc_lowpass;
+  double thetas, phis, thetac, phic;
+  int spectra;           /* 1: unfiltered displacement and traction spectra instead of time series */
+} gem_coupling_params;
+
 /* Context holding the model, nodes and device buffers of one GPU.
  * Replaces the module globals sec_* (splineEarthmodelCoefficients.f90:28-41);
  * one host thread per context. */
@@ -163,6 +185,30 @@ int gem_fk_run_aski(gem_ctx* ctx, const gem_fk_params* p, int nsnod, const int* 
 int gem_fk_run_aski_device(gem_ctx* ctx, const gem_fk_params* p, int nsnod, const int* jsnod, int jf_first,
                            int jf_last, float* d_gfre, float* d_gfim, double* d_gf64, int32_t* d_status,
                            void* stream);
+
+/* Synthetics for SPECFEM coupling of a moment source at npts boundary points of
+ * one node: replaces computeSynthetics and computeTension of
+ * computeSyntheticsForSpecfemCoupling.f90:677-793 in the loops :509-549 and
+ * :571-590.  Per point and frequency: the 42 degree sums of the DSV spectra with
+ * derivatives (harmonicDegreeSums.f90:186-369), displacement and its r, theta
+ * and phi derivatives, strain and stress (singleFrequencyDisplacement.f90:
+ * 108-262), rotation to the box frame (axesRotation.f90), traction = stress *
+ * nrm, then either the unfiltered spectra (p->spectra) or velocity and traction
+ * through the event filter and the time shift, inverse-transformed
+ * (frequencyTime.f90:55-113).  gr/gi: float32 spectra (nkfmax, nsp) of the
+ * points' node; nwn[nf2]; zelcon[nf2*7] the node's complex elastic constants per
+ * frequency (interleaved, getComplexConstantsSelectedExternalRadialNodes);
+ * mt[6]; delta, xi[npts] epicentral distance and azimuth (rad); nrm[npts*3] box
+ * normals.  Output per point: velocity x, y, z then traction x, y, z, as
+ * spec[(p*6 + c)*nf2 + jf-1] (complex) or traces[(p*6 + c)*nsamp + i]. */
+int gem_coupling_run(gem_ctx* ctx, const gem_coupling_params* p, const int* nwn, const float* gr, const float* gi,
+                     const double* zelcon, const double* mt, int npts, const double* delta, const double* xi,
+                     const double* nrm, double* spec, float* traces);
+/* Same with the spectra and the outputs on the device, ordered on `stream`;
+ * nwn, zelcon, mt and the point arrays are host arrays. */
+int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* p, const int* nwn, const float* d_gr,
+                            const float* d_gi, const double* zelcon, const double* mt, int npts, const double* delta,
+                            const double* xi, const double* nrm, double* d_spec, float* d_traces, void* stream);
 
 /* CUDA-graph form of gem_fk_run_device (no counterpart in the reference).
  * gem_fk_graph_build does the host-side preparation of the slab once (item and
