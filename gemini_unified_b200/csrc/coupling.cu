@@ -1,7 +1,7 @@
 // Synthetics for SPECFEM coupling on the GPU: displacement (as velocity) and
 // traction at the boundary points of a SPECFEM box, from the DSV spectra with
 // radial derivatives of the points' node (computeSyntheticsForSpecfemCoupling.f90:
-// computeSynthetics :714-793, computeTension :677-705; moment sources).
+// computeSynthetics :714-793, computeTension :677-705; moment and force sources).
 //
 //   cpl_legendre_kernel  P_l^m, dP/dtheta, P/sin, d2P/dtheta2, d/dtheta(P/sin)
 //                        for m <= 2 at every point (legendreFunctions.f90:48-157)
@@ -42,8 +42,18 @@ __constant__ CplSum c_cpl[CPL_NSUM] = {
     {11, 1, 2.0, 16}, {12, 2, 4.0, 17}, {9, 1, 2.0, 16}, {10, 2, -2.0, 17},
     {11, 1, 2.0, 6}, {12, 2, -4.0, 7}};
 
+// the 21 force sums (harmonicDegreeSums.f90:95-167): columns of U, V, dU/dr,
+// dV/dr (x 2 jumps), W, dW/dr (1 jump)
+__constant__ CplSum c_cplf[21] = {
+    {0, 0, 0.0, 0}, {1, 1, -2.0, 1}, {3, 1, 0.0, 2}, {4, 1, -2.0, 3},
+    {6, 1, -2.0, 8}, {4, 1, 2.0, 8}, {6, 1, 2.0, 3},
+    {0, 0, 0.0, 4}, {1, 1, -2.0, 5}, {3, 1, 0.0, 6}, {4, 1, -2.0, 7},
+    {6, 1, -2.0, 9}, {4, 1, 2.0, 9}, {6, 1, 2.0, 7},
+    {3, 1, 0.0, 0}, {4, 1, -2.0, 1}, {8, 1, 0.0, 2}, {9, 1, -2.0, 3},
+    {11, 1, -2.0, 8}, {9, 1, 2.0, 8}, {11, 1, 2.0, 3}};
+
 struct CplDev {
-  int nf1, nf2, npts, lcap, spectra;
+  int nf1, nf2, npts, lcap, spectra, istyp, nsum;
   long long nkf;
   double df, sigma, re, tred;
   double thetas, phis, thetac, phic;
@@ -138,8 +148,8 @@ __global__ void __launch_bounds__(CPL_SUM_THREADS) cpl_sums_kernel(CplDev S, con
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double* tp = tab + (long long)pt * CPL_NKIND * S.lcap;
   const long long g0 = S.koff[slot];
-  for (int k = warp; k < CPL_NSUM; k += CPL_SUM_THREADS / 32) {
-    const CplSum cs = c_cpl[k];
+  for (int k = warp; k < S.nsum; k += CPL_SUM_THREADS / 32) {
+    const CplSum cs = S.istyp == 1 ? c_cpl[k] : c_cplf[k];
     const double* T = tp + (long long)cs.kind * S.lcap;
     const float* gre = gr + (long long)cs.col * S.nkf + g0;
     const float* gim = gi + (long long)cs.col * S.nkf + g0;
@@ -154,7 +164,7 @@ __global__ void __launch_bounds__(CPL_SUM_THREADS) cpl_sums_kernel(CplDev S, con
       sr += __shfl_xor_sync(0xffffffffu, sr, o);
       si += __shfl_xor_sync(0xffffffffu, si, o);
     }
-    if (lane == 0) hd[((long long)pt * nf + slot) * CPL_NSUM + k] = make_double2(sr, si);
+    if (lane == 0) hd[((long long)pt * nf + slot) * S.nsum + k] = make_double2(sr, si);
   }
 }
 
@@ -207,35 +217,52 @@ __global__ void cpl_point_kernel(CplDev S, const double2* __restrict__ hd, doubl
   const int slot = (int)(idx % nf), pt = (int)(idx / nf);
   const int jf = S.nf1 + slot;
   dz w[CPL_NSUM + 1];
-  for (int k = 0; k < CPL_NSUM; ++k) {
-    const double2 v = hd[((long long)pt * nf + slot) * CPL_NSUM + k];
+  for (int k = 0; k < S.nsum; ++k) {
+    const double2 v = hd[((long long)pt * nf + slot) * S.nsum + k];
     w[k + 1] = dz{v.x, v.y};
   }
   const double* m = S.mt;
   const double phi = S.xi[pt], dl = S.delta[pt], re = S.re;
   const double sphi = sin(phi), cphi = cos(phi), s2phi = sin(2.0 * phi), c2phi = cos(2.0 * phi);
-  const double t1 = m[3] * cphi + m[4] * sphi, t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
-  const double t3 = m[4] * cphi - m[3] * sphi, t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
-  dz u[3], ur[3], ut[3], uf[3];
-  u[0] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
-  u[1] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
-  u[2] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
-  ur[0] = w[15] * m[0] + w[16] * (m[1] + m[2]) + w[17] * t1 + w[18] * t2;
-  ur[1] = w[19] * m[0] + w[20] * (m[1] + m[2]) + (w[21] + w[23]) * t1 + (w[22] + w[24]) * t2;
-  ur[2] = (w[25] + w[27]) * t3 + (w[26] + w[28]) * t4;
-  ut[0] = w[29] * m[0] + w[30] * (m[1] + m[2]) + w[31] * t1 + w[32] * t2;
-  ut[1] = w[33] * m[0] + w[34] * (m[1] + m[2]) + (w[35] + w[37]) * t1 + (w[36] + w[38]) * t2;
-  ut[2] = (w[39] + w[41]) * t3 + (w[40] + w[42]) * t4;
-  for (int c = 0; c < 3; ++c) ut[c] = ut[c] / re;
-  const double p1 = (-m[3]) * sphi + m[4] * cphi;
-  const double p2 = (-2.0) * (m[2] - m[1]) * s2phi - 4.0 * m[5] * c2phi;
-  const double p3 = (-m[4]) * sphi - m[3] * cphi;
-  const double p4 = 2.0 * (m[2] - m[1]) * c2phi - 4.0 * m[5] * s2phi;
   const double rst = re * sin(dl);
-  uf[0] = w[3] * p1 + w[4] * p2;
-  uf[1] = (w[7] + w[9]) * p1 + (w[8] + w[10]) * p2;
-  uf[2] = (w[11] + w[13]) * p3 + (w[12] + w[14]) * p4;
-  for (int c = 0; c < 3; ++c) uf[c] = uf[c] / rst;
+  dz u[3], ur[3], ut[3], uf[3];
+  if (S.istyp == 0) {   // force{,RadDeriv,ThetaDeriv,PhiDeriv}SingleFrequencyDisplacement (:35-103)
+    const double fh = m[1] * cphi + m[2] * sphi, ft = m[1] * sphi - m[2] * cphi;
+    const double fp = (-m[1]) * sphi + m[2] * cphi, fq = m[1] * cphi + m[2] * sphi;
+    for (int q = 0; q < 3; ++q) {
+      dz* v = q == 0 ? u : (q == 1 ? ur : ut);
+      const int o = 7 * q;
+      v[0] = w[o + 1] * m[0] + w[o + 2] * fh;
+      v[1] = w[o + 3] * m[0] + (w[o + 4] + w[o + 5]) * fh;
+      v[2] = (w[o + 6] + w[o + 7]) * ft;
+    }
+    for (int c = 0; c < 3; ++c) ut[c] = ut[c] / re;
+    uf[0] = w[2] * fp;
+    uf[1] = (w[4] + w[5]) * fp;
+    uf[2] = (w[6] + w[7]) * fq;
+    for (int c = 0; c < 3; ++c) uf[c] = uf[c] / rst;
+  } else {
+    const double t1 = m[3] * cphi + m[4] * sphi, t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
+    const double t3 = m[4] * cphi - m[3] * sphi, t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
+    u[0] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
+    u[1] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
+    u[2] = (w[11] + w[13]) * t3 + (w[12] + w[14]) * t4;
+    ur[0] = w[15] * m[0] + w[16] * (m[1] + m[2]) + w[17] * t1 + w[18] * t2;
+    ur[1] = w[19] * m[0] + w[20] * (m[1] + m[2]) + (w[21] + w[23]) * t1 + (w[22] + w[24]) * t2;
+    ur[2] = (w[25] + w[27]) * t3 + (w[26] + w[28]) * t4;
+    ut[0] = w[29] * m[0] + w[30] * (m[1] + m[2]) + w[31] * t1 + w[32] * t2;
+    ut[1] = w[33] * m[0] + w[34] * (m[1] + m[2]) + (w[35] + w[37]) * t1 + (w[36] + w[38]) * t2;
+    ut[2] = (w[39] + w[41]) * t3 + (w[40] + w[42]) * t4;
+    for (int c = 0; c < 3; ++c) ut[c] = ut[c] / re;
+    const double p1 = (-m[3]) * sphi + m[4] * cphi;
+    const double p2 = (-2.0) * (m[2] - m[1]) * s2phi - 4.0 * m[5] * c2phi;
+    const double p3 = (-m[4]) * sphi - m[3] * cphi;
+    const double p4 = 2.0 * (m[2] - m[1]) * c2phi - 4.0 * m[5] * s2phi;
+    uf[0] = w[3] * p1 + w[4] * p2;
+    uf[1] = (w[7] + w[9]) * p1 + (w[8] + w[10]) * p2;
+    uf[2] = (w[11] + w[13]) * p3 + (w[12] + w[14]) * p4;
+    for (int c = 0; c < 3; ++c) uf[c] = uf[c] / rst;
+  }
   // strain and stress (singleFrequencyDisplacement.f90:229-262)
   const double rtd = re * tan(dl);
   dz e[3][3];
@@ -294,7 +321,7 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 using namespace gem;
 
-// SPECFEM-coupling synthetics of a moment source at npts boundary points of one
+// SPECFEM-coupling synthetics of a moment or force source at npts boundary points of one
 // node (the loops of computeSyntheticsForSpecfemCoupling.f90:509-549, 571-590 over
 // computeSynthetics :714-793).  d_gr/d_gi: float32 DSV spectra with radial
 // derivatives of the node, (nkfmax, nsp >= 20).  Host arrays: nwn[nf2], zelcon
@@ -312,7 +339,9 @@ extern "C" int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* 
     return gem_set_error(ctx, "coupling: null argument");
   if (npts < 1) return gem_set_error(ctx, "coupling: no boundary points");
   if (p->nf2 - p->nf1 + 1 > 65535) return gem_set_error(ctx, "coupling: more than 65535 frequencies");
-  if (p->nsp < 20) return gem_set_error(ctx, "coupling: the DSV spectra need radial derivatives (nsp >= 20)");
+  if (p->istyp != 0 && p->istyp != 1) return gem_set_error(ctx, "coupling: invalid source type");
+  if (p->nsp < (p->istyp == 1 ? 20 : 10))
+    return gem_set_error(ctx, "coupling: the DSV spectra need radial derivatives (nsp >= 20 moment, 10 force)");
   if (p->nf1 < 1 || p->nf2 < p->nf1 || p->nwnmax < 1 || !(p->re > 0))
     return gem_set_error(ctx, "coupling: invalid frequency range, degrees or radius");
   if (p->spectra ? !d_spec : !d_traces) return gem_set_error(ctx, "coupling: null output");
@@ -340,7 +369,7 @@ extern "C" int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* 
   // workspace: tables, sums, spectra, small inputs
   const int lcap = p->nwnmax;
   const size_t b_tab = align256((size_t)npts * CPL_NKIND * lcap * sizeof(double));
-  const size_t b_hd = align256((size_t)npts * nf * CPL_NSUM * sizeof(double2));
+  const size_t b_hd = align256((size_t)npts * nf * (p->istyp == 1 ? CPL_NSUM : 21) * sizeof(double2));
   const size_t b_x = align256((size_t)npts * 6 * p->nf2 * sizeof(double2));
   const size_t b_in = align256((size_t)nf * sizeof(int)) + align256((size_t)p->nf2 * sizeof(int)) +
                       3 * align256((size_t)npts * 3 * sizeof(double)) + align256(evf.size() * sizeof(double2)) +
@@ -373,7 +402,8 @@ extern "C" int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* 
   S.nf1 = p->nf1; S.nf2 = p->nf2; S.npts = npts; S.lcap = lcap; S.spectra = p->spectra; S.nkf = p->nkfmax;
   S.df = p->df; S.sigma = p->sigma; S.re = p->re; S.tred = p->tred;
   S.thetas = p->thetas; S.phis = p->phis; S.thetac = p->thetac; S.phic = p->phic;
-  for (int i = 0; i < 6; ++i) S.mt[i] = mt[i];
+  S.istyp = p->istyp; S.nsum = p->istyp == 1 ? CPL_NSUM : 21;
+  for (int i = 0; i < (p->istyp == 1 ? 6 : 3); ++i) S.mt[i] = mt[i];
   S.nwn = d_nwn; S.koff = d_koff; S.delta = d_delta; S.xi = d_xi; S.nrm = d_nrm; S.evf = d_evf; S.zel = d_zel;
   cpl_legendre_kernel<<<(npts * 3 + 127) / 128, 128, 0, st>>>(npts, p->nwnmax - 1, lcap, d_delta, tab);
   const size_t smem = (size_t)p->nwnmax * sizeof(double);

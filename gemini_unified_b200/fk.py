@@ -116,7 +116,11 @@ class CouplingParams(ctypes.Structure):
                 ("dt", ctypes.c_double), ("tred", ctypes.c_double), ("order_highpass", ctypes.c_int),
                 ("fc_highpass", ctypes.c_double), ("order_lowpass", ctypes.c_int), ("fc_lowpass", ctypes.c_double),
                 ("thetas", ctypes.c_double), ("phis", ctypes.c_double), ("thetac", ctypes.c_double),
-                ("phic", ctypes.c_double), ("spectra", ctypes.c_int)]
+                ("phic", ctypes.c_double), ("spectra", ctypes.c_int), ("istyp", ctypes.c_int)]
+
+    def __init__(self, **kw):
+        kw.setdefault("istyp", 1)
+        super().__init__(**kw)
 
 
 class SynthParams(ctypes.Structure):
@@ -396,7 +400,7 @@ class GeminiFK:
         nrm = np.ascontiguousarray(nrm, np.float64)
         npts = len(delta)
         if gr.shape != (cp.nsp, cp.nkfmax) or gi.shape != gr.shape or zel.shape != (cp.nf2, 7) or \
-                nrm.shape != (npts, 3) or len(xi) != npts or len(nwn) < cp.nf2 or len(mt) != 6:
+                nrm.shape != (npts, 3) or len(xi) != npts or len(nwn) < cp.nf2 or len(mt) != (6 if cp.istyp else 3):
             raise GeminiError("coupling: inconsistent input shapes")
         spec = np.zeros((npts, 6, cp.nf2), np.complex128) if cp.spectra else None
         tr = None if cp.spectra else np.zeros((npts, 6, cp.nsamp), np.float32)

@@ -119,6 +119,7 @@ typedef struct gem_coupling_params {
   double fc_lowpass;
   double thetas, phis, thetac, phic;
   int spectra;           /* 1: unfiltered displacement and traction spectra instead of time series */
+  int istyp;             /* 1 MOMENT (mt[6], nsp >= 20, 42 sums), 0 FORCE (mt[3] = Fr, Ft, Ff; nsp >= 10, 21 sums) */
 } gem_coupling_params;
 
 /* Context holding the model, nodes and device buffers of one GPU.
@@ -186,11 +187,12 @@ int gem_fk_run_aski_device(gem_ctx* ctx, const gem_fk_params* p, int nsnod, cons
                            int jf_last, float* d_gfre, float* d_gfim, double* d_gf64, int32_t* d_status,
                            void* stream);
 
-/* Synthetics for SPECFEM coupling of a moment source at npts boundary points of
- * one node: replaces computeSynthetics and computeTension of
+/* Synthetics for SPECFEM coupling of a moment or force source at npts boundary
+ * points of one node: replaces computeSynthetics and computeTension of
  * computeSyntheticsForSpecfemCoupling.f90:677-793 in the loops :509-549 and
- * :571-590.  Per point and frequency: the 42 degree sums of the DSV spectra with
- * derivatives (harmonicDegreeSums.f90:186-369), displacement and its r, theta
+ * :571-590.  Per point and frequency: the 42 (moment) or 21 (force) degree sums
+ * of the DSV spectra with derivatives (harmonicDegreeSums.f90:95-369),
+ * displacement and its r, theta
  * and phi derivatives, strain and stress (singleFrequencyDisplacement.f90:
  * 108-262), rotation to the box frame (axesRotation.f90), traction = stress *
  * nrm, then either the unfiltered spectra (p->spectra) or velocity and traction

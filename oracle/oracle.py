@@ -56,7 +56,7 @@ def lib():
                                            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.oracle_legendre.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
-        L.oracle_coupling.argtypes = ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+        L.oracle_coupling.argtypes = ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_double] * 3 +
                                       [ctypes.c_void_p] * 3 + [ctypes.c_double, ctypes.c_int] + [ctypes.c_double] * 5 +
                                       [ctypes.c_int] + [ctypes.c_void_p] * 3 + [ctypes.c_int] + [ctypes.c_void_p] * 3)
@@ -377,10 +377,11 @@ def synthetics_opts(source_type, global_, nf1, nf2, nwn, nwnmax, df, sigma, dwn,
 
 
 def coupling(nf1, nf2, nwn, nwnmax, gr, gi, df, sigma, re, zelcon, mt, filspecs, tred, nsamp, dt, thetas, phis,
-             thetac, phic, delta, xi, nrm, spectra=False, debug=False):
-    """SPECFEM-coupling synthetics of a moment source at boundary points
+             thetac, phic, delta, xi, nrm, spectra=False, debug=False, istyp=1):
+    """SPECFEM-coupling synthetics at boundary points
     (computeSyntheticsForSpecfemCoupling.f90:677-793).  gr/gi: float32 DSV
-    spectra with derivatives of the points' node, shape (nsp >= 20, nkfmax);
+    spectra with derivatives of the points' node, shape (nsp, nkfmax), nsp >= 20
+    for a moment tensor mt[6] (istyp 1), >= 10 for a force mt[3] (istyp 0);
     zelcon: complex [nf2, 7] elastic constants of the node per frequency.
     Returns (spectra complex [npts, 6, nf2] or None, traces float32 [npts, 6,
     nsamp] or None, debug complex [npts, nf2, 4, 3] or None)."""
@@ -395,7 +396,7 @@ def coupling(nf1, nf2, nwn, nwnmax, gr, gi, df, sigma, re, zelcon, mt, filspecs,
     spec = np.zeros(npts * 6 * nf2, np.complex128) if spectra else None
     tr = None if spectra else np.zeros(npts * 6 * nsamp, np.float32)
     dbg = np.zeros(npts * nf2 * 12, np.complex128) if debug else None
-    rc = lib().oracle_coupling(nf1, nf2, _p(nwn), nwnmax, nkfmax, nsp, _p(gr), _p(gi), df, sigma, re, _p(zel),
+    rc = lib().oracle_coupling(istyp, nf1, nf2, _p(nwn), nwnmax, nkfmax, nsp, _p(gr), _p(gi), df, sigma, re, _p(zel),
                                _p(mt), _p(fs), tred, nsamp, dt, thetas, phis, thetac, phic, npts, _p(delta), _p(xi),
                                _p(nrm), 1 if spectra else 0, _p(spec), _p(tr), _p(dbg))
     if rc:

@@ -716,6 +716,46 @@ const SumDef DSUM[42] = {
     {4, 1, 1, 2.0, 7, 1},  {4, 2, 2, 4.0, 7, 2},  {3, 1, 1, 2.0, 7, 1},  {3, 2, 2, -2.0, 7, 2},
     {4, 1, 1, 2.0, 3, 3},  {4, 2, 2, -4.0, 3, 4}};
 
+// the 21 force sums with derivatives (harmonicDegreeSums.f90:95-167, index map :34-37)
+const SumDef DSUMF[21] = {
+    {0, 0, 0, 0.0, 1, 1},  {0, 1, 1, -2.0, 1, 2}, {1, 0, 1, 0.0, 3, 1},  {1, 1, 1, -2.0, 3, 2},
+    {2, 1, 1, -2.0, 7, 1}, {1, 1, 1, 2.0, 7, 1},  {2, 1, 1, 2.0, 3, 2},
+    {0, 0, 0, 0.0, 5, 1},  {0, 1, 1, -2.0, 5, 2}, {1, 0, 1, 0.0, 6, 1},  {1, 1, 1, -2.0, 6, 2},
+    {2, 1, 1, -2.0, 9, 1}, {1, 1, 1, 2.0, 9, 1},  {2, 1, 1, 2.0, 6, 2},
+    {1, 0, 1, 0.0, 1, 1},  {1, 1, 1, -2.0, 1, 2}, {3, 0, 1, 0.0, 3, 1},  {3, 1, 1, -2.0, 3, 2},
+    {4, 1, 1, -2.0, 7, 1}, {3, 1, 1, 2.0, 7, 1},  {4, 1, 1, 2.0, 3, 2}};
+
+// column of (component, jump) in the force DSV spectra with derivatives
+// (positionDataGreenFKSpectra, greenFKSpectra.f90:204-212: 2 spheroidal jumps, 1 toroidal)
+int dsvColumnForce(int comp, int jump) {
+  switch (comp) {
+    case 1: return jump - 1;
+    case 3: return 2 + jump - 1;
+    case 5: return 4 + jump - 1;
+    case 6: return 6 + jump - 1;
+    case 7: return 8;
+    default: return 9;
+  }
+}
+
+zc derivSumForce(int kint, const float* gr, const float* gi, int nwn, const Legendre& alf,
+                 const std::vector<double>& tap) {
+  const SumDef& s = DSUMF[kint - 1];
+  const std::vector<double>& T = s.kind == 0 ? alf.plm[s.m] : s.kind == 1 ? alf.dpdt[s.m] : s.kind == 2 ?
+                                 alf.pdst[s.m] : s.kind == 3 ? alf.d2pdt2[s.m] : alf.dtpdst[s.m];
+  const double fourpi = 4.0 * PI_F;
+  zc z = Z(0.0);
+  for (int l = s.l0; l <= nwn - 1; ++l) {
+    zc g = Z((double)gr[l], (double)gi[l]);
+    zc t;
+    if (s.fnum == 0.0) t = T[l] * g;
+    else t = (T[l] * (s.fnum / (double)(float)(l * (l + 1)))) * g;
+    t = ((t * (2.0 * (double)l + 1.0)) / fourpi) * tap[l];
+    z = z + t;
+  }
+  return z;
+}
+
 // column of (component, jump) in the DSV spectra with derivatives
 int dsvColumn(int comp, int jump) {
   switch (comp) {
@@ -785,6 +825,8 @@ void vecLSrot(double d, double x, const zc* u, zc* o) { vecLCfromLS(d, x, u, o);
 }  // namespace
 
 extern "C" {
+// istyp 1: moment tensor mt[6] and DSV spectra of a moment (nsp >= 20, 42 sums);
+// istyp 0: force mt[3] = (Fr, Ft, Ff) and those of a force (nsp >= 10, 21 sums).
 // Per boundary point p (epicentral distance delta[p], azimuth xi[p] from south over
 // east, outward normal nrm[3p..3p+2] in box coordinates) at radius re of the DSV node:
 // the 42 degree sums, displacement and its derivatives, strain and stress
@@ -795,12 +837,13 @@ extern "C" {
 // traction through the event filter and the time shift of tred, then the inverse FFT:
 // traces[(p*6 + c)*nsamp + i].  dbg (nullable): the LS displacement, d/dr, (1/r)d/dtheta
 // and (1/(r sin)) d/dphi at dbg[((p*nf2 + jf-1)*12 + 3q + c)*2].
-int oracle_coupling(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp, const float* gr,
+int oracle_coupling(int istyp, int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, int nsp, const float* gr,
                     const float* gi, double df, double sigma, double re, const double* zelcon, const double* mt,
                     const double* filspecs, double tred, int nsamp, double dt, double thetas, double phis,
                     double thetac, double phic, int npts, const double* delta, const double* xi,
                     const double* nrm, int spectra, double* spec, float* traces, double* dbg) {
-  if (nsp < 20) return 2;
+  if (nsp < (istyp == 1 ? 20 : 10)) return 2;
+  const int nsum = istyp == 1 ? 42 : 21;
   std::vector<zc> evf;
   eventFilter((int)std::lround(filspecs[0]), filspecs[1], (int)std::lround(filspecs[2]), filspecs[3], nf1, nf2, df,
               sigma, evf);
@@ -821,15 +864,35 @@ int oracle_coupling(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, in
       std::vector<double> tap;
       taper(nwn[jf - 1] - 1, 0.2, tap);
       zc w[43];
-      for (int k = 1; k <= 42; ++k) {
-        const int col = dsvColumn(DSUM[k - 1].comp, DSUM[k - 1].jump);
-        w[k] = derivSum(k, gr + (size_t)col * nkfmax + (nwa - 1), gi + (size_t)col * nkfmax + (nwa - 1),
-                        nwn[jf - 1], alf, tap);
+      for (int k = 1; k <= nsum; ++k) {
+        const SumDef& sd = istyp == 1 ? DSUM[k - 1] : DSUMF[k - 1];
+        const int col = istyp == 1 ? dsvColumn(sd.comp, sd.jump) : dsvColumnForce(sd.comp, sd.jump);
+        const float* a = gr + (size_t)col * nkfmax + (nwa - 1);
+        const float* b = gi + (size_t)col * nkfmax + (nwa - 1);
+        w[k] = istyp == 1 ? derivSum(k, a, b, nwn[jf - 1], alf, tap) : derivSumForce(k, a, b, nwn[jf - 1], alf, tap);
       }
       const double* m = mt;
+      zc u[3], ur[3], ut[3], uf[3];
+      const double rst = re * std::sin(dl);
+      if (istyp == 0) {
+        // force{,RadDeriv,ThetaDeriv,PhiDeriv}SingleFrequencyDisplacement (:35-103)
+        const double fh = m[1] * cphi + m[2] * sphi, ft = m[1] * sphi - m[2] * cphi;
+        const double fp = (-m[1]) * sphi + m[2] * cphi, fq = m[1] * cphi + m[2] * sphi;
+        for (int q = 0; q < 3; ++q) {
+          zc* v = q == 0 ? u : (q == 1 ? ur : ut);
+          const int o = 7 * q;
+          v[0] = w[o + 1] * m[0] + w[o + 2] * fh;
+          v[1] = w[o + 3] * m[0] + (w[o + 4] + w[o + 5]) * fh;
+          v[2] = (w[o + 6] + w[o + 7]) * ft;
+        }
+        for (int c = 0; c < 3; ++c) ut[c] = ut[c] / re;
+        uf[0] = w[2] * fp;
+        uf[1] = (w[4] + w[5]) * fp;
+        uf[2] = (w[6] + w[7]) * fq;
+        for (int c = 0; c < 3; ++c) uf[c] = uf[c] / rst;
+      } else {
       const double t1 = m[3] * cphi + m[4] * sphi, t2 = (m[2] - m[1]) * c2phi - 2.0 * m[5] * s2phi;
       const double t3 = m[4] * cphi - m[3] * sphi, t4 = (m[2] - m[1]) * s2phi + 2.0 * m[5] * c2phi;
-      zc u[3], ur[3], ut[3], uf[3];
       // momentSingleFrequencyDisplacement (:108-125)
       u[0] = w[1] * m[0] + w[2] * (m[1] + m[2]) + w[3] * t1 + w[4] * t2;
       u[1] = w[5] * m[0] + w[6] * (m[1] + m[2]) + (w[7] + w[9]) * t1 + (w[8] + w[10]) * t2;
@@ -848,11 +911,11 @@ int oracle_coupling(int nf1, int nf2, const int* nwn, int nwnmax, int nkfmax, in
       const double p2 = (-2.0) * (m[2] - m[1]) * s2phi - 4.0 * m[5] * c2phi;
       const double p3 = (-m[4]) * sphi - m[3] * cphi;
       const double p4 = 2.0 * (m[2] - m[1]) * c2phi - 4.0 * m[5] * s2phi;
-      const double rst = re * std::sin(dl);
       uf[0] = w[3] * p1 + w[4] * p2;
       uf[1] = (w[7] + w[9]) * p1 + (w[8] + w[10]) * p2;
       uf[2] = (w[11] + w[13]) * p3 + (w[12] + w[14]) * p4;
       for (int c = 0; c < 3; ++c) uf[c] = uf[c] / rst;
+      }
       if (dbg) {
         const zc* q[4] = {u, ur, ut, uf};
         for (int a = 0; a < 4; ++a)

@@ -2,8 +2,8 @@
 the CPU oracle (computeSyntheticsForSpecfemCoupling.f90:677-793).
 
 Both sides take the same float32 DSV spectra with radial derivatives (from
-gem_fk_run_dsv, a moment source at the surface node) at the node of the
-boundary points.  The degree sums run in FP64 on both sides and differ only in
+gem_fk_run_dsv, a moment source or a force at the surface node) at the node of
+the boundary points.  The degree sums run in FP64 on both sides and differ only in
 the order of the additions.  Spectra must agree to 1e-9 relative to the
 largest value of each (point, component) spectrum.  Time series are float32
 and must agree to 1e-6 relative to the largest sample of each series."""
@@ -17,6 +17,7 @@ from gemini_unified_b200 import configs, model as M
 pytestmark = pytest.mark.gpu
 NPTS = 16
 MT = np.array([1.0, -0.4, 0.7, 0.3, -0.5, 0.2])
+FORCE = np.array([0.8, -0.3, 0.6])
 FS = (2.0, 0.002, 4.0, 0.04)
 
 
@@ -30,7 +31,8 @@ def case(gpu):
     g = M.frequency_grid(w.params, m.rearth)
     fk = GeminiFK(m, ex)
     gre, gim, _, st = fk.run_dsv(w.params, jre, g.nf1, g.nf2, f64=False)
-    assert np.all(st == 0)
+    fre, fim, _, sf = fk.run_dsv(dataclasses.replace(w.params, source_type="FORCE"), jre, g.nf1, g.nf2, f64=False)
+    assert np.all(st == 0) and np.all(sf == 0)
     rng = np.random.default_rng(7)
     delta = np.radians(np.linspace(10.0, 80.0, NPTS))
     xi = np.radians(rng.uniform(-180.0, 180.0, NPTS))
@@ -40,40 +42,47 @@ def case(gpu):
     base = np.array([1.1e11 + 1e8j, 1.2e11 + 1e8j, 4e10, 4.5e10 + 5e7j, 4.4e10, 0, 0])
     zel = base[None, :] * (1.0 + 0.01 * f[:, None])
     node = 1
-    return dict(w=w, g=g, fk=fk, gr=gre[node - 1], gi=gim[node - 1], re=ex.r[node - 1], delta=delta, xi=xi,
-                nrm=nrm, zel=zel, nkf=gre.shape[2])
+    return dict(w=w, g=g, fk=fk, gr={1: gre[node - 1], 0: fre[node - 1]}, gi={1: gim[node - 1], 0: fim[node - 1]},
+                re=ex.r[node - 1], delta=delta, xi=xi, nrm=nrm, zel=zel, nkf=gre.shape[2])
 
 
-def _params(c, spectra):
+def _params(c, spectra, istyp=1):
     from gemini_unified_b200.fk import CouplingParams
     g = c["g"]
-    return CouplingParams(nf1=g.nf1, nf2=g.nf2, nwnmax=g.nwnmax, nkfmax=c["nkf"], nsp=20, df=g.df, sigma=g.sigma,
+    return CouplingParams(nf1=g.nf1, nf2=g.nf2, nwnmax=g.nwnmax, nkfmax=c["nkf"], nsp=20 if istyp else 10,
+                          df=g.df, sigma=g.sigma, istyp=istyp,
                           re=c["re"], nsamp=2048, dt=0.5, tred=0.0, order_highpass=int(FS[0]), fc_highpass=FS[1],
                           order_lowpass=int(FS[2]), fc_lowpass=FS[3], thetas=0.35, phis=1.1, thetac=0.6,
                           phic=1.4, spectra=1 if spectra else 0)
 
 
-def _oracle(c, spectra):
+def _oracle(c, spectra, istyp=1):
     import oracle
     g = c["g"]
-    return oracle.coupling(g.nf1, g.nf2, g.nwn, g.nwnmax, c["gr"], c["gi"], g.df, g.sigma, c["re"], c["zel"], MT, FS,
-                           0.0, 2048, 0.5, 0.35, 1.1, 0.6, 1.4, c["delta"], c["xi"], c["nrm"], spectra=spectra)
+    return oracle.coupling(g.nf1, g.nf2, g.nwn, g.nwnmax, c["gr"][istyp], c["gi"][istyp], g.df, g.sigma, c["re"],
+                           c["zel"], MT if istyp else FORCE, FS, 0.0, 2048, 0.5, 0.35, 1.1, 0.6, 1.4, c["delta"],
+                           c["xi"], c["nrm"], spectra=spectra, istyp=istyp)
 
 
-def test_coupling_spectra_match_oracle(case):
-    got = case["fk"].coupling(_params(case, True), case["g"].nwn, case["gr"], case["gi"], case["zel"], MT,
-                              case["delta"], case["xi"], case["nrm"])
-    ref = _oracle(case, True)[0]
+def _gpu(c, spectra, istyp=1):
+    return c["fk"].coupling(_params(c, spectra, istyp), c["g"].nwn, c["gr"][istyp], c["gi"][istyp], c["zel"],
+                            MT if istyp else FORCE, c["delta"], c["xi"], c["nrm"])
+
+
+@pytest.mark.parametrize("istyp", [1, 0])
+def test_coupling_spectra_match_oracle(case, istyp):
+    got = _gpu(case, True, istyp)
+    ref = _oracle(case, True, istyp)[0]
     assert got.shape == ref.shape == (NPTS, 6, case["g"].nf2)
     scale = np.abs(ref).max(axis=2, keepdims=True)
     assert np.all(scale > 0)
     assert (np.abs(got - ref) / scale).max() <= 1e-9
 
 
-def test_coupling_time_series_match_oracle(case):
-    got = case["fk"].coupling(_params(case, False), case["g"].nwn, case["gr"], case["gi"], case["zel"], MT,
-                              case["delta"], case["xi"], case["nrm"])
-    ref = _oracle(case, False)[1]
+@pytest.mark.parametrize("istyp", [1, 0])
+def test_coupling_time_series_match_oracle(case, istyp):
+    got = _gpu(case, False, istyp)
+    ref = _oracle(case, False, istyp)[1]
     assert got.shape == ref.shape == (NPTS, 6, 2048)
     scale = np.abs(ref).max(axis=2, keepdims=True)
     assert np.all(scale > 0)
@@ -85,5 +94,5 @@ def test_coupling_rejects_spectra_without_derivatives(case):
     p = _params(case, True)
     p.nsp = 10
     with pytest.raises(GeminiError, match="derivatives"):
-        case["fk"].coupling(p, case["g"].nwn, case["gr"][:10], case["gi"][:10], case["zel"], MT, case["delta"],
-                            case["xi"], case["nrm"])
+        case["fk"].coupling(p, case["g"].nwn, case["gr"][1][:10], case["gi"][1][:10], case["zel"], MT,
+                            case["delta"], case["xi"], case["nrm"])
