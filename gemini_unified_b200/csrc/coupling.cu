@@ -5,8 +5,11 @@
 //
 //   cpl_legendre_kernel  P_l^m, dP/dtheta, P/sin, d2P/dtheta2, d/dtheta(P/sin)
 //                        for m <= 2 at every point (legendreFunctions.f90:48-157)
-//   cpl_sums_kernel      the 42 degree sums of each (point, frequency)
-//                        (harmonicDegreeSums.f90:186-369, index map :34-45)
+//   cpl_coef_kernel      coefficient rows (frequency, sum) x degree of each
+//                        table kind: taper, (2l+1)/4pi, factor and spectrum
+//                        (harmonicDegreeSums.f90:95-369, index map :34-45)
+//   cpl_gemm_kernel      the degree sums of every (frequency, sum, point) as one
+//                        FP64 tiled product per table kind
 //   cpl_point_kernel     displacement and its derivatives, strain, stress, the
 //                        rotation to the box frame, traction = stress * n,
 //                        event filter, i omega and time shift
@@ -14,6 +17,7 @@
 //   gem_ifft_run_device  the six time series of every point
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -29,28 +33,32 @@ constexpr int CPL_NKIND = 13;   // plm m0-2, dpdt m0-2, pdst m1-2, d2pdt2 m0-2, 
 // column of its (component, jump) in the DSV spectra U, V, dU/dr, dV/dr (x 4
 // jumps), W, dW/dr (x 2 jumps)
 struct CplSum { int kind, l0; double fac; int col; };
-__constant__ CplSum c_cpl[CPL_NSUM] = {
-    {0, 0, 0.0, 0}, {0, 0, 0.0, 1}, {1, 1, 2.0, 2}, {2, 2, 2.0, 3},
-    {3, 1, 0.0, 4}, {3, 1, 0.0, 5}, {4, 1, 2.0, 6}, {5, 2, 2.0, 7},
-    {6, 1, 2.0, 16}, {7, 2, 4.0, 17}, {4, 1, 2.0, 16}, {5, 2, -2.0, 17},
-    {6, 1, 2.0, 6}, {7, 2, -4.0, 7}, {0, 0, 0.0, 8}, {0, 0, 0.0, 9},
-    {1, 1, 2.0, 10}, {2, 2, 2.0, 11}, {3, 1, 0.0, 12}, {3, 1, 0.0, 13},
-    {4, 1, 2.0, 14}, {5, 2, 2.0, 15}, {6, 1, 2.0, 18}, {7, 2, 4.0, 19},
-    {4, 1, 2.0, 18}, {5, 2, -2.0, 19}, {6, 1, 2.0, 14}, {7, 2, -4.0, 15},
-    {3, 1, 0.0, 0}, {3, 1, 0.0, 1}, {4, 1, 2.0, 2}, {5, 2, 2.0, 3},
-    {8, 1, 0.0, 4}, {8, 1, 0.0, 5}, {9, 1, 2.0, 6}, {10, 2, 2.0, 7},
-    {11, 1, 2.0, 16}, {12, 2, 4.0, 17}, {9, 1, 2.0, 16}, {10, 2, -2.0, 17},
-    {11, 1, 2.0, 6}, {12, 2, -4.0, 7}};
+#define CPL_MOMENT_SUMS {                                   \
+    {0, 0, 0.0, 0}, {0, 0, 0.0, 1}, {1, 1, 2.0, 2}, {2, 2, 2.0, 3}, \
+    {3, 1, 0.0, 4}, {3, 1, 0.0, 5}, {4, 1, 2.0, 6}, {5, 2, 2.0, 7}, \
+    {6, 1, 2.0, 16}, {7, 2, 4.0, 17}, {4, 1, 2.0, 16}, {5, 2, -2.0, 17}, \
+    {6, 1, 2.0, 6}, {7, 2, -4.0, 7}, {0, 0, 0.0, 8}, {0, 0, 0.0, 9}, \
+    {1, 1, 2.0, 10}, {2, 2, 2.0, 11}, {3, 1, 0.0, 12}, {3, 1, 0.0, 13}, \
+    {4, 1, 2.0, 14}, {5, 2, 2.0, 15}, {6, 1, 2.0, 18}, {7, 2, 4.0, 19}, \
+    {4, 1, 2.0, 18}, {5, 2, -2.0, 19}, {6, 1, 2.0, 14}, {7, 2, -4.0, 15}, \
+    {3, 1, 0.0, 0}, {3, 1, 0.0, 1}, {4, 1, 2.0, 2}, {5, 2, 2.0, 3}, \
+    {8, 1, 0.0, 4}, {8, 1, 0.0, 5}, {9, 1, 2.0, 6}, {10, 2, 2.0, 7}, \
+    {11, 1, 2.0, 16}, {12, 2, 4.0, 17}, {9, 1, 2.0, 16}, {10, 2, -2.0, 17}, \
+    {11, 1, 2.0, 6}, {12, 2, -4.0, 7}}
+__constant__ CplSum c_cpl[CPL_NSUM] = CPL_MOMENT_SUMS;
+const CplSum h_cpl[CPL_NSUM] = CPL_MOMENT_SUMS;
 
 // the 21 force sums (harmonicDegreeSums.f90:95-167): columns of U, V, dU/dr,
 // dV/dr (x 2 jumps), W, dW/dr (1 jump)
-__constant__ CplSum c_cplf[21] = {
-    {0, 0, 0.0, 0}, {1, 1, -2.0, 1}, {3, 1, 0.0, 2}, {4, 1, -2.0, 3},
-    {6, 1, -2.0, 8}, {4, 1, 2.0, 8}, {6, 1, 2.0, 3},
-    {0, 0, 0.0, 4}, {1, 1, -2.0, 5}, {3, 1, 0.0, 6}, {4, 1, -2.0, 7},
-    {6, 1, -2.0, 9}, {4, 1, 2.0, 9}, {6, 1, 2.0, 7},
-    {3, 1, 0.0, 0}, {4, 1, -2.0, 1}, {8, 1, 0.0, 2}, {9, 1, -2.0, 3},
-    {11, 1, -2.0, 8}, {9, 1, 2.0, 8}, {11, 1, 2.0, 3}};
+#define CPL_FORCE_SUMS {                                    \
+    {0, 0, 0.0, 0}, {1, 1, -2.0, 1}, {3, 1, 0.0, 2}, {4, 1, -2.0, 3}, \
+    {6, 1, -2.0, 8}, {4, 1, 2.0, 8}, {6, 1, 2.0, 3},        \
+    {0, 0, 0.0, 4}, {1, 1, -2.0, 5}, {3, 1, 0.0, 6}, {4, 1, -2.0, 7}, \
+    {6, 1, -2.0, 9}, {4, 1, 2.0, 9}, {6, 1, 2.0, 7},        \
+    {3, 1, 0.0, 0}, {4, 1, -2.0, 1}, {8, 1, 0.0, 2}, {9, 1, -2.0, 3}, \
+    {11, 1, -2.0, 8}, {9, 1, 2.0, 8}, {11, 1, 2.0, 3}}
+__constant__ CplSum c_cplf[21] = CPL_FORCE_SUMS;
+const CplSum h_cplf[21] = CPL_FORCE_SUMS;
 
 struct CplDev {
   int nf1, nf2, npts, lcap, spectra, istyp, nsum;
@@ -65,21 +73,26 @@ struct CplDev {
   const double* nrm;    // [npts * 3]
   const double2* evf;   // [nf2 + 1]
   const double2* zel;   // [nf2 * 7]
+  // sums per table kind, rank of each sum within its kind, offsets of each kind's
+  // coefficient rows A[row][lcap] and results C[row][npts]; row = 2 (slot nsk + rank) + re/im
+  int nsk[CPL_NKIND];
+  int rank[CPL_NSUM];
+  long long aoff[CPL_NKIND], coff[CPL_NKIND];
 };
 
-// tab[(pt * 13 + kind) * lcap + l]; one thread per (point, m)
+// tab[(kind * lcap + l) * npts + pt]; one thread per (point, m)
 __global__ void cpl_legendre_kernel(int npts, int lmax, int lcap, const double* __restrict__ delta, double* tab) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= npts * 3) return;
   const int pt = idx % npts, m = idx / npts;
   const double ct = cos(delta[pt]), st = sin(delta[pt]);
   const bool atpoles = !(st > 0.0);
-  double* base = tab + (long long)pt * CPL_NKIND * lcap;
-  double* Tp = base + (long long)m * lcap;
-  double* Td = base + (long long)(3 + m) * lcap;
-  double* Ts = m >= 1 ? base + (long long)(5 + m) * lcap : nullptr;
-  double* T2 = base + (long long)(8 + m) * lcap;
-  double* Tt = m >= 1 ? base + (long long)(10 + m) * lcap : nullptr;
+  auto row = [&](int kind) { return tab + (long long)kind * lcap * npts + pt; };
+  double* Tp = row(m);
+  double* Td = row(3 + m);
+  double* Ts = m >= 1 ? row(5 + m) : nullptr;
+  double* T2 = row(8 + m);
+  double* Tt = m >= 1 ? row(10 + m) : nullptr;
   double pmm = 1.0, fact = 1.0;
   for (int j = 1; j <= m; ++j) { pmm = pmm * fact * st; fact = fact + 2.0; }
   const double rst = 1.0 / st;
@@ -112,59 +125,115 @@ __global__ void cpl_legendre_kernel(int npts, int lmax, int lcap, const double* 
       if (m == 2 && l >= 1) dts = 0.125 * q * sl1;
     }
     if (l < lcap) {
-      Tp[l] = p; Td[l] = dp; T2[l] = d2;
-      if (Ts) Ts[l] = ps;
-      if (Tt) Tt[l] = dts;
+      const long long o = (long long)l * npts;
+      Tp[o] = p; Td[o] = dp; T2[o] = d2;
+      if (Ts) Ts[o] = ps;
+      if (Tt) Tt[o] = dts;
     }
     pl2 = pl1;
     pl1 = p;
   }
 }
 
-// hd[((pt * nf) + slot) * 42 + k]; one block of 8 warps per (frequency, point):
-// the block forms w_l = (2l+1)/(4 pi) taper_l in shared memory, each warp then
-// takes every eighth sum and its lanes every 32nd degree
-constexpr int CPL_SUM_THREADS = 256;
-__global__ void __launch_bounds__(CPL_SUM_THREADS) cpl_sums_kernel(CplDev S, const float* __restrict__ gr,
-                                                                   const float* __restrict__ gi,
-                                                                   const double* __restrict__ tab, double2* hd) {
-  extern __shared__ double wl[];
-  const int pt = blockIdx.x, slot = blockIdx.y;
-  const int jf = S.nf1 + slot, nf = S.nf2 - S.nf1 + 1;
-  const int nwn = S.nwn[jf - 1], lmax = nwn - 1;
-  // cos^2 taper of this frequency (harmonicDegreeSums.f90:356-369), TAPFRAC = 0.2
-  const double tapfrac = 0.2;
-  int jt = (int)floor((double)lmax * (1.0 - tapfrac) + 0.5);
-  jt = jt < lmax ? jt : lmax;
-  jt = jt > 1 ? jt : 1;
-  const double c1 = (double)lmax * tapfrac * 2.0 / PI_F;
-  const double c2 = (1.0 - tapfrac) / tapfrac * 0.5 * PI_F;
-  for (int l = threadIdx.x; l < nwn; l += blockDim.x) {
+// A[aoff[kind] + row * lcap + l], row = 2 (slot nsk[kind] + rank) + re/im: the
+// terms of sum k of frequency nf1 + slot without the table value, zero outside
+// the sum's degrees; one thread per (slot, sum, degree)
+__global__ void cpl_coef_kernel(CplDev S, const float* __restrict__ gr, const float* __restrict__ gi, double* A) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = S.nf2 - S.nf1 + 1;
+  if (idx >= (long long)nf * S.nsum * S.lcap) return;
+  const int l = (int)(idx % S.lcap);
+  const int k = (int)((idx / S.lcap) % S.nsum);
+  const int slot = (int)(idx / ((long long)S.lcap * S.nsum));
+  const CplSum cs = S.istyp == 1 ? c_cpl[k] : c_cplf[k];
+  const int jf = S.nf1 + slot, nwn = S.nwn[jf - 1], lmax = nwn - 1;
+  double vr = 0.0, vi = 0.0;
+  if (l >= cs.l0 && l <= lmax) {
+    // cos^2 taper of this frequency (harmonicDegreeSums.f90:356-369), TAPFRAC = 0.2
+    const double tapfrac = 0.2;
+    int jt = (int)floor((double)lmax * (1.0 - tapfrac) + 0.5);
+    jt = jt < lmax ? jt : lmax;
+    jt = jt > 1 ? jt : 1;
     double tap = 1.0;
-    if (l >= jt) { const double c = cos((double)(float)l / c1 - c2); tap = c * c; }
-    wl[l] = (2.0 * (double)l + 1.0) / (4.0 * PI_F) * tap;
+    if (l >= jt) {
+      const double c1 = (double)lmax * tapfrac * 2.0 / PI_F;
+      const double c2 = (1.0 - tapfrac) / tapfrac * 0.5 * PI_F;
+      const double c = cos((double)(float)l / c1 - c2);
+      tap = c * c;
+    }
+    double c = (2.0 * (double)l + 1.0) / (4.0 * PI_F) * tap;
+    if (cs.fac != 0.0) c = c * (cs.fac / (double)(float)(l * (l + 1)));
+    const long long o = (long long)cs.col * S.nkf + S.koff[slot] + l;
+    vr = c * (double)gr[o];
+    vi = c * (double)gi[o];
   }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double* tp = tab + (long long)pt * CPL_NKIND * S.lcap;
-  const long long g0 = S.koff[slot];
-  for (int k = warp; k < S.nsum; k += CPL_SUM_THREADS / 32) {
-    const CplSum cs = S.istyp == 1 ? c_cpl[k] : c_cplf[k];
-    const double* T = tp + (long long)cs.kind * S.lcap;
-    const float* gre = gr + (long long)cs.col * S.nkf + g0;
-    const float* gim = gi + (long long)cs.col * S.nkf + g0;
-    double sr = 0.0, si = 0.0;
-    for (int l = cs.l0 + lane; l < nwn; l += 32) {
-      double c = T[l] * wl[l];
-      if (cs.fac != 0.0) c = c * (cs.fac / (double)(float)(l * (l + 1)));
-      sr += c * (double)gre[l];
-      si += c * (double)gim[l];
+  const long long row = 2LL * ((long long)slot * S.nsk[cs.kind] + S.rank[k]);
+  double* Ar = A + S.aoff[cs.kind] + row * S.lcap;
+  Ar[l] = vr;
+  Ar[S.lcap + l] = vi;
+}
+
+// FP64 tiled product C[kind][row][pt] = sum_l A[kind][row][l] * T[kind][l][pt]:
+// 64 x 64 output tile per block of 256 threads, 4 x 4 per thread, K step 16.  A
+// tile's degree loop ends at the largest degree count of its frequencies (the
+// coefficients beyond a frequency's count are zero).
+constexpr int CT_M = 64, CT_N = 64, CT_K = 16;
+__global__ void __launch_bounds__(256) cpl_gemm_kernel(CplDev S, const double* __restrict__ A,
+                                                       const double* __restrict__ T, double* C) {
+  const int kind = blockIdx.z;
+  const int nsk = S.nsk[kind];
+  const int nf = S.nf2 - S.nf1 + 1;
+  const int M = 2 * nf * nsk, N = S.npts;
+  const int m0 = blockIdx.y * CT_M, n0 = blockIdx.x * CT_N;
+  if (m0 >= M) return;
+  int K = 0;
+  {
+    const int s0 = m0 / (2 * nsk), s1 = min(nf - 1, (m0 + CT_M - 1) / (2 * nsk));
+    for (int sl = s0; sl <= s1; ++sl) K = max(K, S.nwn[S.nf1 - 1 + sl]);
+    K = min(K, S.lcap);
+  }
+  const double* Ak = A + S.aoff[kind];
+  const double* Tk = T + (long long)kind * S.lcap * N;
+  double* Ck = C + S.coff[kind];
+  __shared__ double As[CT_K][CT_M + 1];
+  __shared__ double Bs[CT_K][CT_N];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < K; k0 += CT_K) {
+    for (int i = threadIdx.x; i < CT_M * CT_K; i += 256) {
+      const int mm = i / CT_K, kk = i % CT_K;
+      const int gm = m0 + mm, gk = k0 + kk;
+      As[kk][mm] = (gm < M && gk < K) ? Ak[(long long)gm * S.lcap + gk] : 0.0;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      sr += __shfl_xor_sync(0xffffffffu, sr, o);
-      si += __shfl_xor_sync(0xffffffffu, si, o);
+    for (int i = threadIdx.x; i < CT_K * CT_N; i += 256) {
+      const int kk = i / CT_N, nn = i % CT_N;
+      const int gk = k0 + kk, gn = n0 + nn;
+      Bs[kk][nn] = (gk < K && gn < N) ? Tk[(long long)gk * N + gn] : 0.0;
     }
-    if (lane == 0) hd[((long long)pt * nf + slot) * S.nsum + k] = make_double2(sr, si);
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < CT_K; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + ty * 4 + i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gn = n0 + tx * 4 + j;
+      if (gn < N) Ck[(long long)gm * N + gn] = acc[i][j];
+    }
   }
 }
 
@@ -210,7 +279,7 @@ __device__ __forceinline__ void ten_rot(double a, double b, const dz t[3][3], dz
 
 // one thread per (point, frequency): X[(pt * 6 + c) * nf2 + jf - 1], c = displacement
 // (or velocity) x, y, z, traction x, y, z in the box frame (x east, y north)
-__global__ void cpl_point_kernel(CplDev S, const double2* __restrict__ hd, double2* X) {
+__global__ void cpl_point_kernel(CplDev S, const double* __restrict__ C, double2* X) {
   const int nf = S.nf2 - S.nf1 + 1;
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)S.npts * nf) return;
@@ -218,8 +287,10 @@ __global__ void cpl_point_kernel(CplDev S, const double2* __restrict__ hd, doubl
   const int jf = S.nf1 + slot;
   dz w[CPL_NSUM + 1];
   for (int k = 0; k < S.nsum; ++k) {
-    const double2 v = hd[((long long)pt * nf + slot) * S.nsum + k];
-    w[k + 1] = dz{v.x, v.y};
+    const int kind = S.istyp == 1 ? c_cpl[k].kind : c_cplf[k].kind;
+    const long long row = 2LL * ((long long)slot * S.nsk[kind] + S.rank[k]);
+    const double* Ck = C + S.coff[kind] + row * S.npts + pt;
+    w[k + 1] = dz{Ck[0], Ck[S.npts]};
   }
   const double* m = S.mt;
   const double phi = S.xi[pt], dl = S.delta[pt], re = S.re;
@@ -366,20 +437,33 @@ extern "C" int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* 
   std::vector<double2> evf;
   if (p->spectra) evf.assign(p->nf2 + 1, make_double2(0, 0));
   else event_filter_host(&sp, evf);
-  // workspace: tables, sums, spectra, small inputs
+  // sums per table kind and the rank of each sum within its kind
+  const int nsum = p->istyp == 1 ? CPL_NSUM : 21;
+  const CplSum* sums = p->istyp == 1 ? h_cpl : h_cplf;
+  CplDev S{};
+  for (int k = 0; k < nsum; ++k) S.rank[k] = S.nsk[sums[k].kind]++;
   const int lcap = p->nwnmax;
+  long long ao = 0, co = 0;
+  for (int kd = 0; kd < CPL_NKIND; ++kd) {
+    S.aoff[kd] = ao; S.coff[kd] = co;
+    ao += 2LL * nf * S.nsk[kd] * lcap;
+    co += 2LL * nf * S.nsk[kd] * npts;
+  }
+  // workspace: tables, coefficient rows, sums, spectra, small inputs
   const size_t b_tab = align256((size_t)npts * CPL_NKIND * lcap * sizeof(double));
-  const size_t b_hd = align256((size_t)npts * nf * (p->istyp == 1 ? CPL_NSUM : 21) * sizeof(double2));
+  const size_t b_a = align256((size_t)ao * sizeof(double));
+  const size_t b_hd = align256((size_t)co * sizeof(double));
   const size_t b_x = align256((size_t)npts * 6 * p->nf2 * sizeof(double2));
   const size_t b_in = align256((size_t)nf * sizeof(int)) + align256((size_t)p->nf2 * sizeof(int)) +
                       3 * align256((size_t)npts * 3 * sizeof(double)) + align256(evf.size() * sizeof(double2)) +
                       align256((size_t)p->nf2 * 7 * sizeof(double2));
-  char* ws = (char*)gem_ctx_aux(ctx, 12, b_tab + b_hd + b_x + b_in);
+  char* ws = (char*)gem_ctx_aux(ctx, 12, b_tab + b_a + b_hd + b_x + b_in);
   if (!ws) return GEM_ERROR;
   double* tab = (double*)ws;
-  double2* hd = (double2*)(ws + b_tab);
-  double2* X = p->spectra ? (double2*)d_spec : (double2*)(ws + b_tab + b_hd);
-  char* q = ws + b_tab + b_hd + b_x;
+  double* A = (double*)(ws + b_tab);
+  double* C = (double*)(ws + b_tab + b_a);
+  double2* X = p->spectra ? (double2*)d_spec : (double2*)(ws + b_tab + b_a + b_hd);
+  char* q = ws + b_tab + b_a + b_hd + b_x;
   auto take = [&](size_t bytes) { char* r = q; q += align256(bytes); return r; };
   int* d_koff = (int*)take((size_t)nf * sizeof(int));
   int* d_nwn = (int*)take((size_t)p->nf2 * sizeof(int));
@@ -398,21 +482,21 @@ extern "C" int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* 
           cudaSuccess ||
       cudaMemsetAsync(X, 0, (size_t)npts * 6 * p->nf2 * sizeof(double2), st) != cudaSuccess)
     return gem_set_error(ctx, "coupling: input copy failed");
-  CplDev S{};
   S.nf1 = p->nf1; S.nf2 = p->nf2; S.npts = npts; S.lcap = lcap; S.spectra = p->spectra; S.nkf = p->nkfmax;
   S.df = p->df; S.sigma = p->sigma; S.re = p->re; S.tred = p->tred;
   S.thetas = p->thetas; S.phis = p->phis; S.thetac = p->thetac; S.phic = p->phic;
-  S.istyp = p->istyp; S.nsum = p->istyp == 1 ? CPL_NSUM : 21;
+  S.istyp = p->istyp; S.nsum = nsum;
   for (int i = 0; i < (p->istyp == 1 ? 6 : 3); ++i) S.mt[i] = mt[i];
   S.nwn = d_nwn; S.koff = d_koff; S.delta = d_delta; S.xi = d_xi; S.nrm = d_nrm; S.evf = d_evf; S.zel = d_zel;
   cpl_legendre_kernel<<<(npts * 3 + 127) / 128, 128, 0, st>>>(npts, p->nwnmax - 1, lcap, d_delta, tab);
-  const size_t smem = (size_t)p->nwnmax * sizeof(double);
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(cpl_sums_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return gem_set_error(ctx, "coupling: too many degrees for the shared-memory weights");
-  cpl_sums_kernel<<<dim3((unsigned)npts, (unsigned)nf), CPL_SUM_THREADS, smem, st>>>(S, d_gr, d_gi, tab, hd);
+  const long long ncoef = (long long)nf * nsum * lcap;
+  cpl_coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, A);
+  int maxnsk = 0;
+  for (int kd = 0; kd < CPL_NKIND; ++kd) maxnsk = std::max(maxnsk, S.nsk[kd]);
+  const dim3 ggrid((unsigned)((npts + CT_N - 1) / CT_N), (unsigned)((2 * nf * maxnsk + CT_M - 1) / CT_M), CPL_NKIND);
+  cpl_gemm_kernel<<<ggrid, 256, 0, st>>>(S, A, tab, C);
   const long long nthr = (long long)npts * nf;
-  cpl_point_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, st>>>(S, hd, X);
+  cpl_point_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, st>>>(S, C, X);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return gem_set_error(ctx, cudaGetErrorString(e));
   if (p->spectra) return GEM_OK;
