@@ -174,12 +174,16 @@ __global__ void cpl_coef_kernel(CplDev S, const float* __restrict__ gr, const fl
 }
 
 // FP64 tiled product C[kind][row][pt] = sum_l A[kind][row][l] * T[kind][l][pt]:
-// 64 x 64 output tile per block of 256 threads, 4 x 4 per thread, K step 16.  A
+// 128 x 128 output tile per block of 256 threads, 8 x 8 per thread (rows ty + 16 i,
+// points tx + 16 j: conflict-free shared reads, coalesced stores), K step 16.  The
+// next K tile is loaded into registers while the current one is multiplied.  A
 // tile's degree loop ends at the largest degree count of its frequencies (the
 // coefficients beyond a frequency's count are zero).
-constexpr int CT_M = 64, CT_N = 64, CT_K = 16;
-__global__ void __launch_bounds__(256) cpl_gemm_kernel(CplDev S, const double* __restrict__ A,
-                                                       const double* __restrict__ T, double* C) {
+constexpr int CT_M = 128, CT_N = 128, CT_K = 16;
+constexpr int CT_LOADS = CT_M * CT_K / 256;   // elements of each operand tile per thread
+static_assert(CT_M * CT_K == CT_N * CT_K && CT_LOADS == 8, "tile shape");
+__global__ void __launch_bounds__(256, 1) cpl_gemm_kernel(CplDev S, const double* __restrict__ A,
+                                                          const double* __restrict__ T, double* C) {
   const int kind = blockIdx.z;
   const int nsk = S.nsk[kind];
   const int nf = S.nf2 - S.nf1 + 1;
@@ -197,41 +201,58 @@ __global__ void __launch_bounds__(256) cpl_gemm_kernel(CplDev S, const double* _
   double* Ck = C + S.coff[kind];
   __shared__ double As[CT_K][CT_M + 1];
   __shared__ double Bs[CT_K][CT_N];
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += CT_K) {
-    for (int i = threadIdx.x; i < CT_M * CT_K; i += 256) {
-      const int mm = i / CT_K, kk = i % CT_K;
-      const int gm = m0 + mm, gk = k0 + kk;
-      As[kk][mm] = (gm < M && gk < K) ? Ak[(long long)gm * S.lcap + gk] : 0.0;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  double ra[CT_LOADS], rb[CT_LOADS];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < CT_LOADS; ++q) {
+      const int i = tid + 256 * q;
+      const int gm = m0 + i / CT_K, gk = k0 + i % CT_K;
+      ra[q] = (gm < M && gk < K) ? Ak[(long long)gm * S.lcap + gk] : 0.0;
     }
-    for (int i = threadIdx.x; i < CT_K * CT_N; i += 256) {
-      const int kk = i / CT_N, nn = i % CT_N;
-      const int gk = k0 + kk, gn = n0 + nn;
-      Bs[kk][nn] = (gk < K && gn < N) ? Tk[(long long)gk * N + gn] : 0.0;
+#pragma unroll
+    for (int q = 0; q < CT_LOADS; ++q) {
+      const int i = tid + 256 * q;
+      const int gk = k0 + i / CT_N, gn = n0 + i % CT_N;
+      rb[q] = (gk < K && gn < N) ? Tk[(long long)gk * N + gn] : 0.0;
+    }
+  };
+  if (K > 0) load(0);
+  for (int k0 = 0; k0 < K; k0 += CT_K) {
+#pragma unroll
+    for (int q = 0; q < CT_LOADS; ++q) {
+      const int i = tid + 256 * q;
+      As[i % CT_K][i / CT_K] = ra[q];
+      Bs[i / CT_N][i % CT_N] = rb[q];
     }
     __syncthreads();
+    if (k0 + CT_K < K) load(k0 + CT_K);
 #pragma unroll
     for (int kk = 0; kk < CT_K; ++kk) {
-      double a[4], b[4];
+      double a[8], b[8];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+      for (int i = 0; i < 8; ++i) a[i] = As[kk][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+      for (int j = 0; j < 8; ++j) b[j] = Bs[kk][tx + 16 * j];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int gm = m0 + ty * 4 + i;
+  for (int i = 0; i < 8; ++i) {
+    const int gm = m0 + ty + 16 * i;
     if (gm >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int gn = n0 + tx * 4 + j;
+    for (int j = 0; j < 8; ++j) {
+      const int gn = n0 + tx + 16 * j;
       if (gn < N) Ck[(long long)gm * N + gn] = acc[i][j];
     }
   }
