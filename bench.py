@@ -155,6 +155,35 @@ def cpu_baseline(w, nsample, seed=12345):
                       % (len(pick), seed, len(items), dt)}
 
 
+def cpu_baseline_traces(w, g, nsp, nsta_sample, seed=12345):
+    """CPU FP64 oracle of the synthetics on a random sample of the workload's stations
+    (all six moment tensors, the same seeded FK coefficients), one station per host thread."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from gemini_unified_b200 import configs
+    from gemini_unified_b200.synth_run import fk_coefficients
+    gr, gi = fk_coefficients(nsp, int(g.nkfmax))
+    theta, phi, propdir = w.stations()
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(len(theta), size=min(nsta_sample, len(theta)), replace=False)
+    mt = configs.unit_moment_tensors()
+    ncores = os.cpu_count() or 1
+
+    def one(i):
+        oracle.synthetics(g.nf1, g.nf2, g.nwn, g.nwnmax, g.df, g.sigma, gr, gi, theta[i:i + 1], phi[i:i + 1],
+                          propdir[i:i + 1], mt, w.filspecs, True, 0.0, w.nsamp, w.dt)
+
+    t = time.perf_counter()
+    with cf.ThreadPoolExecutor(ncores) as ex_:
+        list(ex_.map(one, pick))
+    dt = time.perf_counter() - t
+    ntr = len(pick) * len(mt)
+    return {"value": ntr / dt, "unit": "traces/s", "cores": ncores, "kind": "port",
+            "sample": "%d stations drawn uniformly (seed %d) from the %d of the workload, 6 moment tensors each "
+                      "(%d three-component traces of %d samples); %.1f s" % (len(pick), seed, len(theta), ntr,
+                                                                           w.nsamp, dt)}
+
+
 def run_reference(args, rank, size):
     from gemini_unified_b200 import configs
     w = configs.WORKLOADS[args.workload]
@@ -352,6 +381,7 @@ def main():
         if size == 1:
             n = args.cpu_sample or 16384
             line["cpu_baseline"] = cpu_baseline(w, n)
+            line["traces"]["cpu_baseline"] = cpu_baseline_traces(w, g, nsp, 1024)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
