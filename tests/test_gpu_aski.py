@@ -141,3 +141,25 @@ def test_dsv_rejects_fluid_nodes_and_bad_source_sets(aski):
     top = core.node_index(w.rec_radius)
     with pytest.raises(GeminiError, match="fluid"):
         fkc.run_dsv(w.params, top, 10, 10)
+
+
+def test_dsv_regional_mode_matches_oracle(gpu):
+    """Regional (wavenumber) mode on the 8-layer crust: a moment source at an
+    interior node and the force at the receiver, against the oracle's loop over
+    the node range."""
+    import oracle
+    from gemini_unified_b200.fk import GeminiFK
+    w = configs.WORKLOADS["regional_small"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    jf = 40
+    srcs = [3, 12, jre]
+    res = GeminiFK(m, ex).aski_spectra(w.params, srcs, jre, jf, jf, f32=False)
+    ref, st, _ = oracle.Oracle(m, ex).dsv_frequency(M.fk_params_c(w.params, jre), srcs, jf, int(g.nwn[jf - 1]))
+    assert np.all(st == 0)
+    for (_, _, a, sa), b in zip(res, ref):
+        assert np.all(sa == 0)
+        assert np.all(a[:, :, 0] == 0)          # wavenumber 0 stays zero in the regional mode
+        assert _rel(a, b) <= RTOL
