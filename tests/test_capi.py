@@ -56,3 +56,17 @@ def test_product_never_imports_oracle():
         if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
             txt = open(f).read()
             assert "oracle" not in re.sub(r"(#|//).*", "", txt).lower(), f
+
+
+def test_new_entry_points_reject_a_null_context(lib):
+    """The ASKI and coupling entry points return the error level 2 for a null
+    context before touching the GPU; gem_fk_aski_nsp gives the spectra per node."""
+    vp, i = ctypes.c_void_p, ctypes.c_int
+    lib.gem_fk_run_dsv.argtypes = [vp, vp, i, i, vp, vp, vp, vp]
+    lib.gem_fk_run_aski.argtypes = [vp, vp, i, vp, i, i, vp, vp, vp, vp]
+    lib.gem_coupling_run.argtypes = [vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp, vp, vp]
+    lib.gem_fk_aski_nsp.argtypes = [i]
+    assert lib.gem_fk_run_dsv(None, None, 2, 3, None, None, None, None) == 2
+    assert lib.gem_fk_run_aski(None, None, 1, None, 2, 3, None, None, None, None) == 2
+    assert lib.gem_coupling_run(None, None, None, None, None, None, None, 1, None, None, None, None, None) == 2
+    assert lib.gem_fk_aski_nsp(1) == 20 and lib.gem_fk_aski_nsp(0) == 10
