@@ -492,6 +492,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
   L.prop_kopt = nullptr; L.prop_hs = nullptr;
   L.adv_min = 1; L.adv_wait = 0;
+  L.nsrc = 0; L.src_node = nullptr; L.src_type = nullptr; L.src_off = nullptr;
   ctx->last_grid = S.grid[1];
   ctx->last_block = FK_SCHED_BLOCK[S.sched[1]];
   // ---- learned proposer: features / proposals per (phase, item) from the start radii
@@ -575,10 +576,11 @@ int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
 }
 
 // The device work of the ASKI program's FK spectra for a set of source nodes
-// (computeGreenFKSpectraForASKI.f90:451-541): start radii and spheroidal
-// minors once over the node range jsl..jsr of the plan, then per source node
-// (the moment or force sources jsnod[b], then the force at jre) the toroidal
-// phase and the adjoint phase with that node as the source, each writing its
+// (computeGreenFKSpectraForASKI.f90:439-560): start radii; the toroidal phase
+// once, with the minors over the node range jsl..jsr of the plan and the
+// toroidal spectra of every source; the spheroidal minors once over the range;
+// then per source node (the moment or force sources jsnod[b], then the force at
+// jre) the adjoint phase with that node as the source.  Each source writes its
 // own output block (block b at b * blk_m; the force block is blk_f long).
 int fk_enqueue_aski(gem_ctx* ctx, SlabPlan& S, int nsnod, const int* jsnod, int jre, int istyp, float* gre,
                     float* gim, double* g64, size_t blk_m, size_t blk_f, cudaStream_t st) {
@@ -607,8 +609,32 @@ int fk_enqueue_aski(gem_ctx* ctx, SlabPlan& S, int nsnod, const int* jsnod, int 
   FKLaunch L0 = S.L;
   L0.prop_kopt = nullptr; L0.prop_hs = nullptr;
   CK(launch(-1, S.P, L0));
+  // source table of the toroidal phase: nodes, types and output offsets
+  const int nsrc = nsnod + 1;
+  char* tabs = (char*)gem_ctx_aux(ctx, 14, (size_t)nsrc * (2 * sizeof(int) + sizeof(long long)) + 64);
+  if (!tabs) return GEM_ERROR;
+  std::vector<long long> h_off(nsrc);
+  std::vector<int> h_node(nsrc), h_type(nsrc);
+  for (int b = 0; b < nsrc; ++b) {
+    h_node[b] = b == nsnod ? jre : jsnod[b];
+    h_type[b] = b == nsnod ? 0 : istyp;
+    h_off[b] = (long long)((size_t)b * blk_m);
+  }
+  long long* d_off = (long long*)tabs;
+  int* d_node = (int*)(tabs + (size_t)nsrc * sizeof(long long));
+  int* d_type = d_node + nsrc;
+  CK(cudaMemcpyAsync(d_off, h_off.data(), (size_t)nsrc * sizeof(long long), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_node, h_node.data(), (size_t)nsrc * sizeof(int), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_type, h_type.data(), (size_t)nsrc * sizeof(int), cudaMemcpyHostToDevice, st));
+  FKLaunch Lt = L0;
+  Lt.gf64 = reinterpret_cast<double2*>(g64); Lt.gfre = gre; Lt.gfim = gim;
+  Lt.nsrc = nsrc; Lt.src_node = d_node; Lt.src_type = d_type; Lt.src_off = d_off;
+  nvtxRangePushA("gem_fk: toroidal phase over the source-node range");
+  cudaError_t le = launch(0, S.P, Lt);
+  nvtxRangePop();
+  CK(le);
   nvtxRangePushA("gem_fk: spheroidal phase over the source-node range");
-  const cudaError_t le = launch(1, S.P, L0);
+  le = launch(1, S.P, L0);
   nvtxRangePop();
   CK(le);
   for (int b = 0; b <= nsnod; ++b) {
@@ -625,7 +651,6 @@ int fk_enqueue_aski(gem_ctx* ctx, SlabPlan& S, int nsnod, const int* jsnod, int 
     Lb.gfim = gim ? gim + off : nullptr;
     Lb.dets = reinterpret_cast<double2*>(ctx->d_dets) + (size_t)(js - S.P.jsl) * S.nkf;
     CK(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned int), st));
-    CK(launch(0, Pb, Lb));
     CK(launch(2, Pb, Lb));
   }
   // totals only: the per-phase split is not recorded for a set of sources

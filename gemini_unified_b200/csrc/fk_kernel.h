@@ -73,6 +73,12 @@ struct FKLaunch {
   // deferral of the bookkeeping between integrations: a pass runs when
   // adv_min lanes wait, one has waited adv_wait trips, or none integrates
   int adv_min, adv_wait;
+  // toroidal phase of a set of source nodes (nsrc > 0): per source its node, type
+  // (0 force, 1 moment) and the element offset of its output block
+  int nsrc;
+  const int* src_node;
+  const int* src_type;
+  const long long* src_off;
 };
 
 // One Bulirsch-Stoer step attempt as the step log records it (32 bytes).

@@ -286,8 +286,8 @@ __device__ double adjoint_htry(const FKStatic& P, Env& e, double ra, double re) 
   return ((0.25 * v) * TWO_PI_F) / e.omre;
 }
 
-// moment / force source terms at node n (sourceTerms.f90:59-118)
-__device__ void source_terms(const FKStatic& P, const Env& e, int n, dz zsph[4][4], dz ztor[2][2]) {
+// moment (istyp 1) / force (0) source terms at node n (sourceTerms.f90:59-118)
+__device__ void source_terms_of(const FKStatic& P, const Env& e, int n, int istyp, dz zsph[4][4], dz ztor[2][2]) {
   const double r = P.rnod[n];
   const bool fluid = P.state[n] == 1;
   const double rr2 = 1.0 / (r * r), rr3 = rr2 / r, elp1 = e.dll1, om = e.omre;
@@ -295,7 +295,7 @@ __device__ void source_terms(const FKStatic& P, const Env& e, int n, dz zsph[4][
   eval_spline<0x0Eu>(P, e, r, P.layer[n], ro, el);
   for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) zsph[i][j] = dz{0, 0};
   for (int i = 0; i < 2; ++i) for (int j = 0; j < 2; ++j) ztor[i][j] = dz{0, 0};
-  if (P.istyp == 1) {
+  if (istyp == 1) {
     if (fluid) {
       zsph[0][0] = rr2 * (1.0 / el[1] - (elp1 * rr2) / ((om * om) * ro));
       zsph[1][0] = dz{rr3 * 2.0, 0};
@@ -322,6 +322,10 @@ __device__ void source_terms(const FKStatic& P, const Env& e, int n, dz zsph[4][
       ztor[1][0] = dz{0.5 * rr2, 0};
     }
   }
+}
+
+__device__ __forceinline__ void source_terms(const FKStatic& P, const Env& e, int n, dz zsph[4][4], dz ztor[2][2]) {
+  source_terms_of(P, e, n, P.istyp, zsph, ztor);
 }
 
 __device__ __forceinline__ void put_out(const FKStatic& P, const FKLaunch& LL, int k, int isp, int n, dz v) {
@@ -425,6 +429,26 @@ __device__ void output_dsv_tor_node(const FKStatic& P, const Env& e, const dz ti
   int isp = 4 * P.njsph;
   for (int j = 0; j < P.njtor; ++j) put_out(P, LL, k, isp++, n, g[0][j]);
   for (int j = 0; j < P.njtor; ++j) put_out(P, LL, k, isp++, n, d[0][j]);
+}
+
+// toroidal part of node n for one source of a set (node jsh, type ty) into that
+// source's output block at element offset off
+__device__ void output_dsv_tor_src(const FKStatic& P, const Env& e, const dz ti[2][2], int n, const FKLaunch& LL,
+                                   int k, int jsh, int ty, long long off) {
+  dz zsph[4][4], ztor[2][2];
+  source_terms_of(P, e, jsh, ty, zsph, ztor);
+  const int njsph = ty == 0 ? 2 : 4, njtor = ty == 0 ? 1 : 2, nsp = 4 * njsph + 2 * njtor;
+  dz g[2][2], d[2][2];
+  for (int j = 0; j < njtor; ++j)
+    for (int i = 0; i < 2; ++i) g[i][j] = (dz{0.0, 0.0} + ti[i][0] * ztor[0][j]) + ti[i][1] * ztor[1][j];
+  dsv_tor_derivative(P, e, P.rnod[n], njtor, g, d);
+  for (int q = 0; q < 2 * njtor; ++q) {
+    const dz v = q < njtor ? g[0][q] : d[0][q - njtor];
+    const long long o = off + k + LL.nkf * ((long long)(4 * njsph + q) + (long long)nsp * (n - 1));
+    if (LL.gf64) LL.gf64[o] = make_double2(v.re, v.im);
+    if (LL.gfre) LL.gfre[o] = (float)v.re;
+    if (LL.gfim) LL.gfim[o] = (float)v.im;
+  }
 }
 
 // spheroidal spectra of node n: reciprocity (reciprocity.f90:82-153) and
@@ -589,8 +613,9 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
           for (int el = 0; el < 4 * lay.NN; ++el) s.put(el, dz{0.0, 0.0});
           L.up = 0;
           L.st = S_TOR_DONE;
-          if (L.e.dll1 < EPS_D || L.rstart_t >= P.rnod[jre]) { L.st = S_ITEM_END; break; }
-          double rmin = fmax(L.rstart_t, P.rnod[jre]);
+          // minors over the source-node range jsl..jsr (toroidalMinors.f90:129-160)
+          if (L.e.dll1 < EPS_D || L.rstart_t >= P.rnod[P.jsr]) { L.st = S_ITEM_END; break; }
+          double rmin = fmax(L.rstart_t, P.rnod[P.jsl]);
           dz ys[5]; double htry, rsurf; int nl;
           int rc = toroidal_surface_iv(P, L.e, ys, htry, rsurf, nl);
           if (rc) { FAIL(rc); break; }
@@ -641,7 +666,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
       // ---------------- toroidal phase
       case S_TOR_UP: {   // toroidalMinors.f90:206-240
         if (L.jr - L.jl < 0) { FAIL(ST_BOOKKEEPING); break; }
-        double rmax = fmin(P.rnod[jre], L.rend);
+        double rmax = fmin(P.rnod[P.jsr], L.rend);
         int nl, top;
         layer_index(P, L.rstart_t, nl, top);
         if (top == 1) nl = nl + 1;
@@ -655,6 +680,38 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
       }
       case S_TOR_DONE: {   // determinant and toroidal UJGF (unitJumpGreenFunctions.f90:147-175)
         if (L.jr - L.jl < 0) { FAIL(ST_BOOKKEEPING); break; }
+        if constexpr (PH == PH_TOR) {
+          if (LL.nsrc > 0) {   // every source node of a set, each into its own output block
+            for (int b = 0; b < LL.nsrc; ++b) {
+              const int jsh = LL.src_node[b], ty = LL.src_type[b];
+              const dz det =
+                  s.get(lay.ut(jsh, 0)) * s.get(lay.dt(jsh, 1)) - s.get(lay.dt(jsh, 0)) * s.get(lay.ut(jsh, 1));
+              if (!(zabs(det) > TINY_D)) continue;
+              const int mask = ty == 1 ? 3 : 2;
+              dz dcoef[2], ecoef[2];
+              for (int j = 0; j < 2; ++j) {
+                double u1 = j == 0 ? 1.0 : 0.0, u2 = j == 1 ? 1.0 : 0.0;
+                dcoef[j] = (u2 * s.get(lay.dt(jsh, 0)) - u1 * s.get(lay.dt(jsh, 1))) / det;
+                ecoef[j] = (u2 * s.get(lay.ut(jsh, 0)) - u1 * s.get(lay.ut(jsh, 1))) / det;
+              }
+              for (int n = 1; n <= nnod; ++n) {
+                dz ti[2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};   // [comp][jump]
+                for (int j = 0; j < 2; ++j) {
+                  if (!(mask & (1 << j))) continue;
+                  if (n < jsh) {
+                    if (P.state[n] == 0 && P.rnod[n] > L.rstart_t)
+                      for (int c = 0; c < 2; ++c) ti[c][j] = dcoef[j] * s.get(lay.ut(n, c));
+                  } else if (P.state[n] == 0) {
+                    for (int c = 0; c < 2; ++c) ti[c][j] = ecoef[j] * s.get(lay.dt(n, c));
+                  }
+                }
+                output_dsv_tor_src(P, L.e, ti, n, LL, L.k, jsh, ty, LL.src_off[b]);
+              }
+            }
+            L.st = S_ITEM_END;
+            break;
+          }
+        }
         L.det = s.get(lay.ut(jre, 0)) * s.get(lay.dt(jre, 1)) - s.get(lay.dt(jre, 0)) * s.get(lay.ut(jre, 1));
         if (!(zabs(L.det) > TINY_D)) { L.st = S_ITEM_END; break; }
         // jumps whose Green functions are stored: the DSV spectra of a moment
