@@ -104,3 +104,26 @@ def test_aski_first_frequency():
     assert M.aski_nf1(dataclasses.replace(p, fmin=5.0 / 1024.0)) == 6
     assert M.frequency_grid(dataclasses.replace(p, fmin=5.0 / 1024.0), 6371000.0).nf1 == 5
     assert M.nsp_dsv("MOMENT") == 20 and M.nsp_dsv("FORCE") == 10
+
+
+def test_dsv_spectra_obey_reciprocity_in_the_regional_mode():
+    """The same reciprocity in the regional (wavenumber) mode on the 8-layer crust:
+    U, V and W at the receiver of moment sources at two crustal nodes against the
+    synthetics program's spectra of those sources (wavenumbers 2..299)."""
+    w = configs.WORKLOADS["regional_small"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    jf, hi = 40, 300
+    n = int(g.nwn[jf - 1])
+    o = oracle.Oracle(m, ex)
+    pc = M.fk_params_c(w.params, jre)
+    out, st, _ = o.dsv_frequency(pc, [3, 12, jre], jf, n, 1, hi)
+    syn, sts, _ = o.fk_frequency(pc, jf, n, M.nsp_for(w.params), 1, hi)
+    assert np.all(st == 0) and np.all(sts == 0)
+    for i, s in enumerate([3, 12]):
+        a = out[i][jre - 1][:, 1:hi]
+        b = syn[s - 1][:, 1:hi]
+        assert np.abs(a[0:8] - b[0:8]).max() / np.abs(b[0:8]).max() < 5e-4, s
+        assert np.abs(a[16:18] - b[8:10]).max() / np.abs(b[8:10]).max() < 5e-4, s
