@@ -44,6 +44,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "(ω,ℓ) ODE solves/s + seismogram traces/s on 1 B200 vs plain GPU at ≤1e-5 err"
 WORKLOAD = "batched_fk"
+REF_SAMPLE = 16384   # (omega, l) items of a CPU baseline step
 
 
 def parse():
@@ -126,8 +127,9 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(w, nsample, seed=12345):
-    """CPU FP64 oracle on a random sample of the workload's items, all host threads."""
+def cpu_baseline(w, nsample, seed=12345, keep=False):
+    """CPU FP64 oracle on a random sample of the workload's items, all host threads.
+    keep: also return the sampled items and their oracle spectra [item][node][spectrum]."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from gemini_unified_b200 import model as M
@@ -144,24 +146,30 @@ def cpu_baseline(w, nsample, seed=12345):
 
     def one(it):
         jf, iwn = it
-        o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), M.nsp_for(w.params), iwn, iwn)
+        spec = o.fk_frequency(pc, jf, int(g.nwn[jf - 1]), M.nsp_for(w.params), iwn, iwn)[0]
+        return spec[:, :, iwn - 1].copy() if keep else None
 
     t = time.perf_counter()
     with cf.ThreadPoolExecutor(ncores) as ex_:
-        list(ex_.map(one, pick))
+        specs = list(ex_.map(one, pick))
     dt = time.perf_counter() - t
-    return {"value": len(pick) / dt, "unit": "solves/s", "cores": ncores, "kind": "port",
-            "sample": "%d (omega,l) items drawn uniformly (seed %d) from the %d of the workload; %.1f s"
-                      % (len(pick), seed, len(items), dt)}
+    cb = {"value": len(pick) / dt, "unit": "solves/s", "cores": ncores, "kind": "port",
+          "sample": "%d (omega,l) items drawn uniformly (seed %d) from the %d of the workload; %.1f s"
+                    % (len(pick), seed, len(items), dt)}
+    return (cb, pick, np.stack(specs)) if keep else cb
 
 
 def cpu_baseline_traces(w, g, nsp, nsta_sample, seed=12345):
     """CPU FP64 oracle of the synthetics on a random sample of the workload's stations
-    (all six moment tensors, the same seeded FK coefficients), one station per host thread."""
+    (all six moment tensors, the same seeded FK coefficients and float32-rounded df and
+    sigma as the GPU call), one station per host thread.  Returns the baseline, the
+    sampled station indices and the oracle traces [station][mt][component][sample]."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from gemini_unified_b200 import configs
+    from gemini_unified_b200.fk import synth_params
     from gemini_unified_b200.synth_run import fk_coefficients
+    sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs)
     gr, gi = fk_coefficients(nsp, int(g.nkfmax))
     theta, phi, propdir = w.stations()
     rng = np.random.default_rng(seed)
@@ -170,18 +178,19 @@ def cpu_baseline_traces(w, g, nsp, nsta_sample, seed=12345):
     ncores = os.cpu_count() or 1
 
     def one(i):
-        oracle.synthetics(g.nf1, g.nf2, g.nwn, g.nwnmax, g.df, g.sigma, gr, gi, theta[i:i + 1], phi[i:i + 1],
-                          propdir[i:i + 1], mt, w.filspecs, True, 0.0, w.nsamp, w.dt)
+        return oracle.synthetics(g.nf1, g.nf2, g.nwn, g.nwnmax, sp.df, sp.sigma, gr, gi, theta[i:i + 1],
+                                 phi[i:i + 1], propdir[i:i + 1], mt, w.filspecs, False, 0.0, w.nsamp, w.dt)
 
     t = time.perf_counter()
     with cf.ThreadPoolExecutor(ncores) as ex_:
-        list(ex_.map(one, pick))
+        traces = list(ex_.map(one, pick))
     dt = time.perf_counter() - t
     ntr = len(pick) * len(mt)
-    return {"value": ntr / dt, "unit": "traces/s", "cores": ncores, "kind": "port",
-            "sample": "%d stations drawn uniformly (seed %d) from the %d of the workload, 6 moment tensors each "
-                      "(%d three-component traces of %d samples); %.1f s" % (len(pick), seed, len(theta), ntr,
-                                                                           w.nsamp, dt)}
+    cb = {"value": ntr / dt, "unit": "traces/s", "cores": ncores, "kind": "port",
+          "sample": "%d stations drawn uniformly (seed %d) from the %d of the workload, 6 moment tensors each "
+                    "(%d three-component traces of %d samples); %.1f s" % (len(pick), seed, len(theta), ntr,
+                                                                         w.nsamp, dt)}
+    return cb, pick, np.concatenate(traces, axis=0)
 
 
 def run_reference(args, rank, size):
@@ -189,7 +198,10 @@ def run_reference(args, rank, size):
     w = configs.WORKLOADS[args.workload]
     if rank != 0:
         return
-    n = args.cpu_sample or 48
+    # the same 16,384-item sample as the cpu_baseline of the GPU arm: at 16 host
+    # threads that is ~1000 items per thread, so the tail of the thread pool is
+    # small against the step (a few items per thread read ~1.8x slow)
+    n = args.cpu_sample or REF_SAMPLE
     for _ in range(args.warmup):
         cpu_baseline(w, max(8, n // 8), seed=1)
     vals = []
@@ -378,14 +390,54 @@ def main():
             "gpu_launches_traces": SYNTH_LAUNCHES * traces.pop("steps_timed", max(1, min(args.steps, 3))),
             "clocks": clk,
         }
+        out_fast = line["traces"].pop("_out")
         if size == 1:
-            n = args.cpu_sample or 16384
-            line["cpu_baseline"] = cpu_baseline(w, n)
-            line["traces"]["cpu_baseline"] = cpu_baseline_traces(w, g, nsp, 1024)
+            n = args.cpu_sample or REF_SAMPLE
+            cb, pick, ref = cpu_baseline(w, n, keep=True)
+            line["cpu_baseline"] = cb
+            fk_step(fast)   # untimed: the plain form's timing overwrote the output buffers
+            torch.cuda.synchronize()
+            line["error_vs_oracle"] = fk_error_vs_oracle(g, nsp, ex.nnod, gre, gim, pick, ref)
+            cbt, sta, ref_tr = cpu_baseline_traces(w, g, nsp, 1024)
+            line["traces"]["cpu_baseline"] = cbt
+            from gemini_unified_b200.synth_run import trace_errors
+            line["traces"]["error_vs_oracle"] = dict(
+                trace_errors(out_fast[torch.as_tensor(sta, device=dev)], torch.from_numpy(ref_tr).to(dev)),
+                stations=len(sta), note="mixed form of the timed run against the CPU FP64 oracle on the sampled "
+                                        "stations (all six moment tensors)")
+        del out_fast
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fk_error_vs_oracle(g, nsp, nnod, gre, gim, pick, ref):
+    """float32 spectra of the timed run (device, Fortran order (nkf, nsp, nnod)) against the
+    CPU FP64 oracle on the sampled items: |gpu - oracle| relative to the largest value of each
+    spectrum (node, component) of the item's frequency, over all the sample's values."""
+    import torch
+    nkf = int(g.nkfmax)
+    gr = gre[: nkf * nsp * nnod].view(nnod, nsp, nkf)
+    gi = gim[: nkf * nsp * nnod].view(nnod, nsp, nkf)
+    koff = np.concatenate([[0], np.cumsum(g.nwn[g.nf1 - 1: g.nf2])]).astype(np.int64)
+    jfs = sorted({jf for jf, _ in pick})
+    scale = {}
+    for jf in jfs:
+        a, b = int(koff[jf - g.nf1]), int(koff[jf - g.nf1 + 1])
+        mag = torch.sqrt(gr[:, :, a:b].double() ** 2 + gi[:, :, a:b].double() ** 2)
+        scale[jf] = torch.nan_to_num(mag, nan=0.0).amax(dim=-1).cpu().numpy()
+    ks = np.array([koff[jf - g.nf1] + iwn - 1 for jf, iwn in pick], np.int64)
+    kt = torch.as_tensor(ks, device=gre.device)
+    got = (gr[:, :, kt].double().cpu().numpy() + 1j * gi[:, :, kt].double().cpu().numpy()).transpose(2, 0, 1)
+    sc = np.stack([scale[jf] for jf, _ in pick])
+    nan_ok = bool(np.array_equal(np.isnan(got), np.isnan(ref)))
+    ok = ~np.isnan(ref) & (sc > 0)
+    rel = np.abs(got - ref)[ok] / sc[ok]
+    return {"items": len(pick), "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
+            "nan_positions_equal": nan_ok,
+            "note": "float32 spectra of the timed fast run against the CPU FP64 oracle (float32 rounding is "
+                    "6e-8); the FP64 outputs are held to 1e-8 by the GPU tests"}
 
 
 def time_traces(args, w, m, g, nsp, dev, stream, dist, rank, size, timed):
@@ -464,18 +516,19 @@ def time_traces(args, w, m, g, nsp, dev, stream, dist, rank, size, timed):
                            "form": "FP64 tiled degree-sum products (CUDA cores) + reference radix-2 inverse FFT",
                            "speedup_of_value": t_plain / t_fast},
             "error_vs_plain_fp64": err,
+            "_out": out_fast,
             "e2e": {"value": ntr / e2e_s, "unit": "traces/s", "h2d_bytes_per_step": int(gr_h.nbytes * 2),
                     "d2h_bytes_per_step": int(tr_h.nbytes)}}
 
 
 def fp64_peak_tflops(device):
-    """FP64 FMA throughput measured with the library's probe kernel (this run)."""
+    """FP64 FMA throughput measured with the benchmark's own probe kernel (this run);
+    the probe lives in libgem_bench_probe.so, outside the product library."""
     import ctypes
-    from gemini_unified_b200.fk import lib
-    L = lib()
+    from gemini_unified_b200 import build
     try:
-        f = L.gem_probe_fp64_tflops
-    except AttributeError:
+        f = ctypes.CDLL(build.PROBE_LIB).gem_probe_fp64_tflops
+    except (OSError, AttributeError):
         return {"tflops": 37.0, "source": "nominal B200 FP64 (no probe)"}
     f.restype = ctypes.c_double
     f.argtypes = [ctypes.c_int]

@@ -1,8 +1,7 @@
-// FP64 FMA throughput probe, used by the benchmark as the denominator of the
-// solver's FP64 roofline (the measured-peaks file holds HBM and bf16 only).
+// FP64 FMA throughput probe of the benchmark, the denominator of the solver's
+// FP64 roofline (the measured-peaks file holds HBM and bf16 only).  Built as its
+// own library (libgem_bench_probe.so); the product library does not contain it.
 #include <cuda_runtime.h>
-
-#include "../../include/gemini_fk.h"
 
 namespace {
 __global__ void fma_chain(double* out, int iters, double a, double b) {

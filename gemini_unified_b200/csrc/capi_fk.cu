@@ -70,6 +70,7 @@ struct gem_ctx {
   void* d_aux[16] = {};
   size_t aux_cap[16] = {};
   int kopt = 6;   // order target of the step-size control (gem_order_target; fast backend)
+  unsigned long long tc_wait_ns = 0;   // pipeline wait limit of the tensor-core sums (gem_tc_wait_limit; 0: 1 s)
   int dsv = 0;    // set by gem_fk_run_dsv* for the length of one run: DSV spectra with derivatives
   int jsl = 0, jsr = 0;   // set by gem_fk_run_aski* for one run: node range of the minors (0: the receiver)
   // schedule of each solver phase (index into FK_SCHED_*), per build: [0] plain, [1] fast
@@ -197,6 +198,7 @@ int gem_set_error(gem_ctx* ctx, const char* msg) { return fail(ctx, "%s", msg); 
 void gem_note_synth_ms(gem_ctx* ctx, float ms) { if (ctx) ctx->stats.synth_ms = ms; }
 int gem_ctx_device(const gem_ctx* ctx) { return ctx->device; }
 int gem_ctx_backend(const gem_ctx* ctx) { return ctx->backend; }
+unsigned long long gem_ctx_tc_wait_ns(const gem_ctx* ctx) { return ctx->tc_wait_ns; }
 void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes) {
   if (slot < 0 || slot >= 16) return nullptr;
   if (ctx->d_aux[slot] && ctx->aux_cap[slot] >= bytes) return ctx->d_aux[slot];
@@ -492,7 +494,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
   L.prop_kopt = nullptr; L.prop_hs = nullptr;
   L.adv_min = 1; L.adv_wait = 0;
-  L.nsrc = 0; L.src_node = nullptr; L.src_type = nullptr; L.src_off = nullptr;
+  L.nsrc = 0; L.src_blk = 0;
   ctx->last_grid = S.grid[1];
   ctx->last_block = FK_SCHED_BLOCK[S.sched[1]];
   // ---- learned proposer: features / proposals per (phase, item) from the start radii
@@ -609,26 +611,18 @@ int fk_enqueue_aski(gem_ctx* ctx, SlabPlan& S, int nsnod, const int* jsnod, int 
   FKLaunch L0 = S.L;
   L0.prop_kopt = nullptr; L0.prop_hs = nullptr;
   CK(launch(-1, S.P, L0));
-  // source table of the toroidal phase: nodes, types and output offsets
+  // source table of the toroidal phase, passed by value: nodes and types; block b
+  // starts at b * blk_m
   const int nsrc = nsnod + 1;
-  char* tabs = (char*)gem_ctx_aux(ctx, 14, (size_t)nsrc * (2 * sizeof(int) + sizeof(long long)) + 64);
-  if (!tabs) return GEM_ERROR;
-  std::vector<long long> h_off(nsrc);
-  std::vector<int> h_node(nsrc), h_type(nsrc);
-  for (int b = 0; b < nsrc; ++b) {
-    h_node[b] = b == nsnod ? jre : jsnod[b];
-    h_type[b] = b == nsnod ? 0 : istyp;
-    h_off[b] = (long long)((size_t)b * blk_m);
-  }
-  long long* d_off = (long long*)tabs;
-  int* d_node = (int*)(tabs + (size_t)nsrc * sizeof(long long));
-  int* d_type = d_node + nsrc;
-  CK(cudaMemcpyAsync(d_off, h_off.data(), (size_t)nsrc * sizeof(long long), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(d_node, h_node.data(), (size_t)nsrc * sizeof(int), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(d_type, h_type.data(), (size_t)nsrc * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (nsrc > MAXNOD + 2) return fail(ctx, "gem_fk_run_aski: %d source nodes, above the %d supported", nsnod, MAXNOD + 1);
   FKLaunch Lt = L0;
   Lt.gf64 = reinterpret_cast<double2*>(g64); Lt.gfre = gre; Lt.gfim = gim;
-  Lt.nsrc = nsrc; Lt.src_node = d_node; Lt.src_type = d_type; Lt.src_off = d_off;
+  Lt.nsrc = nsrc;
+  Lt.src_blk = (long long)blk_m;
+  for (int b = 0; b < nsrc; ++b) {
+    Lt.src_node[b] = (unsigned char)(b == nsnod ? jre : jsnod[b]);
+    Lt.src_type[b] = (unsigned char)(b == nsnod ? 0 : istyp);
+  }
   nvtxRangePushA("gem_fk: toroidal phase over the source-node range");
   cudaError_t le = launch(0, S.P, Lt);
   nvtxRangePop();
@@ -1179,6 +1173,13 @@ int gem_order_target(gem_ctx* ctx, int k) {
   if (k == 0) k = 6;
   if (k < 3 || k > 7) return fail(ctx, "order target must be 3..7");
   ctx->kopt = k;
+  return GEM_OK;
+}
+
+int gem_tc_wait_limit(gem_ctx* ctx, long long ns) {
+  if (!ctx) return GEM_ERROR;
+  if (ns < 0) return fail(ctx, "wait limit must be >= 0");
+  ctx->tc_wait_ns = (unsigned long long)ns;
   return GEM_OK;
 }
 

@@ -73,13 +73,15 @@ struct FKLaunch {
   // deferral of the bookkeeping between integrations: a pass runs when
   // adv_min lanes wait, one has waited adv_wait trips, or none integrates
   int adv_min, adv_wait;
-  // toroidal phase of a set of source nodes (nsrc > 0): per source its node, type
-  // (0 force, 1 moment) and the element offset of its output block
+  // toroidal phase of a set of source nodes (nsrc > 0): per source b its node and
+  // type (0 force, 1 moment), passed by value; its output block starts at
+  // element b * src_blk
   int nsrc;
-  const int* src_node;
-  const int* src_type;
-  const long long* src_off;
+  long long src_blk;
+  unsigned char src_node[MAXNOD + 2];
+  unsigned char src_type[MAXNOD + 2];
 };
+static_assert(MAXNOD + 1 <= 255, "source-node table entries are bytes");
 
 // One Bulirsch-Stoer step attempt as the step log records it (32 bytes).
 struct StepRec {

@@ -705,7 +705,7 @@ __device__ __noinline__ void advance(const FKStatic& P, const FKLaunch& LL, cons
                     for (int c = 0; c < 2; ++c) ti[c][j] = ecoef[j] * s.get(lay.dt(n, c));
                   }
                 }
-                output_dsv_tor_src(P, L.e, ti, n, LL, L.k, jsh, ty, LL.src_off[b]);
+                output_dsv_tor_src(P, L.e, ti, n, LL, L.k, jsh, ty, (long long)b * LL.src_blk);
               }
             }
             L.st = S_ITEM_END;

@@ -6,11 +6,11 @@
 // run.  It needs no context either.
 //
 // The transform's tables (the twiddles of every radix-2 stage and the
-// exp(sigma t) factors: at most 8192*16 + 8192*8 = 196,608 bytes) live in one
-// file-scope device array of NOALLOC_SCRATCH_BYTES = 256 KiB, which every GPU
-// that loads this library holds until the process exits.  Nothing is allocated
-// per call: no cudaMalloc, no cudaFree, no allocating library routine, no host
-// heap.
+// exp(sigma t) factors: at most 8192*16 + 8192*8 = 196,608 bytes, since the
+// FFT length is limited to 8192) live in one file-scope device array of
+// NOALLOC_SCRATCH_BYTES = 256 KiB, which every GPU that loads this library
+// holds until the process exits.  Nothing is allocated per call: no cudaMalloc,
+// no cudaFree, no allocating library routine, no host heap.
 //
 // Sharing rules: all calls on one device share the array, and it keeps the
 // last call's tables.  Nothing in it has to start at zero: each call rewrites
@@ -19,20 +19,24 @@
 // whose work runs concurrently on the same device) race on the array and give
 // wrong series; order them on one stream.
 //
-// Set-up: the first call on a device, with that device current, looks up the
-// array's device address with cudaGetSymbolAddress; later calls reuse the
-// address.  Make that first call on each device before any stream capture.
+// Set-up: every call, with the caller's device current, looks up the array's
+// device address in the current context with cudaGetSymbolAddress (a lookup,
+// not an allocation), so the address stays right after cudaDeviceReset or in
+// a recreated context.  The first call on a device may load the library's
+// device code into the context (CUDA's lazy module loading); make that first
+// call on each device before any stream capture.
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
-#include <mutex>
 
 #include "synth.h"
 
 namespace {
 
 constexpr size_t NOALLOC_SCRATCH_BYTES = 256 * 1024;
-constexpr int NOALLOC_MAX_DEVICES = 64;
+// the FFT length limit of fft_geometry is what keeps the tables inside the array
+static_assert((size_t)gem::IFFT_MAX_NS * (sizeof(double2) + sizeof(double)) <= NOALLOC_SCRATCH_BYTES,
+              "inverse-FFT tables of the longest transform exceed the no-allocation scratch array");
 
 }  // namespace
 
@@ -41,9 +45,6 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) unsigned char g_ifft_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
 namespace {
-
-void* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
-std::mutex g_setup_lock;
 
 int report(char* errbuf, int errlen, int level, const char* fmt, ...) {
   if (errbuf && errlen > 0) {
@@ -55,23 +56,13 @@ int report(char* errbuf, int errlen, int level, const char* fmt, ...) {
   return level;
 }
 
-// Device address of the scratch array on the current device (set-up on first use).
+// Device address of the scratch array in the current context, looked up on every call.
 int scratch_address(void** out, char* errbuf, int errlen) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-    return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: device %d above the %d devices supported", dev,
-                  NOALLOC_MAX_DEVICES);
-  std::lock_guard<std::mutex> guard(g_setup_lock);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_ifft_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_ifft_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+  *out = p;
   return GEM_OK;
 }
 
@@ -86,10 +77,6 @@ extern "C" int gem_ifft_run_noalloc(int nf1, int nf2, double df, double sigma, i
   if (ntr < 1 || ldsp < nf2) return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: need ntr >= 1 and ldsp >= nf2");
   FftGeometry g;
   if (const char* why = fft_geometry(nf1, nf2, df, nsamp, dt, g)) return report(errbuf, errlen, GEM_ERROR, "%s", why);
-  const size_t need = ifft_table_bytes(g.ns, nsamp);
-  if (need > NOALLOC_SCRATCH_BYTES)
-    return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: tables need %zu bytes, above the %zu-byte scratch", need,
-                  NOALLOC_SCRATCH_BYTES);
   void* scratch = nullptr;
   if (int rc = scratch_address(&scratch, errbuf, errlen)) return rc;
   double2* tw = (double2*)scratch;
@@ -103,10 +90,24 @@ extern "C" int gem_ifft_run_noalloc(int nf1, int nf2, double df, double sigma, i
   if (e != cudaSuccess)
     return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: cudaFuncSetAttribute: %s", cudaGetErrorString(e));
   cudaStream_t st = (cudaStream_t)stream;
-  ifft_tables_kernel<<<8, 256, 0, st>>>(g.ns, g.nslog, nsamp, std::exp(sigma * g.dts), tw, fac);
-  ifft_kernel<<<(unsigned)ntr, IFFT_THREADS, smem, st>>>(S, (const double2*)d_sp, tw, fac, d_ts);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: launch: %s", cudaGetErrorString(e));
+  // launched through cudaLaunchKernel, whose return value is this launch's own
+  // status: an error the caller left pending is neither reported nor cleared
+  int ns = g.ns, nslog = g.nslog, ns_out = nsamp;
+  double efac = std::exp(sigma * g.dts);
+  double2* tw_arg = tw;
+  double* fac_arg = fac;
+  void* targs[] = {&ns, &nslog, &ns_out, &efac, &tw_arg, &fac_arg};
+  e = cudaLaunchKernel((const void*)ifft_tables_kernel, dim3(8), dim3(256), targs, 0, st);
+  if (e != cudaSuccess)
+    return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: table kernel launch: %s", cudaGetErrorString(e));
+  const double2* sp_arg = (const double2*)d_sp;
+  const double2* twc = tw;
+  const double* facc = fac;
+  float* ts_arg = d_ts;
+  void* fargs[] = {&S, &sp_arg, &twc, &facc, &ts_arg};
+  e = cudaLaunchKernel((const void*)ifft_kernel, dim3((unsigned)ntr), dim3(IFFT_THREADS), fargs, smem, st);
+  if (e != cudaSuccess)
+    return report(errbuf, errlen, GEM_ERROR, "ifft_noalloc: transform kernel launch: %s", cudaGetErrorString(e));
   if (g.decimated) return report(errbuf, errlen, GEM_WARNING, "Downsampling to less than 1./(2*fny) requested");
   return GEM_OK;
 }

@@ -23,9 +23,10 @@
 // a 2-stage shared-memory ring; warp 1 issues the S(S+1)/2 slice products (2 MMAs
 // of K 32 each) into S TMEM accumulators of TC_BN columns, one per weight w = i + j;
 // warps 2-5 combine the accumulators in FP64 and write C.  All mbarrier waits
-// are bounded by a 1 s timer: a wait that runs out records an error flag, the
-// CTA stops issuing work, waits (bounded) for its own copies and products,
-// frees its TMEM and returns.
+// of the pipeline are bounded by a timer (1 s unless the context sets another
+// limit): a wait that runs out records an error flag, the CTA stops issuing
+// work, waits (bounded by 1 s, whatever the limit) for its own copies and
+// products, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -58,7 +59,7 @@ constexpr int TC_TMEM_COLS = 512;                       // S accumulators of TC_
 static_assert(TC_S * TC_BN <= TC_TMEM_COLS, "the accumulators must fit the tensor memory");
 static_assert(TC_BN % 16 == 0 && TC_BN >= 16 && TC_BN <= 256, "MMA N of kind::i8 with M = 128");
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
-constexpr unsigned long long TC_WAIT_NS = 1000000000ull;
+constexpr unsigned long long TC_WAIT_NS = 1000000000ull;   // default pipeline wait limit and the drain limit
 
 // ---------------------------------------------------------------------------
 //  Operand preparation (FP64 in, INT8 slices out)
@@ -237,15 +238,16 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: true when the phase completed, false after the time limit or
-// when another role of this CTA has already given up (abort flag).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+// Bounded wait: true when the phase completed, false after limit_ns or when
+// another role of this CTA has already given up (abort flag).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          unsigned long long limit_ns) {
   if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (true) {
     if (mbar_try(bar, parity)) return true;
     if (*abort_flag) return false;
-    if (global_ns() - t0 > TC_WAIT_NS) {
+    if (global_ns() - t0 > limit_ns) {
       *abort_flag = 1;
       return false;
     }
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                    const int4* __restrict__ tiles, const int* __restrict__ kind_rows,
                    const long long* __restrict__ kind_rowoff, const long long* __restrict__ coff, int nsta,
                    long long mtot, const double* __restrict__ rscale, const double* __restrict__ cscale,
-                   double* C, int* err) {
+                   double* C, int* err, unsigned long long wait_ns) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = (uint64_t*)(smem + TC_STAGES * TC_STAGE_BYTES);
@@ -328,7 +330,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     int issued = 0;
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % TC_STAGES;
-      if (kb >= TC_STAGES && !mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1, abort_flag)) break;
+      if (kb >= TC_STAGES && !mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1, abort_flag, wait_ns)) break;
       unsigned char* st = smem + s * TC_STAGE_BYTES;
       mbar_expect_tx(&full[s], TC_STAGE_BYTES);
 #pragma unroll 1
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     bool ok = true;
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % TC_STAGES;
-      if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1, abort_flag)) { ok = false; break; }
+      if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1, abort_flag, wait_ns)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;");
       const unsigned char* st = smem + s * TC_STAGE_BYTES;
 #pragma unroll 1
@@ -378,10 +380,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                      smem_u32(acc_full))
                  : "memory");
     if (!ok) *abort_flag = 1;
+    // the products issued above write TMEM and read the stages.  After an abort
+    // (set here or by the epilogue at any time) nobody else waits for them, so
+    // they are always drained here, before the CTA's closing barrier frees the
+    // tensor memory; without an abort the epilogue has waited for the same phase
+    mbar_drain(acc_full, 0);
   } else if (warp >= 2) {
     // ---- epilogue: TMEM lanes 32*(warp % 4) .. +31 hold rows of the tile
     const int q = warp & 3;
-    const bool done = mbar_wait(acc_full, 0, abort_flag);
+    const bool done = mbar_wait(acc_full, 0, abort_flag, wait_ns);
     asm volatile("tcgen05.fence::after_thread_sync;");
     const int r = m0 + q * 32 + lane;   // row within the kind
     const bool row_ok = done && !*abort_flag && r < Mk;
@@ -503,9 +510,10 @@ size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out) {
 
 // Sliced-integer sums: from the FP64 tables tab[kind][l][sta] and coefficients
 // A[kind rows][lcap], write C[kind][row][sta] in FP64.  ws: device workspace of
-// sums_tc_workspace bytes.  Blocking (synchronises the stream).
+// sums_tc_workspace bytes; wait_ns: limit of each pipeline wait (0: 1 s).
+// Blocking (synchronises the stream).
 const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const double* tab, const double* A,
-                        double* C, void* ws, size_t ws_bytes, cudaStream_t st) {
+                        double* C, void* ws, size_t ws_bytes, unsigned long long wait_ns, cudaStream_t st) {
   TcLayout L = tc_layout(S, mtot);
   if (ws_bytes < L.total) return "sums_tc: workspace too small";
   if (7LL * mtot >= (1LL << 31) || 7LL * 8 * S.nsta >= (1LL << 31)) return "sums_tc: operand rows exceed 2^31";
@@ -572,7 +580,8 @@ const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const
   if (cudaMemsetAsync(ints + 8, 0, sizeof(int), st) != cudaSuccess) return "sums_tc: upload failed";
   dim3 grid((S.nsta + TC_BN - 1) / TC_BN, (unsigned)htiles.size());
   sums_tc_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(mA, mB, tiles, ints, tabs + 8, tabs + 16, S.nsta, mtot,
-                                                    rscale, cscale, C, ints + 8);
+                                                    rscale, cscale, C, ints + 8,
+                                                    wait_ns ? wait_ns : TC_WAIT_NS);
   if (cudaGetLastError() != cudaSuccess) return "sums_tc: launch failed";
   int herr = 0;
   if (cudaMemcpyAsync(&herr, ints + 8, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||

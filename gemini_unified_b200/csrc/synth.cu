@@ -761,7 +761,7 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
     const long long mtot = 2LL * nf * S.nsum;
     const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
     void* ws = gem_ctx_aux(ctx, 3, wsb);
-    const char* why = ws ? sums_tc_run(S, nwn, mtot, b.tab, b.A, b.C, ws, wsb, st) : "";
+    const char* why = ws ? sums_tc_run(S, nwn, mtot, b.tab, b.A, b.C, ws, wsb, gem_ctx_tc_wait_ns(ctx), st) : "";
     if (why) {
       nvtxRangePop();
       cudaEventDestroy(e0); cudaEventDestroy(e1);

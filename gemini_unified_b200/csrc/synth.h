@@ -71,7 +71,7 @@ void event_filter_host(const gem_synth_params* p, std::vector<double2>& h);
 // nwn: host copy of the wavenumber counts per frequency (1-based frequency index)
 size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out);
 const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const double* tab, const double* A,
-                        double* C, void* ws, size_t ws_bytes, cudaStream_t st);
+                        double* C, void* ws, size_t ws_bytes, unsigned long long wait_ns, cudaStream_t st);
 
 }  // namespace gem
 
@@ -80,4 +80,5 @@ int gem_set_error(gem_ctx* ctx, const char* msg);
 void gem_note_synth_ms(gem_ctx* ctx, float ms);
 int gem_ctx_device(const gem_ctx* ctx);
 int gem_ctx_backend(const gem_ctx* ctx);
+unsigned long long gem_ctx_tc_wait_ns(const gem_ctx* ctx);
 void* gem_ctx_aux(gem_ctx* ctx, int slot, size_t bytes);

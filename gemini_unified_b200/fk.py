@@ -87,6 +87,7 @@ def lib() -> ctypes.CDLL:
         L.gem_steplog.argtypes = [vp, ctypes.c_longlong]
         L.gem_steplog_read.argtypes = [vp, vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
         L.gem_order_target.argtypes = [vp, ctypes.c_int]
+        L.gem_tc_wait_limit.argtypes = [vp, ctypes.c_longlong]
         L.gem_ray_table.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp, vp, vp, vp]
         L.gem_travel_times.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int, ctypes.c_double,
@@ -480,6 +481,11 @@ class GeminiFK:
     def order_target(self, k: int):
         """Attempt the step-size control aims at (fast backend; 3..7, 0 restores the reference's 6)."""
         self._check(lib().gem_order_target(self._h, int(k)))
+
+    def tc_wait_limit(self, ns: int):
+        """Time limit in ns of each pipeline wait of the tensor-core degree sums (0 restores 1 s);
+        a wait that runs out makes the synthetics call fail with GeminiError."""
+        self._check(lib().gem_tc_wait_limit(self._h, int(ns)))
 
     def steplog(self, capacity: int):
         """Record every step attempt of the following runs (capacity records; 0 = off)."""

@@ -353,10 +353,21 @@ int gem_ifft_run_device(gem_ctx* ctx, int nf1, int nf2, double df, double sigma,
  * current one; errors and the decimation warning are written to errbuf
  * (errlen bytes, may be NULL).  Returns after queuing its kernels on stream.
  * All calls on a device share the array: calls that overlap on the GPU race and
- * must be ordered on one stream.  The first call on each device looks up the
- * array's address and should come before any stream capture. */
+ * must be ordered on one stream.  Every call looks up the array's address in
+ * the current context (cudaGetSymbolAddress, no allocation), so it stays valid
+ * after cudaDeviceReset; the first call on each device may load the library's
+ * device code and should come before any stream capture. */
 int gem_ifft_run_noalloc(int nf1, int nf2, double df, double sigma, int ntr, const double* d_sp, long long ldsp,
                          int nsamp, double dt, float* d_ts, void* stream, char* errbuf, int errlen);
+
+/* Failure-detection knob (no counterpart in the reference): the time limit, in
+ * ns, of each pipeline wait of the tensor-core degree sums of this context
+ * (fast backend); 0 restores the default of 1 s.  A wait that runs out makes
+ * the kernel stop issuing work, drain its own copies and products (bounded by
+ * 1 s whatever the limit), free its tensor memory and return; the synthetics
+ * call then returns GEM_ERROR with "a pipeline wait timed out".  A limit far
+ * below the pipeline's latency (a few ns) makes every call fail that way. */
+int gem_tc_wait_limit(gem_ctx* ctx, long long ns);
 
 /* Counters of the last run (accepted/rejected steps, attempts, flops, ...). */
 int gem_stats_get(const gem_ctx* ctx, gem_stats* out);
@@ -412,10 +423,6 @@ int gem_proposer_dump_read(gem_ctx* ctx, float* out, long long cap, long long* n
 int gem_prop_grad(const float* w, const float* x, const float* y, const float* mask, int n, float* grad, float* loss);
 int gem_prop_train(float* w, const float* x, const float* y, const float* mask, int n, int epochs, int batch,
                    float lr, unsigned seed, float* loss_hist);
-
-/* Measurement utility (no counterpart in the reference): FP64 FMA throughput
- * of the device in TFLOP/s, the denominator of the solver's FP64 roofline. */
-double gem_probe_fp64_tflops(int device);
 
 #ifdef __cplusplus
 }

@@ -1,8 +1,8 @@
 """Regenerate the committed fixtures under tests/golden/.
 
-Run in the build container, where the reference tree is mounted:
+Run where a reference tree is mounted, giving its root:
 
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py <reference tree>
 
 * models/*.json: the reference's earth-model input files used by the
   configurations and by the reference's own model-reader known-answer test
@@ -55,5 +55,7 @@ def main(ref):
 if __name__ == "__main__":
     if "--oracle" in sys.argv:
         oracle_vectors()
+    elif len(sys.argv) == 2:
+        main(sys.argv[1])
     else:
-        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+        sys.exit("usage: make_fixtures.py <reference tree> | --oracle")

@@ -112,6 +112,32 @@ def test_mixed_precision_synthetics_many_stations(gpu):
     assert np.max(num / den) <= RTOL_MIXED
 
 
+def test_tensor_core_wait_limit_reports_error(fkdata):
+    """Failure detection of the tensor-core sums, without a GPU fault: with a
+    pipeline wait limit of 1 ns the first wait of a tile that is not complete
+    already runs out, the kernel drains its own copies and products, frees its
+    tensor memory and returns, and the call fails with GEM_ERROR.  The context
+    stays usable: with the default limit restored the same call matches the
+    oracle."""
+    import oracle
+    from gemini_unified_b200.fk import GEM_BACKEND_GPU_FAST, GeminiError, GeminiFK, synth_params
+    w, m, ex, g, fk, gr, gi = fkdata
+    theta, phi, propdir = w.stations()
+    theta, phi, propdir = theta[::10], phi[::10], propdir[::10]
+    mt = configs.unit_moment_tensors()[:2]
+    sp = synth_params(g, 10, w.nsamp, w.dt, w.filspecs)
+    fast = GeminiFK(m, ex, backend=GEM_BACKEND_GPU_FAST)
+    fast.tc_wait_limit(1)
+    with pytest.raises(GeminiError, match="timed out"):
+        fast.synthetics(sp, g.nwn, gr, gi, theta, phi, propdir, mt)
+    fast.tc_wait_limit(0)
+    got = fast.synthetics(sp, g.nwn, gr, gi, theta, phi, propdir, mt)
+    ref = oracle.synthetics(g.nf1, g.nf2, g.nwn, g.nwnmax, sp.df, sp.sigma, gr, gi, theta, phi, propdir, mt,
+                            w.filspecs, False, 0.0, w.nsamp, w.dt)
+    num, den = _rel(got, ref, w.nsamp)
+    assert np.max(num / den) <= RTOL_MIXED
+
+
 @pytest.mark.parametrize("backend", [1, 2])
 def test_station_options_match_oracle(fkdata, backend):
     """Per-station reduction times (as AUTOMATIC_TIMESHIFT sets them), samples kept per

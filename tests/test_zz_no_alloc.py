@@ -60,7 +60,10 @@ def test_noalloc_matches_ifft_run_device_on_two_calls(gpu):
     assert free_after[1][0] == free_after[1][1]
 
 
-def test_noalloc_rejects_sizes_beyond_its_scratch(gpu):
+def test_noalloc_rejects_fft_lengths_beyond_its_limit(gpu):
+    """A 16384-sample transform is refused with GEM_ERROR and a message.  The
+    8192-sample length limit is what keeps every call's tables inside the static
+    array (a compile-time check in the library states that relation)."""
     import torch
     f = _noalloc()
     err = ctypes.create_string_buffer(256)
