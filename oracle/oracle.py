@@ -49,6 +49,10 @@ def lib():
         L.oracle_spline.argtypes = [vp, ctypes.c_double, ctypes.c_int] + [ctypes.c_void_p] * 4
         L.oracle_start_radius.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.oracle_start_radius.restype = ctypes.c_double
+        L.oracle_bottom_iv.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_propagate.argtypes = ([vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_int] + [ctypes.c_double] * 4 + [ctypes.c_void_p] * 3)
         L.oracle_nwn.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.oracle_fk_frequency.argtypes = [vp, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
@@ -166,6 +170,24 @@ class Oracle:
 
     def start_radius(self, f, attmode, wn, tor):
         return lib().oracle_start_radius(self.h, ctypes.c_double(f), attmode, ctypes.c_double(wn), int(tor))
+
+    def bottom_iv(self, f, attmode, omim, dll1, r, kind):
+        """Start vector of an upward integration at r (kind 0 toroidal, 1 minors), its
+        initial step and the status of the continued fractions (initialValues.f90:202-416)."""
+        y = np.zeros(4 if kind == 0 else 10)
+        htry = ctypes.c_double()
+        rc = lib().oracle_bottom_iv(self.h, f, attmode, omim, dll1, r, int(kind), _p(y), ctypes.byref(htry))
+        return y.view(np.complex128), htry.value, rc
+
+    def propagate(self, f, attmode, omim, dll1, sys, x1, x2, htry, eps, y0):
+        """y(x2) of system sys (0 minors, 3 toroidal, 4 adjoint solid) from y(x1) = y0, as
+        y1 * 10**lgnorm (propagateOde.f90:132-331); returns (y1, lgnorm, status)."""
+        y0 = np.ascontiguousarray(y0, np.complex128)
+        y1 = np.zeros_like(y0)
+        lg = ctypes.c_double()
+        rc = lib().oracle_propagate(self.h, f, attmode, omim, dll1, int(sys), x1, x2, htry, eps,
+                                    _p(y0.view(np.float64)), _p(y1.view(np.float64)), ctypes.byref(lg))
+        return y1, lg.value, rc
 
     def nwn(self, pc):
         cap = 1 << 16

@@ -1830,6 +1830,62 @@ double oracle_start_radius(void* h, double f, int attmode, double wn, int tor) {
   return startRadius(e, tor != 0);
 }
 
+// Analytic checks of the tests (homogeneous sphere).  Environment of one
+// (omega, dll1) at frequency f with omim the imaginary part of the complex
+// frequency (the FK loop uses -sigma), layer of radius r for an upward start.
+static Env analyticEnv(Ctx* c, const Spline& s, double f, double omim, double dll1, double r) {
+  Env e; e.m = &c->m; e.ex = &c->ex; e.s = &s;
+  e.omre = 2.0 * PI_F * f; e.omim = omim; e.dll1 = dll1;
+  int nl, top;
+  layerIndex(c->m, r, nl, top);
+  if (top == 1) nl = nl + 1;
+  e.nl = nl;
+  return e;
+}
+
+// Start vector of an upward integration at radius r, as the FK loop forms it:
+// kind 0 toroidal (toroidalBottomInitialValues, initialValues.f90:376-416; 2
+// values), 1 spheroidal minors (minorsBottomInitialValues, :202-275; 5 values).
+// y: complex interleaved; returns the status of the continued fractions.
+int oracle_bottom_iv(void* h, double f, int attmode, double omim, double dll1, double r, int kind, double* y,
+                     double* htry) {
+  Ctx* c = (Ctx*)h;
+  Spline s;
+  if (computeSpline(c->m, f, attmode, s)) return 2;
+  Env e = analyticEnv(c, s, f, omim, dll1, r);
+  zc ys[5];
+  const int rc = kind == 0 ? toroidalBottomIV(e, r, ys, *htry) : minorsBottomIV(e, r, ys, *htry);
+  const int nv = kind == 0 ? 2 : 5;
+  for (int v = 0; v < nv; ++v) { y[2 * v] = ys[v].re; y[2 * v + 1] = ys[v].im; }
+  return rc;
+}
+
+// One propagation (propagateOde.f90:132-331, with its renormalisation) of
+// system sys (0 minors, 3 toroidal, 4 adjoint solid) from x1 to x2 with start
+// vector y0 and initial step htry at accuracy eps: y1 = y(x2) / 10^lgnorm.
+int oracle_propagate(void* h, double f, int attmode, double omim, double dll1, int sys, double x1, double x2,
+                     double htry, double eps, const double* y0, double* y1, double* lgnorm) {
+  Ctx* c = (Ctx*)h;
+  if (sys < 0 || sys > 4) return 2;
+  Spline s;
+  if (computeSpline(c->m, f, attmode, s)) return 2;
+  Env e = analyticEnv(c, s, f, omim, dll1, x1);
+  if (x2 < x1) {   // downward: the layer containing x1 from above
+    int nl, top;
+    layerIndex(c->m, x1, nl, top);
+    e.nl = nl;
+  }
+  Stats st{};
+  Prop p; p.sys = sys; p.nv = nvarOf(sys); p.env = &e; p.eps = eps;
+  p.do_norm = true; p.lgnorm = 0.0; p.st = &st;
+  zc ys[5];
+  for (int v = 0; v < p.nv; ++v) ys[v] = Z(y0[2 * v], y0[2 * v + 1]);
+  const int rc = propagate(p, x1, x2, htry, ys);
+  for (int v = 0; v < p.nv; ++v) { y1[2 * v] = p.y[v].re; y1[2 * v + 1] = p.y[v].im; }
+  *lgnorm = p.lgnorm;
+  return rc;
+}
+
 // Number of wavenumbers per frequency (computeGreenFKSpectraForSynthetics.f90:186-236)
 // nwn must hold nf2 entries (index jf-1); returns nf1 and nf2 through pointers.
 int oracle_nwn(void* h, const or_fk_params* p, int* nf1, int* nf2, int* nwn, int nwn_cap) {
