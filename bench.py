@@ -12,9 +12,12 @@ Metric: (omega, l) ODE solves per second.  ``value`` is measured on the device
 (CUDA events around the model preparation and the persistent solver, inputs
 resident); ``e2e`` goes through the public C ABI with host buffers (the float32
 FK spectra are copied back every step).  With N GPUs the frequencies are
-split over the ranks in the reference's zig-zag order
-(computeGreenFKSpectraForSynthetics.f90:361-387); the time is the maximum over
-ranks.
+split over the ranks in contiguous blocks of about equal cost, one FK launch
+per rank (the reference splits them in a zig-zag order,
+computeGreenFKSpectraForSynthetics.f90:361-387); the time is the maximum over
+ranks.  At N > 1 the line also times the whole pipeline of one source node:
+frequency-sharded FK spectra, one NCCL all-gather of that node's spectra,
+station-sharded seismograms (``pipeline``).
 
 Traces leg (``traces``): seismograms of the tensor-core degree-sum configuration
 (seeded log-normal FK coefficients of the batched grid's shape, 4000 stations
@@ -58,18 +61,7 @@ def parse():
     return ap.parse_args()
 
 
-def zigzag(nf1, nf2, rank, size):
-    """Frequencies of one rank (computeGreenFKSpectraForSynthetics.f90:361-387)."""
-    nf = nf2 - nf1 + 1
-    npart = nf // size + (1 if nf % size else 0)
-    out, jfe = [], nf2
-    for k in range(1, npart + 1):
-        jf = jfe - rank if k % 2 == 1 else jfe + rank - size + 1
-        jfe -= size
-        if jf < nf1:
-            break
-        out.append(jf)
-    return sorted(out)
+from gemini_unified_b200.pipeline import contiguous_runs, cost_blocks, zigzag  # noqa: E402  (frequency splits)
 
 
 def sched_names(tune):
@@ -78,20 +70,6 @@ def sched_names(tune):
     from gemini_unified_b200.fk import DEFERRALS, SCHEDULES
     return ["%d%s/defer%d,%d" % (SCHEDULES[s][0], "+cache" if SCHEDULES[s][1] else "", DEFERRALS[d][0],
                                   DEFERRALS[d][1]) for s, d in zip(tune["schedule"], tune["defer"])]
-
-
-def contiguous_runs(js):
-    runs, start = [], None
-    for a in js:
-        if start is None:
-            start = prev = a
-        elif a == prev + 1:
-            prev = a
-        else:
-            runs.append((start, prev)); start = prev = a
-    if start is not None:
-        runs.append((start, prev))
-    return runs
 
 
 class Clocks:
@@ -262,8 +240,9 @@ def main():
     jre = ex.node_index(w.rec_radius)
     g = M.frequency_grid(w.params, m.rearth)
     nsp = M.nsp_for(w.params)
-    mine = zigzag(g.nf1, g.nf2, rank, size)
-    runs = contiguous_runs(mine)
+    # one contiguous block of frequencies of about equal cost per rank: one FK launch
+    # each (the reference's zig-zag order gives a rank many short runs)
+    runs = cost_blocks(g.nwn, g.nf1, g.nf2, size)[rank]
     dev = torch.device("cuda", local)
     nkf = {r: int(g.nwn[r[0] - 1: r[1]].sum()) for r in runs}
     items_rank = sum(nkf.values())
@@ -355,6 +334,8 @@ def main():
 
     # ---------------- seismogram traces: FK spectra of one source node -> traces at all stations
     traces = time_traces(args, w, m, g, nsp, dev, stream, dist, rank, size, timed)
+    # ---------------- N GPUs: frequency-sharded FK -> one all-gather -> station-sharded traces
+    pipe = time_pipeline(w, m, ex, jre, g, nsp, local, dev, stream, rank, size, timed) if size > 1 else None
 
     # ---------------- roofline of the dominant kernel: the spheroidal phase (FP64 pipe)
     peak = fp64_peak_tflops(local)
@@ -390,6 +371,8 @@ def main():
             "gpu_launches_traces": SYNTH_LAUNCHES * traces.pop("steps_timed", max(1, min(args.steps, 3))),
             "clocks": clk,
         }
+        if pipe is not None:
+            line["pipeline"] = pipe
         out_fast = line["traces"].pop("_out")
         if size == 1:
             n = args.cpu_sample or REF_SAMPLE
@@ -410,6 +393,33 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def time_pipeline(w, m, ex, jre, g, nsp, local, dev, stream, rank, size, timed):
+    """The FK-to-seismogram pipeline of the 5 km source node on N GPUs
+    (gemini_unified_b200.pipeline): each rank computes the FK spectra of its
+    block of frequencies (all nodes, fast form), one NCCL all-gather brings the
+    source node's float32 spectra of every frequency to every rank, and each
+    rank computes the seismograms of its share of the 4000 stations (mixed
+    form).  Timed as one step, the maximum over ranks."""
+    from gemini_unified_b200 import configs, pipeline as P
+    from gemini_unified_b200.fk import synth_params
+    sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs)
+    mt = configs.unit_moment_tensors()
+    st = P.GpuStages(m, ex, w.params, jre, sp, w.stations(), mt, device=local, backend=2, stream=stream)
+    src = ex.node_index(m.rearth - 5000.0)
+    nsta = w.ndist
+
+    def one():
+        return P.fk_to_traces(rank, size, g.nwn, g.nf1, g.nf2, nsp, src, nsta, st.fk_fn, st.synth_fn, device=dev)
+
+    one()   # warm-up: buffers of the context
+    t_ms, _ = timed(one, 1)
+    return {"ms_per_step": t_ms, "unit": "ms", "source_node": int(src), "stations": nsta, "moment_tensors": len(mt),
+            "partition": "cost-balanced frequency blocks, stations round robin",
+            "allgather_bytes_per_rank": int(2 * nsp * P.SlabPartition(g.nwn, g.nf1, g.nf2, P.cost_blocks(
+                g.nwn, g.nf1, g.nf2, size)).width * 4),
+            "slab_bytes": int(2 * nsp * int(g.nkfmax) * 4)}
 
 
 def fk_error_vs_oracle(g, nsp, nnod, gre, gim, pick, ref):

@@ -165,3 +165,45 @@ def test_regional_top_frequency_matches_oracle(gpu, backend):
                          RTOL_PLAIN if backend == 1 else RTOL_FAST)
     print("backend %d: worst relative error over %d wavenumbers of %g Hz %.2e" % (backend, len(sample),
                                                                                    (jf - 1) * g.df, worst))
+
+
+def test_pipeline_stages_on_one_rank_equal_the_direct_calls(gpu):
+    """The GPU stages of the multi-GPU pipeline (gemini_unified_b200.pipeline.GpuStages)
+    through a one-rank NCCL group: FK spectra into device buffers, the all-gather, and
+    the device seismogram entry point give the direct host calls' traces bit for bit
+    (FP64 form, global configuration)."""
+    import datetime
+    import socket
+    import torch
+    import torch.distributed as dist
+    from gemini_unified_b200 import pipeline as P
+    from gemini_unified_b200.fk import GeminiFK, synth_params
+    w = configs.WORKLOADS["global_small"]
+    m = w.model()
+    ex = w.nodes(m)
+    jre = ex.node_index(w.rec_radius)
+    g = M.frequency_grid(w.params, m.rearth)
+    nsp = M.nsp_for(w.params)
+    src = ex.node_index(m.rearth - 10000.0)
+    sp = synth_params(g, nsp, w.nsamp, w.dt, w.filspecs)
+    stations = w.stations()
+    mt = configs.unit_moment_tensors()[[0, 5]]
+    s = socket.socket(); s.bind(("127.0.0.1", 0)); port = s.getsockname()[1]; s.close()
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120))
+    try:
+        st = P.GpuStages(m, ex, w.params, jre, sp, stations, mt, device=0, backend=1)
+        traces, sta, full = P.fk_to_traces(0, 1, g.nwn, g.nf1, g.nf2, nsp, src, len(stations[0]), st.fk_fn,
+                                           st.synth_fn, device=torch.device("cuda", 0))
+        torch.cuda.synchronize()
+        got, slab = traces.cpu().numpy(), full.cpu().numpy()
+    finally:
+        dist.destroy_process_group()
+    fk = GeminiFK(m, ex)
+    gre, gim, _, _ = fk.run(w.params, jre, g.nf1, g.nf2, f64=False)
+    assert np.array_equal(slab[0].view(np.uint32), gre[src - 1].view(np.uint32))
+    assert np.array_equal(slab[1].view(np.uint32), gim[src - 1].view(np.uint32))
+    ref = fk.synthetics(sp, g.nwn, gre[src - 1], gim[src - 1], *stations, mt)
+    assert np.array_equal(np.arange(len(stations[0])), sta)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
