@@ -1,6 +1,6 @@
 """FK spectra of a whole frequency band in batches, with a completion record for resume.
 
-    python -m gemini_unified_b200.fk_batches --workload batched_fk --out runs/batched --batch 32
+    python -m gemini_unified_b200.fk_batches --workload batched_fk --out runs/batched --batch 32 [--h5 gfk.MOMENT]
 
 The reference writes each rank's frequency slab to the FK file as it completes it
 (computeGreenFKSpectraForSynthetics.f90:508-519) and has no resume: a stopped run starts
@@ -9,7 +9,9 @@ per-item status go to ``spectra_<jf0>_<jf1>.npz`` in the output folder, and
 ``done.json`` lists the completed batches together with a fingerprint of the run's
 parameters.  A second run with the same parameters skips the completed batches; a run
 with other parameters refuses the folder.  Files are written to a temporary name and
-renamed, so a batch that was interrupted is never recorded.
+renamed, so a batch that was interrupted is never recorded.  ``export`` writes the recorded
+batches into one FK-spectra file in the reference's HDF5 layout (gemini_unified_b200.fkfile),
+which the reference's computeSyntheticSeismograms reads.
 """
 from __future__ import annotations
 
@@ -103,6 +105,24 @@ def load(out_dir: str):
             np.concatenate([p["status"] for p in parts]))
 
 
+def export(out_dir: str, path: str, model, nodes, params: M.FKParams, jre: int, earth_model_name: str = "") -> None:
+    """The recorded batches as one FK-spectra file (HDF5, the reference's layout),
+    written batch by batch.  Every batch of the band must be recorded."""
+    from .fkfile import FKFileWriter
+    rec = _read_record(out_dir)
+    g = M.frequency_grid(params, model.rearth)
+    if not rec or rec.get("fingerprint") != fingerprint(params, jre, nodes.r):
+        raise ValueError("%s holds no batches of this run" % out_dir)
+    done = sorted(tuple(b) for b in rec["done"])
+    covered = sum(b - a + 1 for a, b in done)
+    if covered != g.nf2 - g.nf1 + 1:
+        raise ValueError("only %d of the %d frequencies are recorded" % (covered, g.nf2 - g.nf1 + 1))
+    with FKFileWriter(path, model, nodes, params, jre, earth_model_name=earth_model_name) as fw:
+        for b in done:
+            with np.load(batch_file(out_dir, b)) as z:
+                fw.write_slab(b[0], b[1], z["gfre"], z["gfim"])
+
+
 def main(argv=None):
     from .fk import GeminiFK
     ap = argparse.ArgumentParser()
@@ -111,12 +131,16 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--backend", type=int, default=2, choices=[1, 2])
     ap.add_argument("--no-resume", action="store_true")
+    ap.add_argument("--h5", default="", help="also write the FK-spectra file (reference HDF5 layout) to this path")
     a = ap.parse_args(argv)
     w = configs.WORKLOADS[a.workload]
     m = w.model()
     ex = w.nodes(m)
     fk = GeminiFK(m, ex, backend=a.backend)
-    res = run(fk, w.params, ex.node_index(w.rec_radius), a.out, a.batch, resume=not a.no_resume, log=print)
+    jre = ex.node_index(w.rec_radius)
+    res = run(fk, w.params, jre, a.out, a.batch, resume=not a.no_resume, log=print)
+    if a.h5:
+        export(a.out, a.h5, m, ex, w.params, jre, earth_model_name=m.name)
     print(json.dumps({"batches": len(res), "computed": sum(1 for _, c in res if c)}))
     return 0
 

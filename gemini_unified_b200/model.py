@@ -257,6 +257,97 @@ def node_model_from_dict(d: dict, name: str = "") -> NodeEarthModel:
     return m
 
 
+def _natural_spline_y2(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """Second derivatives of the natural cubic spline through (x, y) from the
+    tridiagonal system of cubicSpline.f90:74-109 (first and last rows set the
+    end second derivatives to zero), solved by elimination."""
+    n = len(x)
+    if n <= 2:
+        return np.zeros(n)
+    lo, di, up, rhs = np.zeros(n), np.ones(n), np.zeros(n), np.zeros(n)
+    for j in range(1, n - 1):
+        lo[j] = (x[j] - x[j - 1]) / 6.0
+        di[j] = (x[j + 1] - x[j - 1]) / 3.0
+        up[j] = (x[j + 1] - x[j]) / 6.0
+        rhs[j] = (y[j + 1] - y[j]) / (x[j + 1] - x[j]) - (y[j] - y[j - 1]) / (x[j] - x[j - 1])
+    for j in range(1, n):              # forward elimination (rows 0 and n-1 are y2 = 0)
+        w = lo[j] / di[j - 1]
+        di[j] -= w * up[j - 1]
+        rhs[j] -= w * rhs[j - 1]
+    y2 = np.zeros(n)
+    y2[n - 1] = rhs[n - 1] / di[n - 1]
+    for j in range(n - 2, -1, -1):
+        y2[j] = (rhs[j] - up[j] * y2[j + 1]) / di[j]
+    return y2
+
+
+def node_elastic_constants(m: NodeEarthModel, nodes: "ExternalRadialNodes"):
+    """Density, inverse Q (kappa, mu) and the seven elastic constants A, C, F,
+    L, N, kappa, mu at the external nodes, from the model's splines at the
+    reference frequency in ELASTIC mode -- what elasticConstantsExternalRadialNodes
+    (externalRadialNodes.f90:423-435) stores with the nodes.  ELASTIC mode
+    (nodeEarthmodel.f90:302-306) makes the constants real; the layer-1
+    halfspace is constant, the other layers are natural cubic splines over
+    their knots (splineEarthmodelCoefficients.f90:46-94,118-162).
+
+    Returns ro [nnod], qinv [nnod, 2], elcon complex [nnod, 7]."""
+    nk = m.nk
+    vph = m.vph if m.aniflag else m.vpv
+    vsh = m.vsh if m.aniflag else m.vsv
+    eta = m.eta if m.aniflag else np.ones(nk)
+    qinv = np.stack([1.0 / m.qk, np.maximum(1.0 / m.qm, 0.0)], axis=1)     # nodeEarthmodel.f90:206-214
+    el = np.zeros((nk, 7))
+    for j in range(nk):   # complexElasticVTIConstants (complexElasticConstants.f90:48-106) without attenuation
+        ro, alfv, alfh, betv, beth, et = m.ro[j], m.vpv[j], vph[j], m.vsv[j], vsh[j], eta[j]
+        if betv > float(np.float32(1e-6)):
+            epa, epc, epn, epl = ro * alfh * alfh, ro * alfv * alfv, ro * beth * beth, ro * betv * betv
+            epf = et * (epa - 2.0 * epl)
+            kappa = (epc + 4.0 * epa - 4.0 * epn + 4.0 * epf) / 9.0
+            mue = (epc + epa + 6.0 * epl + 5.0 * epn - 2.0 * epf) / 15.0
+            el[j] = [epa, epc, epf, epl, epn, kappa, mue]
+        else:
+            kappa = ro * alfv * alfv
+            el[j] = [kappa, kappa, kappa, 0.0, 0.0, kappa, 0.0]
+    rk = m.rk
+    iktop = m.iktop.astype(int)           # 1-based knot index of each layer's top
+    ikbot = m.ikbot.astype(int)
+    fields = np.concatenate([m.ro[:, None], qinv, el], axis=1)   # 10 splined quantities per knot
+    y2 = np.zeros_like(fields)
+    for nl in range(2, m.nlay + 1):
+        j1, j2 = ikbot[nl - 1] - 1, iktop[nl - 1]       # 0-based slice of the layer's knots
+        for q in range(fields.shape[1]):
+            y2[j1:j2, q] = _natural_spline_y2(rk[j1:j2], fields[j1:j2, q])
+    out = np.zeros((nodes.nnod, fields.shape[1]))
+    for i in range(nodes.nnod):
+        r, nl = float(nodes.r[i]), int(nodes.layer[i])
+        if nl == 1:
+            out[i] = fields[iktop[0] - 1]
+            continue
+        j1, j2 = iktop[nl - 2] + 1, iktop[nl - 1]      # 1-based knot range of the layer
+        if j2 - j1 == 1:
+            j = j1
+        else:
+            j = j1 - 1
+            jr = j2 + 1
+            while jr - j > 1:
+                mid = (j + jr) // 2
+                if r > rk[mid - 1]:
+                    j = mid
+                else:
+                    jr = mid
+            j = max(j, j1)
+            j = min(j, j2 - 1)
+        x1, x2 = rk[j - 1], rk[j]
+        h = x2 - x1
+        a = (x2 - r) / h
+        b = 1.0 - a
+        v = a * fields[j - 1] + b * fields[j]
+        if j2 - j1 > 1:
+            v = v + h * h * a * (a * a - 1.0) / 6.0 * y2[j - 1] + h * h * b * (b * b - 1.0) / 6.0 * y2[j]
+        out[i] = v
+    return out[:, 0], out[:, 1:3], out[:, 3:].astype(np.complex128)
+
+
 def property_at_node(m: NodeEarthModel, prop: str, i: int) -> float:
     """getPropertyNodeEarthmodel (nodeEarthmodel.f90:570-590): single-precision result, 1-based i."""
     src = {"node_radius": m.rk, "vp": m.vpv, "vs": m.vsv, "rho": m.ro}.get(prop)

@@ -7,8 +7,11 @@ the workload; six unit moment tensors, or with ``--source FORCE`` three unit
 forces Fr, Ft, Ff).  The FK
 spectra are seeded synthetic coefficients with the shape of the workload's
 spectra: amplitudes log-normal with log10|c| ~ N(-3, 1) clipped to [-6, 0]
-and uniform phases (``fk_coefficients``).  Prints one JSON line with the
-device time per run.
+and uniform phases (``fk_coefficients``), or, with ``--fkfile PATH --node JR``,
+the spectra of node JR of an FK-spectra file (HDF5, the reference's layout;
+its frequency grid replaces the workload's, as readMetaGreenFKSpectra and
+readDataNodeGreenFKSpectra give it to computeSyntheticSeismograms).  Prints
+one JSON line with the device time per run.
 """
 from __future__ import annotations
 
@@ -41,13 +44,24 @@ def main(argv=None):
                     help="1 FP64 degree sums, 2 sliced-integer tensor-core degree sums")
     ap.add_argument("--check", action="store_true", help="also run the FP64 form and report the relative error")
     ap.add_argument("--source", default="MOMENT", choices=["MOMENT", "FORCE"])
+    ap.add_argument("--fkfile", default="", help="FK-spectra file (HDF5) to take the spectra from")
+    ap.add_argument("--node", type=int, default=0, help="external node of the file (1-based; default the deepest)")
     a = ap.parse_args(argv)
     w = configs.WORKLOADS[a.workload]
     m = w.model()
     g = M.frequency_grid(w.params, m.rearth)
     params = dataclasses.replace(w.params, source_type=a.source)
     nsp = M.nsp_for(params)
-    gr, gi = fk_coefficients(nsp, int(g.nkfmax))
+    if a.fkfile:
+        from .fkfile import FKFile
+        with FKFile(a.fkfile) as f:
+            g = f.grid()
+            gr, gi = f.read_node(a.node or 1)
+            if f.meta.nsp != nsp:
+                raise SystemExit("the file holds %d spectra per node, the %s source needs %d" % (f.meta.nsp, a.source,
+                                                                                                 nsp))
+    else:
+        gr, gi = fk_coefficients(nsp, int(g.nkfmax))
     theta, phi, propdir = w.stations()
     if a.stations:
         theta, phi, propdir = theta[: a.stations], phi[: a.stations], propdir[: a.stations]

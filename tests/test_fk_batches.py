@@ -65,3 +65,29 @@ def test_folder_of_another_run_is_refused(setup):
     other = dataclasses.replace(w.params, eps=1e-6)
     with pytest.raises(ValueError):
         fk_batches.run(FakeFK(m, ex), other, jre, out, 16)
+
+
+def test_export_to_the_fk_spectra_file(setup, tmp_path):
+    """The recorded batches become one FK-spectra file in the reference's HDF5
+    layout; a node read from it equals the batches' spectra of that node."""
+    from gemini_unified_b200.fkfile import FKFile
+    w, m, ex, jre, out = setup
+    fk_batches.run(FakeFK(m, ex), w.params, jre, out, 16)
+    path = str(tmp_path / "gfk.MOMENT")
+    fk_batches.export(out, path, m, ex, w.params, jre)
+    gre, gim, _ = fk_batches.load(out)
+    with FKFile(path) as f:
+        assert f.meta.nkfmax == gre.shape[2] and f.meta.nnod == ex.nnod
+        for jr in (1, jre):
+            re, im = f.read_node(jr)
+            np.testing.assert_array_equal(re, gre[jr - 1])
+            np.testing.assert_array_equal(im, gim[jr - 1])
+
+
+def test_export_refuses_an_incomplete_run(setup, tmp_path):
+    w, m, ex, jre, out = setup
+    g = M.frequency_grid(w.params, m.rearth)
+    with pytest.raises(RuntimeError):
+        fk_batches.run(FakeFK(m, ex, fail_at=fk_batches.batches(g.nf1, g.nf2, 8)[2][0]), w.params, jre, out, 8)
+    with pytest.raises(ValueError):
+        fk_batches.export(out, str(tmp_path / "x"), m, ex, w.params, jre)
