@@ -11,11 +11,17 @@ RTOL_L2 = 1e-7
 
 CASES = [
     # nf1, nf2, df, nsamp, dt: the global configuration's series, a decimated
-    # series, the 8192-sample series of the batched configuration, a 512-sample one
+    # series, the 8192-sample series of the batched configuration, a 512-sample
+    # one, a 4096-sample one, and an 8192-sample one with a band wider than 512
+    # bins.  The fast form runs its narrow-band coset transform on the first,
+    # third and fifth (bands below bin 512, 2048-8192 samples) and its radix-16
+    # Stockham transform on the others.
     (2, 52, 1.0 / 1024, 2048, 0.5),
     (3, 300, 1.0 / 1024, 256, 4.0),
     (2, 411, 1.0 / 2048, 8192, 0.25),
     (2, 200, 1.0 / 512, 512, 1.0),
+    (2, 300, 1.0 / 1024, 4096, 0.25),
+    (5, 1500, 1.0 / 2048, 8192, 0.25),
 ]
 
 
@@ -82,7 +88,7 @@ def _exact(nf1, nf2, df, sigma, sp, nsamp, dt):
 
 @pytest.mark.parametrize("case", CASES)
 def test_fast_ifft_exact_and_reference(case):
-    """Fast form (real output from a half-length radix-16 transform): within
+    """Fast form (real output from a half-length complex transform): within
     float32 rounding of the exact inverse DFT, and within the 1e-5 seismogram
     bar of the reference's transform (whose twiddles use single-precision pi)."""
     import oracle
