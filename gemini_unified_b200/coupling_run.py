@@ -37,6 +37,9 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--source", default="MOMENT", choices=["MOMENT", "FORCE"])
     ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--backend", type=int, default=2, choices=[1, 2],
+                    help="1 FP64 degree sums, 2 sliced-integer tensor-core degree sums")
+    ap.add_argument("--check", action="store_true", help="also run the FP64 form and report the difference")
     a = ap.parse_args(argv)
     w = configs.WORKLOADS[a.workload]
     m = w.model()
@@ -47,6 +50,7 @@ def main(argv=None):
     istyp = 1 if a.source == "MOMENT" else 0
     fk = GeminiFK(m, ex, backend=GEM_BACKEND_GPU_FAST)
     gre, gim, _, st = fk.run_dsv(params, jre, g.nf1, g.nf2, f64=False)
+    ctxs = {2: fk, 1: GeminiFK(m, ex)}
     if np.any(st != 0):
         raise SystemExit("DSV spectra: %d items failed" % int(np.sum(st != 0)))
     nsp, nkf = gre.shape[1], gre.shape[2]
@@ -65,8 +69,9 @@ def main(argv=None):
     nwn = np.ascontiguousarray(g.nwn, np.int32)
     P = lambda x: x.ctypes.data_as(ctypes.c_void_p)
     res = {"workload": a.workload, "source": a.source, "points": npts, "frequencies": g.nf2 - g.nf1 + 1,
-           "degrees": nkf, "nsamp": nsamp}
-    for spectra in (1, 0):
+           "degrees": nkf, "nsamp": nsamp, "backend": a.backend}
+    outs = {}
+    for spectra, be in ((1, a.backend), (0, a.backend)) + (((1, 1),) if a.check else ()):
         cp = CouplingParams(nf1=g.nf1, nf2=g.nf2, nwnmax=g.nwnmax, nkfmax=nkf, nsp=nsp, df=g.df, sigma=g.sigma,
                             re=ex.r[0], nsamp=nsamp, dt=dt, tred=0.0, order_highpass=2, fc_highpass=0.002,
                             order_lowpass=4, fc_lowpass=0.8 * g.nf2 * g.df, thetas=0.3, phis=1.0, thetac=0.5,
@@ -78,17 +83,25 @@ def main(argv=None):
         for _ in range(a.repeat):
             torch.cuda.synchronize()
             t0.record()
-            rc = lib().gem_coupling_run_device(fk._h, ctypes.byref(cp), P(nwn), dgr.data_ptr(), dgi.data_ptr(),
+            rc = lib().gem_coupling_run_device(ctxs[be]._h, ctypes.byref(cp), P(nwn), dgr.data_ptr(), dgi.data_ptr(),
                                                P(zel), P(src), npts, P(delta), P(xi), P(nrm),
                                                out.data_ptr() if spectra else None,
                                                None if spectra else out.data_ptr(), None)
             t1.record()
             torch.cuda.synchronize()
             if rc:
-                raise SystemExit(lib().gem_last_error(fk._h).decode())
+                raise SystemExit(lib().gem_last_error(ctxs[be]._h).decode())
             ms.append(t0.elapsed_time(t1))
-        res["spectra_ms" if spectra else "traces_ms"] = round(min(ms), 3)
-        res["finite_" + ("spectra" if spectra else "traces")] = bool(torch.isfinite(out).all().item())
+        tag = ("spectra" if spectra else "traces") + ("" if be == a.backend else "_fp64")
+        res[tag + "_ms"] = round(min(ms), 3)
+        res["finite_" + tag] = bool(torch.isfinite(out).all().item())
+        outs[tag] = out
+    if a.check:   # largest difference relative to each (point, component) spectrum's peak
+        got = outs["spectra"].view(npts, 6, g.nf2, 2)
+        ref = outs["spectra_fp64"].view(npts, 6, g.nf2, 2)
+        mag = torch.sqrt((ref ** 2).sum(-1))
+        scale = mag.amax(dim=2, keepdim=True).clamp_min(1e-300)
+        res["spectra_rel_diff_fp64"] = float((torch.sqrt(((got - ref) ** 2).sum(-1)) / scale).max().item())
     print(json.dumps(res))
 
 

@@ -9,7 +9,9 @@
 //                        table kind: taper, (2l+1)/4pi, factor and spectrum
 //                        (harmonicDegreeSums.f90:95-369, index map :34-45)
 //   cpl_gemm_kernel      the degree sums of every (frequency, sum, point) as one
-//                        FP64 tiled product per table kind
+//                        FP64 tiled product per table kind; with the fast
+//                        backend the same 13 products run on the tensor cores
+//                        as sliced-INT8 integer products (sums_tc.cu)
 //   cpl_point_kernel     displacement and its derivatives, strain, stress, the
 //                        rotation to the box frame, traction = stress * n,
 //                        event filter, i omega and time shift
@@ -28,6 +30,7 @@ namespace {
 
 constexpr int CPL_NSUM = 42;
 constexpr int CPL_NKIND = 13;   // plm m0-2, dpdt m0-2, pdst m1-2, d2pdt2 m0-2, dtpdst m1-2
+static_assert(CPL_NKIND <= TC_MAX_KIND, "the tensor-core sums take at most TC_MAX_KIND table kinds");
 
 // per sum: table kind, first degree, factor numerator over l(l+1) (0: none),
 // column of its (component, jump) in the DSV spectra U, V, dU/dr, dV/dr (x 4
@@ -515,7 +518,25 @@ extern "C" int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* 
   int maxnsk = 0;
   for (int kd = 0; kd < CPL_NKIND; ++kd) maxnsk = std::max(maxnsk, S.nsk[kd]);
   const dim3 ggrid((unsigned)((npts + CT_N - 1) / CT_N), (unsigned)((2 * nf * maxnsk + CT_M - 1) / CT_M), CPL_NKIND);
-  cpl_gemm_kernel<<<ggrid, 256, 0, st>>>(S, A, tab, C);
+  if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST) {
+    // the degree sums on tcgen05: 6 INT8 slices per operand, exact INT32 accumulation
+    TcProblem TP{};
+    TP.nkind = CPL_NKIND; TP.ncol = npts; TP.lcap = lcap; TP.lmax = p->nwnmax - 1; TP.nf1 = p->nf1; TP.nf2 = p->nf2;
+    TP.nslice = 7;   // 49 bits: strain, stress and traction cancel between the 42 sums
+    long long mtot = 0;
+    for (int kd = 0; kd < CPL_NKIND; ++kd) {
+      TP.nsk[kd] = S.nsk[kd];
+      TP.coff[kd] = S.coff[kd];
+      mtot += 2LL * nf * S.nsk[kd];
+    }
+    const size_t wsb = sums_tc_workspace(TP, mtot, nullptr);
+    void* tws = gem_ctx_aux(ctx, 14, wsb);
+    if (!tws) return GEM_ERROR;
+    if (const char* why = sums_tc_run(TP, nwn, mtot, tab, A, C, tws, wsb, gem_ctx_tc_wait_ns(ctx), st))
+      return gem_set_error(ctx, why);
+  } else {
+    cpl_gemm_kernel<<<ggrid, 256, 0, st>>>(S, A, tab, C);
+  }
   const long long nthr = (long long)npts * nf;
   cpl_point_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, st>>>(S, C, X);
   cudaError_t e = cudaGetLastError();

@@ -17,8 +17,6 @@
 // One CTA per trace.
 #include <cuda_runtime.h>
 
-#include <algorithm>
-
 #include "synth.h"
 
 namespace gem {
@@ -242,144 +240,6 @@ __global__ void __launch_bounds__(H / 16, H == 4096 ? 3 : 1) ifft_fast_kernel(Sy
   }
 }
 
-// ---------------------------------------------------------------------------
-//  Narrow-band form.  When every bin of the band lies below M/2 = 512 (nf2 <=
-//  512; true of all configurations here), Z_k is nonzero only for k in
-//  [lo, hi] and [H - hi, H - lo], i.e. within (-M/2, M/2) modulo H.  With
-//  S = H / M and n = S q + s (q < M, s < S):
-//    z_{S q + s} = sum_k (Z_k e^{2 pi i k s/H}) e^{2 pi i k q/M},
-//  and k mod M is one-to-one on the band, so each of the S output cosets is one
-//  M-point inverse DFT of the band's points, folded modulo M and multiplied by
-//  e^{2 pi i k s/H}.  One warp computes one coset as a four-step 32 x 32
-//  transform: a 32-point DFT in each lane's registers over k1 (k = 32 k1 +
-//  lane), the twiddle e^{2 pi i lane q1/M}, a transpose through the warp's own
-//  shared-memory tile, and a second 32-point DFT; no CTA-wide barrier until
-//  the S cosets meet in a shared staging buffer, from which the trace is
-//  written with coalesced stores.  For the band's bins k' (lo <= k' <= hi):
-//    Z_{k'}      = X_{k'} (1 + i w^{k'})              (X_{k'+H} = 0),
-//    Z_{H - k'}  = conj(X_{k'}) (1 - i w^{H - k'})   (X_{H - k'} = 0),
-//  and H - k' folds to M - k'.
-// ---------------------------------------------------------------------------
-
-// e^{2 pi i n/32}, n = 0..15
-__device__ __constant__ const double2 W32[16] = {
-    {1.0, 0.0},
-    {0.9807852804032304491262, 0.1950903220161282678483},
-    {0.9238795325112867561282, 0.3826834323650897717285},
-    {0.8314696123025452370788, 0.5555702330196022247428},
-    {0.7071067811865475244008, 0.7071067811865475244008},
-    {0.5555702330196022247428, 0.8314696123025452370788},
-    {0.3826834323650897717285, 0.9238795325112867561282},
-    {0.1950903220161282678483, 0.9807852804032304491262},
-    {0.0, 1.0},
-    {-0.1950903220161282678483, 0.9807852804032304491262},
-    {-0.3826834323650897717285, 0.9238795325112867561282},
-    {-0.5555702330196022247428, 0.8314696123025452370788},
-    {-0.7071067811865475244008, 0.7071067811865475244008},
-    {-0.8314696123025452370788, 0.5555702330196022247428},
-    {-0.9238795325112867561282, 0.3826834323650897717285},
-    {-0.9807852804032304491262, 0.1950903220161282678483}};
-
-namespace {
-// 32-point inverse DFT in place, natural order: out_k = sum_n v_n e^{2 pi i nk/32}
-__device__ __forceinline__ void dft32(double2* v) {
-  double2 e[16], o[16];
-#pragma unroll
-  for (int n = 0; n < 16; ++n) { e[n] = v[2 * n]; o[n] = v[2 * n + 1]; }
-  dft16(e);
-  dft16(o);
-#pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    const double2 t = k == 0 ? o[0] : cmul(o[k], W32[k]);
-    v[k] = cadd(e[k], t);
-    v[k + 16] = csub(e[k], t);
-  }
-}
-__device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -a.y); }
-}  // namespace
-
-constexpr int IFFT_BAND_M = 1024;        // points of one coset transform (32 x 32)
-constexpr int IFFT_BAND_TILE = 32 * 33;  // double2 per warp transpose tile (padded rows)
-
-template <int S>
-__global__ void __launch_bounds__(32 * S, S == 4 ? 3 : (S == 2 ? 5 : 8))
-    ifft_band_kernel(SynthDev D, const double2* __restrict__ X, const double2* __restrict__ tw,
-                     const double* __restrict__ fac, float* traces) {
-  extern __shared__ double2 smb[];
-  constexpr int M = IFFT_BAND_M, H = M * S, N = 2 * H;
-  const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
-  const long long tr = blockIdx.x;
-  const double2* __restrict__ x = X + tr * D.ldx;
-  const int lo = D.nf1 - 1, hi = D.nf2 - 1;   // 0-based bins of the band, hi < M/2
-  // e^{2 pi i j s/H} = e^{2 pi i 32 k1 s/H} e^{2 pi i lane s/H} for j = 32 k1 + lane
-  const double2 bl = tw[(2 * s * lane) & (N - 1)];
-  double2 v[32];
-#pragma unroll
-  for (int k1 = 0; k1 < 32; ++k1) {
-    double2 y = make_double2(0.0, 0.0);
-    const int j0 = 32 * k1;   // warp-uniform: skip blocks of 32 outside both folded ranges
-    const bool low = j0 <= hi && j0 + 31 >= lo, mirrored = M - (j0 + 31) <= hi && M - j0 >= lo;
-    if (low || mirrored) {
-      const int j = j0 + lane;
-      const double2 ak = tw[(64 * s * k1) & (N - 1)];
-      if (j >= lo && j <= hi) {
-        const double2 a = x[j], w = tw[j];
-        // Z = a (1 + i w)
-        const double2 z = make_double2(a.x - (w.x * a.y + w.y * a.x), a.y + (w.x * a.x - w.y * a.y));
-        y = cmul(cmul(z, ak), bl);
-      } else {
-        const int kp = M - j;   // the bin whose mirror folds to j
-        if (kp >= lo && kp <= hi && kp > 0) {
-          const double2 a = conj2(x[kp]), w = tw[H - kp];
-          // Z = a (1 - i w), times e^{2 pi i (H - kp) s/H} = e^{-2 pi i kp s/H} = conj(e^{2 pi i kp s/H})
-          const double2 z = make_double2(a.x + (w.x * a.y + w.y * a.x), a.y - (w.x * a.x - w.y * a.y));
-          y = cmul(z, conj2(tw[(2 * s * kp) & (N - 1)]));
-        }
-      }
-    }
-    v[k1] = y;
-  }
-  dft32(v);   // v[q1] = sum_k1 Y[32 k1 + lane] e^{2 pi i k1 q1/32}
-#pragma unroll
-  for (int q1 = 1; q1 < 32; ++q1) v[q1] = cmul(v[q1], tw[lane * q1 * 2 * S]);   // e^{2 pi i lane q1/M}
-  double2* T = smb + s * IFFT_BAND_TILE;
-#pragma unroll
-  for (int q1 = 0; q1 < 32; ++q1) T[lane * 33 + q1] = v[q1];
-  __syncwarp();
-#pragma unroll
-  for (int k2 = 0; k2 < 32; ++k2) v[k2] = T[k2 * 33 + lane];
-  dft32(v);   // v[q2] = z_{S (lane + 32 q2) + s}
-  __syncthreads();   // every warp is done with its tile: the staging buffer reuses them
-  float* stage = reinterpret_cast<float*>(smb);
-  const int ndec = D.ndec, nsamp = D.nsamp;
-#pragma unroll
-  for (int q2 = 0; q2 < 32; ++q2) {
-    const int n = S * (lane + 32 * q2) + s;
-    const int t0 = 2 * n, t1 = 2 * n + 1;
-    if (ndec == 1) {
-      if (t0 < nsamp) stage[t0] = (float)(v[q2].x * D.df * fac[t0]);
-      if (t1 < nsamp) stage[t1] = (float)(v[q2].y * D.df * fac[t1]);
-    } else {
-      if (t0 % ndec == 0 && t0 / ndec < nsamp) stage[t0 / ndec] = (float)(v[q2].x * D.df * fac[t0 / ndec]);
-      if (t1 % ndec == 0 && t1 / ndec < nsamp) stage[t1 / ndec] = (float)(v[q2].y * D.df * fac[t1 / ndec]);
-    }
-  }
-  __syncthreads();
-  float* out = traces + tr * nsamp;
-  if ((nsamp & 3) == 0 && ((tr * nsamp) & 3) == 0) {
-    for (int i = 4 * threadIdx.x; i < nsamp; i += 4 * blockDim.x)
-      *reinterpret_cast<float4*>(out + i) = *reinterpret_cast<const float4*>(stage + i);
-  } else {
-    for (int i = threadIdx.x; i < nsamp; i += blockDim.x) out[i] = stage[i];
-  }
-}
-
-// the narrow-band form applies: half length a multiple of M up to 4096, band below M/2
-bool ifft_band_supported(int ns, int nf1, int nf2) {
-  const int H = ns / 2;
-  return (H == 1024 || H == 2048 || H == 4096) && nf1 >= 1 && nf2 <= IFFT_BAND_M / 2;
-}
-
 // Launch: ns in 512..8192.  tw: the ns + IFFT_TW_EXTRA twiddles of ifft_fast_twiddles; fac: nsamp factors.
 cudaError_t ifft_fast_launch(const SynthDev& S, long long ntr, const double2* X, const double2* tw, const double* fac,
                              float* traces, cudaStream_t st) {
@@ -393,21 +253,6 @@ cudaError_t ifft_fast_launch(const SynthDev& S, long long ntr, const double2* X,
     kern<<<(unsigned)ntr, threads, smem, st>>>(S, X, tw, fac, traces);
     return cudaGetLastError();
   };
-  if (ifft_band_supported(S.ns, S.nf1, S.nf2)) {
-    const int Sc = H / IFFT_BAND_M;
-    const size_t sb = std::max((size_t)Sc * IFFT_BAND_TILE * sizeof(double2), (size_t)S.nsamp * sizeof(float));
-    auto band = [&](auto kern) -> cudaError_t {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
-      if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-      if (e != cudaSuccess) return e;
-      kern<<<(unsigned)ntr, 32 * Sc, sb, st>>>(S, X, tw, fac, traces);
-      return cudaGetLastError();
-    };
-    if (Sc == 1) return band(ifft_band_kernel<1>);
-    if (Sc == 2) return band(ifft_band_kernel<2>);
-    return band(ifft_band_kernel<4>);
-  }
   switch (H) {
     case 256: return go(ifft_fast_kernel<256>, 16);
     case 512: return go(ifft_fast_kernel<512>, 32);

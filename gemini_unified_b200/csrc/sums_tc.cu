@@ -18,10 +18,10 @@
 // five orders of magnitude (near-antipodal stations), which FP16 operands with
 // FP32 accumulation cannot.
 //
-// GEMM kernel: one CTA per 128 x 80 output tile (TC_BM x TC_BN).  Per k-block of 64 degrees,
+// GEMM kernel: one CTA per 128 x BN output tile (BN 80 with 6 slices, 64 with 7).  Per k-block of 64 degrees,
 // warp 0 issues TMA loads (64-byte swizzle) of the S slices of A and of T into
 // a 2-stage shared-memory ring; warp 1 issues the S(S+1)/2 slice products (2 MMAs
-// of K 32 each) into S TMEM accumulators of TC_BN columns, one per weight w = i + j;
+// of K 32 each) into S TMEM accumulators of BN columns, one per weight w = i + j;
 // warps 2-5 combine the accumulators in FP64 and write C.  All mbarrier waits
 // of the pipeline are bounded by a timer (1 s unless the context sets another
 // limit): a wait that runs out records an error flag, the CTA stops issuing
@@ -46,19 +46,27 @@ namespace gem {
 // at the same error: each A tile is loaded for 80 stations instead of 64.
 constexpr int TC_S = 6;
 constexpr int TC_BM = 128, TC_BN = 80, TC_BK = 64;      // tile; BK int8 = one swizzle row (64 or 32 bytes)
+// The coupling synthetics combine 42 sums into strain, stress and traction, whose cancellations amplify
+// the products' error: with 6 slices their spectra reach 5e-8 of a spectrum's peak against the oracle,
+// with 7 (49 bits; 7 accumulators of 64 columns) the FP64 level.
+constexpr int TC_S_FINE = 7, TC_BN_FINE = 64;
 static_assert(TC_BK == 64 || TC_BK == 32, "swizzle spans of 64 or 32 bytes");
 // Two stages: measured on the same step, 3 stages at N = 64 (8.51 ms) and 5 stages of BK = 32
 // at N = 80 (8.74 ms) both lose to 2 stages of BK = 64 at N = 80 (7.63 ms): the operand bytes
 // per product from L2 bound the main loop, not the depth of the pipeline.
 constexpr int TC_STAGES = 2;
 constexpr int TC_A_BYTES = TC_BM * TC_BK;               // 8 KiB per slice
-constexpr int TC_B_BYTES = TC_BN * TC_BK;               // 5 KiB per slice (10 swizzle atoms of 512 B)
-constexpr int TC_STAGE_BYTES = TC_S * (TC_A_BYTES + TC_B_BYTES);   // 78 KiB
 constexpr int TC_THREADS = 192;
-constexpr int TC_TMEM_COLS = 512;                       // S accumulators of TC_BN columns (power-of-two allocation)
-static_assert(TC_S * TC_BN <= TC_TMEM_COLS, "the accumulators must fit the tensor memory");
-static_assert(TC_BN % 16 == 0 && TC_BN >= 16 && TC_BN <= 256, "MMA N of kind::i8 with M = 128");
-constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
+constexpr int TC_TMEM_COLS = 512;                       // NS accumulators of BN columns (power-of-two allocation)
+// shape of one product: NS slices per operand, BN stations (columns) per tile
+template <int NS, int BN> struct TcShape {
+  static constexpr int B_BYTES = BN * TC_BK;                        // 5 KiB per slice at BN = 80
+  static constexpr int STAGE_BYTES = NS * (TC_A_BYTES + B_BYTES);   // 78 KiB at (6, 80), 84 KiB at (7, 64)
+  static constexpr int SMEM = TC_STAGES * STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
+  static_assert(NS * BN <= TC_TMEM_COLS, "the accumulators must fit the tensor memory");
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "MMA N of kind::i8 with M = 128");
+  static_assert(SMEM <= 227 * 1024, "stages must fit the shared memory of a CTA");
+};
 constexpr unsigned long long TC_WAIT_NS = 1000000000ull;   // default pipeline wait limit and the drain limit
 
 // ---------------------------------------------------------------------------
@@ -77,13 +85,14 @@ __device__ __forceinline__ double pow2_above(double x) {
 // slices are the base-128 digits of u = trunc(|x| 128^S) with the sign of x
 // (x 128^S is exact and the conversion truncates), the same digits as S
 // rounds of x *= 128, q = trunc(x), x -= q, all of which are exact.
-static_assert(TC_S <= 8, "the digits must fit a 64-bit integer");
-__device__ __forceinline__ void slices_of(double x, signed char q[TC_S]) {
-  const long long y = (long long)(x * (double)(1ull << (7 * TC_S)));
+template <int NS>
+__device__ __forceinline__ void slices_of(double x, signed char q[NS]) {
+  static_assert(NS <= 8, "the digits must fit a 64-bit integer");
+  const long long y = (long long)(x * (double)(1ull << (7 * NS)));
   const unsigned long long u = y < 0 ? (unsigned long long)(-y) : (unsigned long long)y;
 #pragma unroll
-  for (int i = 0; i < TC_S; ++i) {
-    const int d = (int)((u >> (7 * (TC_S - 1 - i))) & 127u);
+  for (int i = 0; i < NS; ++i) {
+    const int d = (int)((u >> (7 * (NS - 1 - i))) & 127u);
     q[i] = (signed char)(y < 0 ? -d : d);
   }
 }
@@ -147,11 +156,12 @@ __global__ void tab_colscale_kernel(int n, const unsigned long long* __restrict_
 // T8[j][kind*nsta + sta][l] = slice j of T / (s_l c_sta) for a tile of 64 degrees x 64
 // stations: slices formed on the coalesced read (consecutive stations) into a
 // shared byte tile [slice][station][degree], written back as 4-degree words
-__global__ void tab_slice_kernel(int nsta, int lcap, int K, int Kp, const double* __restrict__ tab,
+template <int NS>
+__global__ void tab_slice_kernel(int nkind, int nsta, int lcap, int K, int Kp, const double* __restrict__ tab,
                                  const double* __restrict__ lscale, const double* __restrict__ cscale,
                                  signed char* T8) {
   constexpr int ROW = 68;   // bytes per station row: 17 words, so the byte writes of a warp hit distinct banks
-  __shared__ __align__(16) signed char dig[TC_S][64][ROW];
+  __shared__ __align__(16) signed char dig[NS][64][ROW];
   __shared__ double sl[64], il[64];
   const int kind = blockIdx.z;
   const int l0 = blockIdx.x * 64, s0 = blockIdx.y * 64;
@@ -168,30 +178,31 @@ __global__ void tab_slice_kernel(int nsta, int lcap, int K, int Kp, const double
     const int l = l0 + r;
     double v = 0.0;
     if (l < K && sta < nsta) v = div_pow2(div_pow2(tab[((long long)kind * lcap + l) * nsta + sta], sl[r], il[r]), cs, ic);
-    signed char q[TC_S];
-    slices_of(v, q);
+    signed char q[NS];
+    slices_of<NS>(v, q);
 #pragma unroll
-    for (int j = 0; j < TC_S; ++j) dig[j][tx][r] = q[j];
+    for (int j = 0; j < NS; ++j) dig[j][tx][r] = q[j];
   }
   __syncthreads();
-  const long long plane = 8LL * nsta * Kp;
+  const long long plane = (long long)nkind * nsta * Kp;
   for (int e = threadIdx.x; e < 64 * 16; e += 256) {
     const int r = e >> 4, w = e & 15;   // station row of the tile, word of 4 degrees
     if (s0 + r >= nsta) continue;
     const long long o = ((long long)kind * nsta + s0 + r) * Kp + l0 + 4 * w;   // Kp, l0: multiples of 64
 #pragma unroll
-    for (int j = 0; j < TC_S; ++j)
+    for (int j = 0; j < NS; ++j)
       *reinterpret_cast<uint32_t*>(T8 + j * plane + o) = *reinterpret_cast<const uint32_t*>(&dig[j][r][4 * w]);
   }
 }
 
 // A8[i][row][l] = slice i of A[row][l] s_l / r_row; one block per row of every kind
-__global__ void coef_slice_kernel(SynthDev S, long long mtot, int K, int Kp, const double* __restrict__ A,
+template <int NS>
+__global__ void coef_slice_kernel(int lcap, long long mtot, int K, int Kp, const double* __restrict__ A,
                                   const double* __restrict__ lscale, const int* __restrict__ row_kind,
                                   signed char* A8, double* rscale) {
   const long long row = blockIdx.x;
   const int kind = row_kind[row];
-  const double* a = A + row * S.lcap;
+  const double* a = A + row * lcap;
   const double* sl = lscale + (long long)kind * Kp;
   double m = 0.0;
   for (int l = threadIdx.x; l < K; l += blockDim.x) m = fmax(m, fabs(a[l] * sl[l]));
@@ -199,10 +210,10 @@ __global__ void coef_slice_kernel(SynthDev S, long long mtot, int K, int Kp, con
   if (threadIdx.x == 0) rscale[row] = r;
   const long long plane = mtot * Kp;
   for (int l = threadIdx.x; l < Kp; l += blockDim.x) {
-    signed char q[TC_S];
-    slices_of(l < K ? div_pow2(a[l] * sl[l], r, ir) : 0.0, q);
+    signed char q[NS];
+    slices_of<NS>(l < K ? div_pow2(a[l] * sl[l], r, ir) : 0.0, q);
 #pragma unroll
-    for (int i = 0; i < TC_S; ++i) A8[i * plane + row * Kp + l] = q[i];
+    for (int i = 0; i < NS; ++i) A8[i * plane + row * Kp + l] = q[i];
   }
 }
 
@@ -281,19 +292,23 @@ __device__ __forceinline__ uint64_t smem_desc_kmajor(const void* p) {
   return d;
 }
 
-// kind::i8 instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = TC_BN, M = 128
-constexpr uint32_t TC_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
-                              ((uint32_t)(TC_BM >> 4) << 24);
+// kind::i8 instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = BN, M = 128
+template <int BN>
+__host__ __device__ constexpr uint32_t tc_idesc() {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
 
+template <int NS, int BN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     sums_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                    const int4* __restrict__ tiles, const int* __restrict__ kind_rows,
-                   const long long* __restrict__ kind_rowoff, const long long* __restrict__ coff, int nsta,
+                   const long long* __restrict__ kind_rowoff, const long long* __restrict__ coff, int nkind, int nsta,
                    long long mtot, const double* __restrict__ rscale, const double* __restrict__ cscale,
                    double* C, int* err, unsigned long long wait_ns) {
+  using Sh = TcShape<NS, BN>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = (uint64_t*)(smem + TC_STAGES * TC_STAGE_BYTES);
+  uint64_t* full = (uint64_t*)(smem + TC_STAGES * Sh::STAGE_BYTES);
   uint64_t* empty = full + TC_STAGES;
   uint64_t* acc_full = empty + TC_STAGES;
   uint32_t* tmem_slot = (uint32_t*)(acc_full + 1);
@@ -304,7 +319,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   // beyond its largest wavenumber count, so its k-loop stops there
   const int4 t = tiles[blockIdx.y];
   const int kind = t.x, m0 = t.y, nkb = t.z;
-  const int n0 = blockIdx.x * TC_BN;
+  const int n0 = blockIdx.x * BN;
   const int Mk = kind_rows[kind];
   const long long rowA = kind_rowoff[kind] + m0;
   const long long rowB = (long long)kind * nsta + n0;
@@ -331,34 +346,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % TC_STAGES;
       if (kb >= TC_STAGES && !mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1, abort_flag, wait_ns)) break;
-      unsigned char* st = smem + s * TC_STAGE_BYTES;
-      mbar_expect_tx(&full[s], TC_STAGE_BYTES);
+      unsigned char* st = smem + s * Sh::STAGE_BYTES;
+      mbar_expect_tx(&full[s], Sh::STAGE_BYTES);
 #pragma unroll 1
-      for (int i = 0; i < TC_S; ++i)
+      for (int i = 0; i < NS; ++i)
         tma_load_2d(st + i * TC_A_BYTES, &mapA, &full[s], kb * TC_BK, (int)(i * mtot + rowA));
 #pragma unroll 1
-      for (int j = 0; j < TC_S; ++j)
-        tma_load_2d(st + TC_S * TC_A_BYTES + j * TC_B_BYTES, &mapB, &full[s], kb * TC_BK,
-                    (int)(j * 8LL * nsta + rowB));
+      for (int j = 0; j < NS; ++j)
+        tma_load_2d(st + NS * TC_A_BYTES + j * Sh::B_BYTES, &mapB, &full[s], kb * TC_BK,
+                    (int)(j * (long long)nkind * nsta + rowB));
       ++issued;
     }
     for (int kb = (issued > TC_STAGES ? issued - TC_STAGES : 0); kb < issued; ++kb)
       mbar_drain(&full[kb % TC_STAGES], (kb / TC_STAGES) & 1);
   } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer: accumulator w = i + j at TMEM columns TC_BN w
+    // ---- MMA issuer: accumulator w = i + j at TMEM columns BN w
     bool ok = true;
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % TC_STAGES;
       if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1, abort_flag, wait_ns)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;");
-      const unsigned char* st = smem + s * TC_STAGE_BYTES;
+      const unsigned char* st = smem + s * Sh::STAGE_BYTES;
 #pragma unroll 1
-      for (int i = 0; i < TC_S; ++i) {
+      for (int i = 0; i < NS; ++i) {
         const uint64_t da = smem_desc_kmajor(st + i * TC_A_BYTES);
 #pragma unroll 1
-        for (int j = 0; j + i < TC_S; ++j) {
-          const uint64_t db = smem_desc_kmajor(st + TC_S * TC_A_BYTES + j * TC_B_BYTES);
-          const uint32_t dtm = tmem + (uint32_t)((i + j) * TC_BN);
+        for (int j = 0; j + i < NS; ++j) {
+          const uint64_t db = smem_desc_kmajor(st + NS * TC_A_BYTES + j * Sh::B_BYTES);
+          const uint32_t dtm = tmem + (uint32_t)((i + j) * BN);
 #pragma unroll
           for (int kk = 0; kk < TC_BK / 32; ++kk) {
             const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 32 int8 = 32 bytes along K
@@ -367,7 +382,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 "{\n\t.reg .pred p;\n\t"
                 "setp.ne.b32 p, %4, 0;\n\t"
                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtm),
-                "l"(da + adv), "l"(db + adv), "r"(TC_IDESC), "r"(acc));
+                "l"(da + adv), "l"(db + adv), "r"(tc_idesc<BN>()), "r"(acc));
           }
         }
       }
@@ -395,16 +410,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const double rs = row_ok ? rscale[kind_rowoff[kind] + r] : 0.0;
     double* crow = C + coff[kind] + (long long)r * nsta;
     const double* cs = cscale + (long long)kind * nsta;
-    // columns in chunks of 16 (TC_BN is a multiple of 16)
+    // columns in chunks of 16 (BN is a multiple of 16)
 #pragma unroll 1
-    for (int c = 0; c < TC_BN / 16; ++c) {
+    for (int c = 0; c < BN / 16; ++c) {
       double sum[16];
 #pragma unroll
       for (int jj = 0; jj < 16; ++jj) sum[jj] = 0.0;
 #pragma unroll 1
-      for (int w = TC_S - 1; w >= 0; --w) {
+      for (int w = NS - 1; w >= 0; --w) {
         uint32_t v[16];
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * TC_BN + c * 16);
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * BN + c * 16);
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
@@ -475,20 +490,22 @@ struct TcLayout {
   size_t off[10], total;
 };
 
-TcLayout tc_layout(const SynthDev& S, long long mtot) {
+int tc_slices(const TcProblem& P) { return P.nslice == TC_S_FINE ? TC_S_FINE : TC_S; }
+
+TcLayout tc_layout(const TcProblem& P, long long mtot) {
   TcLayout L{};
-  const int K = S.lmax + 1;
+  const int K = P.lmax + 1, nk = P.nkind, ns = tc_slices(P);
   L.Kp = (K + 63) / 64 * 64;   // the slicing kernels work on 64-degree tiles
-  const size_t sz[10] = {(size_t)TC_S * 8 * S.nsta * L.Kp,            // T8
-                        (size_t)TC_S * mtot * L.Kp,                   // A8
-                        (size_t)8 * L.Kp * sizeof(double),            // lscale
-                        (size_t)8 * S.nsta * sizeof(double),          // cscale
+  const size_t sz[10] = {(size_t)ns * nk * P.ncol * L.Kp,             // T8
+                        (size_t)ns * mtot * L.Kp,                     // A8
+                        (size_t)nk * L.Kp * sizeof(double),           // lscale
+                        (size_t)nk * P.ncol * sizeof(double),         // cscale
                         (size_t)mtot * sizeof(double),                // rscale
                         (size_t)mtot * sizeof(int),                   // row kind
-                        (size_t)(mtot / TC_BM + 16) * sizeof(int4),   // tiles
-                        (size_t)24 * sizeof(long long),               // per-kind tables
-                        (size_t)16 * sizeof(int),                     // kind rows + error flag
-                        (size_t)8 * S.nsta * sizeof(unsigned long long)};   // column maxima
+                        (size_t)(mtot / TC_BM + nk + 1) * sizeof(int4),   // tiles
+                        (size_t)3 * TC_MAX_KIND * sizeof(long long),  // per-kind tables
+                        (size_t)(TC_MAX_KIND + 8) * sizeof(int),      // kind rows + error flag
+                        (size_t)nk * P.ncol * sizeof(unsigned long long)};   // column maxima
   size_t b = 0;
   for (int i = 0; i < 10; ++i) {
     L.off[i] = b;
@@ -502,24 +519,67 @@ TcLayout tc_layout(const SynthDev& S, long long mtot) {
 
 namespace gem {
 
-size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out) {
-  TcLayout L = tc_layout(S, mtot);
+TcProblem tc_problem_of(const SynthDev& S) {
+  TcProblem P{};
+  P.nkind = 8; P.ncol = S.nsta; P.lcap = S.lcap; P.lmax = S.lmax; P.nf1 = S.nf1; P.nf2 = S.nf2;
+  for (int k = 0; k < 8; ++k) { P.nsk[k] = S.nsk[k]; P.coff[k] = S.coff[k]; }
+  return P;
+}
+
+size_t sums_tc_workspace(const TcProblem& P, long long mtot, int* Kp_out) {
+  TcLayout L = tc_layout(P, mtot);
   if (Kp_out) *Kp_out = L.Kp;
   return L.total;
 }
 
-// Sliced-integer sums: from the FP64 tables tab[kind][l][sta] and coefficients
-// A[kind rows][lcap], write C[kind][row][sta] in FP64.  ws: device workspace of
+// operand slices of NS digits and the products on BN-column tiles (blocking)
+template <int NS, int BN>
+const char* tc_slice_and_multiply(const TcProblem& P, long long mtot, int K, int Kp, const double* tab, const double* A,
+                                  const double* lscale, const double* cscale, const int* row_kind, signed char* T8,
+                                  signed char* A8, double* rscale, const int4* tiles, size_t ntiles, int* ints,
+                                  const long long* tabs, double* C, unsigned long long wait_ns, cudaStream_t st) {
+  using Sh = TcShape<NS, BN>;
+  const int nk = P.nkind, ncol = P.ncol;
+  tab_slice_kernel<NS><<<dim3(Kp / 64, (ncol + 63) / 64, nk), 256, 0, st>>>(nk, ncol, P.lcap, K, Kp, tab, lscale,
+                                                                            cscale, T8);
+  coef_slice_kernel<NS><<<(unsigned)mtot, 256, 0, st>>>(P.lcap, mtot, K, Kp, A, lscale, row_kind, A8, rscale);
+  // tensor maps over A8 [NS mtot][Kp] and T8 [NS * nkind * ncol][Kp]
+  CUtensorMap mA, mB;
+  if (!make_map(&mA, A8, NS * mtot, Kp, TC_BM) || !make_map(&mB, T8, NS * (long long)nk * ncol, Kp, BN))
+    return "sums_tc: cuTensorMapEncodeTiled failed";
+  if (cudaFuncSetAttribute(sums_tc_kernel<NS, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::SMEM) !=
+      cudaSuccess)
+    return "sums_tc: shared-memory attribute";
+  if (cudaMemsetAsync(ints + TC_MAX_KIND, 0, sizeof(int), st) != cudaSuccess) return "sums_tc: upload failed";
+  dim3 grid((ncol + BN - 1) / BN, (unsigned)ntiles);
+  sums_tc_kernel<NS, BN><<<grid, TC_THREADS, Sh::SMEM, st>>>(mA, mB, tiles, ints, tabs + TC_MAX_KIND,
+                                                             tabs + 2 * TC_MAX_KIND, nk, ncol, mtot, rscale, cscale,
+                                                             C, ints + TC_MAX_KIND, wait_ns ? wait_ns : TC_WAIT_NS);
+  if (cudaGetLastError() != cudaSuccess) return "sums_tc: launch failed";
+  int herr = 0;
+  if (cudaMemcpyAsync(&herr, ints + TC_MAX_KIND, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return "sums_tc: execution failed";
+  if (herr) return "sums_tc: a pipeline wait timed out";
+  return nullptr;
+}
+
+// Sliced-integer sums: from the FP64 tables tab[kind][l][col] and coefficients
+// A[kind rows][lcap], write C[kind][row][col] in FP64.  ws: device workspace of
 // sums_tc_workspace bytes; wait_ns: limit of each pipeline wait (0: 1 s).
 // Blocking (synchronises the stream).
-const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const double* tab, const double* A,
+const char* sums_tc_run(const TcProblem& P, const int* nwn, long long mtot, const double* tab, const double* A,
                         double* C, void* ws, size_t ws_bytes, unsigned long long wait_ns, cudaStream_t st) {
-  TcLayout L = tc_layout(S, mtot);
+  if (P.nkind < 1 || P.nkind > TC_MAX_KIND) return "sums_tc: table kinds outside 1..16";
+  TcLayout L = tc_layout(P, mtot);
   if (ws_bytes < L.total) return "sums_tc: workspace too small";
-  if (7LL * mtot >= (1LL << 31) || 7LL * 8 * S.nsta >= (1LL << 31)) return "sums_tc: operand rows exceed 2^31";
-  if ((long long)L.Kp * TC_S * 127 * 127 >= (1LL << 31)) return "sums_tc: degree range too large for INT32 accumulation";
-  const int K = S.lmax + 1, Kp = L.Kp;
-  const int nf = S.nf2 - S.nf1 + 1;
+  const int nk = P.nkind, ncol = P.ncol;
+  if (7LL * mtot >= (1LL << 31) || 7LL * nk * ncol >= (1LL << 31)) return "sums_tc: operand rows exceed 2^31";
+  if ((long long)L.Kp * tc_slices(P) * 127 * 127 >= (1LL << 31))
+    return "sums_tc: degree range too large for INT32 accumulation";
+  if (P.nslice != 0 && P.nslice != TC_S && P.nslice != TC_S_FINE) return "sums_tc: 6 or 7 slices per operand";
+  const int K = P.lmax + 1, Kp = L.Kp;
+  const int nf = P.nf2 - P.nf1 + 1;
   char* base = (char*)(((uintptr_t)ws + 1023) & ~(uintptr_t)1023);
   signed char* T8 = (signed char*)(base + L.off[0]);
   signed char* A8 = (signed char*)(base + L.off[1]);
@@ -529,24 +589,23 @@ const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const
   int* row_kind = (int*)(base + L.off[5]);
   int4* tiles = (int4*)(base + L.off[6]);
   long long* tabs = (long long*)(base + L.off[7]);
-  int* ints = (int*)(base + L.off[8]);   // [0..7] rows per kind, [8] error flag
+  int* ints = (int*)(base + L.off[8]);   // [0..15] rows per kind, [16] error flag
   unsigned long long* colmax = (unsigned long long*)(base + L.off[9]);
-  int krows[16] = {0};
-  long long htabs[24];
+  int krows[TC_MAX_KIND + 8] = {0};
+  long long htabs[3 * TC_MAX_KIND] = {0};
   std::vector<int4> htiles;
   std::vector<int> hrk((size_t)mtot);
   long long ro = 0;
-  for (int k = 0; k < 8; ++k) {
-    krows[k] = 2 * nf * S.nsk[k];
-    htabs[k] = 0;
-    htabs[8 + k] = ro;
-    htabs[16 + k] = S.coff[k];
+  for (int k = 0; k < nk; ++k) {
+    krows[k] = 2 * nf * P.nsk[k];
+    htabs[TC_MAX_KIND + k] = ro;
+    htabs[2 * TC_MAX_KIND + k] = P.coff[k];
     for (int m = 0; m < krows[k]; m += TC_BM) {
       // rows 2 (slot nsk + rank) + re/im; the coefficients of frequency slot are zero
-      // from degree nwn[nf1 - 1 + slot] on (coef_kernel, bessel_coef_kernel)
-      const int s0 = m / (2 * S.nsk[k]), s1 = std::min(nf - 1, (m + TC_BM - 1) / (2 * S.nsk[k]));
+      // from degree nwn[nf1 - 1 + slot] on
+      const int s0 = m / (2 * P.nsk[k]), s1 = std::min(nf - 1, (m + TC_BM - 1) / (2 * P.nsk[k]));
       int ext = 0;
-      for (int s = s0; s <= s1; ++s) ext = std::max(ext, nwn[S.nf1 - 1 + s]);
+      for (int s = s0; s <= s1; ++s) ext = std::max(ext, nwn[P.nf1 - 1 + s]);
       ext = std::min(ext, K);
       htiles.push_back(make_int4(k, m, std::max(1, (ext + TC_BK - 1) / TC_BK), 0));
     }
@@ -554,6 +613,7 @@ const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const
     ro += krows[k];
   }
   if (ro != mtot) return "sums_tc: row count mismatch";
+  if (htiles.empty()) return nullptr;
   // longest k-loops first: the short tiles fill the last wave
   std::stable_sort(htiles.begin(), htiles.end(), [](const int4& a, const int4& b) { return a.z > b.z; });
   if (cudaMemcpyAsync(tiles, htiles.data(), htiles.size() * sizeof(int4), cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -562,33 +622,17 @@ const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const
       cudaMemcpyAsync(ints, krows, sizeof krows, cudaMemcpyHostToDevice, st) != cudaSuccess)
     return "sums_tc: upload failed";
   // operands
-  tab_scale_kernel<<<dim3(Kp, 8), 256, 0, st>>>(S.nsta, S.lcap, K, tab, lscale, Kp);
-  if (cudaMemsetAsync(colmax, 0, (size_t)8 * S.nsta * sizeof(unsigned long long), st) != cudaSuccess)
+  tab_scale_kernel<<<dim3(Kp, nk), 256, 0, st>>>(ncol, P.lcap, K, tab, lscale, Kp);
+  if (cudaMemsetAsync(colmax, 0, (size_t)nk * ncol * sizeof(unsigned long long), st) != cudaSuccess)
     return "sums_tc: upload failed";
-  tab_colmax_kernel<<<dim3((S.nsta + 127) / 128, (K + 63) / 64, 8), 128, 0, st>>>(S.nsta, S.lcap, K, Kp, tab, lscale,
-                                                                                 colmax);
-  tab_colscale_kernel<<<(8 * S.nsta + 255) / 256, 256, 0, st>>>(8 * S.nsta, colmax, cscale);
-  tab_slice_kernel<<<dim3(Kp / 64, (S.nsta + 63) / 64, 8), 256, 0, st>>>(S.nsta, S.lcap, K, Kp, tab, lscale, cscale,
-                                                                         T8);
-  coef_slice_kernel<<<(unsigned)mtot, 256, 0, st>>>(S, mtot, K, Kp, A, lscale, row_kind, A8, rscale);
-  // tensor maps over A8 [TC_S mtot][Kp] and T8 [TC_S * 8 nsta][Kp]
-  CUtensorMap mA, mB;
-  if (!make_map(&mA, A8, TC_S * mtot, Kp, TC_BM) || !make_map(&mB, T8, TC_S * 8LL * S.nsta, Kp, TC_BN))
-    return "sums_tc: cuTensorMapEncodeTiled failed";
-  if (cudaFuncSetAttribute(sums_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) != cudaSuccess)
-    return "sums_tc: shared-memory attribute";
-  if (cudaMemsetAsync(ints + 8, 0, sizeof(int), st) != cudaSuccess) return "sums_tc: upload failed";
-  dim3 grid((S.nsta + TC_BN - 1) / TC_BN, (unsigned)htiles.size());
-  sums_tc_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(mA, mB, tiles, ints, tabs + 8, tabs + 16, S.nsta, mtot,
-                                                    rscale, cscale, C, ints + 8,
-                                                    wait_ns ? wait_ns : TC_WAIT_NS);
-  if (cudaGetLastError() != cudaSuccess) return "sums_tc: launch failed";
-  int herr = 0;
-  if (cudaMemcpyAsync(&herr, ints + 8, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    return "sums_tc: execution failed";
-  if (herr) return "sums_tc: a pipeline wait timed out";
-  return nullptr;
+  tab_colmax_kernel<<<dim3((ncol + 127) / 128, (K + 63) / 64, nk), 128, 0, st>>>(ncol, P.lcap, K, Kp, tab, lscale,
+                                                                                colmax);
+  tab_colscale_kernel<<<(nk * ncol + 255) / 256, 256, 0, st>>>(nk * ncol, colmax, cscale);
+  if (tc_slices(P) == TC_S_FINE)
+    return tc_slice_and_multiply<TC_S_FINE, TC_BN_FINE>(P, mtot, K, Kp, tab, A, lscale, cscale, row_kind, T8, A8,
+                                                      rscale, tiles, htiles.size(), ints, tabs, C, wait_ns, st);
+  return tc_slice_and_multiply<TC_S, TC_BN>(P, mtot, K, Kp, tab, A, lscale, cscale, row_kind, T8, A8, rscale, tiles,
+                                            htiles.size(), ints, tabs, C, wait_ns, st);
 }
 
 }  // namespace gem

@@ -759,9 +759,10 @@ int synth_run(gem_ctx* ctx, const gem_synth_params* p, const int* nwn, const flo
   if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST) {
     // sliced-integer products on the tensor cores (6 INT8 slices per operand, exact INT32 accumulation)
     const long long mtot = 2LL * nf * S.nsum;
-    const size_t wsb = sums_tc_workspace(S, mtot, nullptr);
+    const TcProblem TP = tc_problem_of(S);
+    const size_t wsb = sums_tc_workspace(TP, mtot, nullptr);
     void* ws = gem_ctx_aux(ctx, 3, wsb);
-    const char* why = ws ? sums_tc_run(S, nwn, mtot, b.tab, b.A, b.C, ws, wsb, gem_ctx_tc_wait_ns(ctx), st) : "";
+    const char* why = ws ? sums_tc_run(TP, nwn, mtot, b.tab, b.A, b.C, ws, wsb, gem_ctx_tc_wait_ns(ctx), st) : "";
     if (why) {
       nvtxRangePop();
       cudaEventDestroy(e0); cudaEventDestroy(e1);

@@ -67,10 +67,23 @@ cudaError_t legendre_fast_launch(int nsta, int lmax, int lcap, const double* the
 // event filter of the synthetics (Butterworth band-pass at f - i sigma/2pi), h[jf] for jf = nf1..nf2
 void event_filter_host(const gem_synth_params* p, std::vector<double2>& h);
 
-// sliced-integer tensor-core degree sums (sums_tc.cu): workspace size and run;
-// nwn: host copy of the wavenumber counts per frequency (1-based frequency index)
-size_t sums_tc_workspace(const SynthDev& S, long long mtot, int* Kp_out);
-const char* sums_tc_run(const SynthDev& S, const int* nwn, long long mtot, const double* tab, const double* A,
+// sliced-integer tensor-core degree sums (sums_tc.cu).  One product per table
+// kind: C[coff[kind] + row * ncol + col] = sum_l A[row][l] T[kind][l][col] for the
+// 2 * nf * nsk[kind] rows of the kind (frequency slot slowest, then sum rank, then
+// re/im; the rows of all kinds contiguous in A with leading dimension lcap), and
+// T[kind][l][col] = tab[(kind * lcap + l) * ncol + col].
+constexpr int TC_MAX_KIND = 16;
+struct TcProblem {
+  int nkind, ncol, lcap, lmax, nf1, nf2;
+  int nslice;   // 7-bit slices per operand: 6 (0 selects it; 42 bits) or 7 (49 bits)
+  int nsk[TC_MAX_KIND];
+  long long coff[TC_MAX_KIND];
+};
+TcProblem tc_problem_of(const SynthDev& S);   // the synthetics' 8 Legendre / Bessel kinds
+// workspace size and run; nwn: host copy of the wavenumber counts per frequency
+// (1-based frequency index); wait_ns: limit of each pipeline wait (0: 1 s)
+size_t sums_tc_workspace(const TcProblem& P, long long mtot, int* Kp_out);
+const char* sums_tc_run(const TcProblem& P, const int* nwn, long long mtot, const double* tab, const double* A,
                         double* C, void* ws, size_t ws_bytes, unsigned long long wait_ns, cudaStream_t st);
 
 }  // namespace gem

@@ -12,10 +12,7 @@ RTOL_L2 = 1e-7
 CASES = [
     # nf1, nf2, df, nsamp, dt: the global configuration's series, a decimated
     # series, the 8192-sample series of the batched configuration, a 512-sample
-    # one, a 4096-sample one, and an 8192-sample one with a band wider than 512
-    # bins.  The fast form runs its narrow-band coset transform on the first,
-    # third and fifth (bands below bin 512, 2048-8192 samples) and its radix-16
-    # Stockham transform on the others.
+    # one, a 4096-sample one, and an 8192-sample one with a band of 1496 bins
     (2, 52, 1.0 / 1024, 2048, 0.5),
     (3, 300, 1.0 / 1024, 256, 4.0),
     (2, 411, 1.0 / 2048, 8192, 0.25),
