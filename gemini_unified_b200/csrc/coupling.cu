@@ -83,12 +83,8 @@ struct CplDev {
   long long aoff[CPL_NKIND], coff[CPL_NKIND];
 };
 
-// tab[(kind * lcap + l) * npts + pt]; one thread per (point, m)
-__global__ void cpl_legendre_kernel(int npts, int lmax, int lcap, const double* __restrict__ delta, double* tab) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= npts * 3) return;
-  const int pt = idx % npts, m = idx / npts;
-  const double ct = cos(delta[pt]), st = sin(delta[pt]);
+// tab[(kind * lcap + l) * npts + pt] of one (point, m), in the reference's operation order
+__device__ void cpl_legendre_series(int pt, int m, int npts, int lmax, int lcap, double ct, double st, double* tab) {
   const bool atpoles = !(st > 0.0);
   auto row = [&](int kind) { return tab + (long long)kind * lcap * npts + pt; };
   double* Tp = row(m);
@@ -133,6 +129,81 @@ __global__ void cpl_legendre_kernel(int npts, int lmax, int lcap, const double* 
       if (Ts) Ts[o] = ps;
       if (Tt) Tt[o] = dts;
     }
+    pl2 = pl1;
+    pl1 = p;
+  }
+}
+// tab[(kind * lcap + l) * npts + pt]; one thread per (point, m)
+__global__ void cpl_legendre_kernel(int npts, int lmax, int lcap, const double* __restrict__ delta, double* tab) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= npts * 3) return;
+  const int pt = idx % npts, m = idx / npts;
+  cpl_legendre_series(pt, m, npts, lmax, lcap, cos(delta[pt]), sin(delta[pt]), tab);
+}
+
+// Fast form (fast backend): the same tables with the upward recurrence written as
+// p_l = alpha_l p_{l-1} + beta_l p_{l-2} and 1/(l - m) from a shared-memory
+// table, so one FMA per degree sits on the dependent chain (the plain form's
+// software division leaves the 3 npts threads of this kernel waiting on it); the
+// derivative tables follow in FMA form.  Rounding differs from the plain form's
+// only (relative 1e-13 at l = 3200).  Poles keep the plain form's special values.
+constexpr int CPL_LF_THREADS = 64;
+__global__ void __launch_bounds__(CPL_LF_THREADS) cpl_legendre_fast_kernel(int npts, int lmax, int lcap,
+                                                                           const double* __restrict__ delta,
+                                                                           double* tab) {
+  extern __shared__ double rcp[];   // rcp[n] = 1/n, n = 1..lmax
+  for (int n = threadIdx.x + 1; n <= lmax; n += blockDim.x) rcp[n] = 1.0 / (double)n;
+  __syncthreads();
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= npts * 3) return;
+  const int pt = idx % npts, m = idx / npts;
+  const double ct = cos(delta[pt]), st = sin(delta[pt]);
+  if (!(st > 0.0)) {
+    cpl_legendre_series(pt, m, npts, lmax, lcap, ct, st, tab);
+    return;
+  }
+  auto row = [&](int kind) { return tab + (long long)kind * lcap * npts + pt; };
+  double* Tp = row(m);
+  double* Td = row(3 + m);
+  double* Ts = m >= 1 ? row(5 + m) : nullptr;
+  double* T2 = row(8 + m);
+  double* Tt = m >= 1 ? row(10 + m) : nullptr;
+  const long long stride = npts;
+  double pmm = 1.0, fact = 1.0;
+  for (int j = 1; j <= m; ++j) { pmm = pmm * fact * st; fact = fact + 2.0; }
+  const double rst = 1.0 / st, ctr = ct * rst, m2r2 = (double)(m * m) * (rst * rst);
+  // d2P/dtheta2 = -(cos/sin) dP/dtheta + (m^2/sin^2 - l(l+1)) P,  d/dtheta (P/sin) = (dP/dtheta - (cos/sin) P)/sin
+  auto put = [&](long long o, double p, double dp, double ll1) {
+    Tp[o] = p;
+    Td[o] = dp;
+    T2[o] = fma(-ctr, dp, (m2r2 - ll1) * p);
+    if (Ts) Ts[o] = p * rst;
+    if (Tt) Tt[o] = rst * fma(-ctr, p, dp);
+  };
+  long long o = 0;
+  for (int l = 0; l < m && l <= lmax; ++l, o += stride) {
+    Tp[o] = 0.0; Td[o] = 0.0; T2[o] = 0.0;
+    if (Ts) Ts[o] = 0.0;
+    if (Tt) Tt[o] = 0.0;
+  }
+  if (m > lmax) return;
+  put(o, pmm, (double)m * ct * pmm * rst, (double)m * (double)(m + 1));   // l = m
+  if (m + 1 > lmax) return;
+  o += stride;
+  const double p1 = ct * (double)(2 * m + 1) * pmm;   // l = m + 1
+  double dl = (double)(m + 1);
+  put(o, p1, fma(dl * ct, p1, -(dl + (double)m) * pmm) * rst, dl * (dl + 1.0));
+  o += stride;
+  double pl2 = pmm, pl1 = p1;
+  const double mm1 = (double)(m - 1), md = (double)m;
+#pragma unroll 2
+  for (int l = m + 2; l <= lmax; ++l, o += stride) {
+    dl += 1.0;
+    const double r = rcp[l - m];
+    const double alpha = ct * fma(2.0, dl, -1.0) * r;
+    const double bp = -(dl + mm1) * r * pl2;   // off the chain: pl2 is known a degree early
+    const double p = fma(alpha, pl1, bp);
+    put(o, p, fma(dl * ct, p, -(dl + md) * pl1) * rst, dl * (dl + 1.0));
     pl2 = pl1;
     pl1 = p;
   }
@@ -512,7 +583,14 @@ extern "C" int gem_coupling_run_device(gem_ctx* ctx, const gem_coupling_params* 
   S.istyp = p->istyp; S.nsum = nsum;
   for (int i = 0; i < (p->istyp == 1 ? 6 : 3); ++i) S.mt[i] = mt[i];
   S.nwn = d_nwn; S.koff = d_koff; S.delta = d_delta; S.xi = d_xi; S.nrm = d_nrm; S.evf = d_evf; S.zel = d_zel;
-  cpl_legendre_kernel<<<(npts * 3 + 127) / 128, 128, 0, st>>>(npts, p->nwnmax - 1, lcap, d_delta, tab);
+  const size_t rcp_bytes = (size_t)p->nwnmax * sizeof(double);
+  if (gem_ctx_backend(ctx) == GEM_BACKEND_GPU_FAST && rcp_bytes <= 200 * 1024) {
+    cudaFuncSetAttribute(cpl_legendre_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rcp_bytes);
+    cpl_legendre_fast_kernel<<<(npts * 3 + CPL_LF_THREADS - 1) / CPL_LF_THREADS, CPL_LF_THREADS, rcp_bytes, st>>>(
+        npts, p->nwnmax - 1, lcap, d_delta, tab);
+  } else {
+    cpl_legendre_kernel<<<(npts * 3 + 127) / 128, 128, 0, st>>>(npts, p->nwnmax - 1, lcap, d_delta, tab);
+  }
   const long long ncoef = (long long)nf * nsum * lcap;
   cpl_coef_kernel<<<(unsigned)((ncoef + 255) / 256), 256, 0, st>>>(S, d_gr, d_gi, A);
   int maxnsk = 0;

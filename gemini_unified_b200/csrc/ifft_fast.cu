@@ -127,8 +127,25 @@ __device__ __forceinline__ void stockham_pass(double2* buf, double2* v, int* idx
     const int j = tid + b * T;
     const int k = j % NS;
     if (NS > 1) {
+      // w^r, r = 1..R-1, of w = e^{2 pi i k/(NS R)}: R = 16 loads w, w^4 and w^8 and forms the
+      // others by products (a few ulps; 3 loads in place of 15, the L1 pipe bounds this kernel)
+      if constexpr (R == 16) {
+        const double2 w1 = twp[k], w4 = twp[3 * NS + k], w8 = twp[7 * NS + k];
+        const double2 w2 = cmul(w1, w1), w3 = cmul(w2, w1);
+        double2* u = v + b * R;
+        u[1] = cmul(u[1], w1); u[2] = cmul(u[2], w2); u[3] = cmul(u[3], w3);
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[b * R + r] = cmul(v[b * R + r], twp[(r - 1) * NS + k]);
+        for (int q = 1; q < 4; ++q) {   // rows 4q .. 4q + 3 with base w^{4q}
+          const double2 wb = q == 1 ? w4 : (q == 2 ? w8 : cmul(w8, w4));
+          u[4 * q] = cmul(u[4 * q], wb);
+          u[4 * q + 1] = cmul(u[4 * q + 1], cmul(wb, w1));
+          u[4 * q + 2] = cmul(u[4 * q + 2], cmul(wb, w2));
+          u[4 * q + 3] = cmul(u[4 * q + 3], cmul(wb, w3));
+        }
+      } else {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[b * R + r] = cmul(v[b * R + r], twp[(r - 1) * NS + k]);
+      }
     }
     dftR<R>(v + b * R);
     const int d = (j / NS) * NS * R + k;
