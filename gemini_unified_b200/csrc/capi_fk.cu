@@ -986,9 +986,6 @@ int gem_proposer_dump_read(gem_ctx* ctx, float* out, long long cap, long long* n
   return GEM_OK;
 }
 
-// Order target of the step-size control (fast backend; no counterpart in the
-// reference, which fixes it at 6, parametersBulirschStep.f90:28-48): k in 3..7;
-// 0 restores 6.
 // Solver schedules (no counterpart in the reference): per phase (toroidal,
 // spheroidal, adjoint) an index into FK_SCHED_BLOCK / FK_SCHED_BIGCACHE, kept
 // per backend.  Every schedule gives bit-identical spectra; only the time differs.
@@ -1168,6 +1165,9 @@ int gem_ray_table(gem_ctx* ctx, int stype, int attmode, double eps, double drtp,
   return GEM_OK;
 }
 
+// Order target of the step-size control (fast backend; no counterpart in the
+// reference, which fixes it at 6, parametersBulirschStep.f90:28-48): k in 3..7;
+// 0 restores 6.
 int gem_order_target(gem_ctx* ctx, int k) {
   if (!ctx) return GEM_ERROR;
   if (k == 0) k = 6;
