@@ -121,11 +121,12 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
   dz t0[NV];
   constexpr bool CACHE = SysCache<SYS, BIG>::value;
   SysM<SYS> Mh, Me;
+  const double h48 = h / 48.0;   // grid spacing of the step's sub-steps
   if (need) {
     apply_sys<SYS>(P, e, x, ys, t0);
     if constexpr (CACHE) {
-      sys_eval<SYS>(P, e, x + (24.0 * h) / 48.0, Mh);
-      sys_eval<SYS>(P, e, x + (48.0 * h) / 48.0, Me);
+      sys_eval<SYS>(P, e, x + 24.0 * h48, Mh);
+      sys_eval<SYS>(P, e, x + 48.0 * h48, Me);
     }
   }
 #endif
@@ -138,7 +139,7 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
     if (!need) continue;
     dz Y[NV];
 #if GEM_FAST
-    midpoint<SYS, CACHE>(P, e, j, h, x, ys, t0, Mh, Me, Y);
+    midpoint<SYS, CACHE>(P, e, j, h48, x, ys, t0, Mh, Me, Y);
 #else
     midpoint<SYS>(P, e, j, h, x, ys, Y);
 #endif
@@ -151,12 +152,14 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
     dz yy[NV], dy[NV], c[NV], pend[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) { yy[v] = Y[v]; c[v] = Y[v]; pend[v] = Y[v]; dy[v] = dz{0.0, 0.0}; }
+#if GEM_FAST
+    for (int m = 1; m <= p; ++m) {
+      const double na = NEV.a[p][m], nb = NEV.b[p][m];
+#else
     const double xp = h / (double)SEQDIV[p];
     for (int m = 1; m <= p; ++m) {
       const double xi = h / (double)SEQDIV[p - m];
       const double hh = xi - xp;
-#if GEM_FAST
-      const double rhh = __drcp_rn(hh);
 #endif
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
@@ -165,12 +168,14 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
         dz pv = dlast[v];
         if (shared_level) { double2 q = *slot; pv = dz{q.x, q.y}; }
 #if GEM_FAST
-        dz u = (c[v] - pv) * rhh;
+        const dz u = c[v] - pv;
+        c[v] = na * u;
+        dz nd = nb * u;
 #else
         dz u = (c[v] - pv) / hh;
-#endif
         c[v] = xi * u;
         dz nd = xp * u;
+#endif
         if (shared_level) *slot = make_double2(pend[v].re, pend[v].im);   // level m-1 of the new diagonal
         else dlast[v] = pend[v];
         pend[v] = nd;

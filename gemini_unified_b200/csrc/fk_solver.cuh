@@ -394,17 +394,37 @@ template <int SYS, bool BIG> struct SysCache {
   static constexpr bool value = BIG || SYS == SYS_TOROIDAL || SYS == SYS_FLUID || SYS == SYS_RADIAL;
 };
 
+// Neville coefficients of the fast build.  With x_k = h / n_k, the update of
+// level m of diagonal p, u = (c - d) / (x_{p-m} - x_p), c' = x_{p-m} u,
+// d' = x_p u, is c' = a (c - d), d' = b (c - d) with a = n_p / (n_p - n_{p-m})
+// and b = n_{p-m} / (n_p - n_{p-m}): h cancels, so no division is left.
+struct NevTab {
+  double a[7][7], b[7][7];
+};
+constexpr NevTab make_nev() {
+  const int n[7] = {2, 4, 6, 8, 12, 16, 24};
+  NevTab t{};
+  for (int p = 1; p < 7; ++p)
+    for (int m = 1; m <= p; ++m) {
+      t.a[p][m] = (double)n[p] / (double)(n[p] - n[p - m]);
+      t.b[p][m] = (double)n[p - m] / (double)(n[p] - n[p - m]);
+    }
+  return t;
+}
+__device__ __constant__ const NevTab NEV = make_nev();
+
 // Modified midpoint of attempt jtry with t0 = A(xstart) y0 given, and with
 // CACHE the matrices at xstart + h/2 (Mh) and xstart + h (Me): the parts every
-// attempt of a step shares.
+// attempt of a step shares.  The grid point g (in 48ths of the step) sits at
+// xstart + g h48, h48 = h / 48 rounded once per step.
 template <int SYS, bool CACHE>
-__device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jtry, double h, double xstart,
+__device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jtry, double h48, double xstart,
                                          const dz* y0, const dz* t0, const SysM<SYS>& Mh, const SysM<SYS>& Me,
                                          dz* out) {
   constexpr int NV = SysNV<SYS>::NV;
   const int nstep = SEQDIV[jtry - 1];
-  const double hdiv = h / (double)nstep;
   const int dix = 48 / nstep;
+  const double hdiv = (double)dix * h48;
   dz z0[NV], z1[NV], t[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) { z0[v] = y0[v]; z1[v] = y0[v] + hdiv * t0[v]; }
@@ -413,7 +433,7 @@ __device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jt
     if (CACHE && m * dix == 24) {
       sys_apply<SYS>(Mh, e, z1, t);
     } else {
-      const double x = xstart + ((double)(m * dix) * h) / 48.0;
+      const double x = xstart + (double)(m * dix) * h48;
       apply_sys<SYS>(P, e, x, z1, t);
     }
 #pragma unroll
@@ -424,7 +444,7 @@ __device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jt
     }
   }
   if constexpr (CACHE) sys_apply<SYS>(Me, e, z1, t);
-  else apply_sys<SYS>(P, e, xstart + (48.0 * h) / 48.0, z1, t);
+  else apply_sys<SYS>(P, e, xstart + 48.0 * h48, z1, t);
 #pragma unroll
   for (int v = 0; v < NV; ++v) out[v] = 0.5 * ((z1[v] + z0[v]) + hdiv * t[v]);
 }
