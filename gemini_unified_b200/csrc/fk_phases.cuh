@@ -99,6 +99,26 @@ struct ItemStore {
   }
 };
 
+// Reference-algorithm work of a step whose lane made attempts 1..j: sub-step
+// matrix-vector products (mv), system matrices on the 1/48 grid (sm), and the
+// extrapolation flops from the third attempt on for NV variables (ext) -- the
+// oracle's accounting, summed once per step from these tables.
+struct StepWork {
+  int mv[8], sm[8], ext[6][8];
+};
+constexpr StepWork make_stepwork() {
+  const int seq[7] = {2, 4, 6, 8, 12, 16, 24}, nx[7] = {3, 2, 4, 4, 4, 8, 8};
+  StepWork w{};
+  for (int j = 1; j <= 7; ++j) {
+    w.mv[j] = w.mv[j - 1] + seq[j - 1] + 1;
+    w.sm[j] = w.sm[j - 1] + nx[j - 1];
+    for (int nv = 0; nv < 6; ++nv)
+      w.ext[nv][j] = w.ext[nv][j - 1] + (j >= 3 ? (j * (j - 1) / 2) * 8 * nv + (j - 1) * 2 * nv + 8 * nv + 3 : 0);
+  }
+  return w;
+}
+__device__ __constant__ const StepWork STEPWORK = make_stepwork();
+
 // ------------------------------------------------------------------------
 //  Lockstep Bulirsch-Stoer step of all lanes with `active` set
 //  (complexBulirschStep.f90:111-170,180-238,297-340)
@@ -107,10 +127,10 @@ template <int SYS, int NVD, int DL, bool BIG>
 __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool active, double h, double x,
                                      const dz* y0, dz* yext, int& result, double2* D, int lane, Counters& cnt_out) {
   constexpr int NV = SysNV<SYS>::NV;
-  // the lane state lives in local memory: work on register copies of the
-  // environment and the counters for the whole step
+  // the lane state lives in local memory: work on a register copy of the
+  // environment; the counters follow from the attempts made (added at the end)
   const Env e = e_in;
-  Counters cnt{};
+  int lane_att = 0, warp_att = 0, jdone = 0;
   bool need = active;
   int res = 0;   // 0: failed; > 0: number of attempts of a successful step
   dz ys[NV];
@@ -134,8 +154,8 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
   for (int j = 1; j <= 7; ++j) {
     unsigned needm = __ballot_sync(0xffffffffu, need);
     if (!needm) break;
-    cnt.lane_attempts += __popc(needm);
-    cnt.warp_attempts += 1;
+    lane_att += __popc(needm);
+    warp_att += 1;
     if (!need) continue;
     dz Y[NV];
 #if GEM_FAST
@@ -143,10 +163,7 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
 #else
     midpoint<SYS>(P, e, j, h, x, ys, Y);
 #endif
-    cnt.attempts++;
-    cnt.matvecs += SEQDIV[j - 1] + 1;
-    cnt.sysmats += NXDIV[j - 1];
-    cnt.flops += (long long)NXDIV[j - 1] * FLOP_SYSMAT[SYS] + (long long)(SEQDIV[j - 1] + 1) * FLOP_MV[SYS];
+    jdone = j;
     // new diagonal of the Neville tableau for point p = j-1 (0-based)
     const int p = j - 1;
     dz yy[NV], dy[NV], c[NV], pend[NV];
@@ -191,7 +208,6 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
       for (int v = 0; v < NV; ++v) dlast[v] = pend[v];
     }
     if (j >= 3) {
-      cnt.flops += (long long)(j * (j - 1) / 2) * 8 * NV + (long long)(j - 1) * 2 * NV + 8 * NV + 3;
       double s1 = 0.0, s2 = 0.0;
 #if GEM_FAST
 #pragma unroll
@@ -218,12 +234,13 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
     }
   }
   result = res;
-  cnt_out.lane_attempts += cnt.lane_attempts;
-  cnt_out.warp_attempts += cnt.warp_attempts;
-  cnt_out.attempts += cnt.attempts;
-  cnt_out.matvecs += cnt.matvecs;
-  cnt_out.sysmats += cnt.sysmats;
-  cnt_out.flops += cnt.flops;
+  const int mv = STEPWORK.mv[jdone], sm = STEPWORK.sm[jdone];
+  cnt_out.lane_attempts += lane_att;
+  cnt_out.warp_attempts += warp_att;
+  cnt_out.attempts += jdone;
+  cnt_out.matvecs += mv;
+  cnt_out.sysmats += sm;
+  cnt_out.flops += (long long)sm * FLOP_SYSMAT[SYS] + (long long)mv * FLOP_MV[SYS] + STEPWORK.ext[NV][jdone];
 }
 
 // ------------------------------------------------------------------------
