@@ -298,6 +298,48 @@ __host__ __device__ constexpr uint32_t tc_idesc() {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
 }
 
+// The 16 columns [taddr + w stride, + 16) of the NS accumulators w = 0..NS-1,
+// loaded by one asm statement that ends with the wait for all of them: the NS
+// loads are in flight together, and the compiler sees the registers defined
+// only after the wait.
+#define GEM_TM16(a, k)                                                                                        \
+  "=r"(a[k][0]), "=r"(a[k][1]), "=r"(a[k][2]), "=r"(a[k][3]), "=r"(a[k][4]), "=r"(a[k][5]), "=r"(a[k][6]),    \
+      "=r"(a[k][7]), "=r"(a[k][8]), "=r"(a[k][9]), "=r"(a[k][10]), "=r"(a[k][11]), "=r"(a[k][12]),             \
+      "=r"(a[k][13]), "=r"(a[k][14]), "=r"(a[k][15])
+template <int NS>
+__device__ __forceinline__ void tmem_ld_acc16(uint32_t taddr, uint32_t stride, uint32_t (&v)[NS][16]) {
+  static_assert(NS == 6 || NS == 7, "six or seven accumulators");
+  if constexpr (NS == 6) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%96];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%97];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, [%98];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%99];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%64,%65,%66,%67,%68,%69,%70,%71,%72,%73,%74,%75,%76,%77,%78,%79}, [%100];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%80,%81,%82,%83,%84,%85,%86,%87,%88,%89,%90,%91,%92,%93,%94,%95}, [%101];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : GEM_TM16(v, 0), GEM_TM16(v, 1), GEM_TM16(v, 2), GEM_TM16(v, 3),
+          GEM_TM16(v, 4), GEM_TM16(v, 5)
+        : "r"(taddr + 0u * stride), "r"(taddr + 1u * stride), "r"(taddr + 2u * stride), "r"(taddr + 3u * stride),
+          "r"(taddr + 4u * stride), "r"(taddr + 5u * stride));
+  } else {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%112];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%113];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, [%114];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%115];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%64,%65,%66,%67,%68,%69,%70,%71,%72,%73,%74,%75,%76,%77,%78,%79}, [%116];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%80,%81,%82,%83,%84,%85,%86,%87,%88,%89,%90,%91,%92,%93,%94,%95}, [%117];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%96,%97,%98,%99,%100,%101,%102,%103,%104,%105,%106,%107,%108,%109,%110,%111}, [%118];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : GEM_TM16(v, 0), GEM_TM16(v, 1), GEM_TM16(v, 2), GEM_TM16(v, 3),
+          GEM_TM16(v, 4), GEM_TM16(v, 5), GEM_TM16(v, 6)
+        : "r"(taddr + 0u * stride), "r"(taddr + 1u * stride), "r"(taddr + 2u * stride), "r"(taddr + 3u * stride),
+          "r"(taddr + 4u * stride), "r"(taddr + 5u * stride), "r"(taddr + 6u * stride));
+  }
+}
+#undef GEM_TM16
+
 template <int NS, int BN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     sums_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
@@ -406,35 +448,41 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const bool done = mbar_wait(acc_full, 0, abort_flag, wait_ns);
     asm volatile("tcgen05.fence::after_thread_sync;");
     const int r = m0 + q * 32 + lane;   // row within the kind
-    const bool row_ok = done && !*abort_flag && r < Mk;
-    const double rs = row_ok ? rscale[kind_rowoff[kind] + r] : 0.0;
-    double* crow = C + coff[kind] + (long long)r * nsta;
+    // the ring is idle once every product has completed: each warp stages its
+    // 32 rows x 16 columns there and writes them row by row (a row's 16
+    // doubles are one 128-byte segment), not as 32 strided rows per store
+    const bool store = __all_sync(0xffffffffu, done && !*abort_flag);
+    const double rs = (store && r < Mk) ? rscale[kind_rowoff[kind] + r] : 0.0;
+    double* ck = C + coff[kind];
     const double* cs = cscale + (long long)kind * nsta;
-    // columns in chunks of 16 (BN is a multiple of 16)
+    double* stg = reinterpret_cast<double*>(smem) + q * (32 * 17);   // 17: one pad double per row
+    // columns in chunks of 16 (BN is a multiple of 16); the NS accumulators of a
+    // chunk are loaded together, then combined smallest weights first
 #pragma unroll 1
     for (int c = 0; c < BN / 16; ++c) {
+      uint32_t v[NS][16];
+      tmem_ld_acc16<NS>(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 16), (uint32_t)BN, v);
       double sum[16];
 #pragma unroll
       for (int jj = 0; jj < 16; ++jj) sum[jj] = 0.0;
-#pragma unroll 1
+#pragma unroll
       for (int w = NS - 1; w >= 0; --w) {
-        uint32_t v[16];
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * BN + c * 16);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const double wgt = ldexp(1.0, -7 * (w + 2));
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) sum[jj] += (double)(int)v[jj] * wgt;   // smallest weights first
+        for (int jj = 0; jj < 16; ++jj) sum[jj] += (double)(int)v[w][jj] * wgt;
       }
-      if (row_ok) {
-        const int nb = n0 + c * 16;
+      if (store) {
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj)
-          if (nb + jj < nsta) crow[nb + jj] = sum[jj] * rs * cs[nb + jj];
+        for (int jj = 0; jj < 16; ++jj) stg[lane * 17 + jj] = sum[jj] * rs;
+        __syncwarp();
+        const int col = lane & 15, n = n0 + c * 16 + col;
+        const double csn = n < nsta ? cs[n] : 0.0;
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k) {
+          const int row = 2 * k + (lane >> 4), rg = m0 + q * 32 + row;
+          if (rg < Mk && n < nsta) ck[(long long)rg * nsta + n] = stg[row * 17 + col] * csn;
+        }
+        __syncwarp();
       }
     }
   }
