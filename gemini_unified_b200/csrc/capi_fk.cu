@@ -480,7 +480,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
     S.grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph, sc) : gem_plain::fk_phase_blocks_per_sm(ph, sc));
     nthreads = std::max(nthreads, (long long)S.grid[ph] * FK_SCHED_BLOCK[sc]);
   }
-  size_t scratch_n = (size_t)nthreads * (ctx->nnod + 1) * gem_plain::fk_lane_slot_per_node();
+  size_t scratch_n = (size_t)nthreads * ((ctx->nnod + 1) * gem_plain::fk_lane_slot_per_node() + FK_LANE_STEP_SLOTS);
   if (grow(ctx, ctx->d_scratch, ctx->scratch_cap, scratch_n)) return GEM_ERROR;
   FKLaunch& L = S.L;
   L.spl = ctx->d_spl; L.poly = fast ? ctx->d_poly : nullptr; L.jf = ctx->d_slots; L.koff = ctx->d_slots + nslot; L.items = ctx->d_items;

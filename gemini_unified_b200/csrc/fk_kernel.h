@@ -23,6 +23,9 @@ constexpr int FK_DEFER_MIN[FK_NDEFER] = {1, 8, 16, 32, 32, 32};
 constexpr int FK_DEFER_WAIT[FK_NDEFER] = {0, 6, 10, 24, 48, 1000000};
 constexpr int FK_DEFER_DEFAULT = 4;
 constexpr int MAX_LAYER_KNOTS = 64;    // knots per layer handled by the spline kernel
+// per-lane scratch elements (double2) of one Bulirsch-Stoer step, after the
+// lane's node storage: A(x0) y0 and the last level of the Neville diagonal
+constexpr int FK_LANE_STEP_SLOTS = 10;
 
 struct PrepArgs {
   int nslot, nk, nlay, attmode;

@@ -125,32 +125,46 @@ __device__ __constant__ const StepWork STEPWORK = make_stepwork();
 // ------------------------------------------------------------------------
 template <int SYS, int NVD, int DL, bool BIG>
 __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool active, double h, double x,
-                                     const dz* y0, dz* yext, int& result, double2* D, int lane, Counters& cnt_out) {
+                                     const dz* y0, dz* yext, int& result, double2* D, int lane, const Slot& xs,
+                                     Counters& cnt_out) {
   constexpr int NV = SysNV<SYS>::NV;
   // the lane state lives in local memory: work on a register copy of the
   // environment; the counters follow from the attempts made (added at the end)
+#if GEM_FAST
+  const EnvF e = make_envf(P, e_in, active);
+#else
   const Env e = e_in;
+#endif
   int lane_att = 0, warp_att = 0, jdone = 0;
   bool need = active;
   int res = 0;   // 0: failed; > 0: number of attempts of a successful step
-  dz ys[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) ys[v] = y0[v];
 #if GEM_FAST
-  // what every attempt shares: A(x) y0 and the matrices at x + h/2 and x + h
-  dz t0[NV];
+  // What every attempt shares: y0 (read from the lane state), A(x) y0 and the
+  // matrices at x + h/2 and x + h.  y0 and A(x) y0 are read once per attempt,
+  // so they stay in memory (A(x) y0 in the lane's scratch elements 0..4)
+  // instead of holding 20 registers each through the sub-step loop.
   constexpr bool CACHE = SysCache<SYS, BIG>::value;
   SysM<SYS> Mh, Me;
   const double h48 = h / 48.0;   // grid spacing of the step's sub-steps
   if (need) {
+    dz ys[NV], t0[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) ys[v] = y0[v];
     apply_sys<SYS>(P, e, x, ys, t0);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) xs.put(v, t0[v]);
     if constexpr (CACHE) {
       sys_eval<SYS>(P, e, x + 24.0 * h48, Mh);
       sys_eval<SYS>(P, e, x + 48.0 * h48, Me);
     }
   }
+#else
+  (void)xs;
+  dz ys[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) ys[v] = y0[v];
 #endif
-  dz dlast[NV];   // diagonal level DL when DL < 6
+  dz dlast[NV];   // diagonal level DL when DL < 6 (fast build: scratch elements 5..9)
   for (int j = 1; j <= 7; ++j) {
     unsigned needm = __ballot_sync(0xffffffffu, need);
     if (!needm) break;
@@ -159,7 +173,7 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
     if (!need) continue;
     dz Y[NV];
 #if GEM_FAST
-    midpoint<SYS, CACHE>(P, e, j, h48, x, ys, t0, Mh, Me, Y);
+    midpoint<SYS, CACHE>(P, e, j, h48, x, y0, xs, Mh, Me, Y);
 #else
     midpoint<SYS>(P, e, j, h, x, ys, Y);
 #endif
@@ -182,7 +196,11 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
       for (int v = 0; v < NV; ++v) {
         const bool shared_level = DL == 6 || m - 1 < DL;
         double2* slot = D + ((m - 1) * NVD + v) * 32 + lane;
+#if GEM_FAST
+        dz pv = shared_level ? dz{0.0, 0.0} : xs.get(5 + v);
+#else
         dz pv = dlast[v];
+#endif
         if (shared_level) { double2 q = *slot; pv = dz{q.x, q.y}; }
 #if GEM_FAST
         const dz u = c[v] - pv;
@@ -194,7 +212,11 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
         dz nd = xp * u;
 #endif
         if (shared_level) *slot = make_double2(pend[v].re, pend[v].im);   // level m-1 of the new diagonal
+#if GEM_FAST
+        else xs.put(5 + v, pend[v]);
+#else
         else dlast[v] = pend[v];
+#endif
         pend[v] = nd;
         yy[v] = yy[v] + nd;
         dy[v] = nd;
@@ -204,8 +226,13 @@ __device__ __noinline__ void bs_step(const FKStatic& P, const Env& e_in, bool ac
 #pragma unroll
       for (int v = 0; v < NV; ++v) D[(p * NVD + v) * 32 + lane] = make_double2(pend[v].re, pend[v].im);
     } else if (p < 6) {
+#if GEM_FAST
+#pragma unroll
+      for (int v = 0; v < NV; ++v) xs.put(5 + v, pend[v]);
+#else
 #pragma unroll
       for (int v = 0; v < NV; ++v) dlast[v] = pend[v];
+#endif
     }
     if (j >= 3) {
       double s1 = 0.0, s2 = 0.0;
@@ -1010,6 +1037,8 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   Slot s{LL.scratch + tid, LL.nthreads};
   LaneLayout lay{P.nnod + 1};
+  // the step's own scratch elements follow the node storage
+  const Slot xs{LL.scratch + tid + (long long)LaneLayout::PER_NODE * lay.NN * LL.nthreads, LL.nthreads};
   Counters cnt{0, 0, 0, 0, 0, 0, 0, 0};
   unsigned long long trips = 0, integ_lanes = 0, t_start = 0;
   if (LL.warp_ns) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
@@ -1066,23 +1095,26 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
     dz yext[5];
     int result = 0;
     if (PH == PH_TOR) {
-      bs_step<SYS_TOROIDAL, NVD, DL, BIG>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
+      bs_step<SYS_TOROIDAL, NVD, DL, BIG>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, xs, cnt);
     } else if (PH == PH_ADJ) {
-      bs_step<SYS_SOLIDT, NVD, DL, BIG>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, cnt);
+      bs_step<SYS_SOLIDT, NVD, DL, BIG>(P, L.e, integ, L.h, L.x, L.y, yext, result, D, lane, xs, cnt);
     } else {
       unsigned sysmask = __reduce_or_sync(FULL, integ ? (1u << L.sys) : 0u);
       mixed_trips += __popc(sysmask) > 1;
       if (sysmask & (1u << SYS_MINORS))
-        bs_step<SYS_MINORS, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_MINORS, L.h, L.x, L.y, yext, result, D, lane, cnt);
+        bs_step<SYS_MINORS, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_MINORS, L.h, L.x, L.y, yext, result, D, lane, xs,
+                                          cnt);
       const unsigned long long c2 = clock64();
       if (sysmask & (1u << SYS_FLUID)) {
         int r = 0;
-        bs_step<SYS_FLUID, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_FLUID, L.h, L.x, L.y, yext, r, D, lane, cnt);
+        bs_step<SYS_FLUID, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_FLUID, L.h, L.x, L.y, yext, r, D, lane, xs,
+                                          cnt);
         if (integ && L.sys == SYS_FLUID) result = r;
       }
       if (sysmask & (1u << SYS_RADIAL)) {
         int r = 0;
-        bs_step<SYS_RADIAL, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_RADIAL, L.h, L.x, L.y, yext, r, D, lane, cnt);
+        bs_step<SYS_RADIAL, NVD, DL, BIG>(P, L.e, integ && L.sys == SYS_RADIAL, L.h, L.x, L.y, yext, r, D, lane, xs,
+                                          cnt);
         if (integ && L.sys == SYS_RADIAL) result = r;
       }
       cyc_minor_sys += clock64() - c2;

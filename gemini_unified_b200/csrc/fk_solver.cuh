@@ -154,6 +154,62 @@ __device__ __forceinline__ void eval_spline(const FKStatic& P, const Env& e, dou
     }
 }
 
+#if GEM_FAST
+// The environment of one Bulirsch-Stoer step (fast build): the knot range of
+// the step's layer is looked up once per step instead of at every sub-step.
+// The interval and t = r - rk(j) are the ones eval_spline finds.
+struct EnvF : Env {
+  int sj1, sjhi;       // first and last knot interval of the layer
+  int sflat;           // layer 1: the homogeneous sphere, evaluated at its knot (t = 0)
+  int sequi;           // equidistant knots: direct index; else the search of eval_spline
+  double srk1, srdrk;  // rk(j1) and 1/drk of the layer
+};
+// Lanes without a step (active false) may hold no layer yet (a lane that never
+// took an item): they read the tables of layer 1 and evaluate nothing.
+__device__ __forceinline__ EnvF make_envf(const FKStatic& P, const Env& e, bool active) {
+  EnvF f;
+  static_cast<Env&>(f) = e;
+  const Tab* __restrict__ T = e.tab;
+  const int nl = (active && e.nl >= 1 && e.nl <= P.nlay) ? e.nl : 1;
+  f.sflat = nl == 1;
+  f.sequi = P.equidis == 1;
+  if (nl == 1) {
+    f.sj1 = f.sjhi = T->iktop[1];
+    f.srk1 = 0.0; f.srdrk = 0.0;
+  } else {
+    const int j1 = T->iktop[nl - 1] + 1, j2 = T->iktop[nl];
+    f.sj1 = j1; f.sjhi = j2 - 1;
+    f.srk1 = T->rk[j1]; f.srdrk = T->rdrk[nl];
+  }
+  return f;
+}
+template <unsigned MASK>
+__device__ __forceinline__ void eval_spline(const FKStatic& P, const EnvF& e, double r, double& ro, dz* el) {
+  if (!e.sequi) { eval_spline<MASK>(P, static_cast<const Env&>(e), r, e.nl, ro, el); return; }
+  const Tab* __restrict__ T = e.tab;
+  int j = e.sj1;
+  double t = 0.0;
+  if (!e.sflat) {
+    if (e.sjhi > e.sj1) {
+      j = (int)((r - e.srk1) * e.srdrk) + e.sj1;
+      j = j < e.sj1 ? e.sj1 : (j > e.sjhi ? e.sjhi : j);
+    }
+    j = j < 1 ? 1 : (j > P.nk - 1 ? P.nk - 1 : j);
+    t = r - T->rk[j];
+  }
+  const double* __restrict__ q = e.poly + (long long)j * POLY_STRIDE;
+  auto horner = [&](int v) {
+    double2 c32 = __ldg(reinterpret_cast<const double2*>(q + 4 * v));
+    double2 c10 = __ldg(reinterpret_cast<const double2*>(q + 4 * v + 2));
+    return fma(fma(fma(c32.x, t, c32.y), t, c10.x), t, c10.y);
+  };
+  ro = horner(0);
+#pragma unroll
+  for (int c = 0; c < 7; ++c)
+    if (MASK & (1u << c)) el[c] = dz{horner(1 + 2 * c), horner(2 + 2 * c)};
+}
+#endif
+
 // ------------------------------------------------------------------------
 //  ODE systems: y = A(x) z, nonzero entries only, column order as matmul
 // ------------------------------------------------------------------------
@@ -194,13 +250,13 @@ template <> struct SysM<SYS_TOROIDAL> { dz m12, m21; double rr; };
 template <> struct SysM<SYS_SOLIDT> { dz z2, zrpc, w, c, a43; double rr, ro; };  // w = z1/r^2, c = N/r^2
 
 template <int SYS>
-__device__ __forceinline__ void sys_eval(const FKStatic& P, const Env& e, double x, SysM<SYS>& M) {
+__device__ __forceinline__ void sys_eval(const FKStatic& P, const EnvF& e, double x, SysM<SYS>& M) {
   double ro;
   dz el[7];
   const dz zom{e.omre, e.omim};
   const double dll1 = e.dll1;
   if constexpr (SYS == SYS_MINORS) {          // minorsOdeSystem.f90:77-126
-    eval_spline<0x1Fu>(P, e, x, e.nl, ro, el);
+    eval_spline<0x1Fu>(P, e, x, ro, el);
     const double rr = rinv(x), rr2 = rr * rr;
     const dz zrpc = zinv(el[1]);
     const dz z1 = el[0] - (el[2] * el[2]) * zrpc - el[4];
@@ -212,13 +268,13 @@ __device__ __forceinline__ void sys_eval(const FKStatic& P, const Env& e, double
     M.rr = rr;
     M.ro = ro;
   } else if constexpr (SYS == SYS_FLUID) {   // fluidOdeSystem.f90:78-95
-    eval_spline<0x02u>(P, e, x, e.nl, ro, el);
+    eval_spline<0x02u>(P, e, x, ro, el);
     const dz zomro = zom * zom * ro;
     M.m11 = -2.0 * rinv(x);
     M.m12 = zinv(el[1]) - dll1 * zinv((zomro * x) * x);
     M.ro = ro;
   } else if constexpr (SYS == SYS_RADIAL) {  // radialOdeSystem.f90:78-99
-    eval_spline<0x17u>(P, e, x, e.nl, ro, el);
+    eval_spline<0x17u>(P, e, x, ro, el);
     const dz zomro = zom * zom * ro;
     const double rr = rinv(x), rr2 = rr * rr;
     const dz rc = zinv(el[1]);
@@ -227,14 +283,14 @@ __device__ __forceinline__ void sys_eval(const FKStatic& P, const Env& e, double
     M.m21 = (-zomro) + (4.0 * rr2) * ((el[0] - (el[2] * el[2]) * rc) - el[4]);
     M.m22 = (2.0 * rr) * (el[2] * rc - 1.0);
   } else if constexpr (SYS == SYS_TOROIDAL) {  // toroidalOdeSystem.f90:81-102
-    eval_spline<0x18u>(P, e, x, e.nl, ro, el);
+    eval_spline<0x18u>(P, e, x, ro, el);
     const dz zomro = zom * zom * ro;
     const double rr = rinv(x), rr2 = rr * rr;
     M.m12 = zinv(el[3]);
     M.m21 = (-zomro) - (el[4] * rr2) * (2.0 - dll1);
     M.rr = rr;
   } else {                                    // solidtOdeSystem.f90:77-114
-    eval_spline<0x1Fu>(P, e, x, e.nl, ro, el);
+    eval_spline<0x1Fu>(P, e, x, ro, el);
     const double rr = rinv(x), rr2 = rr * rr;
     const dz zrpc = zinv(el[1]);
     M.z2 = (el[2] * rr) * zrpc;
@@ -293,7 +349,7 @@ __device__ __forceinline__ void sys_apply(const SysM<SYS>& M, const Env& e, cons
 }
 
 template <int SYS>
-__device__ __forceinline__ void apply_sys(const FKStatic& P, const Env& e, double x, const dz* z, dz* y) {
+__device__ __forceinline__ void apply_sys(const FKStatic& P, const EnvF& e, double x, const dz* z, dz* y) {
   SysM<SYS> M;
   sys_eval<SYS>(P, e, x, M);
   sys_apply<SYS>(M, e, z, y);
@@ -413,13 +469,13 @@ constexpr NevTab make_nev() {
 }
 __device__ __constant__ const NevTab NEV = make_nev();
 
-// Modified midpoint of attempt jtry with t0 = A(xstart) y0 given, and with
+// Modified midpoint of attempt jtry with t0 = A(xstart) y0 given (in memory), and with
 // CACHE the matrices at xstart + h/2 (Mh) and xstart + h (Me): the parts every
 // attempt of a step shares.  The grid point g (in 48ths of the step) sits at
 // xstart + g h48, h48 = h / 48 rounded once per step.
 template <int SYS, bool CACHE>
-__device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jtry, double h48, double xstart,
-                                         const dz* y0, const dz* t0, const SysM<SYS>& Mh, const SysM<SYS>& Me,
+__device__ __forceinline__ void midpoint(const FKStatic& P, const EnvF& e, int jtry, double h48, double xstart,
+                                         const dz* y0, const Slot& t0, const SysM<SYS>& Mh, const SysM<SYS>& Me,
                                          dz* out) {
   constexpr int NV = SysNV<SYS>::NV;
   const int nstep = SEQDIV[jtry - 1];
@@ -427,7 +483,7 @@ __device__ __forceinline__ void midpoint(const FKStatic& P, const Env& e, int jt
   const double hdiv = (double)dix * h48;
   dz z0[NV], z1[NV], t[NV];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) { z0[v] = y0[v]; z1[v] = y0[v] + hdiv * t0[v]; }
+  for (int v = 0; v < NV; ++v) { z0[v] = y0[v]; z1[v] = y0[v] + hdiv * t0.get(v); }
   const double h2 = 2.0 * hdiv;
   for (int m = 1; m <= nstep - 1; ++m) {
     if (CACHE && m * dix == 24) {
