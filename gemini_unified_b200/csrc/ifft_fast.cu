@@ -239,6 +239,25 @@ __global__ void __launch_bounds__(H / 16, H == 4096 ? 3 : 1) ifft_fast_kernel(Sy
   // ---- x_{2n} = Re z_n, x_{2n+1} = Im z_n; ts(i) = x(ndec i) df fac(i)
   float* out = traces + tr * S.nsamp;
   const int ndec = S.ndec;
+  if constexpr (H == 4096) {
+    // the last pass leaves thread tid the points n = tid + 256 q: samples 2 tid + 512 q (+1), whose factors are
+    // df fac(2 tid) expo^(512 q) (+1), formed by products with fac(512) = expo^512 instead of 32 table loads
+    // (the table is the running product expo^i; the products differ from it by a few ulps of a double)
+    if (ndec == 1 && S.nsamp > 512) {
+      const double2 f01 = *reinterpret_cast<const double2*>(fac + 2 * tid);
+      const double ratio = fac[512];
+      double g0 = S.df * f01.x, g1 = S.df * f01.y;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int t0 = 2 * tid + 512 * q, t1 = t0 + 1;
+        if (t1 < S.nsamp) *reinterpret_cast<float2*>(out + t0) = make_float2((float)(v[q].x * g0), (float)(v[q].y * g1));
+        else if (t0 < S.nsamp) out[t0] = (float)(v[q].x * g0);
+        g0 *= ratio;
+        g1 *= ratio;
+      }
+      return;
+    }
+  }
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
     const int n = idx[q];
