@@ -12,13 +12,16 @@ RTOL_L2 = 1e-7
 CASES = [
     # nf1, nf2, df, nsamp, dt: the global configuration's series, a decimated
     # series, the 8192-sample series of the batched configuration, a 512-sample
-    # one, a 4096-sample one, and an 8192-sample one with a band of 1496 bins
+    # one, a 4096-sample one, an 8192-sample one with a band of 1496 bins, and
+    # 4096 samples decimated by 2 from an 8192-point transform (the fast form's
+    # table path for the output factors)
     (2, 52, 1.0 / 1024, 2048, 0.5),
     (3, 300, 1.0 / 1024, 256, 4.0),
     (2, 411, 1.0 / 2048, 8192, 0.25),
     (2, 200, 1.0 / 512, 512, 1.0),
     (2, 300, 1.0 / 1024, 4096, 0.25),
     (5, 1500, 1.0 / 2048, 8192, 0.25),
+    (2, 3000, 1.0 / 2048, 4096, 0.5),
 ]
 
 
