@@ -66,10 +66,11 @@ from gemini_unified_b200.pipeline import contiguous_runs, cost_blocks, zigzag  #
 
 def sched_names(tune):
     """Autotuned schedule per phase (toroidal, spheroidal, adjoint) as
-    'threads[+cache]/defer<lanes>,<steps>' strings."""
-    from gemini_unified_b200.fk import DEFERRALS, SCHEDULES
-    return ["%d%s/defer%d,%d" % (SCHEDULES[s][0], "+cache" if SCHEDULES[s][1] else "", DEFERRALS[d][0],
-                                  DEFERRALS[d][1]) for s, d in zip(tune["schedule"], tune["defer"])]
+    'threads[+cache]/defer<lanes>,<steps>/q<granularity>' strings."""
+    from gemini_unified_b200.fk import DEFERRALS, GRANULARITIES, SCHEDULES
+    return ["%d%s/defer%d,%d/q%d" % (SCHEDULES[s][0], "+cache" if SCHEDULES[s][1] else "", DEFERRALS[d][0],
+                                     DEFERRALS[d][1], GRANULARITIES[q])
+            for s, d, q in zip(tune["schedule"], tune["defer"], tune["queue"])]
 
 
 class Clocks:

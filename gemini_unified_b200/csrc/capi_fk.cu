@@ -80,6 +80,9 @@ struct gem_ctx {
   // bookkeeping deferral of each phase (index into FK_DEFER_*), per build
   int defer[2][3] = {{FK_DEFER_DEFAULT, FK_DEFER_DEFAULT, FK_DEFER_DEFAULT},
                      {FK_DEFER_DEFAULT, FK_DEFER_DEFAULT, FK_DEFER_DEFAULT}};
+  // queue granularity of each phase (index into FK_GRAN), per build
+  int qgran[2][3] = {{FK_GRAN_DEFAULT, FK_GRAN_DEFAULT, FK_GRAN_DEFAULT},
+                     {FK_GRAN_DEFAULT, FK_GRAN_DEFAULT, FK_GRAN_DEFAULT}};
   // captured launch sequence of one slab (gem_fk_graph_build)
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t graph_stream = nullptr;
@@ -369,7 +372,7 @@ struct SlabPlan {
   long long nkf;
   size_t spl_n, nout, nu, nd, ndet;
   bool fast, propose;
-  int sched[3], defer[3];
+  int sched[3], defer[3], qgran[3];
   float* gfre;
   float* gfim;
   double* gf64;
@@ -477,6 +480,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
     const int sc = ctx->sched[fast ? 1 : 0][ph];
     S.sched[ph] = sc;
     S.defer[ph] = ctx->defer[fast ? 1 : 0][ph];
+    S.qgran[ph] = ctx->qgran[fast ? 1 : 0][ph];
     S.grid[ph] = ctx->nsm * (fast ? gem_fast::fk_phase_blocks_per_sm(ph, sc) : gem_plain::fk_phase_blocks_per_sm(ph, sc));
     nthreads = std::max(nthreads, (long long)S.grid[ph] * FK_SCHED_BLOCK[sc]);
   }
@@ -493,7 +497,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   L.warp_ns = nullptr;
   L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
   L.prop_kopt = nullptr; L.prop_hs = nullptr;
-  L.adv_min = 1; L.adv_wait = 0;
+  L.adv_min = 1; L.adv_wait = 0; L.qgran = 1;
   L.nsrc = 0; L.src_blk = 0;
   ctx->last_grid = S.grid[1];
   ctx->last_block = FK_SCHED_BLOCK[S.sched[1]];
@@ -563,6 +567,7 @@ int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
     FKLaunch Lp = S.L;
     Lp.adv_min = FK_DEFER_MIN[S.defer[ph]];
     Lp.adv_wait = FK_DEFER_WAIT[S.defer[ph]];
+    Lp.qgran = FK_GRAN[S.qgran[ph]];
     if (ctx->d_prof) Lp.prof = ctx->d_prof + 8 * ph;
     if (ctx->d_warp_ns && ph == 1) Lp.warp_ns = ctx->d_warp_ns;
     const cudaError_t le = launch(ph, Lp, S.grid[ph]);
@@ -604,7 +609,10 @@ int fk_enqueue_aski(gem_ctx* ctx, SlabPlan& S, int nsnod, const int* jsnod, int 
   if (ctx->d_prof) CK(cudaMemsetAsync(ctx->d_prof, 0, 32 * sizeof(unsigned long long), st));
   auto launch = [&](int ph, const FKStatic& PX, FKLaunch LX) {
     const int sc = ph >= 0 ? S.sched[ph] : 0;
-    if (ph >= 0) { LX.adv_min = FK_DEFER_MIN[S.defer[ph]]; LX.adv_wait = FK_DEFER_WAIT[S.defer[ph]]; }
+    if (ph >= 0) {
+      LX.adv_min = FK_DEFER_MIN[S.defer[ph]]; LX.adv_wait = FK_DEFER_WAIT[S.defer[ph]];
+      LX.qgran = FK_GRAN[S.qgran[ph]];
+    }
     const int g = ph >= 0 ? S.grid[ph] : ctx->nsm * 8;
     return S.fast ? gem_fast::launch_fk_phase(ph, sc, PX, LX, g, st) : gem_plain::launch_fk_phase(ph, sc, PX, LX, g, st);
   };
@@ -1025,12 +1033,33 @@ int gem_fk_defer_get(const gem_ctx* ctx, int* defer3) {
   return GEM_OK;
 }
 
+// Queue granularity (no counterpart in the reference): per phase an index into
+// FK_GRAN, the queue positions a lane reserves per fetch, kept per backend.
+int gem_fk_queue_set(gem_ctx* ctx, const int* gran3) {
+  if (!ctx || !gran3) return GEM_ERROR;
+  for (int ph = 0; ph < 3; ++ph)
+    if (gran3[ph] < 0 || gran3[ph] >= FK_NGRAN) return fail(ctx, "queue granularity index must be 0..%d", FK_NGRAN - 1);
+  const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
+  for (int ph = 0; ph < 3; ++ph) ctx->qgran[b][ph] = gran3[ph];
+  ctx->graph_valid = false;
+  return GEM_OK;
+}
+
+int gem_fk_queue_get(const gem_ctx* ctx, int* gran3) {
+  if (!ctx || !gran3) return GEM_ERROR;
+  const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
+  for (int ph = 0; ph < 3; ++ph) gran3[ph] = ctx->qgran[b][ph];
+  return GEM_OK;
+}
+
 // Autotuner: runs frequencies jf_first..jf_last once per candidate (all three
 // phases at once, repeats times, the minimum kept) and keeps per phase the
 // fastest.  Stage 1 tries the schedules (block size, matrix caching) under the
-// current deferral, stage 2 the deferrals under the chosen schedules.
-// ms[c*3 + ph]: stage-1 times for c < GEM_FK_NSCHED, stage-2 times after them;
-// -1 for candidates not run (the plain build has no matrix-caching variants).
+// current deferral and queue granularity, stage 2 the deferrals under the
+// chosen schedules, stage 3 the queue granularities under both.
+// ms[c*3 + ph]: stage-1 times for c < GEM_FK_NSCHED, then the stage-2 and the
+// stage-3 times; -1 for candidates not run (the plain build has no
+// matrix-caching variants).
 int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, int repeats, float* ms,
                     int* sched3, int* defer3) {
   if (!ctx) return GEM_ERROR;
@@ -1051,7 +1080,8 @@ int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_l
   const int b = ctx->backend == GEM_BACKEND_GPU_FAST ? 1 : 0;
   const int saved_s[3] = {ctx->sched[b][0], ctx->sched[b][1], ctx->sched[b][2]};
   const int saved_d[3] = {ctx->defer[b][0], ctx->defer[b][1], ctx->defer[b][2]};
-  float t[FK_NSCHED + FK_NDEFER][3];
+  const int saved_q[3] = {ctx->qgran[b][0], ctx->qgran[b][1], ctx->qgran[b][2]};
+  float t[FK_NSCHED + FK_NDEFER + FK_NGRAN][3];
   for (auto& row : t)
     for (float& v : row) v = -1.0f;
   auto run = [&](float* tc) -> int {
@@ -1067,7 +1097,9 @@ int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_l
     return GEM_OK;
   };
   auto restore = [&]() {
-    for (int ph = 0; ph < 3; ++ph) { ctx->sched[b][ph] = saved_s[ph]; ctx->defer[b][ph] = saved_d[ph]; }
+    for (int ph = 0; ph < 3; ++ph) {
+      ctx->sched[b][ph] = saved_s[ph]; ctx->defer[b][ph] = saved_d[ph]; ctx->qgran[b][ph] = saved_q[ph];
+    }
   };
   auto argmin = [&](int c0, int n, int ph) {
     int best = c0;
@@ -1088,12 +1120,18 @@ int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_l
     if ((rc = run(t[FK_NSCHED + c]))) { restore(); return rc; }
   }
   for (int ph = 0; ph < 3; ++ph) ctx->defer[b][ph] = argmin(FK_NSCHED, FK_NDEFER, ph);
+  // stage 3: queue granularities under the chosen schedules and deferrals
+  for (int c = 0; c < FK_NGRAN; ++c) {
+    for (int ph = 0; ph < 3; ++ph) ctx->qgran[b][ph] = c;
+    if ((rc = run(t[FK_NSCHED + FK_NDEFER + c]))) { restore(); return rc; }
+  }
+  for (int ph = 0; ph < 3; ++ph) ctx->qgran[b][ph] = argmin(FK_NSCHED + FK_NDEFER, FK_NGRAN, ph);
   for (int ph = 0; ph < 3; ++ph) {
     if (sched3) sched3[ph] = ctx->sched[b][ph];
     if (defer3) defer3[ph] = ctx->defer[b][ph];
   }
   if (ms)
-    for (int c = 0; c < FK_NSCHED + FK_NDEFER; ++c)
+    for (int c = 0; c < FK_NSCHED + FK_NDEFER + FK_NGRAN; ++c)
       for (int ph = 0; ph < 3; ++ph) ms[c * 3 + ph] = t[c][ph];
   ctx->graph_valid = false;
   return GEM_OK;

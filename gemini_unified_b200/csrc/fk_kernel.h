@@ -22,6 +22,11 @@ constexpr int FK_NDEFER = 6;
 constexpr int FK_DEFER_MIN[FK_NDEFER] = {1, 8, 16, 32, 32, 32};
 constexpr int FK_DEFER_WAIT[FK_NDEFER] = {0, 6, 10, 24, 48, 1000000};
 constexpr int FK_DEFER_DEFAULT = 4;
+// queue granularity: consecutive queue positions a lane reserves per fetch (it
+// takes the next of its run without the queue until the run is used up)
+constexpr int FK_NGRAN = 3;
+constexpr int FK_GRAN[FK_NGRAN] = {1, 2, 4};
+constexpr int FK_GRAN_DEFAULT = 0;
 constexpr int MAX_LAYER_KNOTS = 64;    // knots per layer handled by the spline kernel
 // per-lane scratch elements (double2) of one Bulirsch-Stoer step, after the
 // lane's node storage: A(x0) y0 and the last level of the Neville diagonal
@@ -76,6 +81,7 @@ struct FKLaunch {
   // deferral of the bookkeeping between integrations: a pass runs when
   // adv_min lanes wait, one has waited adv_wait trips, or none integrates
   int adv_min, adv_wait;
+  int qgran;            // queue positions reserved per fetch (FK_GRAN)
   // toroidal phase of a set of source nodes (nsrc > 0): per source b its node and
   // type (0 force, 1 moment), passed by value; its output block starts at
   // element b * src_blk

@@ -76,6 +76,7 @@ struct Lane {
   int kopt;   // target attempt of the step-size control
   double hs;  // multiplier of the initial steps given by the initial-value formulas
   dz y[5];
+  unsigned qnext, qend;   // queue positions reserved by the lane and not yet taken
 };
 
 // ------------------------------------------------------------------------
@@ -1046,6 +1047,8 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
   Lane L;
   L.e.tab = &tab;
   L.st = S_FETCH;
+  L.qnext = 0; L.qend = 0;
+  const unsigned qg = LL.qgran > 1 ? (unsigned)LL.qgran : 1u;
   unsigned long long cyc_adv = 0, cyc_step = 0, mixed_trips = 0, cyc_minor_sys = 0;
   int waited = 0;   // trips this lane has waited for its bookkeeping
   for (;;) {
@@ -1066,15 +1069,20 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
       if (__any_sync(FULL, pshort) && pshort) advance<PH>(P, LL, s, lay, L);
     }
     for (int round = 0; go && round < 64; ++round) {
+      // the next position of the lane's reserved run, without the queue
+      if (L.st == S_FETCH && L.qnext < L.qend) {
+        if (L.qnext < (unsigned)LL.nitems) { L.k = LL.order[L.qnext++]; L.st = S_ITEM_INIT; }
+        else L.qnext = L.qend;
+      }
       unsigned fm = __ballot_sync(FULL, L.st == S_FETCH);
       if (fm) {
         int leader = __ffs(fm) - 1;
         unsigned base = 0;
-        if (lane == leader) base = atomicAdd(queue, (unsigned)__popc(fm));
+        if (lane == leader) base = atomicAdd(queue, (unsigned)__popc(fm) * qg);
         base = __shfl_sync(FULL, base, leader);
         if (L.st == S_FETCH) {
-          unsigned my = base + __popc(fm & ((1u << lane) - 1u));
-          if (my < (unsigned)LL.nitems) { L.k = LL.order[my]; L.st = S_ITEM_INIT; }
+          const unsigned my = base + (unsigned)__popc(fm & ((1u << lane) - 1u)) * qg;
+          if (my < (unsigned)LL.nitems) { L.k = LL.order[my]; L.st = S_ITEM_INIT; L.qnext = my + 1; L.qend = my + qg; }
           else L.st = S_IDLE;
         }
       }

@@ -29,6 +29,9 @@ NSCHED = len(SCHEDULES)
 # bookkeeping deferrals (lanes waiting, steps waited)
 DEFERRALS = [(1, 0), (8, 6), (16, 10), (32, 24), (32, 48), (32, 1000000)]
 NDEFER = len(DEFERRALS)
+# queue granularities: consecutive work-queue positions a lane reserves per fetch
+GRANULARITIES = [1, 2, 4]
+NGRAN = len(GRANULARITIES)
 STATUS_TEXT = {0: "ok", 1: "step size smaller than minimum", 2: "maximum number of steps reached",
                3: "continued fraction did not converge", 4: "node/discontinuity bookkeeping",
                5: "non-finite value", 7: "ocean receiver or source not supported"}
@@ -97,6 +100,8 @@ def lib() -> ctypes.CDLL:
         L.gem_fk_autotune.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
         L.gem_fk_defer_set.argtypes = [vp, vp]
         L.gem_fk_defer_get.argtypes = [vp, vp]
+        L.gem_fk_queue_set.argtypes = [vp, vp]
+        L.gem_fk_queue_get.argtypes = [vp, vp]
         L.gem_instrument.argtypes = [vp, ctypes.c_int]
         L.gem_instrument_read.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_int)]
         _lib = L
@@ -429,23 +434,35 @@ class GeminiFK:
         s = (ctypes.c_int * 3)(*[int(x) for x in defer])
         self._check(lib().gem_fk_defer_set(self._h, s))
 
+    def queue(self):
+        """Queue granularity index per phase; see GRANULARITIES."""
+        s = (ctypes.c_int * 3)()
+        self._check(lib().gem_fk_queue_get(self._h, s))
+        return [int(x) for x in s]
+
+    def queue_set(self, gran):
+        s = (ctypes.c_int * 3)(*[int(x) for x in gran])
+        self._check(lib().gem_fk_queue_set(self._h, s))
+
     def autotune(self, params: FKParams, jre: int, jf_first: int = 0, jf_last: int = 0, repeats: int = 1):
         """Pick per phase the fastest schedule, then the fastest bookkeeping
-        deferral, on frequencies jf_first..jf_last (default: the top quarter of
-        the band, which holds about 44% of the solves).  Returns {"schedule":
-        [tor, sph, adj], "defer": [...], "ms": (NSCHED + NDEFER, 3) phase times}."""
+        deferral, then the fastest queue granularity, on frequencies
+        jf_first..jf_last (default: the top quarter of the band, which holds
+        about 44% of the solves).  Returns {"schedule": [tor, sph, adj],
+        "defer": [...], "queue": [...], "ms": (NSCHED + NDEFER + NGRAN, 3)
+        phase times}."""
         if not jf_first:
             grid = frequency_grid(params, self.model.rearth)
             jf_last = grid.nf2
             jf_first = max(grid.nf1, grid.nf2 - (grid.nf2 - grid.nf1 + 1) // 4)
         pc = fk_params_c(params, jre)
-        ms = np.zeros(3 * (NSCHED + NDEFER), np.float32)
+        ms = np.zeros(3 * (NSCHED + NDEFER + NGRAN), np.float32)
         s = (ctypes.c_int * 3)()
         d = (ctypes.c_int * 3)()
         self._check(lib().gem_fk_autotune(self._h, ctypes.byref(pc), int(jf_first), int(jf_last), int(repeats),
                                           _ptr(ms), s, d))
-        return {"schedule": [int(x) for x in s], "defer": [int(x) for x in d],
-                "ms": ms.reshape(NSCHED + NDEFER, 3), "jf": [int(jf_first), int(jf_last)]}
+        return {"schedule": [int(x) for x in s], "defer": [int(x) for x in d], "queue": self.queue(),
+                "ms": ms.reshape(NSCHED + NDEFER + NGRAN, 3), "jf": [int(jf_first), int(jf_last)]}
 
     def ray_table(self, stype: str = "P", attmode: int = 3, eps: float = 1e-6, drtp: float = 10000.0,
                   rtmax: float = 0.0):

@@ -243,12 +243,22 @@ int gem_fk_schedule_get(const gem_ctx* ctx, int* sched3);
 #define GEM_FK_NDEFER 6
 int gem_fk_defer_set(gem_ctx* ctx, const int* defer3);
 int gem_fk_defer_get(const gem_ctx* ctx, int* defer3);
+/* Queue granularity of each phase (no counterpart in the reference): a lane
+ * that fetches work reserves (1, 2, 4) consecutive positions of the phase's
+ * work queue and takes the next of them without the queue until they are used
+ * up.  Index 0..GEM_FK_NGRAN-1, kept per context and backend, default 0;
+ * bit-identical spectra. */
+#define GEM_FK_NGRAN 3
+int gem_fk_queue_set(gem_ctx* ctx, const int* gran3);
+int gem_fk_queue_get(const gem_ctx* ctx, int* gran3);
 /* Autotuner: runs frequencies jf_first..jf_last once per candidate (repeats
  * times, minimum kept), first the schedules, then the deferrals under the
- * chosen schedules, and keeps per phase the fastest of each.  ms (may be NULL,
- * (GEM_FK_NSCHED + GEM_FK_NDEFER) * 3 floats) receives the phase times in ms
- * of every candidate, -1 for candidates not run (the plain backend tries
- * schedules 0..2 only); sched3 and defer3 (may be NULL) the choice. */
+ * chosen schedules, then the queue granularities under both, and keeps per
+ * phase the fastest of each.  ms (may be NULL,
+ * (GEM_FK_NSCHED + GEM_FK_NDEFER + GEM_FK_NGRAN) * 3 floats) receives the phase
+ * times in ms of every candidate, -1 for candidates not run (the plain backend
+ * tries schedules 0..2 only); sched3 and defer3 (may be NULL) the choice, and
+ * gem_fk_queue_get the chosen granularities. */
 int gem_fk_autotune(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, int repeats, float* ms,
                     int* sched3, int* defer3);
 

@@ -224,7 +224,7 @@ def test_every_schedule_gives_identical_spectra(small):
     """Block size, matrix caching and the bookkeeping deferral change the time
     only: every schedule and deferral of both backends gives the default's
     spectra bit for bit."""
-    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NDEFER, NSCHED
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NDEFER, NGRAN, NSCHED
     from gemini_unified_b200.model import GeminiError
     w, m, ex, jre, _, o = small
     for backend in (1, GEM_BACKEND_GPU_FAST):
@@ -241,6 +241,13 @@ def test_every_schedule_gives_identical_spectra(small):
             fk.defer_set([d, d, d])
             _, _, got, st = fk.run(w.params, jre, 40, 52, f32=False)
             assert np.all(st == 0) and same(got), (backend, "deferral", d)
+        assert fk.queue() == [0, 0, 0]
+        for q in range(NGRAN):
+            fk.queue_set([q, q, q])
+            _, _, got, st = fk.run(w.params, jre, 40, 52, f32=False)
+            assert np.all(st == 0) and same(got), (backend, "queue granularity", q)
+        with pytest.raises(GeminiError):
+            fk.queue_set([0, NGRAN, 0])
         with pytest.raises(GeminiError):
             fk.schedule_set([0, NSCHED, 0])
         with pytest.raises(GeminiError):
@@ -248,17 +255,19 @@ def test_every_schedule_gives_identical_spectra(small):
 
 
 def test_autotune_keeps_the_fastest_schedule(small):
-    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NDEFER, NSCHED
+    from gemini_unified_b200.fk import GeminiFK, GEM_BACKEND_GPU_FAST, NDEFER, NGRAN, NSCHED
     w, m, ex, jre, _, o = small
     for backend, ncand in ((1, 3), (GEM_BACKEND_GPU_FAST, NSCHED)):
         fk = GeminiFK(m, ex, backend=backend)
         r = fk.autotune(w.params, jre, 44, 52)
         ms = r["ms"]
+        assert ms.shape == (NSCHED + NDEFER + NGRAN, 3)
         assert np.all(ms[:ncand] > 0) and np.all(ms[ncand:NSCHED] == -1) and np.all(ms[NSCHED:] > 0)
         for ph in range(3):
             assert r["schedule"][ph] == int(np.argmin(ms[:ncand, ph]))
-            assert r["defer"][ph] == int(np.argmin(ms[NSCHED:, ph]))
-        assert fk.schedule() == r["schedule"] and fk.defer() == r["defer"]
+            assert r["defer"][ph] == int(np.argmin(ms[NSCHED:NSCHED + NDEFER, ph]))
+            assert r["queue"][ph] == int(np.argmin(ms[NSCHED + NDEFER:, ph]))
+        assert fk.schedule() == r["schedule"] and fk.defer() == r["defer"] and fk.queue() == r["queue"]
         _, _, g64, st = fk.run(w.params, jre, 44, 52, f32=False)
         assert np.all(st == 0)
 
