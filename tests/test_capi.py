@@ -70,3 +70,16 @@ def test_new_entry_points_reject_a_null_context(lib):
     assert lib.gem_fk_run_aski(None, None, 1, None, 2, 3, None, None, None, None) == 2
     assert lib.gem_coupling_run(None, None, None, None, None, None, None, 1, None, None, None, None, None) == 2
     assert lib.gem_fk_aski_nsp(1) == 20 and lib.gem_fk_aski_nsp(0) == 10
+
+
+def test_tuning_calls_reject_a_null_context(lib):
+    """The schedule, deferral and queue-granularity calls return the error
+    level 2 for a null context or a null array, before touching the GPU."""
+    vp = ctypes.c_void_p
+    three = (ctypes.c_int * 3)(0, 0, 0)
+    for name in ("gem_fk_schedule_set", "gem_fk_schedule_get", "gem_fk_defer_set", "gem_fk_defer_get",
+                 "gem_fk_queue_set", "gem_fk_queue_get"):
+        f = getattr(lib, name)
+        f.argtypes = [vp, vp]
+        assert f(None, three) == 2, name
+        assert f(None, None) == 2, name
