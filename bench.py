@@ -66,10 +66,13 @@ from gemini_unified_b200.pipeline import contiguous_runs, cost_blocks, zigzag  #
 
 def sched_names(tune):
     """Autotuned schedule per phase (toroidal, spheroidal, adjoint) as
-    'threads[+cache]/defer<lanes>,<steps>/q<granularity>' strings."""
+    'threads[+cache]/defer<lanes>,<steps>/q<lane run> or /qblock<block run>' strings."""
     from gemini_unified_b200.fk import DEFERRALS, GRANULARITIES, SCHEDULES
-    return ["%d%s/defer%d,%d/q%d" % (SCHEDULES[s][0], "+cache" if SCHEDULES[s][1] else "", DEFERRALS[d][0],
-                                     DEFERRALS[d][1], GRANULARITIES[q])
+    def gran(q):
+        lane, block = GRANULARITIES[q]
+        return "q%d" % lane if not block else "qblock%d" % block
+    return ["%d%s/defer%d,%d/%s" % (SCHEDULES[s][0], "+cache" if SCHEDULES[s][1] else "", DEFERRALS[d][0],
+                                    DEFERRALS[d][1], gran(q))
             for s, d, q in zip(tune["schedule"], tune["defer"], tune["queue"])]
 
 

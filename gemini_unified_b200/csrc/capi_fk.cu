@@ -497,7 +497,7 @@ int fk_prepare(gem_ctx* ctx, const gem_fk_params* p, int jf_first, int jf_last, 
   L.warp_ns = nullptr;
   L.steplog = ctx->d_steplog; L.steplog_cap = ctx->steplog_cap; L.steplog_n = ctx->d_steplog_n;
   L.prop_kopt = nullptr; L.prop_hs = nullptr;
-  L.adv_min = 1; L.adv_wait = 0; L.qgran = 1;
+  L.adv_min = 1; L.adv_wait = 0; L.qgran = 1; L.qchunk = 0;
   L.nsrc = 0; L.src_blk = 0;
   ctx->last_grid = S.grid[1];
   ctx->last_block = FK_SCHED_BLOCK[S.sched[1]];
@@ -568,6 +568,7 @@ int fk_enqueue(gem_ctx* ctx, SlabPlan& S, cudaStream_t st, bool timed) {
     Lp.adv_min = FK_DEFER_MIN[S.defer[ph]];
     Lp.adv_wait = FK_DEFER_WAIT[S.defer[ph]];
     Lp.qgran = FK_GRAN[S.qgran[ph]];
+    Lp.qchunk = FK_QCHUNK[S.qgran[ph]];
     if (ctx->d_prof) Lp.prof = ctx->d_prof + 8 * ph;
     if (ctx->d_warp_ns && ph == 1) Lp.warp_ns = ctx->d_warp_ns;
     const cudaError_t le = launch(ph, Lp, S.grid[ph]);
@@ -612,6 +613,7 @@ int fk_enqueue_aski(gem_ctx* ctx, SlabPlan& S, int nsnod, const int* jsnod, int 
     if (ph >= 0) {
       LX.adv_min = FK_DEFER_MIN[S.defer[ph]]; LX.adv_wait = FK_DEFER_WAIT[S.defer[ph]];
       LX.qgran = FK_GRAN[S.qgran[ph]];
+      LX.qchunk = FK_QCHUNK[S.qgran[ph]];
     }
     const int g = ph >= 0 ? S.grid[ph] : ctx->nsm * 8;
     return S.fast ? gem_fast::launch_fk_phase(ph, sc, PX, LX, g, st) : gem_plain::launch_fk_phase(ph, sc, PX, LX, g, st);
@@ -1034,7 +1036,8 @@ int gem_fk_defer_get(const gem_ctx* ctx, int* defer3) {
 }
 
 // Queue granularity (no counterpart in the reference): per phase an index into
-// FK_GRAN, the queue positions a lane reserves per fetch, kept per backend.
+// FK_GRAN / FK_QCHUNK, the queue positions a lane or a block reserves per
+// fetch, kept per backend.
 int gem_fk_queue_set(gem_ctx* ctx, const int* gran3) {
   if (!ctx || !gran3) return GEM_ERROR;
   for (int ph = 0; ph < 3; ++ph)

@@ -23,9 +23,11 @@ constexpr int FK_DEFER_MIN[FK_NDEFER] = {1, 8, 16, 32, 32, 32};
 constexpr int FK_DEFER_WAIT[FK_NDEFER] = {0, 6, 10, 24, 48, 1000000};
 constexpr int FK_DEFER_DEFAULT = 4;
 // queue granularity: consecutive queue positions a lane reserves per fetch (it
-// takes the next of its run without the queue until the run is used up)
-constexpr int FK_NGRAN = 3;
-constexpr int FK_GRAN[FK_NGRAN] = {1, 2, 4};
+// takes the next of its run without the queue until the run is used up), or,
+// with FK_QCHUNK > 0, runs of that many positions the warps of a block share
+constexpr int FK_NGRAN = 4;
+constexpr int FK_GRAN[FK_NGRAN] = {1, 2, 4, 1};
+constexpr int FK_QCHUNK[FK_NGRAN] = {0, 0, 0, 1024};
 constexpr int FK_GRAN_DEFAULT = 0;
 constexpr int MAX_LAYER_KNOTS = 64;    // knots per layer handled by the spline kernel
 // per-lane scratch elements (double2) of one Bulirsch-Stoer step, after the
@@ -82,6 +84,7 @@ struct FKLaunch {
   // adv_min lanes wait, one has waited adv_wait trips, or none integrates
   int adv_min, adv_wait;
   int qgran;            // queue positions reserved per fetch (FK_GRAN)
+  int qchunk;           // > 0: runs of queue positions shared by the warps of a block (FK_QCHUNK)
   // toroidal phase of a set of source nodes (nsrc > 0): per source b its node and
   // type (0 force, 1 moment), passed by value; its output block starts at
   // element b * src_blk

@@ -1026,10 +1026,15 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
   constexpr int NVD = PhaseNV<PH>::NV;
   extern __shared__ double2 smem_diag[];
   __shared__ Tab tab;
+  // block-shared run of queue positions (LL.qchunk > 0): (end << 32) | next,
+  // refilled from the phase's queue under blk_lock
+  __shared__ unsigned long long blk_q;
+  __shared__ int blk_lock;
   for (int i = threadIdx.x; i <= MAXKNOT; i += blockDim.x) tab.rk[i] = P.rk[i];
   for (int i = threadIdx.x; i <= MAXLAY; i += blockDim.x) {
     tab.drk[i] = P.drk[i]; tab.iktop[i] = P.iktop[i]; tab.rdrk[i] = 1.0 / P.drk[i];
   }
+  if (threadIdx.x == 0) { blk_q = 0ull; blk_lock = 0; }
   __syncthreads();
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -1075,7 +1080,39 @@ __global__ void __launch_bounds__(BLK, 1) fk_phase_kernel(const __grid_constant_
         else L.qnext = L.qend;
       }
       unsigned fm = __ballot_sync(FULL, L.st == S_FETCH);
-      if (fm) {
+      if (fm && LL.qchunk > 0) {
+        // the block's warps share runs of qchunk consecutive positions (one
+        // frequency's adjacent degrees), so their spline tables stay in L1.  The
+        // positions of a run go out by an atomic add on its next position; the
+        // warp that finds the run used up and takes the lock installs the next
+        // run from the queue.  Lanes left without a position retry.
+        const int leader = __ffs(fm) - 1;
+        unsigned base = 0, got = 0;
+        if (lane == leader) {
+          const unsigned n = (unsigned)__popc(fm);
+          const unsigned long long q = atomicAdd(&blk_q, (unsigned long long)n);
+          const unsigned next = (unsigned)q, end = (unsigned)(q >> 32);
+          if (next < end) { base = next; got = min(n, end - next); }
+          if (got < n && atomicCAS(&blk_lock, 0, 1) == 0) {
+            const unsigned long long cur = atomicAdd(&blk_q, 0ull);
+            if ((unsigned)cur >= (unsigned)(cur >> 32)) {
+              const unsigned nb = atomicAdd(queue, (unsigned)LL.qchunk);
+              atomicExch(&blk_q, ((unsigned long long)(nb + (unsigned)LL.qchunk) << 32) | nb);
+            }
+            atomicExch(&blk_lock, 0);
+          }
+        }
+        base = __shfl_sync(FULL, base, leader);
+        got = __shfl_sync(FULL, got, leader);
+        if (L.st == S_FETCH) {
+          const unsigned r = (unsigned)__popc(fm & ((1u << lane) - 1u));
+          if (r < got) {
+            const unsigned my = base + r;
+            if (my < (unsigned)LL.nitems) { L.k = LL.order[my]; L.st = S_ITEM_INIT; }
+            else L.st = S_IDLE;
+          }
+        }
+      } else if (fm) {
         int leader = __ffs(fm) - 1;
         unsigned base = 0;
         if (lane == leader) base = atomicAdd(queue, (unsigned)__popc(fm) * qg);

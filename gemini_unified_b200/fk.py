@@ -29,8 +29,9 @@ NSCHED = len(SCHEDULES)
 # bookkeeping deferrals (lanes waiting, steps waited)
 DEFERRALS = [(1, 0), (8, 6), (16, 10), (32, 24), (32, 48), (32, 1000000)]
 NDEFER = len(DEFERRALS)
-# queue granularities: consecutive work-queue positions a lane reserves per fetch
-GRANULARITIES = [1, 2, 4]
+# queue granularities: (positions a lane reserves per fetch, positions of the
+# runs the warps of a block share; 0: none)
+GRANULARITIES = [(1, 0), (2, 0), (4, 0), (1, 1024)]
 NGRAN = len(GRANULARITIES)
 STATUS_TEXT = {0: "ok", 1: "step size smaller than minimum", 2: "maximum number of steps reached",
                3: "continued fraction did not converge", 4: "node/discontinuity bookkeeping",

@@ -39,6 +39,7 @@ def main(argv=None):
     ap.add_argument("--sched", default="", help="schedule index per phase (toroidal,spheroidal,adjoint), "
                     "see fk.SCHEDULES; default: the library's")
     ap.add_argument("--defer", default="", help="bookkeeping deferral index per phase, see fk.DEFERRALS")
+    ap.add_argument("--queue", default="", help="queue granularity index per phase, see fk.GRANULARITIES")
     a = ap.parse_args(argv)
     w = configs.WORKLOADS[a.workload]
     m = w.model()
@@ -53,6 +54,8 @@ def main(argv=None):
         fk.schedule_set([int(x) for x in a.sched.split(",")])
     if a.defer:
         fk.defer_set([int(x) for x in a.defer.split(",")])
+    if a.queue:
+        fk.queue_set([int(x) for x in a.queue.split(",")])
     if a.aski:
         return aski(fk, w, ex, jre, lo, hi, a)
     best = None
@@ -63,7 +66,7 @@ def main(argv=None):
             best = s
     s = best
     print(json.dumps({"workload": a.workload, "jf": [lo, hi], "backend": a.backend, "items": int(s["items"]),
-                      "schedule": fk.schedule(), "defer": fk.defer(),
+                      "schedule": fk.schedule(), "defer": fk.defer(), "queue": fk.queue(),
                       "phase_ms": [round(float(x), 3) for x in s["phase_ms"]],
                       "failed": int(np.count_nonzero(st)), "solve_ms": s["solve_ms"],
                       "solves_per_s": s["items"] / s["solve_ms"] * 1e3, "steps_ok": int(s["steps_ok"]),

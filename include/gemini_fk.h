@@ -246,9 +246,10 @@ int gem_fk_defer_get(const gem_ctx* ctx, int* defer3);
 /* Queue granularity of each phase (no counterpart in the reference): a lane
  * that fetches work reserves (1, 2, 4) consecutive positions of the phase's
  * work queue and takes the next of them without the queue until they are used
- * up.  Index 0..GEM_FK_NGRAN-1, kept per context and backend, default 0;
- * bit-identical spectra. */
-#define GEM_FK_NGRAN 3
+ * up (indices 0..2), or the warps of a block share runs of 1024 consecutive
+ * positions (index 3).  Index 0..GEM_FK_NGRAN-1, kept per context and backend,
+ * default 0; bit-identical spectra. */
+#define GEM_FK_NGRAN 4
 int gem_fk_queue_set(gem_ctx* ctx, const int* gran3);
 int gem_fk_queue_get(const gem_ctx* ctx, int* gran3);
 /* Autotuner: runs frequencies jf_first..jf_last once per candidate (repeats
